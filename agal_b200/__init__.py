@@ -1,0 +1,198 @@
+"""agal_b200 - B200-native octree-AMR lattice Boltzmann time step.
+
+Python mirror of the reference's host interface (Parser, Mesh, Solver_LBM of
+AGAL: inc/parser.h, inc/mesh.h, inc/solver_lbm.h) over the C ABI of
+libagal_b200.so.  Every numerical operation runs in the CUDA library; this
+module only marshals parameters and host buffers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import AgalError, AgalParams
+
+__all__ = ["Parser", "Case", "Mesh", "Solver_LBM", "AgalError", "AgalParams", "default_params"]
+
+
+def _check(rc: int, ctx: Optional[C.c_void_p] = None) -> None:
+    if rc != _lib.OK:
+        msg = _lib.lib().agal_last_error(ctx)
+        raise AgalError(rc, msg.decode() if msg else "")
+
+
+def default_params(**kw) -> AgalParams:
+    """agal_params with the reference defaults (parser.h:62-144), then ``kw``."""
+    p = AgalParams()
+    _check(_lib.lib().agal_params_default(C.byref(p)))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        if isinstance(v, str):
+            v = v.encode()
+        setattr(p, k, v)
+    return p
+
+
+class Parser:
+    """input.txt reader with the reference's rules (inc/parser.h:58-183)."""
+
+    def __init__(self, input_file_directory: Optional[str] = None, params: Optional[AgalParams] = None):
+        self.params = params if params is not None else default_params()
+        self.input_file_directory = input_file_directory
+        if input_file_directory is not None:
+            _check(_lib.lib().agal_params_read(input_file_directory.encode(), C.byref(self.params)))
+
+    @property
+    def params_int(self) -> dict:
+        return {k: getattr(self.params, k) for k in _lib.INT_KEYS}
+
+    @property
+    def params_dbl(self) -> dict:
+        return {k: getattr(self.params, k) for k in _lib.DBL_KEYS}
+
+    @property
+    def params_str(self) -> dict:
+        return {k: getattr(self.params, k).decode() for k in _lib.STR_KEYS}
+
+    def set(self, key: str, value) -> None:
+        _check(_lib.lib().agal_params_set(C.byref(self.params), key.encode(), str(value).encode()))
+
+
+class Case:
+    """One simulation case: an agal_ctx and its device arrays."""
+
+    def __init__(self, params: AgalParams):
+        self._lib = _lib.lib()
+        self.params = params
+        h = C.c_void_p()
+        rc = self._lib.agal_ctx_create(C.byref(params), C.byref(h))
+        if rc != _lib.OK:
+            raise AgalError(rc, self._lib.agal_last_error(None).decode())
+        self._h = h
+        self.dim = 2 if params.velocity_set == _lib.D2Q9 else 3
+        self.Q = {_lib.D2Q9: 9, _lib.D3Q19: 19, _lib.D3Q27: 27}[params.velocity_set]
+        self.M_CBLOCK = 16 if self.dim == 2 else 64
+        self.N_Q_max = 9 if self.dim == 2 else 27
+
+    # -- life cycle -----------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.agal_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc: int) -> None:
+        _check(rc, self._h)
+
+    # -- counts ---------------------------------------------------------
+    def counts(self) -> dict:
+        n_ids = (C.c_int * 17)()
+        id_max = (C.c_int * 17)()
+        n_gaps = C.c_int()
+        nmb = C.c_int64()
+        ml = C.c_int()
+        self._c(self._lib.agal_get_counts(self._h, n_ids, id_max, C.byref(n_gaps), C.byref(nmb), C.byref(ml)))
+        L = ml.value
+        return {"n_ids": list(n_ids[: L + 1]), "id_max": list(id_max[: L + 1]), "n_gaps": n_gaps.value,
+                "n_maxcblocks": nmb.value, "max_levels": L}
+
+    # -- solver entry points -------------------------------------------
+    def set_ic(self, L: int = 0) -> None:
+        self._c(self._lib.agal_set_ic(self._h, L))
+
+    def set_ic_all(self) -> None:
+        for L in range(self.counts()["max_levels"]):
+            self.set_ic(L)
+
+    def refresh(self, L: int = 0) -> None:
+        self._c(self._lib.agal_refresh(self._h, L))
+
+    def advance(self, L: Optional[int] = None) -> None:
+        if L is None:
+            L = self.params.N_LEVEL_START
+        self._c(self._lib.agal_advance(self._h, L))
+
+    def advance_n(self, n: int, use_graph: bool = True) -> None:
+        self._c(self._lib.agal_advance_n(self._h, n, 1 if use_graph else 0))
+
+    def sync(self) -> None:
+        self._c(self._lib.agal_sync(self._h))
+
+    def stream_ptr(self) -> int:
+        """The library's cudaStream_t for this case, as an integer."""
+        s = C.c_void_p()
+        self._c(self._lib.agal_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def mass_momentum(self) -> np.ndarray:
+        out = (C.c_double * 4)()
+        self._c(self._lib.agal_mass_momentum(self._h, out))
+        return np.array(out[: self.dim + 1])
+
+    # -- arrays ---------------------------------------------------------
+    _DTYPES = {_lib.ARR_F: np.float64, _lib.ARR_MACROS: np.float64, _lib.ARR_CBLOCK_F_X: np.float32}
+
+    def array_bytes(self, which: int) -> int:
+        n = C.c_size_t()
+        self._c(self._lib.agal_array_bytes(self._h, which, C.byref(n)))
+        return n.value
+
+    def dump(self, which: int) -> np.ndarray:
+        dt = self._DTYPES.get(which, np.int32)
+        out = np.empty(self.array_bytes(which) // np.dtype(dt).itemsize, dtype=dt)
+        self._c(self._lib.agal_dump(self._h, which, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def load(self, which: int, arr: np.ndarray) -> None:
+        dt = self._DTYPES.get(which, np.int32)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        self._c(self._lib.agal_load(self._h, which, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+
+class Mesh(Case):
+    """Facade with the reference Mesh method names (inc/mesh.h)."""
+
+    def __init__(self, parser: Parser):
+        super().__init__(parser.params)
+        self.parser = parser
+
+    def M_Advance_Step(self) -> None:
+        self.advance()
+
+    def M_AdvanceLoop(self, n_iter: Optional[int] = None) -> None:
+        n = self.params.N_ITER_TOTAL if n_iter is None else n_iter
+        self.advance_n(n, use_graph=True)
+
+
+class Solver_LBM:
+    """Facade with the reference Solver_LBM method names (inc/solver_lbm.h:153-179)."""
+
+    def __init__(self, mesh: Mesh):
+        self.mesh = mesh
+
+    def S_SetIC(self, i_dev: int, L: int) -> int:
+        self.mesh.set_ic(L)
+        return 0
+
+    def S_RefreshVariables(self, i_dev: int, L: int, var: int = 0) -> int:
+        self.mesh.refresh(L)
+        return 0
+
+    def S_Advance(self, i_dev: int, L: int, tmp=None) -> int:
+        self.mesh.advance(L)
+        return 0

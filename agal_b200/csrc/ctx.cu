@@ -1,0 +1,538 @@
+// Context life cycle, root grid, host<->device array transfers and the
+// advance entry points of the C ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "ctx.h"
+#include "lattice.cuh"
+#include "storage.cuh"
+
+using namespace agal;
+
+static std::string g_create_err;
+
+int agal_set_err(agal_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg; else g_create_err = msg;
+    return code;
+}
+
+int agal_cuda_check(agal_ctx *c, cudaError_t e, const char *what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return agal_set_err(c, AGAL_ERR_OOM, m);
+    return agal_set_err(c, AGAL_ERR_CUDA, m);
+}
+
+namespace {
+
+// Padded root-grid value (mesh_init.cu:406-460): boundaries are written z,
+// then y, then x, so x wins at edges/corners; periodic faces wrap.
+int root_padded_id(const agal_ctx *c, int bx, int by, int bz, int i, int j, int k)
+{
+    if (i < 1 || i > bx) {
+        if (!c->P.PERIODIC_X) return (i < 1) ? -1 : -2;
+        i = (i < 1) ? bx : 1;
+    }
+    if (j < 1 || j > by) {
+        if (!c->P.PERIODIC_Y) return (j < 1) ? -3 : -4;
+        j = (j < 1) ? by : 1;
+    }
+    if (c->dim == 3 && (k < 1 || k > bz)) {
+        if (!c->P.PERIODIC_Z) return (k < 1) ? -5 : -6;
+        k = (k < 1) ? bz : 1;
+    }
+    if (c->dim == 2) k = 1;
+    return (i - 1) + bx * ((j - 1) + by * (k - 1));
+}
+
+template <typename T>
+__global__ void k_fill(T *p, long long n, T v)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+template <typename T>
+int fill(agal_ctx *c, T *p, long long n, T v)
+{
+    if (n <= 0) return AGAL_OK;
+    k_fill<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(p, n, v);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
+size_t compute_size(const agal_ctx *c) { return c->storage == AGAL_STORE_FP64 ? 8 : 4; }
+
+void release(agal_ctx *c)
+{
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
+                    c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
+                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+}  // namespace
+
+extern "C" const char *agal_last_error(const agal_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : g_create_err.c_str();
+}
+
+extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
+{
+    if (!p || !out) return agal_set_err(nullptr, AGAL_ERR_PARAM, "null argument");
+    *out = nullptr;
+    agal_ctx *c = new (std::nothrow) agal_ctx();
+    if (!c) return agal_set_err(nullptr, AGAL_ERR_OOM, "host allocation failed");
+    c->P = *p;
+    switch (p->velocity_set) {
+    case AGAL_D2Q9: c->dim = 2; c->Q = 9; break;
+    case AGAL_D3Q19: c->dim = 3; c->Q = 19; break;
+    case AGAL_D3Q27: c->dim = 3; c->Q = 27; break;
+    default: delete c; return agal_set_err(nullptr, AGAL_ERR_PARAM, "velocity_set");
+    }
+    if (p->collision != AGAL_BGK) { delete c; return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "collision operator not built yet"); }
+    c->Qmax = (c->dim == 2) ? 9 : 27;
+    c->MC = (c->dim == 2) ? 16 : 64;
+    c->NCH = (c->dim == 2) ? 4 : 8;
+    c->storage = p->storage;
+    switch (p->storage) {
+    case AGAL_STORE_FP32: c->esize = 4; break;
+    case AGAL_STORE_FP64: c->esize = 8; break;
+    case AGAL_STORE_FP16:
+    case AGAL_STORE_BF16: c->esize = 2; break;
+    default: delete c; return agal_set_err(nullptr, AGAL_ERR_PARAM, "storage");
+    }
+
+    // mesh_init.cu:22-91
+    const float Lx = (float)p->L_c;
+    const float Ly = (float)(p->L_fy * Lx);
+    const float Lz = (float)(p->L_fz * Lx);
+    c->Nx = p->Nx;
+    c->Ny = (int)(c->Nx * (Ly / Lx));
+    c->Nz = (c->dim == 2) ? 1 : (int)(c->Nx * (Lz / Lx));
+    if (c->Nx <= 0 || c->Nx % 4 || c->Ny <= 0 || c->Ny % 4 || (c->dim == 3 && (c->Nz <= 0 || c->Nz % 4))) {
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_PARAM, "grid sizes must be positive multiples of 4");
+    }
+    c->dx = Lx / (float)c->Nx;
+    c->dx_cblock = 4.0f * c->dx;
+    c->max_levels = std::max(p->MAX_LEVELS_WALL, p->MAX_LEVELS_INTERIOR);
+    if (c->max_levels < 1 || c->max_levels > 16) { delete c; return agal_set_err(nullptr, AGAL_ERR_PARAM, "MAX_LEVELS"); }
+    c->L0 = p->N_LEVEL_START;
+    if (c->max_levels == 1) c->L0 = 0;
+    if (c->L0 > c->max_levels - 1) c->L0 = c->max_levels - 1;
+    const bool fp64 = (p->storage == AGAL_STORE_FP64);
+    c->dxf.resize(c->max_levels);
+    c->tau.resize(c->max_levels);
+    for (int L = 0; L < c->max_levels; L++) {
+        const double d = (double)c->dx / std::pow(2.0, (double)L);
+        c->dxf[L] = fp64 ? d : (double)(float)d;
+        // solver_lbm_init.cu:51: tau_L = v0*3 + 0.5*dx_L, rounded to ufloat_t.
+        const double t = p->v0 * 3.0 + 0.5 * c->dxf[L];
+        c->tau[L] = fp64 ? t : (double)(float)t;
+    }
+
+    const int bx = c->Nx / 4, by = c->Ny / 4, bz = (c->dim == 2) ? 1 : c->Nz / 4;
+    const long long n_coarse = (long long)bx * by * bz;
+
+    int rc;
+    if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) {
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_CUDA, "cudaSetDevice failed");
+    }
+    if ((rc = cudaGetDevice(&c->device)) != cudaSuccess) { delete c; return agal_set_err(nullptr, AGAL_ERR_CUDA, "no CUDA device"); }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_CUDA, "stream creation failed");
+    }
+
+    // Capacity: explicit, or from free memory like mesh_init.cu:155-169.
+    const size_t per_block =
+        (size_t)c->MC * (2 * c->Q * c->esize + (c->dim + 1) * compute_size(c) + sizeof(int)) +
+        sizeof(float) * c->dim + sizeof(int) * (2 * c->Qmax + 5 + c->max_levels);
+    if (p->n_maxcblocks > 0) {
+        c->nmb = p->n_maxcblocks;
+    } else {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        const double frac = (p->mem_frac > 0 && p->mem_frac < 1) ? p->mem_frac : 0.975;
+        long long ncell = (long long)((double)fr * frac / (double)per_block) * c->MC;
+        ncell = ((ncell + 1024) / 2048) * 2048;   // M_RNDOFF
+        c->nmb = ncell / c->MC;
+    }
+    if (n_coarse > c->nmb) {
+        release(c);
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_OOM, "ERROR: Root grid size exceeds limits...");
+    }
+    c->nmc = c->nmb * c->MC;
+    const long long nmb = c->nmb, nmc = c->nmc;
+
+#define ALLOC(ptr, bytes)                                                              \
+    do {                                                                               \
+        if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                     \
+            cudaGetLastError();                                                        \
+            release(c);                                                                \
+            delete c;                                                                  \
+            return agal_set_err(nullptr, AGAL_ERR_OOM, "device allocation failed: " #ptr); \
+        }                                                                              \
+    } while (0)
+    ALLOC(c->F[0], c->esize * (size_t)c->Q * nmc);
+    ALLOC(c->F[1], c->esize * (size_t)c->Q * nmc);
+    ALLOC(c->macro, compute_size(c) * (size_t)(c->dim + 1) * nmc);
+    ALLOC(c->cells_ID_mask, sizeof(int) * nmc);
+    ALLOC(c->cblock_f_X, sizeof(float) * c->dim * nmb);
+    ALLOC(c->cblock_ID_mask, sizeof(int) * nmb);
+    ALLOC(c->cblock_ID_nbr, sizeof(int) * c->Qmax * nmb);
+    ALLOC(c->cblock_ID_nbr_child, sizeof(int) * c->Qmax * nmb);
+    ALLOC(c->cblock_ID_onb, sizeof(int) * nmb);
+    ALLOC(c->cblock_ID_ref, sizeof(int) * nmb);
+    ALLOC(c->cblock_level, sizeof(int) * nmb);
+    ALLOC(c->id_set, sizeof(int) * c->max_levels * nmb);
+    ALLOC(c->gap_set, sizeof(int) * nmb);
+    ALLOC(c->red_out, sizeof(double) * 4);
+#undef ALLOC
+
+    // Reset values, mesh_init.cu:285-304.
+    if ((rc = fill<int>(c, c->cells_ID_mask, nmc, CELL_INTERIOR)) ||
+        (rc = fill<int>(c, c->cblock_ID_mask, nmb, BLOCK_REGULAR)) ||
+        (rc = fill<int>(c, c->cblock_ID_nbr, c->Qmax * nmb, N_SKIPID)) ||
+        (rc = fill<int>(c, c->cblock_ID_nbr_child, c->Qmax * nmb, N_SKIPID)) ||
+        (rc = fill<int>(c, c->cblock_ID_ref, nmb, REF_INACTIVE)) ||
+        (rc = fill<int>(c, c->cblock_level, nmb, 0)) || (rc = fill<int>(c, c->cblock_ID_onb, nmb, 0)) ||
+        (rc = fill<int>(c, c->id_set, c->max_levels * nmb, -1)) || (rc = fill<int>(c, c->gap_set, nmb, -1)) ||
+        (rc = fill<float>(c, c->cblock_f_X, c->dim * nmb, 0.0f))) {
+        std::string m = c->err;
+        release(c);
+        delete c;
+        return agal_set_err(nullptr, rc, m);
+    }
+    cudaMemsetAsync(c->F[0], 0, c->esize * (size_t)c->Q * nmc, c->stream);
+    cudaMemsetAsync(c->F[1], 0, c->esize * (size_t)c->Q * nmc, c->stream);
+    cudaMemsetAsync(c->macro, 0, compute_size(c) * (size_t)(c->dim + 1) * nmc, c->stream);
+
+    // Root grid (mesh_init.cu:354-516), built on the host and copied in.
+    std::vector<int> nbr((size_t)c->Qmax * n_coarse), onb(n_coarse), ref(n_coarse, REF_UNREFINED);
+    std::vector<float> fX((size_t)c->dim * n_coarse);
+    for (int k = 1; k <= bz; k++)
+        for (int j = 1; j <= by; j++)
+            for (int i = 1; i <= bx; i++) {
+                const int b = root_padded_id(c, bx, by, bz, i, j, k);
+                fX[b] = (float)(i - 1) * c->dx_cblock;
+                fX[b + n_coarse] = (float)(j - 1) * c->dx_cblock;
+                if (c->dim == 3) fX[b + 2 * n_coarse] = (float)(k - 1) * c->dx_cblock;
+                int on = 0;
+                for (int q = 0; q < c->Qmax; q++) {
+                    const int nb = root_padded_id(c, bx, by, bz, i + lat_c(c->dim, 0, q), j + lat_c(c->dim, 1, q),
+                                                  k + lat_c(c->dim, 2, q));
+                    nbr[b + (size_t)q * n_coarse] = nb;
+                    if (nb < 0) on = 1;
+                }
+                onb[b] = on;
+            }
+    std::vector<int> gaps(nmb - n_coarse), ids(n_coarse);
+    for (long long x = 0; x < n_coarse; x++) ids[x] = (int)x;
+    for (long long x = 0; x < nmb - n_coarse; x++) gaps[x] = (int)((nmb - 1) - x);
+#define H2D(dst, src, bytes) \
+    do { cudaError_t e_ = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice); \
+         if (e_ != cudaSuccess) { int r_ = agal_cuda_check(c, e_, "root grid copy"); std::string m = c->err; release(c); delete c; return agal_set_err(nullptr, r_, m); } } while (0)
+    cudaStreamSynchronize(c->stream);
+    H2D(c->cblock_ID_ref, ref.data(), sizeof(int) * n_coarse);
+    for (int q = 0; q < c->Qmax; q++) {
+        H2D(c->cblock_ID_nbr + (size_t)q * nmb, nbr.data() + (size_t)q * n_coarse, sizeof(int) * n_coarse);
+        // nbr_child: boundary IDs copied, N_SKIPID elsewhere (mesh_init.cu:489)
+        std::vector<int> ch(n_coarse);
+        for (long long b = 0; b < n_coarse; b++) {
+            const int v = nbr[b + (size_t)q * n_coarse];
+            ch[b] = v < 0 ? v : N_SKIPID;
+        }
+        H2D(c->cblock_ID_nbr_child + (size_t)q * nmb, ch.data(), sizeof(int) * n_coarse);
+    }
+    H2D(c->cblock_ID_onb, onb.data(), sizeof(int) * n_coarse);
+    for (int d = 0; d < c->dim; d++)
+        H2D(c->cblock_f_X + (size_t)d * nmb, fX.data() + (size_t)d * n_coarse, sizeof(float) * n_coarse);
+    H2D(c->id_set, ids.data(), sizeof(int) * n_coarse);
+    if (!gaps.empty()) H2D(c->gap_set, gaps.data(), sizeof(int) * gaps.size());
+#undef H2D
+    c->n_ids.assign(c->max_levels + 1, 0);
+    c->id_max.assign(c->max_levels + 1, 0);
+    c->n_ids[0] = (int)n_coarse;
+    c->id_max[0] = c->id_max[c->max_levels] = (int)n_coarse;
+    c->n_gaps = (int)(nmb - n_coarse);
+    c->cur.assign(c->max_levels, 0);
+    *out = c;
+    return AGAL_OK;
+}
+
+extern "C" int agal_ctx_destroy(agal_ctx *ctx)
+{
+    if (!ctx) return AGAL_ERR_PARAM;
+    cudaStreamSynchronize(ctx->stream);
+    release(ctx);
+    delete ctx;
+    return AGAL_OK;
+}
+
+extern "C" int agal_get_counts(const agal_ctx *c, int *n_ids, int *id_max, int *n_gaps, int64_t *n_maxcblocks,
+                               int *max_levels)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    for (int L = 0; L <= c->max_levels; L++) {
+        if (n_ids) n_ids[L] = c->n_ids[L];
+        if (id_max) id_max[L] = c->id_max[L];
+    }
+    if (n_gaps) *n_gaps = c->n_gaps;
+    if (n_maxcblocks) *n_maxcblocks = c->nmb;
+    if (max_levels) *max_levels = c->max_levels;
+    return AGAL_OK;
+}
+
+extern "C" int agal_sync(agal_ctx *c)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
+extern "C" int agal_get_stream(const agal_ctx *c, void **stream)
+{
+    if (!c || !stream) return AGAL_ERR_PARAM;
+    *stream = (void *)c->stream;
+    return AGAL_OK;
+}
+
+extern "C" int agal_set_ic(agal_ctx *c, int L)
+{
+    if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;
+    return agal_launch_set_ic(c, L);
+}
+
+extern "C" int agal_refresh(agal_ctx *c, int L)
+{
+    if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;
+    return agal_launch_refresh(c, L);
+}
+
+extern "C" int agal_mass_momentum(agal_ctx *c, double *out)
+{
+    if (!c || !out) return AGAL_ERR_PARAM;
+    return agal_launch_mass(c, out);
+}
+
+// ---------------------------------------------------------------------------
+// Advance (solver_lbm_advance.cu:31-174).  The single-level branch
+// (:239-251) is one fused kernel per step.
+static int advance_level(agal_ctx *c, int L)
+{
+    if (c->max_levels > 1 && c->max_levels != c->L0 + 1)
+        return agal_set_err(c, AGAL_ERR_UNSUPPORTED, "multi-level advance not built yet");
+    return agal_launch_step(c, L);
+}
+
+extern "C" int agal_advance(agal_ctx *c, int L)
+{
+    if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;
+    return advance_level(c, L);
+}
+
+extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
+{
+    if (!c || n < 0) return AGAL_ERR_PARAM;
+    if (!use_graph) {
+        for (int i = 0; i < n; i++) {
+            int rc = advance_level(c, c->L0);
+            if (rc) return rc;
+        }
+        return AGAL_OK;
+    }
+    // Capture n steps once; replay while the captured buffer parity matches.
+    if (!c->graph_exec || c->graph_steps != n || c->graph_cur_in != c->cur) {
+        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+        std::vector<int> cur0 = c->cur;
+        cudaGraph_t g = nullptr;
+        AGAL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = AGAL_OK;
+        for (int i = 0; i < n && rc == AGAL_OK; i++) rc = advance_level(c, c->L0);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->cur = cur0;   // capture only recorded the launches
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGraphInstantiate");
+        c->graph_steps = n;
+        c->graph_cur_in = cur0;
+    }
+    AGAL_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+    for (int L = 0; L < c->max_levels; L++)
+        if (n & 1) c->cur[L] = 1 - c->cur[L];   // single-level: every level stepped n times
+    return AGAL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Array transfers.
+extern "C" int agal_array_bytes(const agal_ctx *c, int which, size_t *bytes)
+{
+    if (!c || !bytes) return AGAL_ERR_PARAM;
+    const size_t nmb = (size_t)c->nmb, nmc = (size_t)c->nmc;
+    switch (which) {
+    case AGAL_ARR_F: *bytes = sizeof(double) * (size_t)c->Q * nmc; break;
+    case AGAL_ARR_MACROS: *bytes = sizeof(double) * (size_t)(c->dim + 1) * nmc; break;
+    case AGAL_ARR_CELLS_ID_MASK: *bytes = sizeof(int) * nmc; break;
+    case AGAL_ARR_CBLOCK_F_X: *bytes = sizeof(float) * (size_t)c->dim * nmb; break;
+    case AGAL_ARR_CBLOCK_ID_MASK:
+    case AGAL_ARR_CBLOCK_ID_ONB:
+    case AGAL_ARR_CBLOCK_ID_REF:
+    case AGAL_ARR_CBLOCK_LEVEL:
+    case AGAL_ARR_GAP_SET: *bytes = sizeof(int) * nmb; break;
+    case AGAL_ARR_CBLOCK_ID_NBR:
+    case AGAL_ARR_CBLOCK_ID_NBR_CHILD: *bytes = sizeof(int) * (size_t)c->Qmax * nmb; break;
+    case AGAL_ARR_ID_SET: *bytes = sizeof(int) * (size_t)c->max_levels * nmb; break;
+    default: return AGAL_ERR_PARAM;
+    }
+    return AGAL_OK;
+}
+
+static void *int_array(agal_ctx *c, int which)
+{
+    switch (which) {
+    case AGAL_ARR_CELLS_ID_MASK: return c->cells_ID_mask;
+    case AGAL_ARR_CBLOCK_F_X: return c->cblock_f_X;
+    case AGAL_ARR_CBLOCK_ID_MASK: return c->cblock_ID_mask;
+    case AGAL_ARR_CBLOCK_ID_NBR: return c->cblock_ID_nbr;
+    case AGAL_ARR_CBLOCK_ID_NBR_CHILD: return c->cblock_ID_nbr_child;
+    case AGAL_ARR_CBLOCK_ID_ONB: return c->cblock_ID_onb;
+    case AGAL_ARR_CBLOCK_ID_REF: return c->cblock_ID_ref;
+    case AGAL_ARR_CBLOCK_LEVEL: return c->cblock_level;
+    case AGAL_ARR_ID_SET: return c->id_set;
+    case AGAL_ARR_GAP_SET: return c->gap_set;
+    default: return nullptr;
+    }
+}
+
+template <typename T>
+static void decode(const std::vector<unsigned char> &raw, size_t i, int Q, int p, double *o)
+{
+    const T v = reinterpret_cast<const T *>(raw.data())[i];
+    *o = (double)ST<T>::dec(v) + (ST<T>::OFF ? lat_w(Q, p) : 0.0);
+}
+
+template <typename T>
+static void encode(std::vector<unsigned char> &raw, size_t i, int Q, int p, double v)
+{
+    using C = typename ST<T>::C;
+    reinterpret_cast<T *>(raw.data())[i] = ST<T>::enc((C)(v - (ST<T>::OFF ? lat_w(Q, p) : 0.0)));
+}
+
+// Buffer index each block's populations currently live in.
+static int block_buffers(agal_ctx *c, std::vector<int> &which_buf)
+{
+    std::vector<int> lev(c->nmb), ref(c->nmb);
+    AGAL_CUDA(c, cudaMemcpy(lev.data(), c->cblock_level, sizeof(int) * c->nmb, cudaMemcpyDeviceToHost));
+    AGAL_CUDA(c, cudaMemcpy(ref.data(), c->cblock_ID_ref, sizeof(int) * c->nmb, cudaMemcpyDeviceToHost));
+    which_buf.resize(c->nmb);
+    for (long long b = 0; b < c->nmb; b++) {
+        const int L = (ref[b] != REF_INACTIVE && lev[b] >= 0 && lev[b] < c->max_levels) ? lev[b] : 0;
+        which_buf[b] = c->cur[L];
+    }
+    return AGAL_OK;
+}
+
+extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
+{
+    size_t need = 0;
+    int rc = agal_array_bytes(c, which, &need);
+    if (rc) return rc;
+    if (!host_buf || bytes != need) return agal_set_err(c, AGAL_ERR_PARAM, "dump size mismatch");
+    AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (which == AGAL_ARR_F) {
+        const size_t n = (size_t)c->Q * c->nmc;
+        std::vector<unsigned char> raw[2];
+        for (int k = 0; k < 2; k++) {
+            raw[k].resize(n * c->esize);
+            AGAL_CUDA(c, cudaMemcpy(raw[k].data(), c->F[k], n * c->esize, cudaMemcpyDeviceToHost));
+        }
+        std::vector<int> wb, cm(c->nmc);
+        if ((rc = block_buffers(c, wb))) return rc;
+        AGAL_CUDA(c, cudaMemcpy(cm.data(), c->cells_ID_mask, sizeof(int) * c->nmc, cudaMemcpyDeviceToHost));
+        double *o = static_cast<double *>(host_buf);
+        for (int s = 0; s < c->Q; s++) {
+            const int p = lat_pb(c->dim, s);   // slot s holds f_p, w_p == w_s
+            for (long long cell = 0; cell < c->nmc; cell++) {
+                const size_t i = (size_t)s * c->nmc + cell;
+                const auto &r = raw[wb[cell / c->MC]];
+                switch (c->storage) {
+                case AGAL_STORE_FP32: decode<float>(r, i, c->Q, p, &o[i]); break;
+                case AGAL_STORE_FP64: decode<double>(r, i, c->Q, p, &o[i]); break;
+                case AGAL_STORE_FP16: decode<__half>(r, i, c->Q, p, &o[i]); break;
+                case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, i, c->Q, p, &o[i]); break;
+                }
+                if (cm[cell] == CELL_SOLID) o[i] = -1.0;
+            }
+        }
+        return AGAL_OK;
+    }
+    if (which == AGAL_ARR_MACROS) {
+        const size_t n = (size_t)(c->dim + 1) * c->nmc;
+        double *o = static_cast<double *>(host_buf);
+        if (c->storage == AGAL_STORE_FP64) {
+            AGAL_CUDA(c, cudaMemcpy(o, c->macro, n * 8, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> t(n);
+            AGAL_CUDA(c, cudaMemcpy(t.data(), c->macro, n * 4, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; i++) o[i] = t[i];
+        }
+        return AGAL_OK;
+    }
+    AGAL_CUDA(c, cudaMemcpy(host_buf, int_array(c, which), need, cudaMemcpyDeviceToHost));
+    return AGAL_OK;
+}
+
+extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t bytes)
+{
+    size_t need = 0;
+    int rc = agal_array_bytes(c, which, &need);
+    if (rc) return rc;
+    if (!host_buf || bytes != need) return agal_set_err(c, AGAL_ERR_PARAM, "load size mismatch");
+    AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (which == AGAL_ARR_F) {
+        // The same values go to both buffers.
+        const size_t n = (size_t)c->Q * c->nmc;
+        std::vector<unsigned char> raw(n * c->esize);
+        const double *in = static_cast<const double *>(host_buf);
+        for (int s = 0; s < c->Q; s++) {
+            const int p = lat_pb(c->dim, s);
+            for (long long cell = 0; cell < c->nmc; cell++) {
+                const size_t i = (size_t)s * c->nmc + cell;
+                switch (c->storage) {
+                case AGAL_STORE_FP32: encode<float>(raw, i, c->Q, p, in[i]); break;
+                case AGAL_STORE_FP64: encode<double>(raw, i, c->Q, p, in[i]); break;
+                case AGAL_STORE_FP16: encode<__half>(raw, i, c->Q, p, in[i]); break;
+                case AGAL_STORE_BF16: encode<__nv_bfloat16>(raw, i, c->Q, p, in[i]); break;
+                }
+            }
+        }
+        for (int k = 0; k < 2; k++) AGAL_CUDA(c, cudaMemcpy(c->F[k], raw.data(), raw.size(), cudaMemcpyHostToDevice));
+        return AGAL_OK;
+    }
+    if (which == AGAL_ARR_MACROS) return agal_set_err(c, AGAL_ERR_PARAM, "macros are derived, not loaded");
+    AGAL_CUDA(c, cudaMemcpy(int_array(c, which), host_buf, need, cudaMemcpyHostToDevice));
+    if (which == AGAL_ARR_CELLS_ID_MASK) {
+        // Geometry present when any cell is solid.
+        std::vector<int> cm(c->nmc);
+        std::memcpy(cm.data(), host_buf, need);
+        c->geometry_init = std::any_of(cm.begin(), cm.end(), [](int v) { return v == CELL_SOLID; }) ? 1 : 0;
+    }
+    return AGAL_OK;
+}

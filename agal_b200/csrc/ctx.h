@@ -1,0 +1,79 @@
+// Private state of one simulation case (the object behind agal_ctx*).
+//
+// Device layout in HBM, per case:
+//   F[2]            two population buffers, each Q slots x n_maxcells of the
+//                   storage type (float, double, or half/bf16 weight offsets),
+//                   slot s of a cell holding f_{pb(s)} (the reference's
+//                   post-stream convention, solver_lbm_kernels.cu:67/251).
+//                   Level L's current buffer is cur[L]; a step of level L
+//                   reads F[cur[L]] and writes F[1-cur[L]].
+//   macro           (dim+1) x n_maxcells float/double, written on demand.
+//   block arrays    structure-of-arrays over n_maxcblocks exactly as
+//                   inc/mesh.h:366-459 (neighbours [Qmax][n_maxcblocks], ...).
+//   id_set          [MAX_LEVELS][n_maxcblocks], sorted block IDs per level.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/agal_b200.h"
+
+struct agal_ctx {
+    agal_params P{};
+    int dim = 2, Q = 9, Qmax = 9, MC = 16, NCH = 4;
+    int storage = AGAL_STORE_FP32;
+    size_t esize = 4;                  // bytes per stored population
+    int64_t nmb = 0, nmc = 0;          // n_maxcblocks, n_maxcells
+    int max_levels = 1, L0 = 0;
+    int Nx = 0, Ny = 0, Nz = 1;
+    float dx = 0.f, dx_cblock = 0.f;
+    std::vector<double> dxf;           // dxf_vec (rounded to the compute type)
+    std::vector<double> tau;           // tau_vec (rounded to the compute type)
+    // host mirrors (authoritative for launch sizes, as in the reference)
+    std::vector<int> n_ids, id_max;
+    int n_gaps = 0;
+    int geometry_init = 0;
+    // device arrays
+    void *F[2] = {nullptr, nullptr};
+    std::vector<int> cur;              // current population buffer per level
+    void *macro = nullptr;
+    int *cells_ID_mask = nullptr;
+    float *cblock_f_X = nullptr;
+    int *cblock_ID_mask = nullptr;
+    int *cblock_ID_nbr = nullptr;
+    int *cblock_ID_nbr_child = nullptr;
+    int *cblock_ID_onb = nullptr;
+    int *cblock_ID_ref = nullptr;
+    int *cblock_level = nullptr;
+    int *id_set = nullptr;
+    int *gap_set = nullptr;
+    double *red = nullptr;             // reduction scratch for FP64 sums
+    int red_len = 0;
+    double *red_out = nullptr;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    // graph of n coarse steps (agal_advance_n)
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_steps = 0;
+    std::vector<int> graph_cur_in;     // cur[] the graph was captured with
+    int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
+    std::string err;
+};
+
+// Error helpers shared by the translation units.
+int agal_set_err(agal_ctx *c, int code, const std::string &msg);
+int agal_cuda_check(agal_ctx *c, cudaError_t e, const char *what);
+#define AGAL_CUDA(c, call)                                             \
+    do {                                                               \
+        cudaError_t e_ = (call);                                       \
+        if (e_ != cudaSuccess) return agal_cuda_check((c), e_, #call); \
+    } while (0)
+
+// Kernel launchers (step_kernels.cu).
+int agal_launch_set_ic(agal_ctx *c, int L);
+int agal_launch_step(agal_ctx *c, int L);
+int agal_launch_refresh(agal_ctx *c, int L);
+int agal_launch_mass(agal_ctx *c, double *out);

@@ -1,0 +1,80 @@
+// Lattice tables and block-local index maths for the device kernels.
+//
+// The direction order, opposite map and weights must be those of the
+// reference (inc/util.h:94-101, solver_lbm_init.cu:79-91): they define the slot
+// convention of the population arrays that callers read and write.  All
+// functions are constexpr so that, inside fully unrolled loops over p, every
+// table lookup folds to an immediate.
+#pragma once
+
+#include <cstdint>
+
+namespace agal {
+
+constexpr int N_SKIPID = -999;   // cppspec.h:125
+constexpr int N_SPECID = -998;   // cppspec.h:124
+
+// Reference enumerations (inc/mesh.h:34-105).
+constexpr int REF_UNREFINED = 0, REF_REFINED = 1, REF_REFINED_WCHILD = 2, REF_REFINED_PERM = 3,
+              REF_MARK_REFINE = 4, REF_MARK_COARSEN = 5, REF_NEW = 6, REF_REMOVE = 7,
+              REF_INACTIVE = 8, REF_UNREFINED_VIO = 9, REF_REFINED_WCHILD_PERM = 10;
+constexpr int CELL_INTERIOR = 0, CELL_INTERFACE = 1, CELL_GHOST = 2, CELL_SOLID = -1,
+              CELL_GUARD = -2, CELL_BOUNDARY = -6;
+constexpr int BLOCK_REGULAR = 0, BLOCK_INTERFACE = 1, BLOCK_SOLIDB = -1, BLOCK_SOLIDA = -2,
+              BLOCK_SOLID = -3;
+
+template <int DIM> struct Geo;
+template <> struct Geo<2> { static constexpr int MC = 16, QMAX = 9, NCH = 4; };
+template <> struct Geo<3> { static constexpr int MC = 64, QMAX = 27, NCH = 8; };
+
+__host__ __device__ constexpr int lat_c(int dim, int axis, int p)
+{
+    constexpr int c2[3][9] = {{0, 1, 0, -1, 0, 1, -1, -1, 1},
+                              {0, 0, 1, 0, -1, 1, 1, -1, -1},
+                              {0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    constexpr int c3[3][27] = {
+        {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1},
+        {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1},
+        {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1}};
+    return dim == 2 ? c2[axis][p] : c3[axis][p];
+}
+
+__host__ __device__ constexpr int lat_pb(int dim, int p)
+{
+    constexpr int pb2[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+    constexpr int pb3[27] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13,
+                             16, 15, 18, 17, 20, 19, 22, 21, 24, 23, 26, 25};
+    return dim == 2 ? pb2[p] : pb3[p];
+}
+
+// Weights: D2Q9 4/9,1/9,1/36; D3Q19 1/3,1/18,1/36; D3Q27 8/27,2/27,1/54,1/216.
+__host__ __device__ constexpr double lat_w(int Q, int p)
+{
+    return Q == 9 ? (p == 0 ? 4.0 / 9.0 : (p < 5 ? 1.0 / 9.0 : 1.0 / 36.0))
+         : Q == 19 ? (p == 0 ? 1.0 / 3.0 : (p < 7 ? 1.0 / 18.0 : 1.0 / 36.0))
+         : (p == 0 ? 8.0 / 27.0 : (p < 7 ? 2.0 / 27.0 : (p < 19 ? 1.0 / 54.0 : 1.0 / 216.0)));
+}
+
+// Neighbour-array index of the lexicographic neighbour slot S (util.h:100-101).
+__host__ __device__ constexpr int lat_map(int dim, int S)
+{
+    constexpr int m2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
+    constexpr int m3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
+                            1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
+    return dim == 2 ? m2[S] : m3[S];
+}
+
+// Lexicographic neighbour slot of a cell index in {-1..4}^dim (util_index.h:45-66).
+__host__ __device__ constexpr int nbr_slot(int dim, int I, int J, int K)
+{
+    return ((I >= 4) ? 2 : (I >= 0 ? 1 : 0)) + 3 * ((J >= 4) ? 2 : (J >= 0 ? 1 : 0)) +
+           (dim == 3 ? 9 * ((K >= 4) ? 2 : (K >= 0 ? 1 : 0)) : 0);
+}
+// Cell id after wrapping into the neighbour block (util_index.h:88-98).
+__host__ __device__ constexpr int nbr_cell(int dim, int I, int J, int K)
+{
+    return ((I + 4) & 3) + 4 * ((J + 4) & 3) + (dim == 3 ? 16 * ((K + 4) & 3) : 0);
+}
+__host__ __device__ constexpr int center_slot(int dim) { return dim == 2 ? 4 : 13; }
+
+}  // namespace agal

@@ -1,0 +1,523 @@
+// Per-level LBM kernels: initial conditions, the fused collide + boundary +
+// stream step, macro refresh and FP64 mass/momentum sums.
+//
+// The fused step replaces the reference's sequence
+//   Cu_RefreshVariables -> Cu_Collide -> Cu_ImposeBC -> Cu_Stream
+// (solver_lbm_kernels.cu:112, 206, 693, 534), which reads and writes the
+// populations in place four times per step, by ONE pass that reads the Q
+// populations of a cell from buffer A and pushes the Q post-collision values
+// to their destination cells in buffer B.  Buffer B then holds exactly what
+// the reference's in-place swap leaves behind: slot pb(p) of cell x + c_p
+// holds f*_p(x) when the link is open; when it is closed (domain boundary,
+// missing same-level neighbour, solid neighbour cell) slot p of x holds
+// f*_p(x), passed through the boundary hook for a domain boundary.
+// Algorithmic traffic: 2 * Q * sizeof(storage) bytes per cell update.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "ctx.h"
+#include "lattice.cuh"
+#include "storage.cuh"
+
+namespace agal {
+
+__constant__ int c_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
+__constant__ int c_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
+                               1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
+
+struct StepArgs {
+    const int *ids;
+    int n;
+    const void *fin;
+    void *fout;
+    long long nmc, nmb;
+    const int *nbr, *nbr_child, *bmask, *onb, *cmask;
+    double omega;
+    double u_ref;
+    int bc_preset;
+    int has_solid;
+};
+
+// Boundary hook presets (inc/custom.h:79-122); f is the full population.
+template <typename C>
+__device__ __forceinline__ C bc_hook(int preset, int nb, C f, C rho, C u, C v, C w, C wp, int cx,
+                                     int cy, int cz, C U)
+{
+    (void)rho;
+    bool inflow = false, outflow = false;
+    switch (preset) {
+    case AGAL_BC_LDC2D: inflow = (nb == -4); break;
+    case AGAL_BC_LDC3D: inflow = (nb == -6); break;
+    case AGAL_BC_FPSC2D: inflow = (nb == -1 || nb == -3 || nb == -4); outflow = (nb == -2); break;
+    case AGAL_BC_FPSC3D:
+        inflow = (nb == -1 || nb == -3 || nb == -4 || nb == -5 || nb == -6);
+        outflow = (nb == -2);
+        break;
+    default: break;
+    }
+    if (inflow) return f - C(2) * wp * (C(3) * (C(cx) * U));
+    if (outflow) {
+        C cu = C(cx) * u + C(cy) * v + C(cz) * w;
+        C e = C(1) + C(4.5) * cu * cu - C(1.5) * (u * u + v * v + w * w);
+        return -f + C(2) * wp * e;
+    }
+    return f;
+}
+
+template <int DIM, int Q, typename T, int BPC>
+__global__ void __launch_bounds__(BPC *Geo<DIM>::MC)
+k_step(const StepArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX;
+    __shared__ int s_nbr[BPC][QMAX];
+    __shared__ int s_blk[BPC];
+    __shared__ int s_flag[BPC];
+    const int tid = threadIdx.x;
+    const long long base = (long long)blockIdx.x * BPC;
+
+    if (tid < BPC) {
+        long long kap = base + tid;
+        int b = -1, fl = 0;
+        if (kap < a.n) {
+            b = a.ids[kap];
+            if (b >= 0) {
+                if (a.nbr_child[b] < 0 || a.bmask[b] != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
+                if (a.onb[b] == 1) fl |= 2;                                     // kernels.cu:736
+            }
+        }
+        s_blk[tid] = b;
+        s_flag[tid] = fl;
+    }
+    __syncthreads();
+    for (int i = tid; i < BPC * QMAX; i += BPC * MC) {
+        const int S = i / BPC, lb = i % BPC;
+        const int b = s_blk[lb];
+        const int m = (DIM == 2) ? c_map2[S] : c_map3[S];
+        s_nbr[lb][S] = (b >= 0) ? a.nbr[b + (long long)m * a.nmb] : N_SKIPID;
+    }
+    __syncthreads();
+
+    const int lb = tid / MC, t = tid % MC;
+    const int b = s_blk[lb];
+    const int fl = s_flag[lb];
+    if (b < 0 || !(fl & 1)) return;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const long long cell = (long long)b * MC + t;
+    if (a.has_solid && a.cmask[cell] == CELL_SOLID) return;   // solid cells keep their guard
+
+    const T *__restrict__ fin = static_cast<const T *>(a.fin);
+    T *__restrict__ fout = static_cast<T *>(a.fout);
+    const long long nmc = a.nmc;
+
+    // Load: slot pb(p) holds f_p (offset form g_p for half storage).
+    C g[Q];
+#pragma unroll
+    for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(__ldg(&fin[(long long)lat_pb(DIM, p) * nmc + cell]));
+
+    C rho, drho = C(0), jx = C(0), jy = C(0), jz = C(0);
+    if (!ST<T>::OFF) {
+        // Direct form, operation order of Cu_Collide (kernels.cu:249-263).
+#pragma unroll
+        for (int p = 0; p < Q; p++) {
+            drho += g[p];
+            jx += C(lat_c(DIM, 0, p)) * g[p];
+            jy += C(lat_c(DIM, 1, p)) * g[p];
+            if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
+        }
+        rho = drho;
+    } else {
+        // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
+#pragma unroll
+        for (int p = 0; p < Q; p++) {
+            drho += g[p];
+            jx += C(lat_c(DIM, 0, p)) * g[p];
+            jy += C(lat_c(DIM, 1, p)) * g[p];
+            if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
+        }
+        rho = C(1) + drho;
+    }
+    const C ux = jx / rho, uy = jy / rho, uz = (DIM == 3) ? jz / rho : C(0);
+    const C udotu = ux * ux + uy * uy + uz * uz;
+    const C omeg = C(a.omega);
+    const C omegp = C(1) - omeg;
+
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const C cu = C(lat_c(DIM, 0, p)) * ux + C(lat_c(DIM, 1, p)) * uy + C(lat_c(DIM, 2, p)) * uz;
+        const C wp = C(lat_w(Q, p));
+        if (!ST<T>::OFF) {
+            g[p] = g[p] * omegp + (wp * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu)) * omeg;
+        } else {
+            // f' - w = g (1 - omega) + omega (feq - w),  feq - w = w (drho + rho X)
+            g[p] = g[p] * omegp + omeg * (wp * (drho + rho * (C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu)));
+        }
+    }
+
+    // Push to destinations, bounce back on closed links.
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        constexpr int dummy = 0;
+        (void)dummy;
+        const int cx = lat_c(DIM, 0, p), cy = lat_c(DIM, 1, p), cz = lat_c(DIM, 2, p);
+        const int Ip = I + cx, Jp = J + cy, Kp = K + cz;
+        const int S = nbr_slot(DIM, Ip, Jp, Kp);
+        const int nb = (S == center_slot(DIM)) ? b : s_nbr[lb][S];
+        const int nc = nbr_cell(DIM, Ip, Jp, Kp);
+        bool open = nb >= 0;
+        if (open && a.has_solid) open = a.cmask[(long long)nb * MC + nc] != CELL_SOLID;
+        if (open) {
+            fout[(long long)lat_pb(DIM, p) * nmc + (long long)nb * MC + nc] = ST<T>::enc(g[p]);
+        } else {
+            C v = g[p];
+            if ((fl & 2) && nb < 0 && nb != N_SKIPID && a.bc_preset != AGAL_BC_NONE) {
+                const C wp = C(lat_w(Q, p));
+                const C off = ST<T>::OFF ? wp : C(0);
+                v = bc_hook<C>(a.bc_preset, nb, v + off, rho, ux, uy, uz, wp, cx, cy, cz, C(a.u_ref)) - off;
+            }
+            fout[(long long)p * nmc + cell] = ST<T>::enc(v);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Initial conditions (Cu_SetInitialConditions, kernels.cu:15-77); writes both
+// buffers so that cells never written by a step (solid cells) agree.
+struct IcArgs {
+    const int *ids;
+    int n;
+    void *f0, *f1;
+    long long nmc, nmb;
+    const int *cmask;
+    const float *fX;
+    double dxL, u_ref, noise;
+    unsigned long long seed;
+    int ic_preset, L;
+};
+
+__host__ __device__ inline double ic_noise(unsigned long long seed, int L, long long ix, long long iy,
+                                           long long iz, int comp)
+{
+    unsigned long long z = seed ^ ((unsigned long long)(unsigned)L << 56) ^
+                           ((unsigned long long)(ix & 0xFFFFF) << 36) ^
+                           ((unsigned long long)(iy & 0xFFFFF) << 16) ^ ((unsigned long long)(iz & 0xFFFF)) ^
+                           ((unsigned long long)comp << 60);
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+template <int DIM, int Q, typename T>
+__global__ void k_set_ic(const IcArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long kap = gid / MC;
+    const int t = (int)(gid % MC);
+    if (kap >= a.n) return;
+    const int b = a.ids[kap];
+    if (b < 0) return;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const long long cell = (long long)b * MC + t;
+    C rho = C(1), u = C(0), v = C(0), w = C(0);
+    if (a.ic_preset == AGAL_IC_UNIFORM) {
+        u = C(a.u_ref);
+        if (a.noise != 0.0) {
+            const double amp = a.noise * a.u_ref;
+            const long long ix = llrint((double)a.fX[b] / a.dxL) + I;
+            const long long iy = llrint((double)a.fX[b + a.nmb] / a.dxL) + J;
+            const long long iz = (DIM == 3) ? llrint((double)a.fX[b + 2 * a.nmb] / a.dxL) + K : 0;
+            u = C(a.u_ref + amp * ic_noise(a.seed, a.L, ix, iy, iz, 0));
+            v = C(amp * ic_noise(a.seed, a.L, ix, iy, iz, 1));
+            if (DIM == 3) w = C(amp * ic_noise(a.seed, a.L, ix, iy, iz, 2));
+        }
+    }
+    const C udotu = u * u + v * v + w * w;
+    const bool solid = a.cmask[cell] == CELL_SOLID;
+    T *f0 = static_cast<T *>(a.f0), *f1 = static_cast<T *>(a.f1);
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const C cu = C(lat_c(DIM, 0, p)) * u + C(lat_c(DIM, 1, p)) * v + C(lat_c(DIM, 2, p)) * w;
+        const C wp = C(lat_w(Q, p));
+        C val;
+        if (solid) val = C(-1) - (ST<T>::OFF ? wp : C(0));
+        else if (!ST<T>::OFF) val = rho * wp * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu);
+        else val = wp * ((rho - C(1)) + rho * (C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu));
+        const long long o = (long long)lat_pb(DIM, p) * a.nmc + cell;
+        f0[o] = ST<T>::enc(val);
+        f1[o] = ST<T>::enc(val);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Macros of one level from its current buffer (Cu_RefreshVariables,
+// kernels.cu:112-159), into the separate macro array.
+struct MacroArgs {
+    const int *ids;
+    int n;
+    const void *f;
+    void *macro;
+    long long nmc;
+};
+
+template <int DIM, int Q, typename T>
+__global__ void k_refresh(const MacroArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long kap = gid / MC;
+    const int t = (int)(gid % MC);
+    if (kap >= a.n) return;
+    const int b = a.ids[kap];
+    if (b < 0) return;
+    const long long cell = (long long)b * MC + t;
+    const T *f = static_cast<const T *>(a.f);
+    C rho = 0, u = 0, v = 0, w = 0;
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const C fp = ST<T>::dec(f[(long long)lat_pb(DIM, p) * a.nmc + cell]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        rho += fp;
+        u += C(lat_c(DIM, 0, p)) * fp;
+        v += C(lat_c(DIM, 1, p)) * fp;
+        if (DIM == 3) w += C(lat_c(DIM, 2, p)) * fp;
+    }
+    u /= rho;
+    v /= rho;
+    if (DIM == 3) w /= rho;
+    C *m = static_cast<C *>(a.macro);
+    m[cell] = rho;
+    m[a.nmc + cell] = u;
+    m[2 * a.nmc + cell] = v;
+    if (DIM == 3) m[3 * a.nmc + cell] = w;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 mass and momentum of the leaf fluid cells of one level; one partial
+// per CTA, summed in a fixed order by k_sum_partials (deterministic).
+struct MassArgs {
+    const int *ids;
+    int n;
+    const void *f;
+    long long nmc;
+    const int *nbr_child, *cmask;
+    double vol;
+    double *partial;   // [gridDim.x][4]
+};
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(256) k_mass(const MassArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC;
+    __shared__ double s[4][256];
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long kap = gid / MC;
+    const int t = (int)(gid % MC);
+    double m = 0, mx = 0, my = 0, mz = 0;
+    if (kap < a.n) {
+        const int b = a.ids[kap];
+        if (b >= 0 && a.nbr_child[b] < 0) {
+            const long long cell = (long long)b * MC + t;
+            if (a.cmask[cell] != CELL_SOLID) {
+                const T *f = static_cast<const T *>(a.f);
+#pragma unroll
+                for (int p = 0; p < Q; p++) {
+                    const double fp = (double)ST<T>::dec(f[(long long)lat_pb(DIM, p) * a.nmc + cell]) +
+                                      (ST<T>::OFF ? lat_w(Q, p) : 0.0);
+                    m += fp;
+                    mx += lat_c(DIM, 0, p) * fp;
+                    my += lat_c(DIM, 1, p) * fp;
+                    mz += lat_c(DIM, 2, p) * fp;
+                }
+            }
+        }
+    }
+    s[0][threadIdx.x] = m * a.vol;
+    s[1][threadIdx.x] = mx * a.vol;
+    s[2][threadIdx.x] = my * a.vol;
+    s[3][threadIdx.x] = mz * a.vol;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int k = 0; k < 4; k++) s[k][threadIdx.x] += s[k][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) a.partial[blockIdx.x * 4 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_sum_partials(const double *partial, int n, double *out)
+{
+    // One thread per component, fixed summation order.
+    const int k = threadIdx.x;
+    if (k >= 4) return;
+    double acc = 0.0;
+    for (int i = 0; i < n; i++) acc += partial[i * 4 + k];
+    out[k] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// Dispatch on (velocity set, storage type).
+template <template <int, int, typename> class Fn, typename... Args>
+int dispatch(agal_ctx *c, Args... args)
+{
+    switch (c->Q) {
+    case 9:
+        switch (c->storage) {
+        case AGAL_STORE_FP32: return Fn<2, 9, float>::run(c, args...);
+        case AGAL_STORE_FP64: return Fn<2, 9, double>::run(c, args...);
+        case AGAL_STORE_FP16: return Fn<2, 9, __half>::run(c, args...);
+        case AGAL_STORE_BF16: return Fn<2, 9, __nv_bfloat16>::run(c, args...);
+        }
+        break;
+    case 19:
+        switch (c->storage) {
+        case AGAL_STORE_FP32: return Fn<3, 19, float>::run(c, args...);
+        case AGAL_STORE_FP64: return Fn<3, 19, double>::run(c, args...);
+        case AGAL_STORE_FP16: return Fn<3, 19, __half>::run(c, args...);
+        case AGAL_STORE_BF16: return Fn<3, 19, __nv_bfloat16>::run(c, args...);
+        }
+        break;
+    case 27:
+        switch (c->storage) {
+        case AGAL_STORE_FP32: return Fn<3, 27, float>::run(c, args...);
+        case AGAL_STORE_FP64: return Fn<3, 27, double>::run(c, args...);
+        case AGAL_STORE_FP16: return Fn<3, 27, __half>::run(c, args...);
+        case AGAL_STORE_BF16: return Fn<3, 27, __nv_bfloat16>::run(c, args...);
+        }
+        break;
+    }
+    return agal_set_err(c, AGAL_ERR_UNSUPPORTED, "velocity set / storage combination not built");
+}
+
+template <int DIM, int Q, typename T> struct RunStep {
+    static int run(agal_ctx *c, int L)
+    {
+        constexpr int BPC = (DIM == 2) ? 16 : 4;
+        const int n = c->n_ids[L];
+        if (n <= 0) return AGAL_OK;
+        StepArgs a;
+        a.ids = c->id_set + (long long)L * c->nmb;
+        a.n = n;
+        a.fin = c->F[c->cur[L]];
+        a.fout = c->F[1 - c->cur[L]];
+        a.nmc = c->nmc;
+        a.nmb = c->nmb;
+        a.nbr = c->cblock_ID_nbr;
+        a.nbr_child = c->cblock_ID_nbr_child;
+        a.bmask = c->cblock_ID_mask;
+        a.onb = c->cblock_ID_onb;
+        a.cmask = c->cells_ID_mask;
+        a.omega = c->dxf[L] / c->tau[L];
+        if (sizeof(typename ST<T>::C) == 4) a.omega = (double)((float)c->dxf[L] / (float)c->tau[L]);
+        a.u_ref = c->P.u_ref;
+        a.bc_preset = c->P.bc_preset;
+        a.has_solid = c->geometry_init;
+        const unsigned grid = (unsigned)((n + BPC - 1) / BPC);
+        k_step<DIM, Q, T, BPC><<<grid, BPC * Geo<DIM>::MC, 0, c->stream>>>(a);
+        AGAL_CUDA(c, cudaGetLastError());
+        c->cur[L] = 1 - c->cur[L];
+        return AGAL_OK;
+    }
+};
+
+template <int DIM, int Q, typename T> struct RunIc {
+    static int run(agal_ctx *c, int L)
+    {
+        const int n = c->n_ids[L];
+        if (n <= 0) return AGAL_OK;
+        IcArgs a;
+        a.ids = c->id_set + (long long)L * c->nmb;
+        a.n = n;
+        a.f0 = c->F[0];
+        a.f1 = c->F[1];
+        a.nmc = c->nmc;
+        a.nmb = c->nmb;
+        a.cmask = c->cells_ID_mask;
+        a.fX = c->cblock_f_X;
+        a.dxL = c->dxf[L];
+        a.u_ref = c->P.u_ref;
+        a.noise = c->P.ic_noise;
+        a.seed = c->P.seed;
+        a.ic_preset = c->P.ic_preset;
+        a.L = L;
+        const long long cells = (long long)n * Geo<DIM>::MC;
+        k_set_ic<DIM, Q, T><<<(unsigned)((cells + 255) / 256), 256, 0, c->stream>>>(a);
+        AGAL_CUDA(c, cudaGetLastError());
+        return AGAL_OK;
+    }
+};
+
+template <int DIM, int Q, typename T> struct RunRefresh {
+    static int run(agal_ctx *c, int L)
+    {
+        const int n = c->n_ids[L];
+        if (n <= 0) return AGAL_OK;
+        MacroArgs a;
+        a.ids = c->id_set + (long long)L * c->nmb;
+        a.n = n;
+        a.f = c->F[c->cur[L]];
+        a.macro = c->macro;
+        a.nmc = c->nmc;
+        const long long cells = (long long)n * Geo<DIM>::MC;
+        k_refresh<DIM, Q, T><<<(unsigned)((cells + 255) / 256), 256, 0, c->stream>>>(a);
+        AGAL_CUDA(c, cudaGetLastError());
+        return AGAL_OK;
+    }
+};
+
+template <int DIM, int Q, typename T> struct RunMass {
+    static int run(agal_ctx *c, double *out)
+    {
+        // Partials of all levels, laid out level after level.
+        long long total = 0;
+        std::vector<long long> grids(c->max_levels);
+        for (int L = 0; L < c->max_levels; L++) {
+            grids[L] = ((long long)c->n_ids[L] * Geo<DIM>::MC + 255) / 256;
+            total += grids[L];
+        }
+        if (total > c->red_len) {
+            if (c->red) cudaFree(c->red);
+            c->red = nullptr;
+            AGAL_CUDA(c, cudaMalloc(&c->red, sizeof(double) * 4 * (size_t)total));
+            c->red_len = (int)total;
+        }
+        long long off = 0;
+        for (int L = 0; L < c->max_levels; L++) {
+            if (grids[L] == 0) continue;
+            MassArgs a;
+            a.ids = c->id_set + (long long)L * c->nmb;
+            a.n = c->n_ids[L];
+            a.f = c->F[c->cur[L]];
+            a.nmc = c->nmc;
+            a.nbr_child = c->cblock_ID_nbr_child;
+            a.cmask = c->cells_ID_mask;
+            a.vol = std::ldexp(1.0, -L * DIM);
+            a.partial = c->red + 4 * off;
+            k_mass<DIM, Q, T><<<(unsigned)grids[L], 256, 0, c->stream>>>(a);
+            AGAL_CUDA(c, cudaGetLastError());
+            off += grids[L];
+        }
+        k_sum_partials<<<1, 32, 0, c->stream>>>(c->red, (int)total, c->red_out);
+        AGAL_CUDA(c, cudaGetLastError());
+        double h[4];
+        AGAL_CUDA(c, cudaMemcpyAsync(h, c->red_out, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+        out[0] = h[0];
+        out[1] = h[1];
+        out[2] = h[2];
+        if (DIM == 3) out[3] = h[3];
+        return AGAL_OK;
+    }
+};
+
+}  // namespace agal
+
+int agal_launch_step(agal_ctx *c, int L) { return agal::dispatch<agal::RunStep>(c, L); }
+int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }
+int agal_launch_refresh(agal_ctx *c, int L) { return agal::dispatch<agal::RunRefresh>(c, L); }
+int agal_launch_mass(agal_ctx *c, double *out) { return agal::dispatch<agal::RunMass>(c, out); }

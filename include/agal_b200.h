@@ -1,0 +1,188 @@
+/*
+ * agal_b200.h - C ABI of the B200-native octree-AMR lattice Boltzmann time step.
+ *
+ * The library (agal_b200/libagal_b200.so) owns every device array of one
+ * simulation case in an opaque context.  All entry points take plain pointers
+ * and sizes, return an int status (AGAL_OK or a negative AGAL_ERR_* code) and
+ * never call exit().  Kernels run on the context's CUDA stream.
+ *
+ * Reference interface replaced (paths relative to the AGAL source tree):
+ *   Solver<...> virtuals          inc/solver.h:62-71
+ *   Solver_LBM<...> routines      inc/solver_lbm.h:153-179
+ *   Mesh<...> AMR/advance entry   inc/mesh.h:676-727
+ *   Parser input.txt maps          inc/parser.h:58-183
+ */
+#ifndef AGAL_B200_H
+#define AGAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with -fvisibility=hidden; the entry points declared
+   here are the only exported symbols. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define AGAL_OK                 0
+#define AGAL_ERR_PARAM         -1   /* invalid argument or input.txt value       */
+#define AGAL_ERR_OOM           -2   /* device allocation failed / capacity short  */
+#define AGAL_ERR_GAPS          -3   /* block-ID gap set exhausted during refine   */
+#define AGAL_ERR_TIMEOUT       -4   /* a bounded device wait gave up              */
+#define AGAL_ERR_CUDA          -5   /* CUDA runtime error (see agal_last_error)   */
+#define AGAL_ERR_IO            -6   /* file missing, unreadable or corrupt        */
+#define AGAL_ERR_STATE         -7   /* call not valid in the context's state      */
+#define AGAL_ERR_UNSUPPORTED   -8   /* option combination not built               */
+
+/* ---- enumerations (runtime forms of the reference's compile-time packs) -- */
+/* velocity set: inc/solver_lbm.h:13-18 */
+#define AGAL_D2Q9   0
+#define AGAL_D3Q19  1
+#define AGAL_D3Q27  2
+/* collision operator: inc/solver_lbm.h:19-24 (TRT not built) */
+#define AGAL_BGK    0
+#define AGAL_MRT    2
+/* interpolation order: inc/solver_lbm.h:25-30 */
+#define AGAL_INTERP_LINEAR 0
+#define AGAL_INTERP_CUBIC  2
+/* population storage in HBM */
+#define AGAL_STORE_FP32 0
+#define AGAL_STORE_FP64 1
+#define AGAL_STORE_FP16 2   /* weight offsets g = f - w_p, collided in FP32 */
+#define AGAL_STORE_BF16 3   /* weight offsets g = f - w_p, collided in FP32 */
+/* boundary-condition presets of the Cu_ImposeBC hook, inc/custom.h:79-117 */
+#define AGAL_BC_NONE    0   /* plain half-way bounce-back on every wall        */
+#define AGAL_BC_LDC2D   1   /* moving lid on boundary -4 (y+), custom.h:80-84   */
+#define AGAL_BC_LDC3D   2   /* moving lid on boundary -6 (z+), custom.h:100-104 */
+#define AGAL_BC_FPSC2D  3   /* inflow -1,-3,-4; outflow -2, custom.h:87-97      */
+#define AGAL_BC_FPSC3D  4   /* inflow -1,-3..-6; outflow -2, custom.h:107-117   */
+/* initial-condition presets of the Cu_ComputeIC hook, inc/custom.h:50-60 */
+#define AGAL_IC_REST    0   /* rho = 1, u = 0                                   */
+#define AGAL_IC_UNIFORM 1   /* rho = 1, u = (u_ref, 0, 0) (+ seeded noise)      */
+
+/* interpolation / averaging modes, inc/mesh.h:58-62 */
+#define AGAL_INTERP_INTERFACE 0
+#define AGAL_INTERP_ADDED     1
+#define AGAL_AVERAGE_INTERFACE 0
+#define AGAL_AVERAGE_BLOCK     1
+#define AGAL_AVERAGE_GRID      2
+
+/* array selectors for agal_dump / agal_load */
+#define AGAL_ARR_F              0  /* populations, reference slot layout [Q][n_maxcells], float64, solid = -1 */
+#define AGAL_ARR_MACROS         1  /* rho,u,v(,w) [dim+1][n_maxcells], float64 (after agal_refresh)          */
+#define AGAL_ARR_CELLS_ID_MASK  2  /* int32 [n_maxcells]                      mesh.h:366                     */
+#define AGAL_ARR_CBLOCK_F_X     3  /* float32 [dim][n_maxcblocks]             mesh.h:389                     */
+#define AGAL_ARR_CBLOCK_ID_MASK 4  /* int32 [n_maxcblocks]                    mesh.h:393                     */
+#define AGAL_ARR_CBLOCK_ID_NBR  5  /* int32 [N_Q_max][n_maxcblocks]           mesh.h:397                     */
+#define AGAL_ARR_CBLOCK_ID_NBR_CHILD 6 /* int32 [N_Q_max][n_maxcblocks]       mesh.h:404                     */
+#define AGAL_ARR_CBLOCK_ID_ONB  7  /* int32 [n_maxcblocks]                    mesh.h:407                     */
+#define AGAL_ARR_CBLOCK_ID_REF  8  /* int32 [n_maxcblocks]                    mesh.h:416                     */
+#define AGAL_ARR_CBLOCK_LEVEL   9  /* int32 [n_maxcblocks]                    mesh.h:419                     */
+#define AGAL_ARR_ID_SET        10  /* int32 [MAX_LEVELS][n_maxcblocks]        mesh.h:428                     */
+#define AGAL_ARR_GAP_SET       11  /* int32 [n_maxcblocks] (first n_gaps valid) mesh.h:459                   */
+
+/* ---- parameters: every input.txt key of inc/parser.h:62-144 ------------- */
+typedef struct agal_params {
+    /* MESH (integer keys) */
+    int MAX_LEVELS_WALL, MAX_LEVELS_INTERIOR, N_ITER_TOTAL, N_LEVEL_START, Nx, N_RESTART;
+    int PERIODIC_X, PERIODIC_Y, PERIODIC_Z;
+    /* GEOMETRY (integer keys) */
+    int G_LOADTYPE, G_PRINT, G_VIS_TREE, G_BIN_DENSITY, G_BIN_APPROACH, G_BIN_LEVELS, G_BIN_SPEC, G_BIN_MAKE_LINKS;
+    /* SOLVER (integer keys) */
+    int S_COLLISION, S_INTERP, S_INTERP_HYBRID, S_AVERAGE, S_CRITERION, S_LES, S_FORCE_ORDER, S_FORCE_TYPE, S_BC_TYPE;
+    /* REFINEMENT / PROBING / OUTPUT (integer keys) */
+    int P_REFINE, N_PROBE, N_PROBE_DENSITY, N_PROBE_FREQUENCY, N_PROBE_FORCE, N_PROBE_F_START, N_PROBE_F_FREQUENCY;
+    int N_PROBE_AVE, N_PROBE_AVE_FREQUENCY, N_PROBE_AVE_START;
+    int N_PRINT_LEVELS, N_PRINT_LEVELS_VTHB, N_PRINT_LEVELS_PATCH, N_PRINT_LEVELS_IMAGE, P_OUTPUT, N_OUTPUT, N_OUTPUT_START;
+    int VOL_I_MIN, VOL_I_MAX, VOL_J_MIN, VOL_J_MAX, VOL_K_MIN, VOL_K_MAX, USE_CPU;
+    /* double keys */
+    double L_c, L_fy, L_fz, v0, G_NEAR_WALL_DISTANCE, s1, s2, s3, s4, s5, s6, V_PROBE_TOL;
+    double N_REFINE_START, N_REFINE_INC, N_REFINE_MAX;
+    double S_FORCEVOLUME_Xm, S_FORCEVOLUME_XM, S_FORCEVOLUME_Ym, S_FORCEVOLUME_YM, S_FORCEVOLUME_Zm, S_FORCEVOLUME_ZM;
+    /* string keys */
+    char I_DIR_NAME[256], P_DIR_NAME[256], G_FILENAME[256];
+
+    /* Runtime selections that the reference fixes at compile time
+       (main.cu:48-77 ArgsPack/LBMPack, custom.h hooks). */
+    int velocity_set;     /* AGAL_D2Q9 / AGAL_D3Q19 / AGAL_D3Q27 */
+    int collision;        /* AGAL_BGK / AGAL_MRT                 */
+    int interp_order;     /* AGAL_INTERP_LINEAR / AGAL_INTERP_CUBIC */
+    int storage;          /* AGAL_STORE_*                        */
+    int bc_preset;        /* AGAL_BC_*                           */
+    int ic_preset;        /* AGAL_IC_*                           */
+    double u_ref;         /* velocity of the presets (custom.h hard-codes 0.05) */
+    double ic_noise;      /* relative amplitude of seeded IC noise (0 = none)   */
+    uint64_t seed;        /* seed of the IC noise                               */
+    /* Capacity in cell-blocks.  0 = size from free device memory with
+       mem_frac, as mesh_init.cu:155-169 does with M_FRAC = 0.975. */
+    int64_t n_maxcblocks;
+    double mem_frac;
+    /* CUDA device ordinal of the context (-1 = the calling thread's current device). */
+    int device;
+} agal_params;
+
+typedef struct agal_ctx agal_ctx;
+
+/* Defaults of inc/parser.h:62-144 plus D2Q9/BGK/cubic/FP32/no-BC presets. */
+int agal_params_default(agal_params *p);
+/* sizeof(agal_params), for foreign-function bindings to check their layout. */
+size_t agal_params_size(void);
+/* Parse <input_dir>/input.txt with the reference's rules (parser.h:146-180):
+   '#' comments, "A*Nx" integer factors, unknown keys reported and skipped.
+   Starts from the values already in *p. */
+int agal_params_read(const char *input_dir, agal_params *p);
+/* Set one key by name from its text value (same rules as a file line). */
+int agal_params_set(agal_params *p, const char *key, const char *value);
+
+/* Mesh::M_Init (mesh_init.cu:11-567) + Solver_LBM::S_Init (solver_lbm_init.cu:4-102):
+   allocate the block pool, build the root grid, set tau per level. */
+int agal_ctx_create(const agal_params *p, agal_ctx **out);
+int agal_ctx_destroy(agal_ctx *ctx);
+/* Text of the last error on this context (or of the last failed create). */
+const char *agal_last_error(const agal_ctx *ctx);
+
+/* Host mirrors: n_ids[MAX_LEVELS+1], id_max[MAX_LEVELS+1], n_gaps, capacity. */
+int agal_get_counts(const agal_ctx *ctx, int *n_ids, int *id_max, int *n_gaps,
+                    int64_t *n_maxcblocks, int *max_levels);
+
+/* Solver::S_SetIC (solver_lbm_kernels.cu:79-98). */
+int agal_set_ic(agal_ctx *ctx, int L);
+/* Solver::S_RefreshVariables (solver_lbm_kernels.cu:161-175): macros of level L. */
+int agal_refresh(agal_ctx *ctx, int L);
+/* Solver::S_Advance(i_dev, L, tmp) (solver_lbm_advance.cu:31-174): one step of
+   level L and, recursively, of every finer level.  L = N_LEVEL_START is one
+   coarse step. */
+int agal_advance(agal_ctx *ctx, int L);
+/* n coarse steps; with use_graph != 0 the steps are captured once into a CUDA
+   graph and replayed (same kernels, no per-step host work). */
+int agal_advance_n(agal_ctx *ctx, int n, int use_graph);
+
+/* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
+   bytes must equal the size reported by agal_array_bytes. */
+int agal_array_bytes(const agal_ctx *ctx, int which, size_t *bytes);
+int agal_dump(agal_ctx *ctx, int which, void *host_buf, size_t bytes);
+int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
+
+/* FP64 sums over every fluid leaf cell: out[0] = mass, out[1..dim] = momentum.
+   Reads the macros of agal_refresh-free state (computes them itself). */
+int agal_mass_momentum(agal_ctx *ctx, double *out);
+
+/* Synchronise the context's stream; returns the first pending CUDA error. */
+int agal_sync(agal_ctx *ctx);
+/* The context's cudaStream_t (as void*), so that callers can order their own
+   work and CUDA events with the library's kernels. */
+int agal_get_stream(const agal_ctx *ctx, void **stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AGAL_B200_H */

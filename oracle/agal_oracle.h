@@ -1,0 +1,69 @@
+/*
+ * ORACLE - CPU restatement of AGAL's octree-AMR lattice Boltzmann time step.
+ *
+ * This is test infrastructure: the checker that the CUDA product is compared
+ * against, and the timed CPU baseline of bench.py.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.  The
+ * product library never links or calls it.
+ *
+ * It restates the reference algorithm step by step in plain C with OpenMP,
+ * using the reference's own data layout (structure-of-arrays populations with
+ * the in-place swap-streaming slot convention) so that its arrays compare
+ * element-wise with dumps of the reference CUDA build and of the product.
+ *
+ * Parity: the integer arrays of the root grid and the lattice tables are
+ * pinned to golden vectors extracted from the reference sources
+ * (tests/golden/make_golden.py).  The floating-point path is pinned against
+ * the reference's own CUDA build when that build has been run (oracle/_ref);
+ * otherwise it is "parity unpinned" for floating point.
+ */
+#ifndef AGAL_ORACLE_H
+#define AGAL_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "../include/agal_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_case orc_case;
+
+/* Mesh::M_Init root grid (mesh_init.cu:325-516) and Solver_LBM::S_Init
+   (solver_lbm_init.cu:4-76) with a fixed capacity of n_maxcblocks blocks.
+   fp64 != 0 runs the arithmetic in double (ufloat_t = double). */
+orc_case *orc_create(const agal_params *p, int64_t n_maxcblocks, int fp64);
+void orc_destroy(orc_case *c);
+
+/* Number of OpenMP threads used by the step routines (0 = library default). */
+void orc_set_threads(int n);
+
+int orc_get_counts(const orc_case *c, int *n_ids, int *id_max, int *n_gaps,
+                   int64_t *n_maxcblocks, int *max_levels);
+
+/* Solver_LBM::S_SetIC (solver_lbm_kernels.cu:15-98). */
+int orc_set_ic(orc_case *c, int L);
+/* Solver_LBM::S_RefreshVariables (solver_lbm_kernels.cu:112-175). */
+int orc_refresh(orc_case *c, int L);
+/* Single phases of one level. */
+int orc_collide(orc_case *c, int L);    /* solver_lbm_kernels.cu:206-289, 465-510 */
+int orc_impose_bc(orc_case *c, int L);  /* solver_lbm_kernels.cu:693-920 */
+int orc_stream(orc_case *c, int L);     /* solver_lbm_kernels.cu:534-660 */
+/* Solver_LBM::S_Advance (solver_lbm_advance.cu:31-174). */
+int orc_advance(orc_case *c, int L);
+/* n coarse steps from N_LEVEL_START. */
+int orc_advance_n(orc_case *c, int n);
+
+/* Array sizes and copies with the AGAL_ARR_* selectors of agal_b200.h. */
+size_t orc_array_bytes(const orc_case *c, int which);
+int orc_dump(const orc_case *c, int which, void *buf, size_t bytes);
+int orc_load(orc_case *c, int which, const void *buf, size_t bytes);
+
+/* FP64 mass and momentum over fluid cells of leaf blocks (all levels). */
+int orc_mass_momentum(orc_case *c, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,132 @@
+"""ORACLE (test infrastructure only): ctypes binding of oracle/liborc.so.
+
+Loaded by tests/, __graft_entry__.smoke() and bench.py's CPU baseline; never
+by the agal_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liborc.so"
+
+
+def build(force: bool = False) -> Path:
+    srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h")) + [HERE.parent / "include" / "agal_b200.h"]
+    if force or not LIB_PATH.exists() or any(s.stat().st_mtime > LIB_PATH.stat().st_mtime for s in srcs):
+        env = dict(os.environ)
+        env.pop("CC", None)
+        subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "all"], check=True, env=env)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        from agal_b200._lib import AgalParams
+        L = C.CDLL(str(LIB_PATH))
+        P = C.POINTER(AgalParams)
+        protos = [
+            ("orc_create", C.c_void_p, [P, C.c_int64, C.c_int]),
+            ("orc_destroy", None, [C.c_void_p]),
+            ("orc_set_threads", None, [C.c_int]),
+            ("orc_get_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+            ("orc_set_ic", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_refresh", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_collide", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_impose_bc", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_stream", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_advance", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_advance_n", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_array_bytes", C.c_size_t, [C.c_void_p, C.c_int]),
+            ("orc_dump", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+            ("orc_load", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+            ("orc_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+        ]
+        for name, res, args in protos:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class OracleCase:
+    """CPU oracle case with the same array selectors as agal_b200.Case."""
+
+    def __init__(self, params, n_maxcblocks: int, fp64: bool = False, threads: int = 0):
+        self._lib = lib()
+        if threads:
+            self._lib.orc_set_threads(threads)
+        self._h = self._lib.orc_create(C.byref(params), n_maxcblocks, 1 if fp64 else 0)
+        if not self._h:
+            raise RuntimeError("orc_create failed")
+        self.params = params
+        self.dim = 2 if params.velocity_set == 0 else 3
+        self.Q = {0: 9, 1: 19, 2: 27}[params.velocity_set]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        if rc != 0:
+            raise RuntimeError(f"oracle call failed: {rc}")
+
+    def counts(self):
+        n_ids = (C.c_int * 17)()
+        id_max = (C.c_int * 17)()
+        n_gaps = C.c_int()
+        nmb = C.c_int64()
+        ml = C.c_int()
+        self._c(self._lib.orc_get_counts(self._h, n_ids, id_max, C.byref(n_gaps), C.byref(nmb), C.byref(ml)))
+        L = ml.value
+        return {"n_ids": list(n_ids[: L + 1]), "id_max": list(id_max[: L + 1]), "n_gaps": n_gaps.value,
+                "n_maxcblocks": nmb.value, "max_levels": L}
+
+    def set_ic(self, L=0):
+        self._c(self._lib.orc_set_ic(self._h, L))
+
+    def refresh(self, L=0):
+        self._c(self._lib.orc_refresh(self._h, L))
+
+    def advance(self, L=None):
+        self._c(self._lib.orc_advance(self._h, self.params.N_LEVEL_START if L is None else L))
+
+    def advance_n(self, n):
+        self._c(self._lib.orc_advance_n(self._h, n))
+
+    def mass_momentum(self):
+        out = (C.c_double * 4)()
+        self._c(self._lib.orc_mass_momentum(self._h, out))
+        return np.array(out[: self.dim + 1])
+
+    def dump(self, which):
+        dt = np.float64 if which in (0, 1) else (np.float32 if which == 3 else np.int32)
+        n = self._lib.orc_array_bytes(self._h, which)
+        out = np.empty(n // np.dtype(dt).itemsize, dtype=dt)
+        self._c(self._lib.orc_dump(self._h, which, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def load(self, which, arr):
+        dt = np.float64 if which in (0, 1) else (np.float32 if which == 3 else np.int32)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        self._c(self._lib.orc_load(self._h, which, a.ctypes.data_as(C.c_void_p), a.nbytes))

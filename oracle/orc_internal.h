@@ -1,0 +1,91 @@
+/* ORACLE (test infrastructure only): private state of a CPU oracle case. */
+#ifndef ORC_INTERNAL_H
+#define ORC_INTERNAL_H
+
+#include <stdint.h>
+#include "agal_oracle.h"
+#include "orc_lattice.h"
+
+#define ORC_MAXL 16
+
+/* Constants of inc/mesh.h:34-105 and inc/cppspec.h:124-125. */
+#define ORC_N_SKIPID (-999)
+#define ORC_N_SPECID (-998)
+#define ORC_REF_UNREFINED 0
+#define ORC_REF_REFINED 1
+#define ORC_REF_REFINED_WCHILD 2
+#define ORC_REF_REFINED_PERM 3
+#define ORC_REF_MARK_REFINE 4
+#define ORC_REF_MARK_COARSEN 5
+#define ORC_REF_NEW 6
+#define ORC_REF_REMOVE 7
+#define ORC_REF_INACTIVE 8
+#define ORC_REF_UNREFINED_VIO 9
+#define ORC_REF_REFINED_WCHILD_PERM 10
+#define ORC_CELL_INTERIOR 0
+#define ORC_CELL_INTERFACE 1
+#define ORC_CELL_GHOST 2
+#define ORC_CELL_SOLID (-1)
+#define ORC_CELL_BOUNDARY (-6)
+#define ORC_BLOCK_REGULAR 0
+#define ORC_BLOCK_INTERFACE 1
+#define ORC_BLOCK_SOLIDB (-1)
+#define ORC_BLOCK_SOLIDA (-2)
+#define ORC_BLOCK_SOLID (-3)
+
+struct orc_case {
+    agal_params P;
+    int fp64;
+    int dim, Q, Qmax, MC, NCH;
+    int64_t nmb, nmc;
+    int max_levels, L0;
+    int Nx, Ny, Nz;
+    float dx, dx_cblock;
+    float dxf[ORC_MAXL];     /* dxf_vec as ufloat_t = float */
+    double dxf_d[ORC_MAXL];  /* dxf_vec as ufloat_t = double */
+    double tau[ORC_MAXL];    /* tau_vec, rounded to the case's ufloat_t */
+    const int *cx, *cy, *cz, *pb, *map;
+    const double *w;
+    /* mesh arrays, layouts of inc/mesh.h:366-459 */
+    int *cells_ID_mask;      /* [nmc] */
+    float *cblock_f_X;       /* [dim][nmb] */
+    int *cblock_ID_mask;     /* [nmb] */
+    int *cblock_ID_nbr;      /* [Qmax][nmb] */
+    int *cblock_ID_nbr_child;/* [Qmax][nmb] */
+    int *cblock_ID_onb;      /* [nmb] */
+    int *cblock_ID_ref;      /* [nmb] */
+    int *cblock_level;       /* [nmb] */
+    int *id_set;             /* [max_levels][nmb] */
+    int *gap_set;            /* [nmb] */
+    int n_ids[ORC_MAXL + 1], id_max[ORC_MAXL + 1], n_gaps;
+    int geometry_init;
+    void *F;                 /* [(Q + dim + 1)][nmc] of float or double */
+    int liter;               /* global_Liter of solver_lbm_advance.cu:6 */
+};
+
+static inline int orc_half(int dim, int p)
+{
+    /* Half set of directions that own a swap pair (kernels.cu:597, 769). */
+    if (dim == 2) return p == 1 || (p + 1) % 3 == 0;
+    return p == 26 || ((p - 1) % 2 == 0 && p < 25);
+}
+
+static inline int orc_nbrslot(int dim, int I, int J, int K)
+{
+    /* inc/util_index.h:45-66 */
+    int S = (I >= 4) ? 2 : (I >= 0 ? 1 : 0);
+    S += 3 * ((J >= 4) ? 2 : (J >= 0 ? 1 : 0));
+    if (dim == 3) S += 9 * ((K >= 4) ? 2 : (K >= 0 ? 1 : 0));
+    return S;
+}
+
+static inline int orc_nbrcell(int dim, int I, int J, int K)
+{
+    /* inc/util_index.h:88-98 */
+    I = (4 + (I % 4)) % 4;
+    J = (4 + (J % 4)) % 4;
+    if (dim == 3) K = (4 + (K % 4)) % 4; else K = 0;
+    return I + 4 * J + 16 * K;
+}
+
+#endif

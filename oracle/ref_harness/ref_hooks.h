@@ -1,0 +1,70 @@
+// ORACLE (test infrastructure only): user hooks for the reference CUDA build.
+//
+// AGAL takes its initial and boundary conditions from three user-edited
+// device functions in inc/custom.h (Cu_RefineRegion :17, Cu_ComputeIC :50,
+// Cu_ImposeBC :68).  The shipped file selects flow past a sphere; the
+// lid-driven-cavity presets are commented out there.  This header provides
+// the same three hooks with the preset chosen at compile time, and defines
+// the include guard CUSTOM_H first so that the reference's own custom.h is
+// skipped when inc/mesh.h includes it.
+//   REF_BC: 1 LDC 2D (lid = boundary -4), 2 LDC 3D (lid = -6),
+//           3 flow past a body 2D, 4 flow past a body 3D (custom.h:87-117)
+//   REF_IC: 0 rest (rho = 1, u = 0), 1 uniform u = 0.05
+#ifndef CUSTOM_H
+#define CUSTOM_H
+
+#ifndef REF_BC
+#define REF_BC 1
+#endif
+#ifndef REF_IC
+#define REF_IC 0
+#endif
+
+template <typename ufloat_t>
+__device__ bool Cu_RefineRegion(const int L, const ufloat_t x, const ufloat_t y, const ufloat_t z,
+                                const ufloat_t xp, const ufloat_t yp, const ufloat_t zp, const int onb,
+                                const int nbr_1, const int nbr_2, const int nbr_3, const int nbr_4,
+                                const int nbr_5, const int nbr_6)
+{
+    return false;
+}
+
+template <typename ufloat_t>
+__device__ __forceinline__ void Cu_ComputeIC(ufloat_t &rho, ufloat_t &u, ufloat_t &v, ufloat_t &w,
+                                             const ufloat_t x, const ufloat_t y, const ufloat_t z)
+{
+    rho = (ufloat_t)1.0;
+    u = (REF_IC == 1) ? (ufloat_t)0.05 : (ufloat_t)0.0;
+    v = (ufloat_t)0.0;
+    w = (ufloat_t)0.0;
+}
+
+template <typename ufloat_t>
+__device__ __forceinline__ ufloat_t Cu_ImposeBC(const int nbr_id, const ufloat_t f, const ufloat_t rho,
+                                                const ufloat_t u, const ufloat_t v, const ufloat_t w,
+                                                const ufloat_t x, const ufloat_t y, const ufloat_t z,
+                                                const ufloat_t wp, const ufloat_t cxp, const ufloat_t cyp,
+                                                const ufloat_t czp)
+{
+    const ufloat_t U = (ufloat_t)0.05;
+    bool inflow = false, outflow = false;
+    if (REF_BC == 1) inflow = (nbr_id == -4);
+    if (REF_BC == 2) inflow = (nbr_id == -6);
+    if (REF_BC == 3) { inflow = (nbr_id == -1 || nbr_id == -3 || nbr_id == -4); outflow = (nbr_id == -2); }
+    if (REF_BC == 4) {
+        inflow = (nbr_id == -1 || nbr_id == -3 || nbr_id == -4 || nbr_id == -5 || nbr_id == -6);
+        outflow = (nbr_id == -2);
+    }
+    if (inflow) {
+        ufloat_t cdotu = (ufloat_t)(3.0) * (cxp * U);
+        return f - (ufloat_t)(2.0) * wp * cdotu;
+    }
+    if (outflow) {
+        ufloat_t cdotu = cxp * u + cyp * v + czp * w;
+        cdotu = (ufloat_t)(1.0) + (ufloat_t)(4.5) * cdotu * cdotu - (ufloat_t)(1.5) * (u * u + v * v + w * w);
+        return -f + (ufloat_t)(2.0) * wp * cdotu;
+    }
+    return f;
+}
+
+#endif

@@ -1,0 +1,218 @@
+// ORACLE (test infrastructure only): driver for the reference's own CUDA
+// build.  Compiled by oracle/Makefile (target `ref`) against the AGAL sources
+// where they lie; the binaries go to oracle/_ref/ and run on the GPU box to
+// produce golden dumps and the reference's own timing.
+//
+// It does what the reference's src/main.cu would do with the solver enabled
+// (main.cu:108-120 commented lines): Parser -> Mesh(N_U = N_Q + N_DIM + 1) ->
+// Solver_LBM -> M_AddSolver, then the loop body of M_AdvanceLoop
+// (mesh_advance.cu:381-466) without printing, and writes a binary dump of the
+// active blocks.
+//
+// usage: ref_agal <input_dir/> <dump_file|-> <n_steps> <keep_mb> [n_timed]
+//   keep_mb  device memory left free for the reference's own sizing: the
+//            rest is taken by a ballast allocation first, because M_Init sizes
+//            its pool to 97.5% of free memory (mesh_init.cu:155-169).
+//   n_timed  extra steps timed with CUDA events after the dump (MLUPS line).
+#include "ref_hooks.h"
+
+#include "cppspec.h"
+#include "parser.h"
+#include "geometry.h"
+#include "geometry_bins.h"
+#include "mesh.h"
+#include "solver_lbm.h"
+
+#include "geometry_add.cu"
+#include "geometry_bins.cu"
+#include "geometry_bins_cpu.cu"
+#include "geometry_bins_gpu.cu"
+#include "geometry_bins_draw.cu"
+#include "geometry_convert.cu"
+#include "geometry_dest.cu"
+#include "geometry_import.cu"
+#include "geometry_init.cu"
+#include "geometry_print.cu"
+#include "geometry_refine.cu"
+#include "mesh_advance.cu"
+#include "mesh_amr.cu"
+#include "mesh_comm.cu"
+#include "mesh_voxelizer.cu"
+#include "mesh_criterion.cu"
+#include "mesh_dest.cu"
+#include "mesh_init.cu"
+#include "mesh_output.cu"
+#include "mesh_print_uniform.cu"
+#include "mesh_restart.cu"
+#include "solver_lbm_advance.cu"
+#include "solver_lbm_compute_macro.cu"
+#include "solver_lbm_compute.cu"
+#include "solver_lbm_criterion.cu"
+#include "solver_lbm_init.cu"
+#include "solver_lbm_kernels.cu"
+#include "solver_lbm_kernels_les.cu"
+#include "solver_lbm_kernels_comm.cu"
+#include "solver_lbm_kernels_forces.cu"
+#include "solver_lbm_kernels_debug.cu"
+
+#include <cstdint>
+#include <cstdio>
+#include <set>
+#include <vector>
+
+// VTK writers are not built (VTK is absent); these stubs replace
+// mesh_print_vthb.cu, mesh_print_vthb_patch.cu and mesh_print_image.cu.
+template <typename ufloat_t, typename ufloat_g_t, const ArgsPack *AP>
+int Mesh<ufloat_t, ufloat_g_t, AP>::M_Print_VTHB(int, int) { return 0; }
+template <typename ufloat_t, typename ufloat_g_t, const ArgsPack *AP>
+int Mesh<ufloat_t, ufloat_g_t, AP>::M_Print_VTHB_Patch(int, int) { return 0; }
+template <typename ufloat_t, typename ufloat_g_t, const ArgsPack *AP>
+int Mesh<ufloat_t, ufloat_g_t, AP>::M_Print_ImageData(int, int) { return 0; }
+
+// Argument packs as in main.cu:48-57.
+constexpr ArgsPack AP2D_H = ArgsPack(2, 128, 1, 1, 1, 24, 2048);
+constexpr ArgsPack AP3D_H = ArgsPack(3, 128, 1, 1, 1, 24, 2048);
+#ifndef REF_INTERP2D
+#define REF_INTERP2D InterpOrder::Cubic
+#endif
+#ifndef REF_INTERP3D
+#define REF_INTERP3D InterpOrder::Linear
+#endif
+#if defined(USED2Q9)
+constexpr ArgsPack APh = AP2D_H;
+constexpr LBMPack LPh = LBMPack(&AP2D_H, VelocitySet::D2Q9, CollisionOperator::BGK, REF_INTERP2D, LESModel::None);
+#elif defined(USED3Q19)
+constexpr ArgsPack APh = AP3D_H;
+constexpr LBMPack LPh = LBMPack(&AP3D_H, VelocitySet::D3Q19, CollisionOperator::BGK, REF_INTERP3D, LESModel::None);
+#else
+constexpr ArgsPack APh = AP3D_H;
+constexpr LBMPack LPh = LBMPack(&AP3D_H, VelocitySet::D3Q27, CollisionOperator::BGK, REF_INTERP3D, LESModel::None);
+#endif
+typedef float REAL_h;
+
+template <typename T>
+static void put(FILE *f, const T *p, size_t n) { fwrite(p, sizeof(T), n, f); }
+
+template <typename T>
+static std::vector<T> d2h(const T *d, size_t n)
+{
+    std::vector<T> h(n);
+    if (n) cudaMemcpy(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost);
+    return h;
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 5) {
+        fprintf(stderr, "usage: %s input_dir/ dump_file|- n_steps keep_mb [n_timed]\n", argv[0]);
+        return 2;
+    }
+    const std::string input_dir = argv[1];
+    const std::string dump_file = argv[2];
+    const int n_steps = atoi(argv[3]);
+    const long long keep_mb = atoll(argv[4]);
+    const int n_timed = argc > 5 ? atoi(argv[5]) : 0;
+
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    void *ballast = nullptr;
+    const size_t keep = (size_t)keep_mb << 20;
+    if (fr > keep + (256ull << 20)) {
+        if (cudaMalloc(&ballast, fr - keep) != cudaSuccess) { fprintf(stderr, "ballast failed\n"); return 3; }
+    }
+
+    Parser parser(input_dir);
+    const int N_U = LPh.N_Q + APh.N_DIM + 1;
+    Mesh<REAL_h, REAL_h, &APh> mesh(&parser, N_U);
+    Solver_LBM<REAL_h, REAL_h, &APh, &LPh> solver(&mesh);
+    mesh.M_AddSolver(&solver);
+    for (int L = 0; L < mesh.MAX_LEVELS; L++) solver.S_SetIC(0, L);
+    cudaDeviceSynchronize();
+
+    // Loop body of M_AdvanceLoop (mesh_advance.cu:403-463) without output.
+    const int iter_mult = (int)pow(2.0, (double)mesh.N_LEVEL_START);
+    if (mesh.MAX_LEVELS > 1) mesh.M_Advance_RefineNearWall();
+    for (int i = 0; i < n_steps; i++) {
+        mesh.M_Advance_Step(i, 0, iter_mult);
+        if (mesh.MAX_LEVELS > 1 && (mesh.MAX_LEVELS != mesh.N_LEVEL_START + 1) && (i + 1) % mesh.P_REFINE == 0 && i > 0)
+            mesh.M_Advance_RefineWithSolution(i, 0);
+    }
+    cudaError_t err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) { fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); return 4; }
+
+    if (dump_file != "-") {
+        const int dim = APh.N_DIM, Q = LPh.N_Q, Qmax = APh.N_Q_max, MC = APh.M_CBLOCK, ML = mesh.MAX_LEVELS;
+        const long long nmb = mesh.n_maxcblocks, nmc = mesh.n_maxcells;
+        FILE *f = fopen(dump_file.c_str(), "wb");
+        if (!f) { fprintf(stderr, "cannot open %s\n", dump_file.c_str()); return 5; }
+        fwrite("AGALREF1", 1, 8, f);
+        int hdr[6] = {dim, Q, Qmax, MC, ML, n_steps};
+        put(f, hdr, 6);
+        long long hdr2[2] = {nmb, nmc};
+        put(f, hdr2, 2);
+        put(f, mesh.n_ids[0], ML + 1);
+        put(f, mesh.id_max[0], ML + 1);
+        put(f, &mesh.n_gaps[0], 1);
+        std::set<int> act;
+        for (int L = 0; L < ML; L++) {
+            auto ids = d2h(&mesh.c_id_set[0][(size_t)L * nmb], mesh.n_ids[0][L]);
+            put(f, ids.data(), ids.size());
+            act.insert(ids.begin(), ids.end());
+        }
+        const int n_gap_keep = std::min(mesh.n_gaps[0], 65536);
+        auto gaps = d2h(&mesh.c_gap_set[0][mesh.n_gaps[0] - n_gap_keep], n_gap_keep);
+        put(f, &n_gap_keep, 1);
+        put(f, gaps.data(), gaps.size());
+        std::vector<int> blk(act.begin(), act.end());
+        const int n_act = (int)blk.size();
+        put(f, &n_act, 1);
+        put(f, blk.data(), blk.size());
+        auto fX = d2h(mesh.c_cblock_f_X[0], (size_t)dim * nmb);
+        auto bm = d2h(mesh.c_cblock_ID_mask[0], (size_t)nmb);
+        auto nb = d2h(mesh.c_cblock_ID_nbr[0], (size_t)Qmax * nmb);
+        auto nc = d2h(mesh.c_cblock_ID_nbr_child[0], (size_t)Qmax * nmb);
+        auto onb = d2h(mesh.c_cblock_ID_onb[0], (size_t)nmb);
+        auto ref = d2h(mesh.c_cblock_ID_ref[0], (size_t)nmb);
+        auto lev = d2h(mesh.c_cblock_level[0], (size_t)nmb);
+        auto cm = d2h(mesh.c_cells_ID_mask[0], (size_t)nmc);
+        auto F = d2h(mesh.c_cells_f_F[0], (size_t)N_U * nmc);
+        for (int b : blk) {
+            for (int d = 0; d < dim; d++) put(f, &fX[b + (size_t)d * nmb], 1);
+            put(f, &bm[b], 1);
+            for (int q = 0; q < Qmax; q++) put(f, &nb[b + (size_t)q * nmb], 1);
+            for (int q = 0; q < Qmax; q++) put(f, &nc[b + (size_t)q * nmb], 1);
+            put(f, &onb[b], 1);
+            put(f, &ref[b], 1);
+            put(f, &lev[b], 1);
+            put(f, &cm[(size_t)b * MC], MC);
+            for (int u = 0; u < N_U; u++) put(f, &F[(size_t)u * nmc + (size_t)b * MC], MC);
+        }
+        fclose(f);
+    }
+
+    if (n_timed > 0) {
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, mesh.streams[0]);
+        for (int i = 0; i < n_timed; i++) mesh.M_Advance_Step(n_steps + i, 0, iter_mult);
+        cudaEventRecord(e1, mesh.streams[0]);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        // Cell updates per coarse step as solver_lbm_advance.cu:74-89 counts them.
+        long long cells = 0;
+        int mult = 1;
+        for (int L = mesh.N_LEVEL_START; L < mesh.MAX_LEVELS - 1; L++) {
+            cells += (long long)mult * (mesh.n_ids[0][L] - mesh.n_ids[0][L + 1] / APh.N_CHILDREN);
+            mult *= 2;
+        }
+        cells += (long long)mult * mesh.n_ids[0][mesh.MAX_LEVELS - 1];
+        cells *= APh.M_CBLOCK;
+        const double mlups = (double)cells * n_timed / (ms * 1e-3) / 1e6;
+        printf("{\"ref_timing\": true, \"steps\": %d, \"ms\": %.4f, \"cell_updates_per_step\": %lld, \"mlups\": %.3f}\n",
+               n_timed, ms, cells, mlups);
+    }
+    if (ballast) cudaFree(ballast);
+    return 0;
+}

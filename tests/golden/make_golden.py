@@ -1,0 +1,213 @@
+#!/usr/bin/env python
+"""Generate the golden fixtures that pin the oracle and the CUDA library to
+the reference (KhodrJ/AGAL).
+
+    python tests/golden/make_golden.py tables [--ref /root/reference]
+        Extract the lattice tables (direction vectors, opposites, neighbour
+        slot map, weights, block-neighbour directions) from the reference
+        sources (inc/util.h:94-101, src/solver_lbm/solver_lbm_init.cu:79-91,
+        inc/mesh.h:468-472) into lattice_tables.json.  CPU only; needs the
+        reference tree.
+
+    python tests/golden/make_golden.py ref --out DIR
+        Run the reference's own CUDA build (oracle/_ref/ref_*, built by
+        `make -C oracle ref`) on the cases of CASES and convert each binary
+        dump into DIR/<case>.npz.  Needs a GPU; the reference tree is not
+        needed at run time.
+
+    python tests/golden/make_golden.py time --out DIR
+        Time the reference CUDA build (MLUPS, CUDA events around its
+        M_Advance_Step loop) on the benchmark workloads; writes DIR/ref_timing.json.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+REF_BIN = ROOT / "oracle" / "_ref"
+
+# Golden cases: (binary, input.txt keys, steps, keep_mb)
+CASES = {
+    "d2q9_ldc64_re100": ("ref_d2q9_ldc", dict(Nx=64, v0=5e-4), 1000, 48),
+    "d2q9_ldc64_px": ("ref_d2q9_ldc", dict(Nx=64, v0=5e-4, PERIODIC_X=1), 300, 48),
+    "d2q9_ldc32x64": ("ref_d2q9_ldc", dict(Nx=32, L_fy=2.0, v0=5e-4), 300, 48),
+    "d3q19_ldc16_re400": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4), 200, 48),
+    "d3q27_ldc16_re200": ("ref_d3q27_ldc", dict(Nx=16, v0=2.5e-4), 200, 48),
+    "d3q19_ldc16_pxy": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4, PERIODIC_X=1, PERIODIC_Y=1), 100, 48),
+}
+
+# Timing workloads of the reference build: (binary, keys, timed steps, keep_mb)
+TIMING = {
+    "ldc2d_256": ("ref_d2q9_ldc", dict(Nx=256, v0=5e-4), 2000, 512),
+    "ldc2d_8192": ("ref_d2q9_ldc", dict(Nx=8192, v0=5e-4), 20, 16384),
+    "ldc3d19_384": ("ref_d3q19_ldc", dict(Nx=384, v0=1.25e-4), 10, 24576),
+}
+
+BASE_KEYS = dict(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, N_LEVEL_START=0, L_c=1.0, L_fy=1.0, L_fz=1.0,
+                 N_RESTART=0, PERIODIC_X=0, PERIODIC_Y=0, PERIODIC_Z=0, N_ITER_TOTAL=1000,
+                 S_FORCE_TYPE=2, S_BC_TYPE=0, S_CRITERION=0, N_PROBE=0, N_PROBE_FORCE=0, N_PRINT_LEVELS=0,
+                 N_PRINT_LEVELS_IMAGE=0, P_OUTPUT=100000)
+
+
+# ---------------------------------------------------------------------------
+def _c_array(text: str, name: str) -> list[float]:
+    m = re.search(name + r"\s*\[[^\]]*\]\s*=\s*\{([^}]*)\}", text)
+    if not m:
+        raise ValueError(f"array {name} not found")
+    out = []
+    for tok in m.group(1).split(","):
+        tok = tok.strip()
+        if not tok:
+            continue
+        if "/" in tok:
+            a, b = tok.split("/")
+            out.append(float(a) / float(b))
+        else:
+            out.append(float(tok))
+    return out
+
+
+def cmd_tables(ref: Path) -> None:
+    util = (ref / "inc" / "util.h").read_text()
+    init = (ref / "src" / "solver_lbm" / "solver_lbm_init.cu").read_text()
+    mesh = (ref / "inc" / "mesh.h").read_text()
+    t = {}
+    for nm in ["V_CONN_ID_2D", "V_CONN_ID_3D", "V_CONN_ID_PB_2D", "V_CONN_ID_PB_3D", "V_CONN_MAP_2D", "V_CONN_MAP_3D"]:
+        t[nm] = [int(v) for v in _c_array(util, nm)]
+    for nm in ["LBMw_D2Q9", "LBMw_D3Q19", "LBMw_D3Q27"]:
+        t[nm] = _c_array(init, nm)
+    for nm in ["LBMpb_D2Q9", "LBMpb_D3Q19", "LBMpb_D3Q27"]:
+        t[nm] = [int(v) for v in _c_array(init, nm)]
+    m = re.search(r"c\[2\]\[27\*3\]\s*=\s*\{(.*?)\};", mesh, re.S)
+    rows = re.findall(r"\{([^{}]*)\}", m.group(1))
+    t["MESH_C_2D"] = [int(float(v)) for v in rows[0].split(",") if v.strip()]
+    t["MESH_C_3D"] = [int(float(v)) for v in rows[1].split(",") if v.strip()]
+    (HERE / "lattice_tables.json").write_text(json.dumps(t, indent=1))
+    print("wrote", HERE / "lattice_tables.json")
+
+
+# ---------------------------------------------------------------------------
+def write_input(d: Path, keys: dict, out_dir: Path) -> None:
+    kv = dict(BASE_KEYS)
+    kv.update(keys)
+    kv["P_DIR_NAME"] = str(out_dir) + "/"
+    kv["I_DIR_NAME"] = str(d) + "/"
+    lines = [f"{k} {v}" for k, v in kv.items()]
+    (d / "input.txt").write_text("\n".join(lines) + "\n")
+
+
+def read_dump(path: Path) -> dict:
+    """Parse an AGALREF1 dump written by oracle/ref_harness/ref_main.cu."""
+    b = path.read_bytes()
+    if b[:8] != b"AGALREF1":
+        raise ValueError("bad magic")
+    o = 8
+
+    def take(dt, n):
+        nonlocal o
+        a = np.frombuffer(b, dtype=dt, count=n, offset=o).copy()
+        o += a.nbytes
+        return a
+
+    dim, Q, Qmax, MC, ML, steps = take(np.int32, 6)
+    nmb, nmc = take(np.int64, 2)
+    n_ids = take(np.int32, ML + 1)
+    id_max = take(np.int32, ML + 1)
+    n_gaps = take(np.int32, 1)[0]
+    id_sets = [take(np.int32, int(n_ids[L])) for L in range(ML)]
+    n_gap_keep = take(np.int32, 1)[0]
+    gaps_tail = take(np.int32, int(n_gap_keep))
+    n_act = take(np.int32, 1)[0]
+    blocks = take(np.int32, int(n_act))
+    NU = Q + dim + 1
+    rec = [("fX", np.float32, dim), ("bmask", np.int32, 1), ("nbr", np.int32, Qmax), ("nbr_child", np.int32, Qmax),
+           ("onb", np.int32, 1), ("ref", np.int32, 1), ("level", np.int32, 1), ("cmask", np.int32, MC),
+           ("F", np.float32, NU * MC)]
+    out = {k: [] for k, _, _ in rec}
+    for _ in range(int(n_act)):
+        for k, dt, n in rec:
+            out[k].append(take(dt, n))
+    res = dict(dim=int(dim), Q=int(Q), Qmax=int(Qmax), MC=int(MC), max_levels=int(ML), steps=int(steps),
+               n_maxcblocks=int(nmb), n_maxcells=int(nmc), n_ids=n_ids, id_max=id_max, n_gaps=int(n_gaps),
+               gaps_tail=gaps_tail, blocks=blocks)
+    for L in range(ML):
+        res[f"id_set_{L}"] = id_sets[L]
+    for k, _, _ in rec:
+        res[k] = np.stack(out[k]) if out[k] else np.zeros((0,))
+    res["F"] = res["F"].reshape(int(n_act), NU, int(MC))
+    return res
+
+
+def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0) -> str:
+    exe = REF_BIN / binary
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        (td / "out").mkdir()
+        write_input(td, keys, td / "out")
+        cmd = [str(exe), str(td) + "/", str(dump) if dump else "-", str(steps), str(keep_mb), str(n_timed)]
+        r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            raise RuntimeError(f"{binary} failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
+        return r.stdout
+
+
+def cmd_ref(out: Path, only: list[str] | None) -> None:
+    out.mkdir(parents=True, exist_ok=True)
+    for name, (binary, keys, steps, keep) in CASES.items():
+        if only and name not in only:
+            continue
+        raw = out / f"{name}.bin"
+        run_ref(binary, keys, steps, keep, raw)
+        d = read_dump(raw)
+        d["case_keys"] = json.dumps(keys)
+        d["binary"] = binary
+        np.savez_compressed(out / f"{name}.npz", **d)
+        raw.unlink()
+        print(name, "n_maxcblocks", d["n_maxcblocks"], "active", len(d["blocks"]), flush=True)
+
+
+def cmd_time(out: Path) -> None:
+    out.mkdir(parents=True, exist_ok=True)
+    res = {}
+    for name, (binary, keys, n_timed, keep) in TIMING.items():
+        txt = run_ref(binary, keys, 3, keep, None, n_timed=n_timed)
+        line = [ln for ln in txt.splitlines() if ln.startswith("{\"ref_timing\"")]
+        res[name] = json.loads(line[-1]) if line else {"error": txt[-500:]}
+        print(name, res[name], flush=True)
+    (out / "ref_timing.json").write_text(json.dumps(res, indent=1))
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("tables")
+    t.add_argument("--ref", default="/root/reference")
+    r = sub.add_parser("ref")
+    r.add_argument("--out", default=str(HERE))
+    r.add_argument("--only", nargs="*")
+    tm = sub.add_parser("time")
+    tm.add_argument("--out", required=True)
+    a = ap.parse_args(argv)
+    if a.cmd == "tables":
+        cmd_tables(Path(a.ref))
+    elif a.cmd == "ref":
+        cmd_ref(Path(a.out), a.only)
+    else:
+        cmd_time(Path(a.out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,211 @@
+"""Parity of the CUDA single-level step (fused collide + boundary + stream)
+with the CPU oracle and with the reference's own CUDA build.
+
+Tolerances: FP32 and FP64 storage compare the full population arrays;
+rho and u are held to 1e-5 relative L2 (FP32) as the reference-parity bar.
+FP16/BF16 weight-offset storage is compared with an FP64 oracle run:
+relative L2 of u below 1e-3 (BF16: 1e-2), of rho below 1e-5 (BF16: 1e-4).
+Integer arrays (root grid, masks, ID sets) must be bit-exact."""
+import numpy as np
+import pytest
+
+from helpers import brute_root_grid, lattice, macros_from_F, rel_l2
+from test_oracle import GOLDEN_CASES, compare_to_golden, load_golden, params_for_golden
+
+import agal_b200 as ag
+from agal_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+VS = {9: _lib.D2Q9, 19: _lib.D3Q19, 27: _lib.D3Q27}
+
+
+def ldc_params(Q, N, steps_re=100.0, storage=_lib.STORE_FP32, extra=None):
+    dim = 2 if Q == 9 else 3
+    kw = dict(velocity_set=VS[Q], Nx=N, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, v0=0.05 / steps_re,
+              bc_preset=_lib.BC_LDC2D if dim == 2 else _lib.BC_LDC3D, storage=storage,
+              n_maxcblocks=(N // 4) ** dim + 5)
+    if extra:
+        kw.update(extra)
+    return ag.default_params(**kw)
+
+
+def run_pair(p, steps, fp64_oracle=False, use_graph=False):
+    from oracle.orc import OracleCase
+    o = OracleCase(p, p.n_maxcblocks, fp64=fp64_oracle)
+    o.set_ic(0)
+    o.advance_n(steps)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        if use_graph:
+            c.advance_n(steps, use_graph=True)
+        else:
+            for _ in range(steps):
+                c.advance()
+        c.sync()
+        F = c.dump(_lib.ARR_F)
+        ints = {k: c.dump(k) for k in (_lib.ARR_CBLOCK_ID_NBR, _lib.ARR_CBLOCK_ID_NBR_CHILD, _lib.ARR_CBLOCK_ID_ONB,
+                                       _lib.ARR_ID_SET, _lib.ARR_GAP_SET, _lib.ARR_CBLOCK_F_X)}
+    oints = {k: o.dump(k) for k in ints}
+    return F, o.dump(_lib.ARR_F), ints, oints
+
+
+def active(F, Q, nmb, n):
+    MC = F.size // (Q * nmb)
+    return F.reshape(Q, nmb, MC)[:, :n, :].reshape(Q, -1)
+
+
+@pytest.mark.parametrize("Q,N,steps", [(9, 64, 500), (9, 128, 200), (19, 16, 100), (27, 16, 100), (19, 32, 50)])
+def test_fp32_step_matches_oracle(Q, N, steps):
+    p = ldc_params(Q, N)
+    F, Fo, ints, oints = run_pair(p, steps)
+    for k in ints:
+        assert (ints[k] == oints[k]).all(), k
+    dim = 2 if Q == 9 else 3
+    n = (N // 4) ** dim
+    A, B = active(F, Q, p.n_maxcblocks, n), active(Fo, Q, p.n_maxcblocks, n)
+    pb, c, _ = lattice(Q)
+    rho, u = macros_from_F(A, dim, Q, pb, c)
+    rho_o, u_o = macros_from_F(B, dim, Q, pb, c)
+    assert rel_l2(rho, rho_o) < 1e-5
+    assert rel_l2(np.stack(u), np.stack(u_o)) < 1e-5
+    assert np.abs(A - B).max() < 1e-5
+
+
+@pytest.mark.parametrize("Q", [9, 19, 27])
+def test_fp64_step_matches_fp64_oracle(Q):
+    N = 32 if Q == 9 else 12
+    p = ldc_params(Q, N, storage=_lib.STORE_FP64)
+    F, Fo, _, _ = run_pair(p, 100, fp64_oracle=True)
+    dim = 2 if Q == 9 else 3
+    n = (N // 4) ** dim
+    assert np.abs(active(F, Q, p.n_maxcblocks, n) - active(Fo, Q, p.n_maxcblocks, n)).max() < 1e-12
+
+
+@pytest.mark.parametrize("Q,storage,tol_u,tol_rho", [(9, _lib.STORE_FP16, 1e-3, 1e-5), (9, _lib.STORE_BF16, 1e-2, 1e-4),
+                                                     (19, _lib.STORE_FP16, 1e-3, 1e-5),
+                                                     (27, _lib.STORE_BF16, 1e-2, 1e-4)])
+def test_half_storage_vs_fp64_oracle(Q, storage, tol_u, tol_rho):
+    N = 64 if Q == 9 else 16
+    p = ldc_params(Q, N, storage=storage)
+    F, Fo, _, _ = run_pair(p, 300 if Q == 9 else 100, fp64_oracle=True)
+    dim = 2 if Q == 9 else 3
+    n = (N // 4) ** dim
+    pb, c, _ = lattice(Q)
+    rho, u = macros_from_F(active(F, Q, p.n_maxcblocks, n), dim, Q, pb, c)
+    rho_o, u_o = macros_from_F(active(Fo, Q, p.n_maxcblocks, n), dim, Q, pb, c)
+    assert rel_l2(rho, rho_o) < tol_rho
+    assert rel_l2(np.stack(u), np.stack(u_o)) < tol_u
+
+
+@pytest.mark.parametrize("per", [(1, 0, 0), (0, 1, 0), (1, 1, 0)])
+def test_periodic_2d(per):
+    p = ldc_params(9, 32, extra=dict(PERIODIC_X=per[0], PERIODIC_Y=per[1], L_fy=0.5))
+    p.n_maxcblocks = 8 * 4 + 3
+    F, Fo, ints, oints = run_pair(p, 150)
+    for k in ints:
+        assert (ints[k] == oints[k]).all()
+    assert np.abs(active(F, 9, p.n_maxcblocks, 32) - active(Fo, 9, p.n_maxcblocks, 32)).max() < 1e-5
+
+
+def test_periodic_3d_fpsc_preset():
+    p = ag.default_params(velocity_set=_lib.D3Q27, Nx=16, L_fy=0.5, L_fz=0.5, MAX_LEVELS_WALL=1,
+                          MAX_LEVELS_INTERIOR=1, v0=1e-4, bc_preset=_lib.BC_FPSC3D, ic_preset=_lib.IC_UNIFORM,
+                          ic_noise=0.01, seed=11, PERIODIC_Z=1, n_maxcblocks=20)
+    F, Fo, _, _ = run_pair(p, 60)
+    assert np.abs(active(F, 27, 20, 16) - active(Fo, 27, 20, 16)).max() < 2e-5
+
+
+def test_root_grid_matches_brute_force():
+    p = ag.default_params(velocity_set=_lib.D3Q19, Nx=16, L_fy=0.5, L_fz=0.75, MAX_LEVELS_WALL=1,
+                          MAX_LEVELS_INTERIOR=1, PERIODIC_Y=1, n_maxcblocks=40)
+    nb_exp, onb_exp = brute_root_grid(3, 16, 8, 12, (0, 1, 0))
+    n = nb_exp.shape[1]
+    with ag.Case(p) as c:
+        nbr = c.dump(_lib.ARR_CBLOCK_ID_NBR).reshape(27, 40)
+        onb = c.dump(_lib.ARR_CBLOCK_ID_ONB)
+    assert (nbr[:, :n] == nb_exp).all() and (onb[:n] == onb_exp).all()
+
+
+def test_graph_replay_bit_identical():
+    p = ldc_params(9, 64)
+    with ag.Case(p) as a, ag.Case(p) as b:
+        a.set_ic(0)
+        b.set_ic(0)
+        for _ in range(40):
+            a.advance()
+        b.advance_n(20, use_graph=True)
+        b.advance_n(20, use_graph=True)   # replay of the same graph
+        a.sync()
+        b.sync()
+        assert np.array_equal(a.dump(_lib.ARR_F), b.dump(_lib.ARR_F))
+
+
+def test_deterministic():
+    p = ldc_params(19, 16)
+    out = []
+    for _ in range(2):
+        with ag.Case(p) as c:
+            c.set_ic(0)
+            c.advance_n(30, use_graph=False)
+            out.append(c.dump(_lib.ARR_F))
+    assert np.array_equal(out[0], out[1])
+
+
+def test_mass_momentum_fp64_matches_oracle():
+    from oracle.orc import OracleCase
+    p = ldc_params(9, 64, storage=_lib.STORE_FP64, extra=dict(PERIODIC_X=1, PERIODIC_Y=1, bc_preset=_lib.BC_NONE,
+                                                              ic_preset=_lib.IC_UNIFORM, ic_noise=0.3, seed=3))
+    o = OracleCase(p, p.n_maxcblocks, fp64=True)
+    o.set_ic(0)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        m0 = c.mass_momentum()
+        assert np.allclose(m0, o.mass_momentum(), rtol=1e-13, atol=1e-12)
+        c.advance_n(100, use_graph=False)
+        m1 = c.mass_momentum()
+    # periodic box, no walls: mass and momentum conserved to rounding
+    assert abs(m1[0] - m0[0]) < 1e-10 * m0[0]
+    assert np.abs(m1[1:] - m0[1:]).max() < 1e-9
+
+
+def test_refresh_macros():
+    p = ldc_params(27, 8)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        c.advance_n(10, use_graph=False)
+        c.refresh(0)
+        M = c.dump(_lib.ARR_MACROS).reshape(4, -1)[:, : 8 * 64]
+        F = c.dump(_lib.ARR_F).reshape(27, -1)[:, : 8 * 64]
+    pb, cv, _ = lattice(27)
+    rho, u = macros_from_F(F, 3, 27, pb, cv)
+    assert np.abs(M[0] - rho).max() < 1e-6
+    assert np.abs(M[1:] - np.stack(u)).max() < 1e-6
+
+
+@pytest.mark.skipif(not GOLDEN_CASES, reason="no reference dumps committed")
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_cuda_vs_reference_build(name):
+    g = load_golden(name)
+    p, steps = params_for_golden(g)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        c.advance_n(steps, use_graph=False)
+        c.sync()
+        compare_to_golden(g, c.dump, 1e-5)
+
+
+def test_large_grid_properties():
+    """At benchmark scale (D2Q9 2048^2), where the oracle is too slow to run
+    alongside: a closed cavity with plain bounce-back walls conserves its FP64
+    mass to round-off and keeps zero momentum."""
+    N = 2048
+    p = ag.default_params(velocity_set=_lib.D2Q9, Nx=N, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, v0=5e-4,
+                          bc_preset=_lib.BC_NONE, n_maxcblocks=(N // 4) ** 2)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        m0 = c.mass_momentum()
+        c.advance_n(50, use_graph=True)
+        m1 = c.mass_momentum()
+    assert abs(m1[0] - m0[0]) < 1e-6 * m0[0]
+    assert np.abs(m1[1:]).max() < 1e-6 * m0[0]

@@ -1,0 +1,141 @@
+"""The CPU oracle against the reference: lattice tables and root grid
+bit-exact against the golden vectors extracted from the reference sources,
+and populations against the reference's own CUDA build (golden dumps in
+tests/golden/*.npz, made by tests/golden/make_golden.py on a B200)."""
+import json
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, brute_root_grid, lattice, macros_from_F, rel_l2, tables
+
+import agal_b200 as ag
+from agal_b200 import _lib
+
+
+def test_golden_tables_consistent():
+    t = tables()
+    # D3Q19 is the first 19 directions of the D3Q27 order; opposites are involutions.
+    for key in ["LBMpb_D2Q9", "LBMpb_D3Q19", "LBMpb_D3Q27"]:
+        pb = t[key]
+        assert all(pb[pb[p]] == p for p in range(len(pb)))
+    c = np.array(t["V_CONN_ID_3D"]).reshape(3, 27)
+    for p, q in enumerate(t["LBMpb_D3Q27"]):
+        assert (c[:, p] == -c[:, q]).all()
+    assert abs(sum(t["LBMw_D2Q9"]) - 1) < 1e-15 and abs(sum(t["LBMw_D3Q27"]) - 1) < 1e-15
+    # block-neighbour directions of mesh.h equal the D2Q9 / D3Q27 velocities
+    assert t["MESH_C_3D"] == t["V_CONN_ID_3D"]
+    assert t["MESH_C_2D"] == t["V_CONN_ID_2D"][:9] + t["V_CONN_ID_2D"][27:36]
+
+
+@pytest.mark.parametrize("vs,N,per", [(0, (32, 32, 1), (0, 0, 0)), (0, (32, 16, 1), (1, 0, 0)),
+                                      (0, (16, 32, 1), (0, 1, 0)), (1, (16, 16, 16), (0, 0, 0)),
+                                      (2, (16, 8, 12), (1, 0, 1)), (1, (8, 16, 8), (0, 1, 1))])
+def test_oracle_root_grid_bit_exact(oracle_lib, vs, N, per):
+    from oracle.orc import OracleCase
+    Nx, Ny, Nz = N
+    p = ag.default_params(velocity_set=vs, Nx=Nx, L_fy=Ny / Nx, L_fz=Nz / Nx, MAX_LEVELS_WALL=1,
+                          MAX_LEVELS_INTERIOR=1, PERIODIC_X=per[0], PERIODIC_Y=per[1], PERIODIC_Z=per[2])
+    dim = 2 if vs == 0 else 3
+    nb_exp, onb_exp = brute_root_grid(dim, Nx, Ny, Nz, per)
+    n = nb_exp.shape[1]
+    nmb = n + 37
+    o = OracleCase(p, nmb)
+    Qmax = 9 if dim == 2 else 27
+    nbr = o.dump(_lib.ARR_CBLOCK_ID_NBR).reshape(Qmax, nmb)
+    assert (nbr[:, :n] == nb_exp).all()
+    assert (nbr[:, n:] == -999).all()
+    onb = o.dump(_lib.ARR_CBLOCK_ID_ONB)
+    assert (onb[:n] == onb_exp).all()
+    ch = o.dump(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(Qmax, nmb)
+    assert (ch[:, :n] == np.where(nb_exp < 0, nb_exp, -999)).all()
+    gaps = o.dump(_lib.ARR_GAP_SET)
+    assert (gaps[: nmb - n] == np.arange(nmb - 1, n - 1, -1)).all()
+    ids = o.dump(_lib.ARR_ID_SET)
+    assert (ids[:n] == np.arange(n)).all()
+    c = o.counts()
+    assert c["n_ids"][0] == n and c["n_gaps"] == nmb - n and c["id_max"][0] == n
+
+
+def test_oracle_rest_state_is_fixed_point(oracle_lib):
+    from oracle.orc import OracleCase
+    p = ag.default_params(velocity_set=_lib.D3Q19, Nx=8, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, v0=1e-3)
+    o = OracleCase(p, 8, fp64=True)
+    o.set_ic(0)
+    f0 = o.dump(_lib.ARR_F)
+    o.advance_n(20)
+    assert np.abs(o.dump(_lib.ARR_F) - f0).max() < 1e-15
+
+
+def test_oracle_periodic_mass_momentum_conserved(oracle_lib):
+    from oracle.orc import OracleCase
+    p = ag.default_params(velocity_set=_lib.D2Q9, Nx=32, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, v0=1e-3,
+                          PERIODIC_X=1, PERIODIC_Y=1, ic_preset=_lib.IC_UNIFORM, ic_noise=0.2, seed=7)
+    o = OracleCase(p, 64, fp64=True)
+    o.set_ic(0)
+    m0 = o.mass_momentum()
+    o.advance_n(50)
+    m1 = o.mass_momentum()
+    assert abs(m1[0] - m0[0]) < 1e-10 * m0[0]
+    assert np.abs(m1[1:] - m0[1:]).max() < 1e-10 * m0[0]
+
+
+# ---------------------------------------------------------------------------
+# Against the reference's own CUDA build (fixtures from a B200 run).
+GOLDEN_CASES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load_golden(name):
+    d = np.load(GOLDEN / f"{name}.npz", allow_pickle=False)
+    return {k: d[k] for k in d.files}
+
+
+def params_for_golden(g):
+    keys = json.loads(str(g["case_keys"]))
+    vs = {9: _lib.D2Q9, 19: _lib.D3Q19, 27: _lib.D3Q27}[int(g["Q"])]
+    bc = _lib.BC_LDC2D if int(g["dim"]) == 2 else _lib.BC_LDC3D
+    kw = dict(velocity_set=vs, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, bc_preset=bc,
+              ic_preset=_lib.IC_REST, n_maxcblocks=int(g["n_maxcblocks"]))
+    kw.update(keys)
+    return ag.default_params(**kw), int(g["steps"])
+
+
+def compare_to_golden(g, dumpf, tol_rel_l2):
+    """Integer arrays bit-exact, rho/u within tol_rel_l2 (relative L2)."""
+    blocks = g["blocks"].astype(np.int64)
+    dim, Q, Qmax, MC = int(g["dim"]), int(g["Q"]), int(g["Qmax"]), int(g["MC"])
+    nmb = int(g["n_maxcblocks"])
+    nbr = dumpf(_lib.ARR_CBLOCK_ID_NBR).reshape(Qmax, nmb)[:, blocks].T
+    assert (nbr == g["nbr"]).all()
+    ch = dumpf(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(Qmax, nmb)[:, blocks].T
+    assert (ch == g["nbr_child"]).all()
+    for arr, key in [(_lib.ARR_CBLOCK_ID_ONB, "onb"), (_lib.ARR_CBLOCK_ID_REF, "ref"),
+                     (_lib.ARR_CBLOCK_LEVEL, "level"), (_lib.ARR_CBLOCK_ID_MASK, "bmask")]:
+        assert (dumpf(arr)[blocks] == g[key][:, 0]).all(), key
+    fX = dumpf(_lib.ARR_CBLOCK_F_X).reshape(dim, nmb)[:, blocks].T
+    assert (fX == g["fX"]).all()
+    cm = dumpf(_lib.ARR_CELLS_ID_MASK).reshape(nmb, MC)[blocks]
+    assert (cm == g["cmask"]).all()
+    for L in range(int(g["max_levels"])):
+        n = int(g["n_ids"][L])
+        assert (dumpf(_lib.ARR_ID_SET).reshape(-1, nmb)[L, :n] == g[f"id_set_{L}"]).all()
+    F = dumpf(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks, :].reshape(Q, -1)
+    Fr = np.transpose(g["F"][:, :Q, :], (1, 0, 2)).reshape(Q, -1).astype(np.float64)
+    pb, c, _ = lattice(Q)
+    rho, u = macros_from_F(F, dim, Q, pb, c)
+    rho_r, u_r = macros_from_F(Fr, dim, Q, pb, c)
+    assert rel_l2(rho, rho_r) < tol_rel_l2
+    assert rel_l2(np.stack(u), np.stack(u_r)) < tol_rel_l2
+    return rel_l2(F, Fr)
+
+
+@pytest.mark.skipif(not GOLDEN_CASES, reason="no reference dumps committed")
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_vs_reference_build(oracle_lib, name):
+    from oracle.orc import OracleCase
+    g = load_golden(name)
+    p, steps = params_for_golden(g)
+    o = OracleCase(p, int(g["n_maxcblocks"]))
+    o.set_ic(0)
+    o.advance_n(steps)
+    compare_to_golden(g, o.dump, 1e-5)

@@ -466,17 +466,20 @@ extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
         std::vector<int> wb, cm(c->nmc);
         if ((rc = block_buffers(c, wb))) return rc;
         AGAL_CUDA(c, cudaMemcpy(cm.data(), c->cells_ID_mask, sizeof(int) * c->nmc, cudaMemcpyDeviceToHost));
+        // Device layout F[b][s][c] -> reference layout cells_f_F[s][b*MC + c].
         double *o = static_cast<double *>(host_buf);
         for (int s = 0; s < c->Q; s++) {
             const int p = lat_pb(c->dim, s);   // slot s holds f_p, w_p == w_s
             for (long long cell = 0; cell < c->nmc; cell++) {
                 const size_t i = (size_t)s * c->nmc + cell;
-                const auto &r = raw[wb[cell / c->MC]];
+                const long long b = cell / c->MC;
+                const size_t src = ((size_t)b * c->Q + s) * c->MC + (cell % c->MC);
+                const auto &r = raw[wb[b]];
                 switch (c->storage) {
-                case AGAL_STORE_FP32: decode<float>(r, i, c->Q, p, &o[i]); break;
-                case AGAL_STORE_FP64: decode<double>(r, i, c->Q, p, &o[i]); break;
-                case AGAL_STORE_FP16: decode<__half>(r, i, c->Q, p, &o[i]); break;
-                case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, i, c->Q, p, &o[i]); break;
+                case AGAL_STORE_FP32: decode<float>(r, src, c->Q, p, &o[i]); break;
+                case AGAL_STORE_FP64: decode<double>(r, src, c->Q, p, &o[i]); break;
+                case AGAL_STORE_FP16: decode<__half>(r, src, c->Q, p, &o[i]); break;
+                case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, src, c->Q, p, &o[i]); break;
                 }
                 if (cm[cell] == CELL_SOLID) o[i] = -1.0;
             }
@@ -515,11 +518,12 @@ extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t by
             const int p = lat_pb(c->dim, s);
             for (long long cell = 0; cell < c->nmc; cell++) {
                 const size_t i = (size_t)s * c->nmc + cell;
+                const size_t dst = ((size_t)(cell / c->MC) * c->Q + s) * c->MC + (cell % c->MC);
                 switch (c->storage) {
-                case AGAL_STORE_FP32: encode<float>(raw, i, c->Q, p, in[i]); break;
-                case AGAL_STORE_FP64: encode<double>(raw, i, c->Q, p, in[i]); break;
-                case AGAL_STORE_FP16: encode<__half>(raw, i, c->Q, p, in[i]); break;
-                case AGAL_STORE_BF16: encode<__nv_bfloat16>(raw, i, c->Q, p, in[i]); break;
+                case AGAL_STORE_FP32: encode<float>(raw, dst, c->Q, p, in[i]); break;
+                case AGAL_STORE_FP64: encode<double>(raw, dst, c->Q, p, in[i]); break;
+                case AGAL_STORE_FP16: encode<__half>(raw, dst, c->Q, p, in[i]); break;
+                case AGAL_STORE_BF16: encode<__nv_bfloat16>(raw, dst, c->Q, p, in[i]); break;
                 }
             }
         }

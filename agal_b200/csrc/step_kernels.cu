@@ -1,6 +1,13 @@
 // Per-level LBM kernels: initial conditions, the fused collide + boundary +
 // stream step, macro refresh and FP64 mass/momentum sums.
 //
+// Population layout (block-major): F[b][s][c] = slot s of cell c of block b,
+// so one block's Q x M_CBLOCK values are contiguous and every load of a
+// cell's own populations is (block base + compile-time offset).  Slot s of a
+// cell holds f_{pb(s)}: the reference's post-stream convention
+// (solver_lbm_kernels.cu:67, 251).  agal_dump / agal_load convert to and from
+// the reference's slot-major array cells_f_F[s][n_maxcells].
+//
 // The fused step replaces the reference's sequence
 //   Cu_RefreshVariables -> Cu_Collide -> Cu_ImposeBC -> Cu_Stream
 // (solver_lbm_kernels.cu:112, 206, 693, 534), which reads and writes the
@@ -14,7 +21,9 @@
 // Algorithmic traffic: 2 * Q * sizeof(storage) bytes per cell update.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
+#include <vector>
 
 #include "ctx.h"
 #include "lattice.cuh"
@@ -22,29 +31,29 @@
 
 namespace agal {
 
-__constant__ int c_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
-__constant__ int c_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
-                               1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
+// Neighbour-slot -> neighbour-array index (inc/util.h:100-101).  Read with a
+// different index by every thread, so it lives in global memory (L1-cached)
+// rather than in the constant bank, which serialises divergent reads.
+__device__ const int g_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
+__device__ const int g_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
+                                   1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
 
 struct StepArgs {
     const int *ids;
     int n;
     const void *fin;
     void *fout;
-    long long nmc, nmb;
+    long long nmb;
     const int *nbr, *nbr_child, *bmask, *onb, *cmask;
     double omega;
     double u_ref;
     int bc_preset;
-    int has_solid;
 };
 
 // Boundary hook presets (inc/custom.h:79-122); f is the full population.
 template <typename C>
-__device__ __forceinline__ C bc_hook(int preset, int nb, C f, C rho, C u, C v, C w, C wp, int cx,
-                                     int cy, int cz, C U)
+__device__ __forceinline__ C bc_hook(int preset, int nb, C f, C u, C v, C w, C wp, int cx, int cy, int cz, C U)
 {
-    (void)rho;
     bool inflow = false, outflow = false;
     switch (preset) {
     case AGAL_BC_LDC2D: inflow = (nb == -4); break;
@@ -65,79 +74,65 @@ __device__ __forceinline__ C bc_hook(int preset, int nb, C f, C rho, C u, C v, C
     return f;
 }
 
-template <int DIM, int Q, typename T, int BPC>
-__global__ void __launch_bounds__(BPC *Geo<DIM>::MC)
+// Minimum resident 256-thread CTAs per SM requested from the register
+// allocator: as many as fit without spilling the Q populations held per thread.
+template <int DIM, int Q, typename T> struct StepOcc {
+    static constexpr bool D = sizeof(typename ST<T>::C) == 8;
+    static constexpr int value = (Q == 9) ? (D ? 3 : 6) : (Q == 19) ? (D ? 2 : 4) : (D ? 1 : 3);
+};
+
+template <int DIM, int Q, typename T, int BPC, bool SOLID>
+__global__ void __launch_bounds__(BPC *Geo<DIM>::MC, (StepOcc<DIM, Q, T>::value))
 k_step(const StepArgs a)
 {
     using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX;
+    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
+    constexpr int CENTER = center_slot(DIM);
     __shared__ int s_nbr[BPC][QMAX];
-    __shared__ int s_blk[BPC];
-    __shared__ int s_flag[BPC];
     const int tid = threadIdx.x;
-    const long long base = (long long)blockIdx.x * BPC;
-
-    if (tid < BPC) {
-        long long kap = base + tid;
-        int b = -1, fl = 0;
-        if (kap < a.n) {
-            b = a.ids[kap];
-            if (b >= 0) {
-                if (a.nbr_child[b] < 0 || a.bmask[b] != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
-                if (a.onb[b] == 1) fl |= 2;                                     // kernels.cu:736
-            }
-        }
-        s_blk[tid] = b;
-        s_flag[tid] = fl;
-    }
-    __syncthreads();
-    for (int i = tid; i < BPC * QMAX; i += BPC * MC) {
-        const int S = i / BPC, lb = i % BPC;
-        const int b = s_blk[lb];
-        const int m = (DIM == 2) ? c_map2[S] : c_map3[S];
-        s_nbr[lb][S] = (b >= 0) ? a.nbr[b + (long long)m * a.nmb] : N_SKIPID;
-    }
-    __syncthreads();
-
     const int lb = tid / MC, t = tid % MC;
-    const int b = s_blk[lb];
-    const int fl = s_flag[lb];
-    if (b < 0 || !(fl & 1)) return;
-    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
-    const long long cell = (long long)b * MC + t;
-    if (a.has_solid && a.cmask[cell] == CELL_SOLID) return;   // solid cells keep their guard
+    const int kap = blockIdx.x * BPC + lb;
 
-    const T *__restrict__ fin = static_cast<const T *>(a.fin);
-    T *__restrict__ fout = static_cast<T *>(a.fout);
-    const long long nmc = a.nmc;
+    // Dependency depth 2: the block ID, then (populations | neighbour row |
+    // block flags) all in flight together before the one barrier.
+    const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
+    if (t < QMAX) {
+        int v = b;   // the centre slot is the block itself
+        if (t != CENTER) {
+            const int m = __ldg((DIM == 2) ? &g_map2[t] : &g_map3[t]);
+            v = (b >= 0) ? __ldg(&a.nbr[b + (long long)m * a.nmb]) : N_SKIPID;
+        }
+        s_nbr[lb][t] = v;
+    }
+    int fl = 0;
+    if (b >= 0) {
+        if (__ldg(&a.nbr_child[b]) < 0 || __ldg(&a.bmask[b]) != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
+        if (__ldg(&a.onb[b]) == 1) fl |= 2;                                             // kernels.cu:736
+    }
+    const T *__restrict__ fin = static_cast<const T *>(a.fin) + (long long)(b >= 0 ? b : 0) * BLK + t;
 
     // Load: slot pb(p) holds f_p (offset form g_p for half storage).
     C g[Q];
+    if (b >= 0) {
 #pragma unroll
-    for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(__ldg(&fin[(long long)lat_pb(DIM, p) * nmc + cell]));
+        for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(__ldg(fin + lat_pb(DIM, p) * MC));
+    }
+    __syncthreads();
+
+    if (b < 0 || !(fl & 1)) return;
+    if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) return;   // solid cells keep their guard
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
 
     C rho, drho = C(0), jx = C(0), jy = C(0), jz = C(0);
-    if (!ST<T>::OFF) {
-        // Direct form, operation order of Cu_Collide (kernels.cu:249-263).
 #pragma unroll
-        for (int p = 0; p < Q; p++) {
-            drho += g[p];
-            jx += C(lat_c(DIM, 0, p)) * g[p];
-            jy += C(lat_c(DIM, 1, p)) * g[p];
-            if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
-        }
-        rho = drho;
-    } else {
-        // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
-#pragma unroll
-        for (int p = 0; p < Q; p++) {
-            drho += g[p];
-            jx += C(lat_c(DIM, 0, p)) * g[p];
-            jy += C(lat_c(DIM, 1, p)) * g[p];
-            if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
-        }
-        rho = C(1) + drho;
+    for (int p = 0; p < Q; p++) {
+        drho += g[p];
+        jx += C(lat_c(DIM, 0, p)) * g[p];
+        jy += C(lat_c(DIM, 1, p)) * g[p];
+        if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
     }
+    // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
+    rho = ST<T>::OFF ? C(1) + drho : drho;
     const C ux = jx / rho, uy = jy / rho, uz = (DIM == 3) ? jz / rho : C(0);
     const C udotu = ux * ux + uy * uy + uz * uz;
     const C omeg = C(a.omega);
@@ -148,6 +143,7 @@ k_step(const StepArgs a)
         const C cu = C(lat_c(DIM, 0, p)) * ux + C(lat_c(DIM, 1, p)) * uy + C(lat_c(DIM, 2, p)) * uz;
         const C wp = C(lat_w(Q, p));
         if (!ST<T>::OFF) {
+            // Operation order of Cu_Collide (kernels.cu:282).
             g[p] = g[p] * omegp + (wp * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu)) * omeg;
         } else {
             // f' - w = g (1 - omega) + omega (feq - w),  feq - w = w (drho + rho X)
@@ -156,27 +152,28 @@ k_step(const StepArgs a)
     }
 
     // Push to destinations, bounce back on closed links.
+    T *__restrict__ fo = static_cast<T *>(a.fout);
+    T *__restrict__ own = fo + (long long)b * BLK + t;
+    const bool bnd = (fl & 2) && a.bc_preset != AGAL_BC_NONE;
 #pragma unroll
     for (int p = 0; p < Q; p++) {
-        constexpr int dummy = 0;
-        (void)dummy;
         const int cx = lat_c(DIM, 0, p), cy = lat_c(DIM, 1, p), cz = lat_c(DIM, 2, p);
         const int Ip = I + cx, Jp = J + cy, Kp = K + cz;
-        const int S = nbr_slot(DIM, Ip, Jp, Kp);
-        const int nb = (S == center_slot(DIM)) ? b : s_nbr[lb][S];
-        const int nc = nbr_cell(DIM, Ip, Jp, Kp);
+        const int S = ((Ip >> 2) + 1) + 3 * ((Jp >> 2) + 1) + (DIM == 3 ? 9 * ((Kp >> 2) + 1) : 0);
+        const int nc = (Ip & 3) | ((Jp & 3) << 2) | (DIM == 3 ? ((Kp & 3) << 4) : 0);
+        const int nb = s_nbr[lb][S];
         bool open = nb >= 0;
-        if (open && a.has_solid) open = a.cmask[(long long)nb * MC + nc] != CELL_SOLID;
+        if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
         if (open) {
-            fout[(long long)lat_pb(DIM, p) * nmc + (long long)nb * MC + nc] = ST<T>::enc(g[p]);
+            fo[(long long)nb * BLK + lat_pb(DIM, p) * MC + nc] = ST<T>::enc(g[p]);
         } else {
             C v = g[p];
-            if ((fl & 2) && nb < 0 && nb != N_SKIPID && a.bc_preset != AGAL_BC_NONE) {
+            if (bnd && nb != N_SKIPID) {
                 const C wp = C(lat_w(Q, p));
                 const C off = ST<T>::OFF ? wp : C(0);
-                v = bc_hook<C>(a.bc_preset, nb, v + off, rho, ux, uy, uz, wp, cx, cy, cz, C(a.u_ref)) - off;
+                v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx, cy, cz, C(a.u_ref)) - off;
             }
-            fout[(long long)p * nmc + cell] = ST<T>::enc(v);
+            own[p * MC] = ST<T>::enc(v);
         }
     }
 }
@@ -188,7 +185,7 @@ struct IcArgs {
     const int *ids;
     int n;
     void *f0, *f1;
-    long long nmc, nmb;
+    long long nmb;
     const int *cmask;
     const float *fX;
     double dxL, u_ref, noise;
@@ -214,7 +211,7 @@ template <int DIM, int Q, typename T>
 __global__ void k_set_ic(const IcArgs a)
 {
     using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long kap = gid / MC;
     const int t = (int)(gid % MC);
@@ -222,7 +219,6 @@ __global__ void k_set_ic(const IcArgs a)
     const int b = a.ids[kap];
     if (b < 0) return;
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
-    const long long cell = (long long)b * MC + t;
     C rho = C(1), u = C(0), v = C(0), w = C(0);
     if (a.ic_preset == AGAL_IC_UNIFORM) {
         u = C(a.u_ref);
@@ -237,8 +233,9 @@ __global__ void k_set_ic(const IcArgs a)
         }
     }
     const C udotu = u * u + v * v + w * w;
-    const bool solid = a.cmask[cell] == CELL_SOLID;
-    T *f0 = static_cast<T *>(a.f0), *f1 = static_cast<T *>(a.f1);
+    const bool solid = a.cmask[(long long)b * MC + t] == CELL_SOLID;
+    T *f0 = static_cast<T *>(a.f0) + (long long)b * BLK + t;
+    T *f1 = static_cast<T *>(a.f1) + (long long)b * BLK + t;
 #pragma unroll
     for (int p = 0; p < Q; p++) {
         const C cu = C(lat_c(DIM, 0, p)) * u + C(lat_c(DIM, 1, p)) * v + C(lat_c(DIM, 2, p)) * w;
@@ -247,15 +244,14 @@ __global__ void k_set_ic(const IcArgs a)
         if (solid) val = C(-1) - (ST<T>::OFF ? wp : C(0));
         else if (!ST<T>::OFF) val = rho * wp * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu);
         else val = wp * ((rho - C(1)) + rho * (C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu));
-        const long long o = (long long)lat_pb(DIM, p) * a.nmc + cell;
-        f0[o] = ST<T>::enc(val);
-        f1[o] = ST<T>::enc(val);
+        f0[lat_pb(DIM, p) * MC] = ST<T>::enc(val);
+        f1[lat_pb(DIM, p) * MC] = ST<T>::enc(val);
     }
 }
 
 // ---------------------------------------------------------------------------
 // Macros of one level from its current buffer (Cu_RefreshVariables,
-// kernels.cu:112-159), into the separate macro array.
+// kernels.cu:112-159), into the macro array [dim+1][n_maxcells].
 struct MacroArgs {
     const int *ids;
     int n;
@@ -268,19 +264,18 @@ template <int DIM, int Q, typename T>
 __global__ void k_refresh(const MacroArgs a)
 {
     using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long kap = gid / MC;
     const int t = (int)(gid % MC);
     if (kap >= a.n) return;
     const int b = a.ids[kap];
     if (b < 0) return;
-    const long long cell = (long long)b * MC + t;
-    const T *f = static_cast<const T *>(a.f);
+    const T *f = static_cast<const T *>(a.f) + (long long)b * BLK + t;
     C rho = 0, u = 0, v = 0, w = 0;
 #pragma unroll
     for (int p = 0; p < Q; p++) {
-        const C fp = ST<T>::dec(f[(long long)lat_pb(DIM, p) * a.nmc + cell]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        const C fp = ST<T>::dec(f[lat_pb(DIM, p) * MC]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
         rho += fp;
         u += C(lat_c(DIM, 0, p)) * fp;
         v += C(lat_c(DIM, 1, p)) * fp;
@@ -290,6 +285,7 @@ __global__ void k_refresh(const MacroArgs a)
     v /= rho;
     if (DIM == 3) w /= rho;
     C *m = static_cast<C *>(a.macro);
+    const long long cell = (long long)b * MC + t;
     m[cell] = rho;
     m[a.nmc + cell] = u;
     m[2 * a.nmc + cell] = v;
@@ -303,7 +299,6 @@ struct MassArgs {
     const int *ids;
     int n;
     const void *f;
-    long long nmc;
     const int *nbr_child, *cmask;
     double vol;
     double *partial;   // [gridDim.x][4]
@@ -312,8 +307,7 @@ struct MassArgs {
 template <int DIM, int Q, typename T>
 __global__ void __launch_bounds__(256) k_mass(const MassArgs a)
 {
-    using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
     __shared__ double s[4][256];
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long kap = gid / MC;
@@ -322,13 +316,11 @@ __global__ void __launch_bounds__(256) k_mass(const MassArgs a)
     if (kap < a.n) {
         const int b = a.ids[kap];
         if (b >= 0 && a.nbr_child[b] < 0) {
-            const long long cell = (long long)b * MC + t;
-            if (a.cmask[cell] != CELL_SOLID) {
-                const T *f = static_cast<const T *>(a.f);
+            if (a.cmask[(long long)b * MC + t] != CELL_SOLID) {
+                const T *f = static_cast<const T *>(a.f) + (long long)b * BLK + t;
 #pragma unroll
                 for (int p = 0; p < Q; p++) {
-                    const double fp = (double)ST<T>::dec(f[(long long)lat_pb(DIM, p) * a.nmc + cell]) +
-                                      (ST<T>::OFF ? lat_w(Q, p) : 0.0);
+                    const double fp = (double)ST<T>::dec(f[lat_pb(DIM, p) * MC]) + (ST<T>::OFF ? lat_w(Q, p) : 0.0);
                     m += fp;
                     mx += lat_c(DIM, 0, p) * fp;
                     my += lat_c(DIM, 1, p) * fp;
@@ -405,7 +397,6 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.n = n;
         a.fin = c->F[c->cur[L]];
         a.fout = c->F[1 - c->cur[L]];
-        a.nmc = c->nmc;
         a.nmb = c->nmb;
         a.nbr = c->cblock_ID_nbr;
         a.nbr_child = c->cblock_ID_nbr_child;
@@ -416,9 +407,11 @@ template <int DIM, int Q, typename T> struct RunStep {
         if (sizeof(typename ST<T>::C) == 4) a.omega = (double)((float)c->dxf[L] / (float)c->tau[L]);
         a.u_ref = c->P.u_ref;
         a.bc_preset = c->P.bc_preset;
-        a.has_solid = c->geometry_init;
         const unsigned grid = (unsigned)((n + BPC - 1) / BPC);
-        k_step<DIM, Q, T, BPC><<<grid, BPC * Geo<DIM>::MC, 0, c->stream>>>(a);
+        if (c->geometry_init)
+            k_step<DIM, Q, T, BPC, true><<<grid, BPC * Geo<DIM>::MC, 0, c->stream>>>(a);
+        else
+            k_step<DIM, Q, T, BPC, false><<<grid, BPC * Geo<DIM>::MC, 0, c->stream>>>(a);
         AGAL_CUDA(c, cudaGetLastError());
         c->cur[L] = 1 - c->cur[L];
         return AGAL_OK;
@@ -435,7 +428,6 @@ template <int DIM, int Q, typename T> struct RunIc {
         a.n = n;
         a.f0 = c->F[0];
         a.f1 = c->F[1];
-        a.nmc = c->nmc;
         a.nmb = c->nmb;
         a.cmask = c->cells_ID_mask;
         a.fX = c->cblock_f_X;
@@ -493,7 +485,6 @@ template <int DIM, int Q, typename T> struct RunMass {
             a.ids = c->id_set + (long long)L * c->nmb;
             a.n = c->n_ids[L];
             a.f = c->F[c->cur[L]];
-            a.nmc = c->nmc;
             a.nbr_child = c->cblock_ID_nbr_child;
             a.cmask = c->cells_ID_mask;
             a.vol = std::ldexp(1.0, -L * DIM);

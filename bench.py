@@ -57,6 +57,9 @@ WORKLOADS = {
     "ldc2d_256_fp16": dict(
         desc="D2Q9 BGK lid-driven cavity 256x256, one level, Re=100, lid 0.05, FP16 weight-offset populations",
         velocity_set=_lib.D2Q9, Nx=256, Re=100.0, storage=_lib.STORE_FP16, bc=_lib.BC_LDC2D),
+    "ldc2d_4096": dict(
+        desc="D2Q9 BGK lid-driven cavity 4096x4096, one level, Re=100, lid 0.05, FP32 populations",
+        velocity_set=_lib.D2Q9, Nx=4096, Re=100.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC2D),
     "ldc2d_8192": dict(
         desc="D2Q9 BGK lid-driven cavity 8192x8192, one level, Re=100, lid 0.05, FP32 populations",
         velocity_set=_lib.D2Q9, Nx=8192, Re=100.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC2D),
@@ -229,9 +232,20 @@ def main(argv=None) -> int:
     ap.add_argument("--roofline-workload", default="ldc2d_8192", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
+                    help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     w = WORKLOADS[a.workload]
+    if a.profile:
+        pw = WORKLOADS[a.profile]
+        with ag.Case(make_params(pw, device=0)) as pc:
+            pc.set_ic(0)
+            for _ in range(a.warmup + a.steps):
+                pc.advance()
+            pc.sync()
+        print(f"profile run done: {a.profile}, {a.warmup}+{a.steps} steps")
+        return 0
     ws, rank, local = dist_setup()
     threads = os.cpu_count() or 1
     base = {"metric": "MLUPS (lattice cell updates per second / 1e6), one coarse time step per step",

@@ -101,6 +101,35 @@ static std::vector<T> d2h(const T *d, size_t n)
     return h;
 }
 
+// Gather rows [r][blk*width .. +width) of an SoA array for the listed blocks:
+// out[(i*rows + r)*width + k] = in[r*stride + blk[i]*width + k].
+template <typename T>
+__global__ void k_gather(const T *in, long long stride, int rows, int width, const int *blk, int n, T *out)
+{
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)n * rows * width;
+    if (g >= tot) return;
+    int k = (int)(g % width);
+    long long t = g / width;
+    int r = (int)(t % rows);
+    int i = (int)(t / rows);
+    out[g] = in[(long long)r * stride + (long long)blk[i] * width + k];
+}
+
+template <typename T>
+static std::vector<T> gather(const T *d_in, long long stride, int rows, int width, const int *d_blk, int n)
+{
+    const size_t tot = (size_t)n * rows * width;
+    T *d_out = nullptr;
+    std::vector<T> h(tot);
+    if (!tot) return h;
+    cudaMalloc(&d_out, tot * sizeof(T));
+    k_gather<T><<<(unsigned)((tot + 255) / 256), 256>>>(d_in, stride, rows, width, d_blk, n, d_out);
+    cudaMemcpy(h.data(), d_out, tot * sizeof(T), cudaMemcpyDeviceToHost);
+    cudaFree(d_out);
+    return h;
+}
+
 int main(int argc, char **argv)
 {
     if (argc < 5) {
@@ -167,25 +196,30 @@ int main(int argc, char **argv)
         const int n_act = (int)blk.size();
         put(f, &n_act, 1);
         put(f, blk.data(), blk.size());
-        auto fX = d2h(mesh.c_cblock_f_X[0], (size_t)dim * nmb);
-        auto bm = d2h(mesh.c_cblock_ID_mask[0], (size_t)nmb);
-        auto nb = d2h(mesh.c_cblock_ID_nbr[0], (size_t)Qmax * nmb);
-        auto nc = d2h(mesh.c_cblock_ID_nbr_child[0], (size_t)Qmax * nmb);
-        auto onb = d2h(mesh.c_cblock_ID_onb[0], (size_t)nmb);
-        auto ref = d2h(mesh.c_cblock_ID_ref[0], (size_t)nmb);
-        auto lev = d2h(mesh.c_cblock_level[0], (size_t)nmb);
-        auto cm = d2h(mesh.c_cells_ID_mask[0], (size_t)nmc);
-        auto F = d2h(mesh.c_cells_f_F[0], (size_t)N_U * nmc);
-        for (int b : blk) {
-            for (int d = 0; d < dim; d++) put(f, &fX[b + (size_t)d * nmb], 1);
-            put(f, &bm[b], 1);
-            for (int q = 0; q < Qmax; q++) put(f, &nb[b + (size_t)q * nmb], 1);
-            for (int q = 0; q < Qmax; q++) put(f, &nc[b + (size_t)q * nmb], 1);
-            put(f, &onb[b], 1);
-            put(f, &ref[b], 1);
-            put(f, &lev[b], 1);
-            put(f, &cm[(size_t)b * MC], MC);
-            for (int u = 0; u < N_U; u++) put(f, &F[(size_t)u * nmc + (size_t)b * MC], MC);
+        // Only the active blocks travel to the host (the pool spans GBs).
+        int *d_blk = nullptr;
+        cudaMalloc(&d_blk, sizeof(int) * std::max(n_act, 1));
+        if (n_act) cudaMemcpy(d_blk, blk.data(), sizeof(int) * n_act, cudaMemcpyHostToDevice);
+        auto fX = gather(mesh.c_cblock_f_X[0], nmb, dim, 1, d_blk, n_act);
+        auto bm = gather(mesh.c_cblock_ID_mask[0], nmb, 1, 1, d_blk, n_act);
+        auto nb = gather(mesh.c_cblock_ID_nbr[0], nmb, Qmax, 1, d_blk, n_act);
+        auto nc = gather(mesh.c_cblock_ID_nbr_child[0], nmb, Qmax, 1, d_blk, n_act);
+        auto onb = gather(mesh.c_cblock_ID_onb[0], nmb, 1, 1, d_blk, n_act);
+        auto ref = gather(mesh.c_cblock_ID_ref[0], nmb, 1, 1, d_blk, n_act);
+        auto lev = gather(mesh.c_cblock_level[0], nmb, 1, 1, d_blk, n_act);
+        auto cm = gather(mesh.c_cells_ID_mask[0], nmc, 1, MC, d_blk, n_act);
+        auto F = gather(mesh.c_cells_f_F[0], nmc, N_U, MC, d_blk, n_act);
+        cudaFree(d_blk);
+        for (int i = 0; i < n_act; i++) {
+            put(f, &fX[(size_t)i * dim], dim);
+            put(f, &bm[i], 1);
+            put(f, &nb[(size_t)i * Qmax], Qmax);
+            put(f, &nc[(size_t)i * Qmax], Qmax);
+            put(f, &onb[i], 1);
+            put(f, &ref[i], 1);
+            put(f, &lev[i], 1);
+            put(f, &cm[(size_t)i * MC], MC);
+            put(f, &F[(size_t)i * N_U * MC], (size_t)N_U * MC);
         }
         fclose(f);
     }

@@ -36,19 +36,21 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 REF_BIN = ROOT / "oracle" / "_ref"
 
-# Golden cases: (binary, input.txt keys, steps, keep_mb)
+# Golden cases: (binary, input.txt keys, steps, keep_mb).  keep_mb is the free
+# device memory the reference sizes its block pool from; it must leave room
+# for the 2 MB granularity of its ~25 separate allocations.
 CASES = {
-    "d2q9_ldc64_re100": ("ref_d2q9_ldc", dict(Nx=64, v0=5e-4), 1000, 48),
-    "d2q9_ldc64_px": ("ref_d2q9_ldc", dict(Nx=64, v0=5e-4, PERIODIC_X=1), 300, 48),
-    "d2q9_ldc32x64": ("ref_d2q9_ldc", dict(Nx=32, L_fy=2.0, v0=5e-4), 300, 48),
-    "d3q19_ldc16_re400": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4), 200, 48),
-    "d3q27_ldc16_re200": ("ref_d3q27_ldc", dict(Nx=16, v0=2.5e-4), 200, 48),
-    "d3q19_ldc16_pxy": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4, PERIODIC_X=1, PERIODIC_Y=1), 100, 48),
+    "d2q9_ldc64_re100": ("ref_d2q9_ldc", dict(Nx=64, v0=5e-4), 1000, 4096),
+    "d2q9_ldc64_px": ("ref_d2q9_ldc", dict(Nx=64, v0=5e-4, PERIODIC_X=1), 300, 4096),
+    "d2q9_ldc32x64": ("ref_d2q9_ldc", dict(Nx=32, L_fy=2.0, v0=5e-4), 300, 4096),
+    "d3q19_ldc16_re400": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4), 200, 4096),
+    "d3q27_ldc16_re200": ("ref_d3q27_ldc", dict(Nx=16, v0=2.5e-4), 200, 4096),
+    "d3q19_ldc16_pxy": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4, PERIODIC_X=1, PERIODIC_Y=1), 100, 4096),
 }
 
 # Timing workloads of the reference build: (binary, keys, timed steps, keep_mb)
 TIMING = {
-    "ldc2d_256": ("ref_d2q9_ldc", dict(Nx=256, v0=5e-4), 2000, 512),
+    "ldc2d_256": ("ref_d2q9_ldc", dict(Nx=256, v0=5e-4), 2000, 4096),
     "ldc2d_8192": ("ref_d2q9_ldc", dict(Nx=8192, v0=5e-4), 20, 16384),
     "ldc3d19_384": ("ref_d3q19_ldc", dict(Nx=384, v0=1.25e-4), 10, 24576),
 }
@@ -157,7 +159,14 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
         (td / "out").mkdir()
         write_input(td, keys, td / "out")
         cmd = [str(exe), str(td) + "/", str(dump) if dump else "-", str(steps), str(keep_mb), str(n_timed)]
-        r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900)
+
+        def big_stack():
+            # M_Init builds the padded root grid as a stack VLA
+            # (mesh_init.cu:332): ~50 MB at 8192^2.
+            import resource
+            resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
+
+        r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack)
         if r.returncode != 0:
             raise RuntimeError(f"{binary} failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
         return r.stdout
@@ -203,9 +212,9 @@ def main(argv=None) -> int:
     if a.cmd == "tables":
         cmd_tables(Path(a.ref))
     elif a.cmd == "ref":
-        cmd_ref(Path(a.out), a.only)
+        cmd_ref(Path(a.out).resolve(), a.only)
     else:
-        cmd_time(Path(a.out))
+        cmd_time(Path(a.out).resolve())
     return 0
 
 

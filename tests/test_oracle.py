@@ -94,8 +94,13 @@ def params_for_golden(g):
     keys = json.loads(str(g["case_keys"]))
     vs = {9: _lib.D2Q9, 19: _lib.D3Q19, 27: _lib.D3Q27}[int(g["Q"])]
     bc = _lib.BC_LDC2D if int(g["dim"]) == 2 else _lib.BC_LDC3D
+    # Block IDs are taken from the low end of the gap stack (the stack holds
+    # n_maxcblocks-1 .. n_coarse, popped from the end), so they do not depend
+    # on the pool size: a pool just above the largest active ID reproduces the
+    # reference's IDs without its multi-GB allocation.
+    nmb = int(g["blocks"].max()) + 1 + 64
     kw = dict(velocity_set=vs, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, bc_preset=bc,
-              ic_preset=_lib.IC_REST, n_maxcblocks=int(g["n_maxcblocks"]))
+              ic_preset=_lib.IC_REST, n_maxcblocks=nmb)
     kw.update(keys)
     return ag.default_params(**kw), int(g["steps"])
 
@@ -104,7 +109,7 @@ def compare_to_golden(g, dumpf, tol_rel_l2):
     """Integer arrays bit-exact, rho/u within tol_rel_l2 (relative L2)."""
     blocks = g["blocks"].astype(np.int64)
     dim, Q, Qmax, MC = int(g["dim"]), int(g["Q"]), int(g["Qmax"]), int(g["MC"])
-    nmb = int(g["n_maxcblocks"])
+    nmb = len(dumpf(_lib.ARR_CBLOCK_ID_ONB))
     nbr = dumpf(_lib.ARR_CBLOCK_ID_NBR).reshape(Qmax, nmb)[:, blocks].T
     assert (nbr == g["nbr"]).all()
     ch = dumpf(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(Qmax, nmb)[:, blocks].T
@@ -135,7 +140,7 @@ def test_oracle_vs_reference_build(oracle_lib, name):
     from oracle.orc import OracleCase
     g = load_golden(name)
     p, steps = params_for_golden(g)
-    o = OracleCase(p, int(g["n_maxcblocks"]))
+    o = OracleCase(p, p.n_maxcblocks)
     o.set_ic(0)
     o.advance_n(steps)
     compare_to_golden(g, o.dump, 1e-5)

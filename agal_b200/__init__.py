@@ -133,6 +133,16 @@ class Case:
     def sync(self) -> None:
         self._c(self._lib.agal_sync(self._h))
 
+    def autotune(self, L: int = 0, reps: int = 5) -> dict:
+        """Pick the step kernel's thread mapping by timing each variant."""
+        ms = (C.c_float * 2)()
+        cpt = C.c_int()
+        self._c(self._lib.agal_autotune(self._h, L, reps, ms, C.byref(cpt)))
+        return {"cells_per_thread": cpt.value, "ms": [ms[0], ms[1]]}
+
+    def set_tuning(self, cells_per_thread: int) -> None:
+        self._c(self._lib.agal_set_tuning(self._h, cells_per_thread))
+
     def stream_ptr(self) -> int:
         """The library's cudaStream_t for this case, as an integer."""
         s = C.c_void_p()

@@ -81,6 +81,8 @@ PROTOS = [
     ("agal_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_sync", C.c_int, [C.c_void_p]),
     ("agal_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("agal_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    ("agal_set_tuning", C.c_int, [C.c_void_p, C.c_int]),
 ]
 
 _lib = None

@@ -312,6 +312,24 @@ extern "C" int agal_get_stream(const agal_ctx *c, void **stream)
     return AGAL_OK;
 }
 
+extern "C" int agal_autotune(agal_ctx *c, int L, int reps, float *ms, int *cells_per_thread)
+{
+    if (!c || L < 0 || L >= c->max_levels || reps <= 0) return AGAL_ERR_PARAM;
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }   // launch shape changes
+    int rc = agal_launch_tune(c, L, reps, ms);
+    if (rc) return rc;
+    if (cells_per_thread) *cells_per_thread = c->step_cpt;
+    return AGAL_OK;
+}
+
+extern "C" int agal_set_tuning(agal_ctx *c, int cells_per_thread)
+{
+    if (!c || (cells_per_thread != 1 && cells_per_thread != 2)) return AGAL_ERR_PARAM;
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    c->step_cpt = cells_per_thread;
+    return AGAL_OK;
+}
+
 extern "C" int agal_set_ic(agal_ctx *c, int L)
 {
     if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;

@@ -60,6 +60,7 @@ struct agal_ctx {
     int graph_steps = 0;
     std::vector<int> graph_cur_in;     // cur[] the graph was captured with
     int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
+    int step_cpt = 1;                  // cells per thread of the step kernel (autotuned)
     std::string err;
 };
 
@@ -75,5 +76,6 @@ int agal_cuda_check(agal_ctx *c, cudaError_t e, const char *what);
 // Kernel launchers (step_kernels.cu).
 int agal_launch_set_ic(agal_ctx *c, int L);
 int agal_launch_step(agal_ctx *c, int L);
+int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms);
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);

@@ -76,54 +76,20 @@ __device__ __forceinline__ C bc_hook(int preset, int nb, C f, C u, C v, C w, C w
 
 // Minimum resident 256-thread CTAs per SM requested from the register
 // allocator: as many as fit without spilling the Q populations held per thread.
-template <int DIM, int Q, typename T> struct StepOcc {
-    static constexpr bool D = sizeof(typename ST<T>::C) == 8;
-    static constexpr int value = (Q == 9) ? (D ? 3 : 6) : (Q == 19) ? (D ? 2 : 4) : (D ? 1 : 3);
+template <int DIM, int Q, typename T, int CPT> struct StepOcc {
+    static constexpr int words = CPT * Q * (sizeof(typename ST<T>::C) == 8 ? 2 : 1);   // registers for g[][]
+    static constexpr int value = words <= 9 ? 6 : words <= 19 ? 4 : words <= 27 ? 3 : words <= 38 ? 2 : 1;
 };
 
-template <int DIM, int Q, typename T, int BPC, bool SOLID>
-__global__ void __launch_bounds__(BPC *Geo<DIM>::MC, (StepOcc<DIM, Q, T>::value))
-k_step(const StepArgs a)
+// BGK collision of one cell in place on g[] (full populations, or weight
+// offsets g = f - w for the half-precision forms).  Opposite directions share
+// the even part of the equilibrium, feq_{p,pb} = w rho (1 + 4.5 cu^2 -
+// 1.5 u^2) +- 3 w rho cu, so each pair is evaluated once
+// (Cu_Collide, kernels.cu:249-286).  Returns the macros for the boundary hook.
+template <int DIM, int Q, typename C, bool OFF>
+__device__ __forceinline__ void bgk_collide(C (&g)[Q], C omeg, C &ux, C &uy, C &uz)
 {
-    using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
-    constexpr int CENTER = center_slot(DIM);
-    __shared__ int s_nbr[BPC][QMAX];
-    const int tid = threadIdx.x;
-    const int lb = tid / MC, t = tid % MC;
-    const int kap = blockIdx.x * BPC + lb;
-
-    // Dependency depth 2: the block ID, then (populations | neighbour row |
-    // block flags) all in flight together before the one barrier.
-    const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
-    if (t < QMAX) {
-        int v = b;   // the centre slot is the block itself
-        if (t != CENTER) {
-            const int m = __ldg((DIM == 2) ? &g_map2[t] : &g_map3[t]);
-            v = (b >= 0) ? __ldg(&a.nbr[b + (long long)m * a.nmb]) : N_SKIPID;
-        }
-        s_nbr[lb][t] = v;
-    }
-    int fl = 0;
-    if (b >= 0) {
-        if (__ldg(&a.nbr_child[b]) < 0 || __ldg(&a.bmask[b]) != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
-        if (__ldg(&a.onb[b]) == 1) fl |= 2;                                             // kernels.cu:736
-    }
-    const T *__restrict__ fin = static_cast<const T *>(a.fin) + (long long)(b >= 0 ? b : 0) * BLK + t;
-
-    // Load: slot pb(p) holds f_p (offset form g_p for half storage).
-    C g[Q];
-    if (b >= 0) {
-#pragma unroll
-        for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(__ldg(fin + lat_pb(DIM, p) * MC));
-    }
-    __syncthreads();
-
-    if (b < 0 || !(fl & 1)) return;
-    if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) return;   // solid cells keep their guard
-    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
-
-    C rho, drho = C(0), jx = C(0), jy = C(0), jz = C(0);
+    C drho = C(0), jx = C(0), jy = C(0), jz = C(0);
 #pragma unroll
     for (int p = 0; p < Q; p++) {
         drho += g[p];
@@ -132,48 +98,133 @@ k_step(const StepArgs a)
         if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
     }
     // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
-    rho = ST<T>::OFF ? C(1) + drho : drho;
-    const C ux = jx / rho, uy = jy / rho, uz = (DIM == 3) ? jz / rho : C(0);
-    const C udotu = ux * ux + uy * uy + uz * uz;
-    const C omeg = C(a.omega);
+    const C rho = OFF ? C(1) + drho : drho;
+    const C inv = C(1) / rho;
+    ux = jx * inv;
+    uy = jy * inv;
+    uz = (DIM == 3) ? jz * inv : C(0);
     const C omegp = C(1) - omeg;
-
+    const C h = C(1.5) * (ux * ux + uy * uy + uz * uz);   // 1.5 u^2
+    const C orho = omeg * rho;
+    // Rest population.  The offset form keeps omega (feq - w) as the small
+    // quantity w omega (drho + rho (...)) instead of a difference of O(w) terms.
+    {
+        const C w0 = C(lat_w(Q, 0));
+        g[0] = OFF ? g[0] * omegp + omeg * w0 * (drho - rho * h) : g[0] * omegp + w0 * orho * (C(1) - h);
+    }
 #pragma unroll
-    for (int p = 0; p < Q; p++) {
+    for (int p = 1; p < Q; p++) {
+        const int q = lat_pb(DIM, p);
+        if (q < p) continue;   // each pair once, from its lower index
         const C cu = C(lat_c(DIM, 0, p)) * ux + C(lat_c(DIM, 1, p)) * uy + C(lat_c(DIM, 2, p)) * uz;
         const C wp = C(lat_w(Q, p));
-        if (!ST<T>::OFF) {
-            // Operation order of Cu_Collide (kernels.cu:282).
-            g[p] = g[p] * omegp + (wp * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu)) * omeg;
-        } else {
-            // f' - w = g (1 - omega) + omega (feq - w),  feq - w = w (drho + rho X)
-            g[p] = g[p] * omegp + omeg * (wp * (drho + rho * (C(3) * cu + C(4.5) * cu * cu - C(1.5) * udotu)));
-        }
+        const C wo = wp * orho;
+        const C even = OFF ? wp * omeg * (drho + rho * (C(4.5) * cu * cu - h)) : wo * ((C(1) - h) + C(4.5) * cu * cu);
+        const C odd = C(3) * wo * cu;
+        g[p] = g[p] * omegp + (even + odd);
+        g[q] = g[q] * omegp + (even - odd);
     }
+}
 
-    // Push to destinations, bounce back on closed links.
-    T *__restrict__ fo = static_cast<T *>(a.fout);
-    T *__restrict__ own = fo + (long long)b * BLK + t;
-    const bool bnd = (fl & 2) && a.bc_preset != AGAL_BC_NONE;
+template <int DIM, int Q, typename T, int CPT, bool SOLID>
+__global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
+k_step(const StepArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
+    constexpr int TPB = MC / CPT;          // threads per cell-block
+    constexpr int BPC = 256 / TPB;         // cell-blocks per CTA
+    constexpr int CENTER = center_slot(DIM);
+    __shared__ int s_nbr[BPC][QMAX];
+    const int tid = threadIdx.x;
+    const int lb = tid / TPB, t0 = tid % TPB;
+    const int kap = blockIdx.x * BPC + lb;
+
+    // Dependency depth 2: the block ID, then (populations | neighbour row |
+    // block flags) all in flight together before the one barrier.
+    const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
+    for (int S = t0; S < QMAX; S += TPB) {
+        int v = b;   // the centre slot is the block itself
+        if (S != CENTER) {
+            const int m = __ldg((DIM == 2) ? &g_map2[S] : &g_map3[S]);
+            v = (b >= 0) ? __ldg(&a.nbr[b + (long long)m * a.nmb]) : N_SKIPID;
+        }
+        s_nbr[lb][S] = v;
+    }
+    int fl = 0;
+    if (b >= 0) {
+        if (__ldg(&a.nbr_child[b]) < 0 || __ldg(&a.bmask[b]) != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
+        if (__ldg(&a.onb[b]) == 1) fl |= 2;                                             // kernels.cu:736
+    }
+    const T *__restrict__ fin = static_cast<const T *>(a.fin) + (long long)(b >= 0 ? b : 0) * BLK + t0;
+
+    // Load: slot pb(p) holds f_p (offset form g_p for half storage).  Cell
+    // h of this thread is t0 + h * TPB.
+    C g[CPT][Q];
+    if (b >= 0) {
 #pragma unroll
-    for (int p = 0; p < Q; p++) {
-        const int cx = lat_c(DIM, 0, p), cy = lat_c(DIM, 1, p), cz = lat_c(DIM, 2, p);
-        const int Ip = I + cx, Jp = J + cy, Kp = K + cz;
-        const int S = ((Ip >> 2) + 1) + 3 * ((Jp >> 2) + 1) + (DIM == 3 ? 9 * ((Kp >> 2) + 1) : 0);
-        const int nc = (Ip & 3) | ((Jp & 3) << 2) | (DIM == 3 ? ((Kp & 3) << 4) : 0);
-        const int nb = s_nbr[lb][S];
-        bool open = nb >= 0;
-        if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
-        if (open) {
-            fo[(long long)nb * BLK + lat_pb(DIM, p) * MC + nc] = ST<T>::enc(g[p]);
-        } else {
-            C v = g[p];
-            if (bnd && nb != N_SKIPID) {
-                const C wp = C(lat_w(Q, p));
-                const C off = ST<T>::OFF ? wp : C(0);
-                v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx, cy, cz, C(a.u_ref)) - off;
+        for (int h = 0; h < CPT; h++)
+#pragma unroll
+            for (int p = 0; p < Q; p++) g[h][p] = ST<T>::dec(__ldg(fin + lat_pb(DIM, p) * MC + h * TPB));
+    }
+    __syncthreads();
+    if (b < 0 || !(fl & 1)) return;
+
+    T *__restrict__ fo = static_cast<T *>(a.fout);
+    const int *nrow = s_nbr[lb];
+    const bool hook = (fl & 2) && a.bc_preset != AGAL_BC_NONE;
+#pragma unroll
+    for (int h = 0; h < CPT; h++) {
+        const int t = t0 + h * TPB;
+        if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;   // solid cells keep their guard
+        const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+        C ux, uy, uz;
+        bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], C(a.omega), ux, uy, uz);
+
+        // Neighbour-slot and wrapped-cell components per axis offset -1, 0, +1
+        // (util_index.h:45-98): slot S = sx + sy + sz, cell = nx + ny + nz.
+        const int sx[3] = {I > 0 ? 1 : 0, 1, I < 3 ? 1 : 2};
+        const int nx[3] = {(I + 3) & 3, I, (I + 1) & 3};
+        const int sy[3] = {J > 0 ? 3 : 0, 3, J < 3 ? 3 : 6};
+        const int ny[3] = {4 * ((J + 3) & 3), 4 * J, 4 * ((J + 1) & 3)};
+        const int sz[3] = {DIM == 3 ? (K > 0 ? 9 : 0) : 0, DIM == 3 ? 9 : 0, DIM == 3 ? (K < 3 ? 9 : 18) : 0};
+        const int nz[3] = {16 * ((K + 3) & 3), 16 * K, 16 * ((K + 1) & 3)};
+        T *__restrict__ own = fo + (long long)b * BLK + t;
+
+        // Push to destinations, bounce back on closed links.
+        if (!hook) {
+            // No boundary hook on this block: closed links are plain bounce-back.
+#pragma unroll
+            for (int p = 0; p < Q; p++) {
+                const int cx = lat_c(DIM, 0, p) + 1, cy = lat_c(DIM, 1, p) + 1, cz = lat_c(DIM, 2, p) + 1;
+                const int nb = nrow[sx[cx] + sy[cy] + sz[cz]];
+                const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
+                bool open = nb >= 0;
+                if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
+                T *dst = open ? fo + ((long long)nb * BLK + lat_pb(DIM, p) * MC + nc) : own + p * MC;
+                *dst = ST<T>::enc(g[h][p]);
             }
-            own[p * MC] = ST<T>::enc(v);
+        } else {
+#pragma unroll
+            for (int p = 0; p < Q; p++) {
+                const int cx = lat_c(DIM, 0, p) + 1, cy = lat_c(DIM, 1, p) + 1, cz = lat_c(DIM, 2, p) + 1;
+                const int nb = nrow[sx[cx] + sy[cy] + sz[cz]];
+                const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
+                bool open = nb >= 0;
+                if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
+                if (open) {
+                    fo[(long long)nb * BLK + lat_pb(DIM, p) * MC + nc] = ST<T>::enc(g[h][p]);
+                } else {
+                    C v = g[h][p];
+                    if (nb != N_SKIPID) {   // domain boundary: Cu_ImposeBC hook (kernels.cu:791-792)
+                        const C wp = C(lat_w(Q, p));
+                        const C off = ST<T>::OFF ? wp : C(0);
+                        v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx - 1, cy - 1, cz - 1,
+                                       C(a.u_ref)) - off;
+                    }
+                    own[p * MC] = ST<T>::enc(v);
+                }
+            }
         }
     }
 }
@@ -386,10 +437,25 @@ int dispatch(agal_ctx *c, Args... args)
     return agal_set_err(c, AGAL_ERR_UNSUPPORTED, "velocity set / storage combination not built");
 }
 
+template <int DIM, int Q, typename T, int CPT>
+int launch_step(agal_ctx *c, const StepArgs &a, int n)
+{
+    constexpr int BPC = 256 / (Geo<DIM>::MC / CPT);
+    const unsigned grid = (unsigned)((n + BPC - 1) / BPC);
+    if (c->geometry_init)
+        k_step<DIM, Q, T, CPT, true><<<grid, 256, 0, c->stream>>>(a);
+    else
+        k_step<DIM, Q, T, CPT, false><<<grid, 256, 0, c->stream>>>(a);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
 template <int DIM, int Q, typename T> struct RunStep {
-    static int run(agal_ctx *c, int L)
+    // flip = false launches the kernel from the current buffer into the
+    // other one without making it current (used by the autotuner: the step is
+    // a pure function of the current buffer, so the state is unchanged).
+    static int run(agal_ctx *c, int L, int cpt = 0, bool flip = true)
     {
-        constexpr int BPC = (DIM == 2) ? 16 : 4;
         const int n = c->n_ids[L];
         if (n <= 0) return AGAL_OK;
         StepArgs a;
@@ -407,13 +473,42 @@ template <int DIM, int Q, typename T> struct RunStep {
         if (sizeof(typename ST<T>::C) == 4) a.omega = (double)((float)c->dxf[L] / (float)c->tau[L]);
         a.u_ref = c->P.u_ref;
         a.bc_preset = c->P.bc_preset;
-        const unsigned grid = (unsigned)((n + BPC - 1) / BPC);
-        if (c->geometry_init)
-            k_step<DIM, Q, T, BPC, true><<<grid, BPC * Geo<DIM>::MC, 0, c->stream>>>(a);
-        else
-            k_step<DIM, Q, T, BPC, false><<<grid, BPC * Geo<DIM>::MC, 0, c->stream>>>(a);
-        AGAL_CUDA(c, cudaGetLastError());
-        c->cur[L] = 1 - c->cur[L];
+        if (cpt <= 0) cpt = c->step_cpt;
+        const int rc = (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n) : launch_step<DIM, Q, T, 1>(c, a, n);
+        if (rc) return rc;
+        if (flip) c->cur[L] = 1 - c->cur[L];
+        return AGAL_OK;
+    }
+};
+
+// Autotuner of the step's thread mapping (cells per thread): times every
+// variant on level L's current state, writing only the scratch buffer.
+template <int DIM, int Q, typename T> struct RunTune {
+    static int run(agal_ctx *c, int L, int reps, float *ms_out)
+    {
+        if (c->n_ids[L] <= 0) return AGAL_OK;
+        cudaEvent_t e0, e1;
+        AGAL_CUDA(c, cudaEventCreate(&e0));
+        AGAL_CUDA(c, cudaEventCreate(&e1));
+        float best = 1e30f;
+        int best_cpt = 1;
+        for (int cpt = 1; cpt <= 2; cpt++) {
+            int rc = RunStep<DIM, Q, T>::run(c, L, cpt, false);   // warm-up
+            if (rc) return rc;
+            AGAL_CUDA(c, cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < reps; r++)
+                if ((rc = RunStep<DIM, Q, T>::run(c, L, cpt, false))) return rc;
+            AGAL_CUDA(c, cudaEventRecord(e1, c->stream));
+            AGAL_CUDA(c, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            AGAL_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+            ms /= (float)reps;
+            if (ms_out) ms_out[cpt - 1] = ms;
+            if (ms < best) { best = ms; best_cpt = cpt; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c->step_cpt = best_cpt;
         return AGAL_OK;
     }
 };
@@ -508,7 +603,8 @@ template <int DIM, int Q, typename T> struct RunMass {
 
 }  // namespace agal
 
-int agal_launch_step(agal_ctx *c, int L) { return agal::dispatch<agal::RunStep>(c, L); }
+int agal_launch_step(agal_ctx *c, int L) { return agal::dispatch<agal::RunStep>(c, L, 0, true); }
+int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms) { return agal::dispatch<agal::RunTune>(c, L, reps, ms); }
 int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }
 int agal_launch_refresh(agal_ctx *c, int L) { return agal::dispatch<agal::RunRefresh>(c, L); }
 int agal_launch_mass(agal_ctx *c, double *out) { return agal::dispatch<agal::RunMass>(c, out); }

@@ -234,6 +234,8 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
+    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2],
+                    help="with --profile: cells per thread of the step kernel")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     w = WORKLOADS[a.workload]
@@ -241,6 +243,7 @@ def main(argv=None) -> int:
         pw = WORKLOADS[a.profile]
         with ag.Case(make_params(pw, device=0)) as pc:
             pc.set_ic(0)
+            pc.set_tuning(a.cpt)
             for _ in range(a.warmup + a.steps):
                 pc.advance()
             pc.sync()
@@ -289,6 +292,7 @@ def main(argv=None) -> int:
     p = make_params(w, device=local)
     case = ag.Case(p)
     case.set_ic(0)
+    tune = case.autotune(0, reps=10)
     for _ in range(a.warmup):
         case.advance()
     case.sync()
@@ -306,6 +310,7 @@ def main(argv=None) -> int:
     p = make_params(w, device=local)
     case = ag.Case(p)
     case.set_ic(0)
+    case.set_tuning(tune["cells_per_thread"])
     f0 = case.dump(_lib.ARR_F)
     pinned = torch.from_numpy(f0).pin_memory()
     host_in = pinned.numpy()
@@ -333,6 +338,7 @@ def main(argv=None) -> int:
     rp = make_params(rw, device=local)
     rcase = ag.Case(rp)
     rcase.set_ic(0)
+    rtune = rcase.autotune(0, reps=5)
     for _ in range(3):
         rcase.advance()
     rcase.sync()
@@ -347,7 +353,7 @@ def main(argv=None) -> int:
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind, "kernel": "k_step (fused collide+BC+stream)",
                 "workload": a.roofline_workload, "algorithmic_bytes_per_launch": alg_bytes,
-                "avg_launch_ms": avg_ms}
+                "avg_launch_ms": avg_ms, "autotune": rtune}
 
     # --- CPU baseline (rank 0 only) -------------------------------------------
     cpu = None
@@ -360,7 +366,8 @@ def main(argv=None) -> int:
         line = dict(base, value=value, ms_per_step=t_ms / a.steps,
                     config={"workload": a.workload, "desc": w["desc"], "cells": cells_per_step(w),
                             "parallelism": f"replicas x{ws}",
-                            "l2": "flushed between timed steps" if flush else "inputs larger than L2"},
+                            "l2": "flushed between timed steps" if flush else "inputs larger than L2",
+                            "autotune": tune},
                     e2e=e2e, roofline=roofline, cpu_baseline=cpu, clocks=clk.summary(),
                     gpu_launches=a.steps)
         print(json.dumps(line), flush=True)

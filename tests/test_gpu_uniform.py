@@ -154,6 +154,28 @@ def test_graph_replay_bit_identical():
         assert np.array_equal(a.dump(_lib.ARR_F), b.dump(_lib.ARR_F))
 
 
+@pytest.mark.parametrize("Q,storage", [(9, _lib.STORE_FP32), (19, _lib.STORE_FP16), (27, _lib.STORE_FP32),
+                                       (9, _lib.STORE_FP64)])
+def test_thread_mappings_bit_identical_and_autotune_pure(Q, storage):
+    N = 32 if Q == 9 else 12
+    p = ldc_params(Q, N, storage=storage)
+    out = []
+    for cpt in (1, 2):
+        with ag.Case(p) as c:
+            c.set_ic(0)
+            c.set_tuning(cpt)
+            c.advance_n(17, use_graph=False)
+            out.append(c.dump(_lib.ARR_F))
+    assert np.array_equal(out[0], out[1])
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        c.advance_n(5, use_graph=False)
+        before = c.dump(_lib.ARR_F)
+        r = c.autotune(0, reps=3)
+        assert r["cells_per_thread"] in (1, 2) and min(r["ms"]) > 0
+        assert np.array_equal(c.dump(_lib.ARR_F), before)   # tuning does not advance the state
+
+
 def test_deterministic():
     p = ldc_params(19, 16)
     out = []

@@ -133,15 +133,17 @@ class Case:
     def sync(self) -> None:
         self._c(self._lib.agal_sync(self._h))
 
-    def autotune(self, L: int = 0, reps: int = 5) -> dict:
-        """Pick the step kernel's thread mapping by timing each variant."""
-        ms = (C.c_float * 2)()
-        cpt = C.c_int()
-        self._c(self._lib.agal_autotune(self._h, L, reps, ms, C.byref(cpt)))
-        return {"cells_per_thread": cpt.value, "ms": [ms[0], ms[1]]}
+    STEP_VARIANTS = {1: "1 cell/thread", 2: "2 cells/thread", 3: "TMA-staged persistent pipeline"}
 
-    def set_tuning(self, cells_per_thread: int) -> None:
-        self._c(self._lib.agal_set_tuning(self._h, cells_per_thread))
+    def autotune(self, L: int = 0, reps: int = 5) -> dict:
+        """Pick the step kernel variant by timing each one (state unchanged)."""
+        ms = (C.c_float * 3)()
+        v = C.c_int()
+        self._c(self._lib.agal_autotune(self._h, L, reps, ms, C.byref(v)))
+        return {"variant": v.value, "name": self.STEP_VARIANTS[v.value], "ms": [ms[0], ms[1], ms[2]]}
+
+    def set_tuning(self, variant: int) -> None:
+        self._c(self._lib.agal_set_tuning(self._h, variant))
 
     def stream_ptr(self) -> int:
         """The library's cudaStream_t for this case, as an integer."""

@@ -74,7 +74,7 @@ void release(agal_ctx *c)
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
-                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out};
+                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -201,7 +201,9 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->id_set, sizeof(int) * c->max_levels * nmb);
     ALLOC(c->gap_set, sizeof(int) * nmb);
     ALLOC(c->red_out, sizeof(double) * 4);
+    ALLOC(c->d_status, sizeof(int) * 4);
 #undef ALLOC
+    cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);
 
     // Reset values, mesh_init.cu:285-304.
     if ((rc = fill<int>(c, c->cells_ID_mask, nmc, CELL_INTERIOR)) ||
@@ -302,6 +304,13 @@ extern "C" int agal_sync(agal_ctx *c)
     if (!c) return AGAL_ERR_PARAM;
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
     AGAL_CUDA(c, cudaGetLastError());
+    // A bounded device wait that expired leaves its code in the status word.
+    int st = 0;
+    AGAL_CUDA(c, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0) {
+        cudaMemset(c->d_status, 0, sizeof(int));
+        return agal_set_err(c, st, "a device wait timed out (pipeline stalled)");
+    }
     return AGAL_OK;
 }
 
@@ -324,8 +333,10 @@ extern "C" int agal_autotune(agal_ctx *c, int L, int reps, float *ms, int *cells
 
 extern "C" int agal_set_tuning(agal_ctx *c, int cells_per_thread)
 {
-    if (!c || (cells_per_thread != 1 && cells_per_thread != 2)) return AGAL_ERR_PARAM;
+    if (!c || cells_per_thread < 1 || cells_per_thread > AGAL_STEP_VARIANTS) return AGAL_ERR_PARAM;
     if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    int rc = agal_prepare_step(c);
+    if (rc) return rc;
     c->step_cpt = cells_per_thread;
     return AGAL_OK;
 }

@@ -60,9 +60,14 @@ struct agal_ctx {
     int graph_steps = 0;
     std::vector<int> graph_cur_in;     // cur[] the graph was captured with
     int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
-    int step_cpt = 1;                  // cells per thread of the step kernel (autotuned)
+    int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
+    int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
     std::string err;
 };
+
+// Step kernel variants: 1 and 2 cells per thread (one-shot grid), 3 the
+// TMA-staged persistent pipeline.
+#define AGAL_STEP_VARIANTS 3
 
 // Error helpers shared by the translation units.
 int agal_set_err(agal_ctx *c, int code, const std::string &msg);
@@ -77,5 +82,6 @@ int agal_cuda_check(agal_ctx *c, cudaError_t e, const char *what);
 int agal_launch_set_ic(agal_ctx *c, int L);
 int agal_launch_step(agal_ctx *c, int L);
 int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms);
+int agal_prepare_step(agal_ctx *c);
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);

@@ -1,0 +1,165 @@
+// Shared pieces of the fused step kernels: kernel arguments, the neighbour
+// slot map, the boundary-condition hook presets and the BGK collision.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lattice.cuh"
+#include "storage.cuh"
+#include "../../include/agal_b200.h"
+
+namespace agal {
+
+// Neighbour-slot -> neighbour-array index (inc/util.h:100-101).  Read with a
+// different index by every thread, so it lives in global memory (L1-cached)
+// rather than in the constant bank, which serialises divergent reads.
+static __device__ const int g_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
+static __device__ const int g_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
+                                   1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
+
+struct StepArgs {
+    const int *ids;
+    int n;
+    const void *fin;
+    void *fout;
+    long long nmb;
+    const int *nbr, *nbr_child, *bmask, *onb, *cmask;
+    double omega;
+    double u_ref;
+    int bc_preset;
+};
+
+// Boundary hook presets (inc/custom.h:79-122); f is the full population.
+template <typename C>
+__device__ __forceinline__ C bc_hook(int preset, int nb, C f, C u, C v, C w, C wp, int cx, int cy, int cz, C U)
+{
+    bool inflow = false, outflow = false;
+    switch (preset) {
+    case AGAL_BC_LDC2D: inflow = (nb == -4); break;
+    case AGAL_BC_LDC3D: inflow = (nb == -6); break;
+    case AGAL_BC_FPSC2D: inflow = (nb == -1 || nb == -3 || nb == -4); outflow = (nb == -2); break;
+    case AGAL_BC_FPSC3D:
+        inflow = (nb == -1 || nb == -3 || nb == -4 || nb == -5 || nb == -6);
+        outflow = (nb == -2);
+        break;
+    default: break;
+    }
+    if (inflow) return f - C(2) * wp * (C(3) * (C(cx) * U));
+    if (outflow) {
+        C cu = C(cx) * u + C(cy) * v + C(cz) * w;
+        C e = C(1) + C(4.5) * cu * cu - C(1.5) * (u * u + v * v + w * w);
+        return -f + C(2) * wp * e;
+    }
+    return f;
+}
+
+// Minimum resident 256-thread CTAs per SM requested from the register
+// allocator: as many as fit without spilling the Q populations held per thread.
+template <int DIM, int Q, typename T, int CPT> struct StepOcc {
+    static constexpr int words = CPT * Q * (sizeof(typename ST<T>::C) == 8 ? 2 : 1);   // registers for g[][]
+    static constexpr int value = words <= 9 ? 6 : words <= 19 ? 4 : words <= 27 ? 3 : words <= 38 ? 2 : 1;
+};
+
+// BGK collision of one cell in place on g[] (full populations, or weight
+// offsets g = f - w for the half-precision forms).  Opposite directions share
+// the even part of the equilibrium, feq_{p,pb} = w rho (1 + 4.5 cu^2 -
+// 1.5 u^2) +- 3 w rho cu, so each pair is evaluated once
+// (Cu_Collide, kernels.cu:249-286).  Returns the macros for the boundary hook.
+template <int DIM, int Q, typename C, bool OFF>
+__device__ __forceinline__ void bgk_collide(C (&g)[Q], C omeg, C &ux, C &uy, C &uz)
+{
+    C drho = C(0), jx = C(0), jy = C(0), jz = C(0);
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        drho += g[p];
+        jx += C(lat_c(DIM, 0, p)) * g[p];
+        jy += C(lat_c(DIM, 1, p)) * g[p];
+        if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
+    }
+    // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
+    const C rho = OFF ? C(1) + drho : drho;
+    const C inv = C(1) / rho;
+    ux = jx * inv;
+    uy = jy * inv;
+    uz = (DIM == 3) ? jz * inv : C(0);
+    const C omegp = C(1) - omeg;
+    const C h = C(1.5) * (ux * ux + uy * uy + uz * uz);   // 1.5 u^2
+    const C orho = omeg * rho;
+    // Rest population.  The offset form keeps omega (feq - w) as the small
+    // quantity w omega (drho + rho (...)) instead of a difference of O(w) terms.
+    {
+        const C w0 = C(lat_w(Q, 0));
+        g[0] = OFF ? g[0] * omegp + omeg * w0 * (drho - rho * h) : g[0] * omegp + w0 * orho * (C(1) - h);
+    }
+#pragma unroll
+    for (int p = 1; p < Q; p++) {
+        const int q = lat_pb(DIM, p);
+        if (q < p) continue;   // each pair once, from its lower index
+        const C cu = C(lat_c(DIM, 0, p)) * ux + C(lat_c(DIM, 1, p)) * uy + C(lat_c(DIM, 2, p)) * uz;
+        const C wp = C(lat_w(Q, p));
+        const C wo = wp * orho;
+        const C even = OFF ? wp * omeg * (drho + rho * (C(4.5) * cu * cu - h)) : wo * ((C(1) - h) + C(4.5) * cu * cu);
+        const C odd = C(3) * wo * cu;
+        g[p] = g[p] * omegp + (even + odd);
+        g[q] = g[q] * omegp + (even - odd);
+    }
+}
+
+// Stream one collided cell (cell t of block b, populations g) into the
+// output buffer: push along open links, bounce back along closed ones with
+// the boundary hook on domain boundaries (kernels.cu:534-633, 693-887).
+// nrow[S] = neighbour block in lexicographic neighbour slot S (centre = b).
+template <int DIM, int Q, typename T, bool SOLID>
+__device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typename ST<T>::C ux,
+                                          typename ST<T>::C uy, typename ST<T>::C uz, int b, int t,
+                                          const int *nrow, bool hook, T *__restrict__ fo, const StepArgs &a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    // Neighbour-slot and wrapped-cell components per axis offset -1, 0, +1
+    // (util_index.h:45-98): slot S = sx + sy + sz, cell = nx + ny + nz.
+    const int sx[3] = {I > 0 ? 1 : 0, 1, I < 3 ? 1 : 2};
+    const int nx[3] = {(I + 3) & 3, I, (I + 1) & 3};
+    const int sy[3] = {J > 0 ? 3 : 0, 3, J < 3 ? 3 : 6};
+    const int ny[3] = {4 * ((J + 3) & 3), 4 * J, 4 * ((J + 1) & 3)};
+    const int sz[3] = {DIM == 3 ? (K > 0 ? 9 : 0) : 0, DIM == 3 ? 9 : 0, DIM == 3 ? (K < 3 ? 9 : 18) : 0};
+    const int nz[3] = {16 * ((K + 3) & 3), 16 * K, 16 * ((K + 1) & 3)};
+    T *__restrict__ own = fo + (long long)b * BLK + t;
+    if (!hook) {
+        // No boundary hook on this block: closed links are plain bounce-back.
+#pragma unroll
+        for (int p = 0; p < Q; p++) {
+            const int cx = lat_c(DIM, 0, p) + 1, cy = lat_c(DIM, 1, p) + 1, cz = lat_c(DIM, 2, p) + 1;
+            const int nb = nrow[sx[cx] + sy[cy] + sz[cz]];
+            const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
+            bool open = nb >= 0;
+            if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
+            T *dst = open ? fo + ((long long)nb * BLK + lat_pb(DIM, p) * MC + nc) : own + p * MC;
+            *dst = ST<T>::enc(g[p]);
+        }
+    } else {
+#pragma unroll
+        for (int p = 0; p < Q; p++) {
+            const int cx = lat_c(DIM, 0, p) + 1, cy = lat_c(DIM, 1, p) + 1, cz = lat_c(DIM, 2, p) + 1;
+            const int nb = nrow[sx[cx] + sy[cy] + sz[cz]];
+            const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
+            bool open = nb >= 0;
+            if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
+            if (open) {
+                fo[(long long)nb * BLK + lat_pb(DIM, p) * MC + nc] = ST<T>::enc(g[p]);
+            } else {
+                C v = g[p];
+                if (nb != N_SKIPID) {   // domain boundary: Cu_ImposeBC hook (kernels.cu:791-792)
+                    const C wp = C(lat_w(Q, p));
+                    const C off = ST<T>::OFF ? wp : C(0);
+                    v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx - 1, cy - 1, cz - 1, C(a.u_ref)) -
+                        off;
+                }
+                own[p * MC] = ST<T>::enc(v);
+            }
+        }
+    }
+}
+
+}  // namespace agal

@@ -28,103 +28,9 @@
 #include "ctx.h"
 #include "lattice.cuh"
 #include "storage.cuh"
+#include "step_common.cuh"
 
 namespace agal {
-
-// Neighbour-slot -> neighbour-array index (inc/util.h:100-101).  Read with a
-// different index by every thread, so it lives in global memory (L1-cached)
-// rather than in the constant bank, which serialises divergent reads.
-__device__ const int g_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
-__device__ const int g_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
-                                   1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
-
-struct StepArgs {
-    const int *ids;
-    int n;
-    const void *fin;
-    void *fout;
-    long long nmb;
-    const int *nbr, *nbr_child, *bmask, *onb, *cmask;
-    double omega;
-    double u_ref;
-    int bc_preset;
-};
-
-// Boundary hook presets (inc/custom.h:79-122); f is the full population.
-template <typename C>
-__device__ __forceinline__ C bc_hook(int preset, int nb, C f, C u, C v, C w, C wp, int cx, int cy, int cz, C U)
-{
-    bool inflow = false, outflow = false;
-    switch (preset) {
-    case AGAL_BC_LDC2D: inflow = (nb == -4); break;
-    case AGAL_BC_LDC3D: inflow = (nb == -6); break;
-    case AGAL_BC_FPSC2D: inflow = (nb == -1 || nb == -3 || nb == -4); outflow = (nb == -2); break;
-    case AGAL_BC_FPSC3D:
-        inflow = (nb == -1 || nb == -3 || nb == -4 || nb == -5 || nb == -6);
-        outflow = (nb == -2);
-        break;
-    default: break;
-    }
-    if (inflow) return f - C(2) * wp * (C(3) * (C(cx) * U));
-    if (outflow) {
-        C cu = C(cx) * u + C(cy) * v + C(cz) * w;
-        C e = C(1) + C(4.5) * cu * cu - C(1.5) * (u * u + v * v + w * w);
-        return -f + C(2) * wp * e;
-    }
-    return f;
-}
-
-// Minimum resident 256-thread CTAs per SM requested from the register
-// allocator: as many as fit without spilling the Q populations held per thread.
-template <int DIM, int Q, typename T, int CPT> struct StepOcc {
-    static constexpr int words = CPT * Q * (sizeof(typename ST<T>::C) == 8 ? 2 : 1);   // registers for g[][]
-    static constexpr int value = words <= 9 ? 6 : words <= 19 ? 4 : words <= 27 ? 3 : words <= 38 ? 2 : 1;
-};
-
-// BGK collision of one cell in place on g[] (full populations, or weight
-// offsets g = f - w for the half-precision forms).  Opposite directions share
-// the even part of the equilibrium, feq_{p,pb} = w rho (1 + 4.5 cu^2 -
-// 1.5 u^2) +- 3 w rho cu, so each pair is evaluated once
-// (Cu_Collide, kernels.cu:249-286).  Returns the macros for the boundary hook.
-template <int DIM, int Q, typename C, bool OFF>
-__device__ __forceinline__ void bgk_collide(C (&g)[Q], C omeg, C &ux, C &uy, C &uz)
-{
-    C drho = C(0), jx = C(0), jy = C(0), jz = C(0);
-#pragma unroll
-    for (int p = 0; p < Q; p++) {
-        drho += g[p];
-        jx += C(lat_c(DIM, 0, p)) * g[p];
-        jy += C(lat_c(DIM, 1, p)) * g[p];
-        if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
-    }
-    // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
-    const C rho = OFF ? C(1) + drho : drho;
-    const C inv = C(1) / rho;
-    ux = jx * inv;
-    uy = jy * inv;
-    uz = (DIM == 3) ? jz * inv : C(0);
-    const C omegp = C(1) - omeg;
-    const C h = C(1.5) * (ux * ux + uy * uy + uz * uz);   // 1.5 u^2
-    const C orho = omeg * rho;
-    // Rest population.  The offset form keeps omega (feq - w) as the small
-    // quantity w omega (drho + rho (...)) instead of a difference of O(w) terms.
-    {
-        const C w0 = C(lat_w(Q, 0));
-        g[0] = OFF ? g[0] * omegp + omeg * w0 * (drho - rho * h) : g[0] * omegp + w0 * orho * (C(1) - h);
-    }
-#pragma unroll
-    for (int p = 1; p < Q; p++) {
-        const int q = lat_pb(DIM, p);
-        if (q < p) continue;   // each pair once, from its lower index
-        const C cu = C(lat_c(DIM, 0, p)) * ux + C(lat_c(DIM, 1, p)) * uy + C(lat_c(DIM, 2, p)) * uz;
-        const C wp = C(lat_w(Q, p));
-        const C wo = wp * orho;
-        const C even = OFF ? wp * omeg * (drho + rho * (C(4.5) * cu * cu - h)) : wo * ((C(1) - h) + C(4.5) * cu * cu);
-        const C odd = C(3) * wo * cu;
-        g[p] = g[p] * omegp + (even + odd);
-        g[q] = g[q] * omegp + (even - odd);
-    }
-}
 
 template <int DIM, int Q, typename T, int CPT, bool SOLID>
 __global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
@@ -177,55 +83,9 @@ k_step(const StepArgs a)
     for (int h = 0; h < CPT; h++) {
         const int t = t0 + h * TPB;
         if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;   // solid cells keep their guard
-        const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
         C ux, uy, uz;
         bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], C(a.omega), ux, uy, uz);
-
-        // Neighbour-slot and wrapped-cell components per axis offset -1, 0, +1
-        // (util_index.h:45-98): slot S = sx + sy + sz, cell = nx + ny + nz.
-        const int sx[3] = {I > 0 ? 1 : 0, 1, I < 3 ? 1 : 2};
-        const int nx[3] = {(I + 3) & 3, I, (I + 1) & 3};
-        const int sy[3] = {J > 0 ? 3 : 0, 3, J < 3 ? 3 : 6};
-        const int ny[3] = {4 * ((J + 3) & 3), 4 * J, 4 * ((J + 1) & 3)};
-        const int sz[3] = {DIM == 3 ? (K > 0 ? 9 : 0) : 0, DIM == 3 ? 9 : 0, DIM == 3 ? (K < 3 ? 9 : 18) : 0};
-        const int nz[3] = {16 * ((K + 3) & 3), 16 * K, 16 * ((K + 1) & 3)};
-        T *__restrict__ own = fo + (long long)b * BLK + t;
-
-        // Push to destinations, bounce back on closed links.
-        if (!hook) {
-            // No boundary hook on this block: closed links are plain bounce-back.
-#pragma unroll
-            for (int p = 0; p < Q; p++) {
-                const int cx = lat_c(DIM, 0, p) + 1, cy = lat_c(DIM, 1, p) + 1, cz = lat_c(DIM, 2, p) + 1;
-                const int nb = nrow[sx[cx] + sy[cy] + sz[cz]];
-                const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
-                bool open = nb >= 0;
-                if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
-                T *dst = open ? fo + ((long long)nb * BLK + lat_pb(DIM, p) * MC + nc) : own + p * MC;
-                *dst = ST<T>::enc(g[h][p]);
-            }
-        } else {
-#pragma unroll
-            for (int p = 0; p < Q; p++) {
-                const int cx = lat_c(DIM, 0, p) + 1, cy = lat_c(DIM, 1, p) + 1, cz = lat_c(DIM, 2, p) + 1;
-                const int nb = nrow[sx[cx] + sy[cy] + sz[cz]];
-                const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
-                bool open = nb >= 0;
-                if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
-                if (open) {
-                    fo[(long long)nb * BLK + lat_pb(DIM, p) * MC + nc] = ST<T>::enc(g[h][p]);
-                } else {
-                    C v = g[h][p];
-                    if (nb != N_SKIPID) {   // domain boundary: Cu_ImposeBC hook (kernels.cu:791-792)
-                        const C wp = C(lat_w(Q, p));
-                        const C off = ST<T>::OFF ? wp : C(0);
-                        v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx - 1, cy - 1, cz - 1,
-                                       C(a.u_ref)) - off;
-                    }
-                    own[p * MC] = ST<T>::enc(v);
-                }
-            }
-        }
+        push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
     }
 }
 
@@ -437,6 +297,16 @@ int dispatch(agal_ctx *c, Args... args)
     return agal_set_err(c, AGAL_ERR_UNSUPPORTED, "velocity set / storage combination not built");
 }
 
+// TMA-staged persistent variant (step_tma.cu).
+template <int DIM, int Q, typename T>
+int launch_step_tma(agal_ctx *c, const StepArgs &a);
+template <int DIM, int Q, typename T>
+int prepare_step_tma(agal_ctx *c);
+
+template <int DIM, int Q, typename T> struct RunPrepare {
+    static int run(agal_ctx *c) { return prepare_step_tma<DIM, Q, T>(c); }
+};
+
 template <int DIM, int Q, typename T, int CPT>
 int launch_step(agal_ctx *c, const StepArgs &a, int n)
 {
@@ -474,15 +344,18 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.u_ref = c->P.u_ref;
         a.bc_preset = c->P.bc_preset;
         if (cpt <= 0) cpt = c->step_cpt;
-        const int rc = (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n) : launch_step<DIM, Q, T, 1>(c, a, n);
+        const int rc = (cpt == 3)   ? launch_step_tma<DIM, Q, T>(c, a)
+                       : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
+                                    : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
         if (flip) c->cur[L] = 1 - c->cur[L];
         return AGAL_OK;
     }
 };
 
-// Autotuner of the step's thread mapping (cells per thread): times every
-// variant on level L's current state, writing only the scratch buffer.
+// Autotuner of the step kernel: times every variant (1: one cell per thread,
+// 2: two cells per thread, 3: TMA-staged persistent pipeline) on level L's
+// current state, writing only the scratch buffer.
 template <int DIM, int Q, typename T> struct RunTune {
     static int run(agal_ctx *c, int L, int reps, float *ms_out)
     {
@@ -492,7 +365,7 @@ template <int DIM, int Q, typename T> struct RunTune {
         AGAL_CUDA(c, cudaEventCreate(&e1));
         float best = 1e30f;
         int best_cpt = 1;
-        for (int cpt = 1; cpt <= 2; cpt++) {
+        for (int cpt = 1; cpt <= AGAL_STEP_VARIANTS; cpt++) {
             int rc = RunStep<DIM, Q, T>::run(c, L, cpt, false);   // warm-up
             if (rc) return rc;
             AGAL_CUDA(c, cudaEventRecord(e0, c->stream));
@@ -604,7 +477,12 @@ template <int DIM, int Q, typename T> struct RunMass {
 }  // namespace agal
 
 int agal_launch_step(agal_ctx *c, int L) { return agal::dispatch<agal::RunStep>(c, L, 0, true); }
-int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms) { return agal::dispatch<agal::RunTune>(c, L, reps, ms); }
+int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms)
+{
+    int rc = agal::dispatch<agal::RunPrepare>(c);
+    return rc ? rc : agal::dispatch<agal::RunTune>(c, L, reps, ms);
+}
+int agal_prepare_step(agal_ctx *c) { return agal::dispatch<agal::RunPrepare>(c); }
 int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }
 int agal_launch_refresh(agal_ctx *c, int L) { return agal::dispatch<agal::RunRefresh>(c, L); }
 int agal_launch_mass(agal_ctx *c, double *out) { return agal::dispatch<agal::RunMass>(c, out); }

@@ -234,8 +234,8 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
-    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2],
-                    help="with --profile: cells per thread of the step kernel")
+    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3],
+                    help="with --profile: step kernel variant (1, 2 cells per thread; 3 TMA pipeline)")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     w = WORKLOADS[a.workload]
@@ -310,7 +310,7 @@ def main(argv=None) -> int:
     p = make_params(w, device=local)
     case = ag.Case(p)
     case.set_ic(0)
-    case.set_tuning(tune["cells_per_thread"])
+    case.set_tuning(tune["variant"])
     f0 = case.dump(_lib.ARR_F)
     pinned = torch.from_numpy(f0).pin_memory()
     host_in = pinned.numpy()

@@ -172,17 +172,20 @@ int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
    Reads the macros of agal_refresh-free state (computes them itself). */
 int agal_mass_momentum(agal_ctx *ctx, double *out);
 
-/* Autotuner of the fused step's thread mapping (1 or 2 cells per thread):
-   times each variant reps times on level L's current state without advancing
-   it (the step writes only the scratch population buffer), keeps the fastest
-   for the context.  ms[2] (may be NULL) receives the per-launch times,
-   *cells_per_thread (may be NULL) the choice.  No reference counterpart: the
-   reference launches one fixed 16/64-thread shape (cppspec.h:96). */
-int agal_autotune(agal_ctx *ctx, int L, int reps, float *ms, int *cells_per_thread);
-/* Set the step kernel's thread mapping explicitly (1 or 2 cells per thread). */
-int agal_set_tuning(agal_ctx *ctx, int cells_per_thread);
+/* Autotuner of the fused step kernel.  Variants: 1 = one cell per thread,
+   2 = two cells per thread (one-shot grids), 3 = persistent pipeline with the
+   cell-blocks staged in shared memory by TMA bulk copies.  Times each variant
+   reps times on level L's current state without advancing it (the step
+   writes only the scratch population buffer) and keeps the fastest for the
+   context.  ms[3] (may be NULL) receives the per-launch times, *variant (may
+   be NULL) the choice.  No reference counterpart: the reference launches one
+   fixed 16/64-thread shape (cppspec.h:96). */
+int agal_autotune(agal_ctx *ctx, int L, int reps, float *ms, int *variant);
+/* Set the step kernel variant explicitly (1..3, as for agal_autotune). */
+int agal_set_tuning(agal_ctx *ctx, int variant);
 
-/* Synchronise the context's stream; returns the first pending CUDA error. */
+/* Synchronise the context's stream; returns the first pending CUDA error, or
+   AGAL_ERR_TIMEOUT if a bounded wait inside a kernel expired. */
 int agal_sync(agal_ctx *ctx);
 /* The context's cudaStream_t (as void*), so that callers can order their own
    work and CUDA events with the library's kernels. */

@@ -60,6 +60,44 @@ template <int DIM, int Q, typename T, int CPT> struct StepOcc {
     static constexpr int value = words <= 9 ? 6 : words <= 19 ? 4 : words <= 27 ? 3 : words <= 38 ? 2 : 1;
 };
 
+// Explicitly rounded arithmetic (never contracted or reordered by the
+// compiler), so that every kernel variant that inlines the collision performs
+// the same operation sequence and produces bit-identical populations.
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float r_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float r_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double r_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double r_div(double a, double b) { return __ddiv_rn(a, b); }
+
+// sum_p c_p g_p along one axis for lattice directions with c in {-1, 0, 1}.
+template <int DIM, int Q, int AXIS, typename C>
+__device__ __forceinline__ C moment1(const C (&g)[Q])
+{
+    C s = C(0);
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const int c = lat_c(DIM, AXIS, p);
+        if (c > 0) s = r_add(s, g[p]);
+        if (c < 0) s = r_add(s, -g[p]);
+    }
+    return s;
+}
+
+// c_p . u for c in {-1, 0, 1}^3.
+template <int DIM, typename C>
+__device__ __forceinline__ C cdot(int p, C ux, C uy, C uz)
+{
+    C s = C(0);
+    const int cx = lat_c(DIM, 0, p), cy = lat_c(DIM, 1, p), cz = lat_c(DIM, 2, p);
+    s = cx > 0 ? ux : (cx < 0 ? -ux : s);
+    if (cy != 0) s = r_add(s, cy > 0 ? uy : -uy);
+    if (cz != 0) s = r_add(s, cz > 0 ? uz : -uz);
+    return s;
+}
+
 // BGK collision of one cell in place on g[] (full populations, or weight
 // offsets g = f - w for the half-precision forms).  Opposite directions share
 // the even part of the equilibrium, feq_{p,pb} = w rho (1 + 4.5 cu^2 -
@@ -68,40 +106,42 @@ template <int DIM, int Q, typename T, int CPT> struct StepOcc {
 template <int DIM, int Q, typename C, bool OFF>
 __device__ __forceinline__ void bgk_collide(C (&g)[Q], C omeg, C &ux, C &uy, C &uz)
 {
-    C drho = C(0), jx = C(0), jy = C(0), jz = C(0);
+    C drho = C(0);
 #pragma unroll
-    for (int p = 0; p < Q; p++) {
-        drho += g[p];
-        jx += C(lat_c(DIM, 0, p)) * g[p];
-        jy += C(lat_c(DIM, 1, p)) * g[p];
-        if (DIM == 3) jz += C(lat_c(DIM, 2, p)) * g[p];
-    }
+    for (int p = 0; p < Q; p++) drho = r_add(drho, g[p]);
+    const C jx = moment1<DIM, Q, 0>(g), jy = moment1<DIM, Q, 1>(g);
+    const C jz = (DIM == 3) ? moment1<DIM, Q, 2>(g) : C(0);
     // Offset form: sum_p w_p = 1 and sum_p w_p c_p = 0.
-    const C rho = OFF ? C(1) + drho : drho;
-    const C inv = C(1) / rho;
-    ux = jx * inv;
-    uy = jy * inv;
-    uz = (DIM == 3) ? jz * inv : C(0);
-    const C omegp = C(1) - omeg;
-    const C h = C(1.5) * (ux * ux + uy * uy + uz * uz);   // 1.5 u^2
-    const C orho = omeg * rho;
+    const C rho = OFF ? r_add(C(1), drho) : drho;
+    const C inv = r_div(C(1), rho);
+    ux = r_mul(jx, inv);
+    uy = r_mul(jy, inv);
+    uz = (DIM == 3) ? r_mul(jz, inv) : C(0);
+    const C omegp = r_add(C(1), -omeg);
+    const C usq = r_fma(uz, uz, r_fma(uy, uy, r_mul(ux, ux)));
+    const C h = r_mul(C(1.5), usq);   // 1.5 u^2
+    const C one_h = r_add(C(1), -h);
+    const C orho = r_mul(omeg, rho);
     // Rest population.  The offset form keeps omega (feq - w) as the small
     // quantity w omega (drho + rho (...)) instead of a difference of O(w) terms.
     {
         const C w0 = C(lat_w(Q, 0));
-        g[0] = OFF ? g[0] * omegp + omeg * w0 * (drho - rho * h) : g[0] * omegp + w0 * orho * (C(1) - h);
+        const C e0 = OFF ? r_mul(r_mul(omeg, w0), r_fma(-rho, h, drho)) : r_mul(r_mul(w0, orho), one_h);
+        g[0] = r_fma(g[0], omegp, e0);
     }
 #pragma unroll
     for (int p = 1; p < Q; p++) {
         const int q = lat_pb(DIM, p);
         if (q < p) continue;   // each pair once, from its lower index
-        const C cu = C(lat_c(DIM, 0, p)) * ux + C(lat_c(DIM, 1, p)) * uy + C(lat_c(DIM, 2, p)) * uz;
+        const C cu = cdot<DIM>(p, ux, uy, uz);
         const C wp = C(lat_w(Q, p));
-        const C wo = wp * orho;
-        const C even = OFF ? wp * omeg * (drho + rho * (C(4.5) * cu * cu - h)) : wo * ((C(1) - h) + C(4.5) * cu * cu);
-        const C odd = C(3) * wo * cu;
-        g[p] = g[p] * omegp + (even + odd);
-        g[q] = g[q] * omegp + (even - odd);
+        const C wo = r_mul(wp, orho);
+        const C cu2 = r_mul(cu, cu);
+        const C even = OFF ? r_mul(r_mul(wp, omeg), r_fma(rho, r_fma(C(4.5), cu2, -h), drho))
+                           : r_mul(wo, r_fma(C(4.5), cu2, one_h));
+        const C odd = r_mul(r_mul(C(3), wo), cu);
+        g[p] = r_fma(g[p], omegp, r_add(even, odd));
+        g[q] = r_fma(g[q], omegp, r_add(even, -odd));
     }
 }
 

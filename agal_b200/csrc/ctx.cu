@@ -74,7 +74,7 @@ void release(agal_ctx *c)
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
-                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status};
+                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -202,6 +202,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->gap_set, sizeof(int) * nmb);
     ALLOC(c->red_out, sizeof(double) * 4);
     ALLOC(c->d_status, sizeof(int) * 4);
+    ALLOC(c->meta, sizeof(int) * (size_t)(c->dim == 2 ? 12 : 28) * nmb);
 #undef ALLOC
     cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);
 
@@ -272,6 +273,12 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     c->id_max[0] = c->id_max[c->max_levels] = (int)n_coarse;
     c->n_gaps = (int)(nmb - n_coarse);
     c->cur.assign(c->max_levels, 0);
+    if ((rc = agal_build_meta(c))) {
+        std::string m = c->err;
+        release(c);
+        delete c;
+        return agal_set_err(nullptr, rc, m);
+    }
     *out = c;
     return AGAL_OK;
 }
@@ -561,6 +568,7 @@ extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t by
     }
     if (which == AGAL_ARR_MACROS) return agal_set_err(c, AGAL_ERR_PARAM, "macros are derived, not loaded");
     AGAL_CUDA(c, cudaMemcpy(int_array(c, which), host_buf, need, cudaMemcpyHostToDevice));
+    if ((rc = agal_build_meta(c))) return rc;
     if (which == AGAL_ARR_CELLS_ID_MASK) {
         // Geometry present when any cell is solid.
         std::vector<int> cm(c->nmc);

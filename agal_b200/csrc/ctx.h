@@ -62,6 +62,7 @@ struct agal_ctx {
     int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
+    int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
     std::string err;
 };
 
@@ -83,5 +84,6 @@ int agal_launch_set_ic(agal_ctx *c, int L);
 int agal_launch_step(agal_ctx *c, int L);
 int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms);
 int agal_prepare_step(agal_ctx *c);
+int agal_build_meta(agal_ctx *c);   // after any change of the block arrays
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);

@@ -17,13 +17,26 @@ static __device__ const int g_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
 static __device__ const int g_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
                                    1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
 
+// Per-block step metadata row, rebuilt whenever the mesh changes
+// (agal_build_meta): the neighbour block in each lexicographic neighbour slot
+// S (the centre slot holds the block itself) and the step flags.  One
+// contiguous 16-byte-multiple row per block, so the step kernels fetch it
+// with one coalesced load or one bulk copy instead of Q_max strided loads
+// from the structure-of-arrays neighbour table.
+template <int DIM> struct Meta {
+    static constexpr int W = (DIM == 2) ? 12 : 28;        // ints per row (48 / 112 bytes)
+    static constexpr int FLAGS = (DIM == 2) ? 9 : 27;     // index of the flag word
+};
+constexpr int META_ACTIVE = 1;   // collide/stream this block (kernels.cu:236)
+constexpr int META_ONB = 2;      // block touches a domain boundary (kernels.cu:736)
+
 struct StepArgs {
     const int *ids;
     int n;
     const void *fin;
     void *fout;
-    long long nmb;
-    const int *nbr, *nbr_child, *bmask, *onb, *cmask;
+    const int *meta;
+    const int *cmask;
     double omega;
     double u_ref;
     int bc_preset;

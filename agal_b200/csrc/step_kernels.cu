@@ -40,28 +40,16 @@ k_step(const StepArgs a)
     constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
     constexpr int TPB = MC / CPT;          // threads per cell-block
     constexpr int BPC = 256 / TPB;         // cell-blocks per CTA
-    constexpr int CENTER = center_slot(DIM);
-    __shared__ int s_nbr[BPC][QMAX];
+    constexpr int W = Meta<DIM>::W;
+    __shared__ int s_meta[BPC][W];
     const int tid = threadIdx.x;
     const int lb = tid / TPB, t0 = tid % TPB;
     const int kap = blockIdx.x * BPC + lb;
 
-    // Dependency depth 2: the block ID, then (populations | neighbour row |
-    // block flags) all in flight together before the one barrier.
+    // Dependency depth 2: the block ID, then (populations | metadata row) in
+    // flight together before the one barrier.
     const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
-    for (int S = t0; S < QMAX; S += TPB) {
-        int v = b;   // the centre slot is the block itself
-        if (S != CENTER) {
-            const int m = __ldg((DIM == 2) ? &g_map2[S] : &g_map3[S]);
-            v = (b >= 0) ? __ldg(&a.nbr[b + (long long)m * a.nmb]) : N_SKIPID;
-        }
-        s_nbr[lb][S] = v;
-    }
-    int fl = 0;
-    if (b >= 0) {
-        if (__ldg(&a.nbr_child[b]) < 0 || __ldg(&a.bmask[b]) != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
-        if (__ldg(&a.onb[b]) == 1) fl |= 2;                                             // kernels.cu:736
-    }
+    for (int i = t0; i < W; i += TPB) s_meta[lb][i] = (b >= 0) ? __ldg(&a.meta[(long long)b * W + i]) : 0;
     const T *__restrict__ fin = static_cast<const T *>(a.fin) + (long long)(b >= 0 ? b : 0) * BLK + t0;
 
     // Load: slot pb(p) holds f_p (offset form g_p for half storage).  Cell
@@ -74,11 +62,12 @@ k_step(const StepArgs a)
             for (int p = 0; p < Q; p++) g[h][p] = ST<T>::dec(__ldg(fin + lat_pb(DIM, p) * MC + h * TPB));
     }
     __syncthreads();
-    if (b < 0 || !(fl & 1)) return;
+    const int fl = s_meta[lb][Meta<DIM>::FLAGS];
+    if (b < 0 || !(fl & META_ACTIVE)) return;
 
     T *__restrict__ fo = static_cast<T *>(a.fout);
-    const int *nrow = s_nbr[lb];
-    const bool hook = (fl & 2) && a.bc_preset != AGAL_BC_NONE;
+    const int *nrow = s_meta[lb];
+    const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
 #pragma unroll
     for (int h = 0; h < CPT; h++) {
         const int t = t0 + h * TPB;
@@ -264,6 +253,28 @@ __global__ void k_sum_partials(const double *partial, int n, double *out)
 }
 
 // ---------------------------------------------------------------------------
+// Step metadata rows (Meta<DIM>) of every block from the mesh arrays: the
+// neighbour table in lexicographic slot order (util.h:100-101 map) and the
+// flags of kernels.cu:236 (collide/stream) and :736 (boundary hook).
+template <int DIM>
+__global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child, const int *bmask,
+                             const int *onb, int *meta)
+{
+    constexpr int W = Meta<DIM>::W, QMAX = Geo<DIM>::QMAX;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nmb * W) return;
+    const long long b = g / W;
+    const int i = (int)(g % W);
+    int v = 0;
+    if (i < QMAX) {
+        v = (i == center_slot(DIM)) ? (int)b : nbr[b + (long long)((DIM == 2) ? g_map2[i] : g_map3[i]) * nmb];
+    } else if (i == Meta<DIM>::FLAGS) {
+        if (nbr_child[b] < 0 || bmask[b] != BLOCK_SOLID) v |= META_ACTIVE;
+        if (onb[b] == 1) v |= META_ONB;
+    }
+    meta[g] = v;
+}
+
 // Dispatch on (velocity set, storage type).
 template <template <int, int, typename> class Fn, typename... Args>
 int dispatch(agal_ctx *c, Args... args)
@@ -333,11 +344,7 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.n = n;
         a.fin = c->F[c->cur[L]];
         a.fout = c->F[1 - c->cur[L]];
-        a.nmb = c->nmb;
-        a.nbr = c->cblock_ID_nbr;
-        a.nbr_child = c->cblock_ID_nbr_child;
-        a.bmask = c->cblock_ID_mask;
-        a.onb = c->cblock_ID_onb;
+        a.meta = c->meta;
         a.cmask = c->cells_ID_mask;
         a.omega = c->dxf[L] / c->tau[L];
         if (sizeof(typename ST<T>::C) == 4) a.omega = (double)((float)c->dxf[L] / (float)c->tau[L]);
@@ -483,6 +490,20 @@ int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms)
     return rc ? rc : agal::dispatch<agal::RunTune>(c, L, reps, ms);
 }
 int agal_prepare_step(agal_ctx *c) { return agal::dispatch<agal::RunPrepare>(c); }
+
+int agal_build_meta(agal_ctx *c)
+{
+    const long long tot = c->nmb * (c->dim == 2 ? agal::Meta<2>::W : agal::Meta<3>::W);
+    const unsigned grid = (unsigned)((tot + 255) / 256);
+    if (c->dim == 2)
+        agal::k_build_meta<2><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
+                                                           c->cblock_ID_mask, c->cblock_ID_onb, c->meta);
+    else
+        agal::k_build_meta<3><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
+                                                           c->cblock_ID_mask, c->cblock_ID_onb, c->meta);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
 int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }
 int agal_launch_refresh(agal_ctx *c, int L) { return agal::dispatch<agal::RunRefresh>(c, L); }
 int agal_launch_mass(agal_ctx *c, double *out) { return agal::dispatch<agal::RunMass>(c, out); }

@@ -96,19 +96,22 @@ constexpr size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
 
-// Stage geometry: ~18-28 KB of populations per stage, 3 or 4 stages.
+// Stage geometry: ~20 KB of populations per stage (at most 64 blocks), 3 or
+// 4 stages.  A stage holds, per block: populations, metadata row, block ID.
 template <int DIM, int Q, typename T> struct TmaCfg {
-    static constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
+    static constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, W = Meta<DIM>::W;
     static constexpr int BLK_BYTES = BLK * (int)sizeof(T);   // multiple of 16 for every set/type
-    static constexpr int BPS = (20480 / BLK_BYTES) > 0 ? (20480 / BLK_BYTES) : 1;
+    static constexpr int META_BYTES = W * 4;                  // 48 / 112
+    static constexpr int BPS_RAW = 20480 / BLK_BYTES;
+    static constexpr int BPS = BPS_RAW < 1 ? 1 : (BPS_RAW > 64 ? 64 : BPS_RAW);
     static constexpr size_t POP = (size_t)BPS * BLK_BYTES;
-    static constexpr size_t STAGE = align_up(POP + (size_t)BPS * QMAX * 4 + (size_t)BPS * 8, 128);
+    static constexpr size_t STAGE = align_up(POP + (size_t)BPS * META_BYTES + (size_t)BPS * 4, 128);
     static constexpr int NS = STAGE <= 24 * 1024 ? 4 : 3;
     static constexpr size_t BARS = 128;   // 2 * NS mbarriers, padded
     static constexpr size_t SMEM = BARS + NS * STAGE;
     static constexpr int CONSUMERS = 256;
     static constexpr int THREADS = CONSUMERS + 32;
-    static_assert(BLK_BYTES % 16 == 0, "bulk copies need 16-byte multiples");
+    static_assert(BLK_BYTES % 16 == 0 && META_BYTES % 16 == 0, "bulk copies need 16-byte multiples");
 };
 
 template <int DIM, int Q, typename T, bool SOLID>
@@ -117,8 +120,7 @@ k_step_tma(const StepArgs a, int *status)
 {
     using Cfg = TmaCfg<DIM, Q, T>;
     using C = typename ST<T>::C;
-    constexpr int MC = Cfg::MC, QMAX = Cfg::QMAX, BLK = Cfg::BLK, BPS = Cfg::BPS, NS = Cfg::NS;
-    constexpr int CENTER = center_slot(DIM);
+    constexpr int MC = Cfg::MC, BLK = Cfg::BLK, BPS = Cfg::BPS, NS = Cfg::NS, W = Cfg::W;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem);
     uint64_t *empty = full + NS;
@@ -137,48 +139,45 @@ k_step_tma(const StepArgs a, int *status)
 
     if (warp == Cfg::CONSUMERS / 32) {
         // ---------------- producer warp ----------------
+        // Its only global loads are the block IDs, prefetched one chunk
+        // ahead; populations and metadata rows arrive by bulk copy.
         const T *fin = static_cast<const T *>(a.fin);
+        int bn[2] = {-1, -1};   // IDs of blocks lane and lane+32 of the next chunk
+        auto fetch_ids = [&](int chunk) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int lb = lane + 32 * h;
+                const int kap = chunk * BPS + lb;
+                bn[h] = (lb < BPS && chunk < nchunks && kap < a.n) ? __ldg(&a.ids[kap]) : -1;
+            }
+        };
+        fetch_ids(blockIdx.x);
         int k = 0;
         for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x, ++k) {
             const int s = k % NS;
             const unsigned ph = (unsigned)(k / NS) & 1u;
+            const int b0 = bn[0], b1 = bn[1];
+            fetch_ids(chunk + gridDim.x);
             if (!mbar_wait(&empty[s], ph ^ 1u, status)) break;
             unsigned char *st = stages + (size_t)s * Cfg::STAGE;
             T *pop = reinterpret_cast<T *>(st);
-            int *nbr = reinterpret_cast<int *>(st + Cfg::POP);
-            int *blk = nbr + BPS * QMAX;
-            int *flg = blk + BPS;
-            int valid = 0;
-            for (int lb = lane; lb < BPS; lb += 32) {
-                const int kap = chunk * BPS + lb;
-                const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
-                int fl = 0;
-                if (b >= 0) {
-                    if (__ldg(&a.nbr_child[b]) < 0 || __ldg(&a.bmask[b]) != BLOCK_SOLID) fl |= 1;   // kernels.cu:236
-                    if (__ldg(&a.onb[b]) == 1) fl |= 2;                                             // kernels.cu:736
-                }
-                blk[lb] = b;
-                flg[lb] = fl;
-                valid += (b >= 0);
-            }
+            int *meta = reinterpret_cast<int *>(st + Cfg::POP);
+            int *blk = meta + BPS * W;
+            if (lane < BPS) blk[lane] = b0;
+            if (lane + 32 < BPS) blk[lane + 32] = b1;
+            int valid = (b0 >= 0) + (b1 >= 0);
             for (int off = 16; off > 0; off >>= 1) valid += __shfl_xor_sync(0xffffffffu, valid, off);
             __syncwarp();
-            for (int i = lane; i < BPS * QMAX; i += 32) {
-                const int lb = i % BPS, S = i / BPS;
-                const int b = blk[lb];
-                int v = b;   // the centre slot is the block itself
-                if (S != CENTER) {
-                    const int m = __ldg((DIM == 2) ? &g_map2[S] : &g_map3[S]);
-                    v = (b >= 0) ? __ldg(&a.nbr[b + (long long)m * a.nmb]) : N_SKIPID;
+            if (lane == 0) mbar_arrive_expect_tx(&full[s], (unsigned)(valid * (Cfg::BLK_BYTES + Cfg::META_BYTES)));
+            __syncwarp();
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int lb = lane + 32 * h;
+                const int b = h ? b1 : b0;
+                if (lb < BPS && b >= 0) {
+                    bulk_g2s(pop + (size_t)lb * BLK, fin + (long long)b * BLK, Cfg::BLK_BYTES, &full[s]);
+                    bulk_g2s(meta + lb * W, a.meta + (long long)b * W, Cfg::META_BYTES, &full[s]);
                 }
-                nbr[lb * QMAX + S] = v;
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive_expect_tx(&full[s], (unsigned)(valid * Cfg::BLK_BYTES));
-            __syncwarp();
-            for (int lb = lane; lb < BPS; lb += 32) {
-                const int b = blk[lb];
-                if (b >= 0) bulk_g2s(pop + (size_t)lb * BLK, fin + (long long)b * BLK, Cfg::BLK_BYTES, &full[s]);
             }
         }
         // Drain: the last phase armed on each stage must complete before exit.
@@ -199,21 +198,23 @@ k_step_tma(const StepArgs a, int *status)
             if (!mbar_wait(&full[s], ph, status)) break;
             const unsigned char *st = stages + (size_t)s * Cfg::STAGE;
             const T *pop = reinterpret_cast<const T *>(st);
-            const int *nbr = reinterpret_cast<const int *>(st + Cfg::POP);
-            const int *blk = nbr + BPS * QMAX;
-            const int *flg = blk + BPS;
+            const int *meta = reinterpret_cast<const int *>(st + Cfg::POP);
+            const int *blk = meta + BPS * W;
             for (int c = threadIdx.x; c < BPS * MC; c += Cfg::CONSUMERS) {
                 const int lb = c / MC, t = c % MC;
-                const int b = blk[lb], fl = flg[lb];
-                if (b < 0 || !(fl & 1)) continue;
+                const int b = blk[lb];
+                if (b < 0) continue;
+                const int *row = meta + lb * W;
+                const int fl = row[Meta<DIM>::FLAGS];
+                if (!(fl & META_ACTIVE)) continue;
                 if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;
                 C g[Q];
 #pragma unroll
                 for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(pop[(size_t)lb * BLK + lat_pb(DIM, p) * MC + t]);
                 C ux, uy, uz;
                 bgk_collide<DIM, Q, C, ST<T>::OFF>(g, omeg, ux, uy, uz);
-                const bool hook = (fl & 2) && a.bc_preset != AGAL_BC_NONE;
-                push_cell<DIM, Q, T, SOLID>(g, ux, uy, uz, b, t, nbr + lb * QMAX, hook, fo, a);
+                const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
+                push_cell<DIM, Q, T, SOLID>(g, ux, uy, uz, b, t, row, hook, fo, a);
             }
             mbar_arrive(&empty[s]);
         }

@@ -109,7 +109,7 @@ template <int DIM, int Q, typename T> struct TmaCfg {
     static constexpr int NS = STAGE <= 24 * 1024 ? 4 : 3;
     static constexpr size_t BARS = 128;   // 2 * NS mbarriers, padded
     static constexpr size_t SMEM = BARS + NS * STAGE;
-    static constexpr int CONSUMERS = 256;
+    static constexpr int CONSUMERS = 512;   // 16 consumer warps: enough to overlap smem latency
     static constexpr int THREADS = CONSUMERS + 32;
     static_assert(BLK_BYTES % 16 == 0 && META_BYTES % 16 == 0, "bulk copies need 16-byte multiples");
 };

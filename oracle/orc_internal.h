@@ -61,6 +61,10 @@ struct orc_case {
     int geometry_init;
     void *F;                 /* [(Q + dim + 1)][nmc] of float or double */
     int liter;               /* global_Liter of solver_lbm_advance.cu:6 */
+    int *emap;               /* [nmb] efficient map of the refinement pass (c_tmp_8), -1 = absent */
+    int *first_child;        /* [nmb] scattered first-child IDs (c_tmp_2), -1 = none */
+    long iter;               /* coarse steps taken (M_AdvanceLoop counter i) */
+    int n_ref_last, n_coarse_last;  /* marks acted on by the last refinement pass */
 };
 
 static inline int orc_half(int dim, int p)

@@ -290,3 +290,241 @@ static void FN(mass_momentum)(const orc_case *c, double *out)
     out[0] = m; out[1] = mx; out[2] = my;
     if (dim == 3) out[3] = mz;
 }
+
+/* ---------------------------------------------------------------------------
+ * Level-interface transfers (solver_lbm_kernels_comm.cu) and the refinement
+ * criterion (solver_lbm_criterion.cu).  They read the macros stored in slots
+ * Q..Q+dim by the last refresh, as the reference does.
+ */
+
+/* Rescaled population g = feq + (f - feq) * ratio of slot pb(p) of cell o. */
+static inline R FN(rescaled)(const orc_case *c, const R *F, int64_t o, int p, R ratio)
+{
+    const int64_t nmc = c->nmc;
+    const int Q = c->Q;
+    R rho = F[o + (int64_t)(Q + 0) * nmc];
+    R u = F[o + (int64_t)(Q + 1) * nmc];
+    R v = F[o + (int64_t)(Q + 2) * nmc];
+    R w = (c->dim == 3) ? F[o + (int64_t)(Q + 3) * nmc] : (R)0.0;
+    R udotu = u * u + v * v + w * w;
+    R cdotu = (R)c->cx[p] * u + (R)c->cy[p] * v + (R)c->cz[p] * w;
+    R feq = (R)c->w[p] * rho * ((R)1.0 + (R)3.0 * cdotu + (R)4.5 * cdotu * cdotu - (R)1.5 * udotu);
+    R f = F[o + (int64_t)c->pb[p] * nmc];
+    return feq + (f - feq) * ratio;
+}
+
+/* Lagrange weight of node a (nodes at 0, 1/3, 2/3, 1) at position x. */
+static inline double FN(lag4)(int a, double x)
+{
+    static const double t[4] = {0.0, 1.0 / 3.0, 2.0 / 3.0, 1.0};
+    double r = 1.0;
+    for (int k = 0; k < 4; k++)
+        if (k != a) r *= (x - t[k]) / (t[a] - t[k]);
+    return r;
+}
+
+static int FN(interpolate)(orc_case *c, int L, int var)
+{
+    /* Cu_Interpolate_Linear (kernels_comm.cu:15-138) and Cu_Interpolate_Cubic
+       (:406-640): parent cells rescaled by tau_{L+1}/tau_L, then bilinear /
+       trilinear (offsets -0.25 + 0.5 I from parent cell 2ci) or tricubic
+       Lagrange on the 4^d parent cells (children at -1/12 + m/6 in units where
+       parent cell k sits at k/3) into the children's ghost cells (mask 2) or,
+       for newly added children, into all their cells. */
+    R *F = (R *)c->F;
+    const int64_t nmc = c->nmc, nmb = c->nmb;
+    const int Q = c->Q, MC = c->MC, dim = c->dim, NCH = c->NCH;
+    const int n = c->n_ids[L];
+    const int *ids = &c->id_set[(int64_t)L * nmb];
+    const R ratio = c->fp64 ? (R)(c->tau[L + 1] / c->tau[L]) : (R)((float)c->tau[L + 1] / (float)c->tau[L]);
+    const int cubic = (c->P.interp_order == AGAL_INTERP_CUBIC);
+    /* cubic weights: positions m = 0..7 along an axis */
+    double W[4][8];
+    for (int a = 0; a < 4; a++)
+        for (int m = 0; m < 8; m++) W[a][m] = FN(lag4)(a, -1.0 / 12.0 + m / 6.0);
+#pragma omp parallel for schedule(static)
+    for (int kap = 0; kap < n; kap++) {
+        int b = ids[kap];
+        int bc = c->cblock_ID_nbr_child[b];
+        int b1 = (var == AGAL_INTERP_INTERFACE) && (c->cblock_ID_mask[b] == ORC_BLOCK_INTERFACE);
+        int b2 = (var == AGAL_INTERP_ADDED) && (c->cblock_ID_ref[b] == ORC_REF_MARK_REFINE);
+        if (!(b1 || b2)) continue;
+        R sF[64];
+        for (int p = 0; p < Q; p++) {
+            for (int t = 0; t < MC; t++) sF[t] = FN(rescaled)(c, F, (int64_t)b * MC + t, p, ratio);
+            for (int ch = 0; ch < NCH; ch++) {
+                int ci = ch & 1, cj = (ch >> 1) & 1, ck = (ch >> 2) & 1;
+                int64_t cb = (int64_t)(bc + ch);
+                for (int t = 0; t < MC; t++) {
+                    if (var == AGAL_INTERP_INTERFACE && c->cells_ID_mask[cb * MC + t] != ORC_CELL_GHOST) continue;
+                    int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
+                    R val;
+                    if (!cubic) {
+                        int s = 2 * ci + 8 * cj + 32 * ck;
+                        R Ix = (R)(-0.25) + (R)(0.5) * (R)I, Iy = (R)(-0.25) + (R)(0.5) * (R)J;
+                        if (dim == 2) {
+                            val = sF[0 + s] + (sF[1 + s] - sF[0 + s]) * Ix + (sF[4 + s] - sF[0 + s]) * Iy +
+                                  (sF[5 + s] - sF[4 + s] - sF[1 + s] + sF[0 + s]) * Ix * Iy;
+                        } else {
+                            R Iz = (R)(-0.25) + (R)(0.5) * (R)K;
+                            val = sF[0 + s] + (sF[1 + s] - sF[0 + s]) * Ix + (sF[4 + s] - sF[0 + s]) * Iy +
+                                  (sF[16 + s] - sF[0 + s]) * Iz +
+                                  (sF[5 + s] - sF[1 + s] - sF[4 + s] + sF[0 + s]) * Ix * Iy +
+                                  (sF[17 + s] - sF[1 + s] - sF[16 + s] + sF[0 + s]) * Ix * Iz +
+                                  (sF[20 + s] - sF[4 + s] - sF[16 + s] + sF[0 + s]) * Iy * Iz +
+                                  (sF[21 + s] + sF[1 + s] + sF[4 + s] + sF[16 + s] - sF[5 + s] - sF[17 + s] -
+                                   sF[20 + s] - sF[0 + s]) * Ix * Iy * Iz;
+                        }
+                    } else {
+                        int mx = I + 4 * ci, my = J + 4 * cj, mz = K + 4 * ck;
+                        double acc = 0.0;
+                        if (dim == 2) {
+                            for (int bj = 0; bj < 4; bj++)
+                                for (int ai = 0; ai < 4; ai++) acc += W[ai][mx] * W[bj][my] * (double)sF[ai + 4 * bj];
+                        } else {
+                            for (int ck2 = 0; ck2 < 4; ck2++)
+                                for (int bj = 0; bj < 4; bj++)
+                                    for (int ai = 0; ai < 4; ai++)
+                                        acc += W[ai][mx] * W[bj][my] * W[ck2][mz] * (double)sF[ai + 4 * bj + 16 * ck2];
+                        }
+                        val = (R)acc;
+                    }
+                    F[cb * MC + t + (int64_t)c->pb[p] * nmc] = val;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+static int FN(average)(orc_case *c, int L, int var)
+{
+    /* Cu_Average (kernels_comm.cu:174-347): parent cell = mean of the 2^d child
+       cells under it, rescaled by tau_L/tau_{L+1}, where the child cell at the
+       quadrant's corner has mask 1 (INTERFACE) or mask < 2 (BLOCK, GRID). */
+    R *F = (R *)c->F;
+    const int64_t nmc = c->nmc, nmb = c->nmb;
+    const int Q = c->Q, MC = c->MC, dim = c->dim, NCH = c->NCH;
+    const int n = c->n_ids[L];
+    const int *ids = &c->id_set[(int64_t)L * nmb];
+    const R ratio = c->fp64 ? (R)(c->tau[L] / c->tau[L + 1]) : (R)((float)c->tau[L] / (float)c->tau[L + 1]);
+#pragma omp parallel for schedule(static)
+    for (int kap = 0; kap < n; kap++) {
+        int b = ids[kap];
+        int bc = c->cblock_ID_nbr_child[b];
+        if (!(bc > -1 && (var == AGAL_AVERAGE_GRID || c->cblock_ID_mask[b] == ORC_BLOCK_INTERFACE))) continue;
+        for (int ch = 0; ch < NCH; ch++) {
+            int ci = ch & 1, cj = (ch >> 1) & 1, ck = (ch >> 2) & 1;
+            int64_t cb = (int64_t)(bc + ch);
+            int mask[64];
+            for (int t = 0; t < MC; t++) {
+                mask[t] = c->cells_ID_mask[cb * MC + t];
+                if (var > 0 && mask[t] < 2) mask[t] = 1;
+            }
+            R g[64];
+            for (int p = 0; p < Q; p++) {
+                for (int t = 0; t < MC; t++) g[t] = FN(rescaled)(c, F, cb * MC + t, p, ratio);
+                for (int t = 0; t < MC; t++) {
+                    int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
+                    if (!(I >= 2 * ci && I < 2 + 2 * ci && J >= 2 * cj && J < 2 + 2 * cj)) continue;
+                    if (dim == 3 && !(K >= 2 * ck && K < 2 + 2 * ck)) continue;
+                    int c0 = 2 * (I % 2) + 4 * (2 * (J % 2)) + (dim == 3 ? 16 * (2 * (K % 2)) : 0);
+                    if (mask[c0] != 1) continue;
+                    R val;
+                    if (dim == 2)
+                        val = (R)0.25 * (g[c0 + 0] + g[c0 + 1] + g[c0 + 4] + g[c0 + 5]);
+                    else
+                        val = (R)0.125 * (g[c0 + 0] + g[c0 + 1] + g[c0 + 4] + g[c0 + 5] + g[c0 + 16] + g[c0 + 17] +
+                                          g[c0 + 20] + g[c0 + 21]);
+                    F[(int64_t)b * MC + t + (int64_t)c->pb[p] * nmc] = val;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+static int FN(ref_criteria)(orc_case *c)
+{
+    /* Cu_ComputeRefCriteria (solver_lbm_criterion.cu:440-592), launched over
+       every block ID below id_max[MAX_LEVELS] with the level-0 spacing (the
+       reference passes dxf_vec[0], criterion.cu:604).  Halo by 4th-order
+       extrapolation (util_math.h:56-116), central differences, floor(log2 |w|)
+       (S_CRITERION 0) or of |Q| (1), ghost cells 0, block maximum. */
+    const R *F = (const R *)c->F;
+    const int64_t nmc = c->nmc, nmb = c->nmb;
+    const int Q = c->Q, MC = c->MC, dim = c->dim, Qmax = c->Qmax;
+    const int idm = c->id_max[c->max_levels];
+    const R dxL = c->fp64 ? (R)c->dxf_d[0] : (R)c->dxf[0];
+    const int MLI = c->P.MAX_LEVELS_INTERIOR;
+    const R NRS = (R)c->P.N_REFINE_START, NRI = (R)c->P.N_REFINE_INC, NRM = (R)c->P.N_REFINE_MAX;
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < idm; b++) {
+        if (c->cblock_ID_ref[b] == ORC_REF_INACTIVE) continue;
+        R h[3][216];
+        for (int comp = 0; comp < dim; comp++)
+            for (int t = 0; t < MC; t++) {
+                int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
+                int hi = (I + 1) + 6 * (J + 1) + (dim == 3 ? 36 * (K + 1) : 0);
+                h[comp][hi] = F[(int64_t)b * MC + t + (int64_t)(Q + 1 + comp) * nmc];
+            }
+        for (int comp = 0; comp < dim; comp++) {
+            R *s = h[comp];
+#define HI(i, j, k) (((i) + 1) + 6 * ((j) + 1) + (dim == 3 ? 36 * ((k) + 1) : 0))
+            for (int t = 0; t < MC; t++) {
+                int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
+                if (I == 0) {
+                    s[HI(-1, J, K)] = (R)4.0 * s[HI(0, J, K)] + (R)(-6.0) * s[HI(1, J, K)] + (R)4.0 * s[HI(2, J, K)] + (R)(-1.0) * s[HI(3, J, K)];
+                    s[HI(4, J, K)] = (R)4.0 * s[HI(3, J, K)] + (R)(-6.0) * s[HI(2, J, K)] + (R)4.0 * s[HI(1, J, K)] + (R)(-1.0) * s[HI(0, J, K)];
+                }
+                if (J == 0) {
+                    s[HI(I, -1, K)] = (R)4.0 * s[HI(I, 0, K)] + (R)(-6.0) * s[HI(I, 1, K)] + (R)4.0 * s[HI(I, 2, K)] + (R)(-1.0) * s[HI(I, 3, K)];
+                    s[HI(I, 4, K)] = (R)4.0 * s[HI(I, 3, K)] + (R)(-6.0) * s[HI(I, 2, K)] + (R)4.0 * s[HI(I, 1, K)] + (R)(-1.0) * s[HI(I, 0, K)];
+                }
+                if (dim == 3 && K == 0) {
+                    s[HI(I, J, -1)] = (R)4.0 * s[HI(I, J, 0)] + (R)(-6.0) * s[HI(I, J, 1)] + (R)4.0 * s[HI(I, J, 2)] + (R)(-1.0) * s[HI(I, J, 3)];
+                    s[HI(I, J, 4)] = (R)4.0 * s[HI(I, J, 3)] + (R)(-6.0) * s[HI(I, J, 2)] + (R)4.0 * s[HI(I, J, 1)] + (R)(-1.0) * s[HI(I, J, 0)];
+                }
+            }
+        }
+        R Wmax = -INFINITY;
+        for (int t = 0; t < MC; t++) {
+            int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
+            R d[3][3] = {{0}};   /* d[comp][axis] */
+            for (int comp = 0; comp < dim; comp++) {
+                const R *s = h[comp];
+                if (dim == 2) {
+                    /* 2D divides by the double 2.0*dx_L (criterion.cu:502-505) */
+                    d[comp][0] = (R)((double)(s[HI(I + 1, J, K)] - s[HI(I - 1, J, K)]) / (2.0 * (double)dxL));
+                    d[comp][1] = (R)((double)(s[HI(I, J + 1, K)] - s[HI(I, J - 1, K)]) / (2.0 * (double)dxL));
+                } else {
+                    d[comp][0] = (s[HI(I + 1, J, K)] - s[HI(I - 1, J, K)]) / ((R)2 * dxL);
+                    d[comp][1] = (s[HI(I, J + 1, K)] - s[HI(I, J - 1, K)]) / ((R)2 * dxL);
+                    d[comp][2] = (s[HI(I, J, K + 1)] - s[HI(I, J, K - 1)]) / ((R)2 * dxL);
+                }
+            }
+#undef HI
+            R uX = d[0][0], uY = d[0][1], uZ = d[0][2], vX = d[1][0], vY = d[1][1], vZ = d[1][2];
+            R wX = d[2][0], wY = d[2][1], wZ = d[2][2];
+            R Wt = (R)0;
+            if (c->P.S_CRITERION == 0)
+                Wt = (R)floor(log2((double)(R)sqrt((double)((wY - vZ) * (wY - vZ) + (uZ - wX) * (uZ - wX) + (vX - uY) * (vX - uY)))));
+            if (c->P.S_CRITERION == 1)
+                Wt = (R)floor(log2((double)(R)fabs((double)((R)0.5 * (uX * uX + vY * vY + wZ * wZ + (R)2.0 * (uY * vX + uZ * wX + wY * vZ))))));
+            if (c->cells_ID_mask[(int64_t)b * MC + t] == ORC_CELL_GHOST) Wt = (R)0;
+            Wmax = (R)fmax((double)Wmax, (double)Wt);   /* BlockwiseMaximum with fmaxf (util.h:29, 787) */
+        }
+        if (Wmax > NRM) Wmax = NRM;
+        int ref_kap = c->cblock_ID_ref[b], level_kap = c->cblock_level[b];
+        int L_desired = MLI - 1;
+        for (int p = 1; p <= MLI - 1; p++)
+            if (Wmax < NRS - NRI * (R)p) L_desired = (MLI - 1) - p;
+        int eligible = 1;
+        for (int p = 0; p < Qmax; p++)
+            if (c->cblock_ID_nbr[b + (int64_t)p * nmb] == ORC_N_SKIPID) eligible = 0;
+        if (eligible && level_kap != MLI - 1 && ref_kap == ORC_REF_UNREFINED && L_desired > level_kap)
+            c->cblock_ID_ref[b] = ORC_REF_MARK_REFINE;
+        if (ref_kap == ORC_REF_REFINED && L_desired < level_kap + 1) c->cblock_ID_ref[b] = ORC_REF_MARK_COARSEN;
+    }
+    return 0;
+}

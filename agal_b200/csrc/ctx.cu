@@ -213,7 +213,10 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         (rc = fill<int>(c, c->cblock_ID_nbr_child, c->Qmax * nmb, N_SKIPID)) ||
         (rc = fill<int>(c, c->cblock_ID_ref, nmb, REF_INACTIVE)) ||
         (rc = fill<int>(c, c->cblock_level, nmb, 0)) || (rc = fill<int>(c, c->cblock_ID_onb, nmb, 0)) ||
-        (rc = fill<int>(c, c->id_set, c->max_levels * nmb, -1)) || (rc = fill<int>(c, c->gap_set, nmb, -1)) ||
+        // id_set / gap_set start zeroed as in the reference (mesh_init.cu
+        // allocates them and fills only the live prefix); the refinement
+        // pass reads slot 0 of an empty level as its id_max.
+        (rc = fill<int>(c, c->id_set, c->max_levels * nmb, 0)) || (rc = fill<int>(c, c->gap_set, nmb, 0)) ||
         (rc = fill<float>(c, c->cblock_f_X, c->dim * nmb, 0.0f))) {
         std::string m = c->err;
         release(c);

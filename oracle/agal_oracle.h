@@ -50,9 +50,20 @@ int orc_refresh(orc_case *c, int L);
 int orc_collide(orc_case *c, int L);    /* solver_lbm_kernels.cu:206-289, 465-510 */
 int orc_impose_bc(orc_case *c, int L);  /* solver_lbm_kernels.cu:693-920 */
 int orc_stream(orc_case *c, int L);     /* solver_lbm_kernels.cu:534-660 */
+/* S_Interpolate / S_Average with their refresh (solver_lbm_kernels_comm.cu). */
+int orc_interpolate(orc_case *c, int L, int var);
+int orc_average(orc_case *c, int L, int var);
+/* Solver_LBM::S_ComputeRefCriteria (solver_lbm_criterion.cu:440-613). */
+int orc_ref_criteria(orc_case *c);
+/* Mesh::M_RefineAndCoarsenBlocks (mesh_amr.cu:2162-2744). */
+int orc_refine_coarsen(orc_case *c);
+/* Mesh::M_Advance_RefineWithSolution (mesh_advance.cu:185-243). */
+int orc_refine_with_solution(orc_case *c);
 /* Solver_LBM::S_Advance (solver_lbm_advance.cu:31-174). */
 int orc_advance(orc_case *c, int L);
-/* n coarse steps from N_LEVEL_START. */
+/* n coarse steps of the M_AdvanceLoop body (mesh_advance.cu:421-463):
+   S_Advance from N_LEVEL_START, then every P_REFINE steps the
+   solution-based refinement. */
 int orc_advance_n(orc_case *c, int n);
 
 /* Array sizes and copies with the AGAL_ARR_* selectors of agal_b200.h. */

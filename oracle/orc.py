@@ -48,6 +48,11 @@ def lib() -> C.CDLL:
             ("orc_impose_bc", C.c_int, [C.c_void_p, C.c_int]),
             ("orc_stream", C.c_int, [C.c_void_p, C.c_int]),
             ("orc_advance", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_interpolate", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+            ("orc_average", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+            ("orc_ref_criteria", C.c_int, [C.c_void_p]),
+            ("orc_refine_coarsen", C.c_int, [C.c_void_p]),
+            ("orc_refine_with_solution", C.c_int, [C.c_void_p]),
             ("orc_advance_n", C.c_int, [C.c_void_p, C.c_int]),
             ("orc_array_bytes", C.c_size_t, [C.c_void_p, C.c_int]),
             ("orc_dump", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
@@ -113,6 +118,21 @@ class OracleCase:
 
     def advance_n(self, n):
         self._c(self._lib.orc_advance_n(self._h, n))
+
+    def interpolate(self, L, var):
+        self._c(self._lib.orc_interpolate(self._h, L, var))
+
+    def average(self, L, var):
+        self._c(self._lib.orc_average(self._h, L, var))
+
+    def ref_criteria(self):
+        self._c(self._lib.orc_ref_criteria(self._h))
+
+    def refine_coarsen(self):
+        self._c(self._lib.orc_refine_coarsen(self._h))
+
+    def refine_with_solution(self):
+        self._c(self._lib.orc_refine_with_solution(self._h))
 
     def mass_momentum(self):
         out = (C.c_double * 4)()

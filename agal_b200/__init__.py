@@ -156,6 +156,12 @@ class Case:
         self._c(self._lib.agal_mass_momentum(self._h, out))
         return np.array(out[: self.dim + 1])
 
+    def mass_momentum_noalloc(self) -> np.ndarray:
+        """mass_momentum with a fixed static device scratch (allocates nothing)."""
+        out = (C.c_double * 4)()
+        self._c(self._lib.agal_mass_momentum_noalloc(self._h, out))
+        return np.array(out[: self.dim + 1])
+
     # -- arrays ---------------------------------------------------------
     _DTYPES = {_lib.ARR_F: np.float64, _lib.ARR_MACROS: np.float64, _lib.ARR_CBLOCK_F_X: np.float32}
 

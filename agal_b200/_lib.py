@@ -79,6 +79,7 @@ PROTOS = [
     ("agal_dump", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("agal_load", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("agal_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("agal_mass_momentum_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_sync", C.c_int, [C.c_void_p]),
     ("agal_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("agal_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),

@@ -23,6 +23,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "ctx.h"
@@ -481,7 +482,97 @@ template <int DIM, int Q, typename T> struct RunMass {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Allocation-free mass/momentum: the same k_mass / k_sum_partials kernels with
+// their partials and result in a fixed file-scope device array instead of
+// the context's cudaMalloc'd scratch.  Every partial slot the final sum reads
+// is written by k_mass in the same call, and k_sum_partials overwrites the
+// result, so nothing has to start at zero.  All contexts on one device share
+// the array: calls that overlap in time (other host threads or streams on the
+// same device) race on it and must be serialised by the caller.
+__device__ __align__(256) static double g_mass_scratch[4 * AGAL_MASS_NOALLOC_MAX_PARTIALS + 4];
+
+static std::mutex g_mass_scratch_mu;
+static double *g_mass_scratch_ptr[128];   // per device ordinal, set on first use
+
+// Device address of g_mass_scratch on device dev, looked up once per device
+// with that device current (cudaGetSymbolAddress may initialise the module,
+// so the first call on a device belongs before any stream capture).
+static int mass_scratch_on(agal_ctx *c, double **out)
+{
+    const int dev = c->device;
+    if (dev < 0 || dev >= 128) return agal_set_err(c, AGAL_ERR_PARAM, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_mass_scratch_mu);
+    if (!g_mass_scratch_ptr[dev]) {
+        int prev = -1;
+        AGAL_CUDA(c, cudaGetDevice(&prev));
+        if (prev != dev) AGAL_CUDA(c, cudaSetDevice(dev));
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_scratch);
+        if (prev != dev) cudaSetDevice(prev);
+        if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGetSymbolAddress(g_mass_scratch)");
+        g_mass_scratch_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_mass_scratch_ptr[dev];
+    return AGAL_OK;
+}
+
+template <int DIM, int Q, typename T> struct RunMassNoAlloc {
+    static int run(agal_ctx *c, double *out)
+    {
+        long long total = 0;
+        std::vector<long long> grids(c->max_levels);
+        for (int L = 0; L < c->max_levels; L++) {
+            grids[L] = ((long long)c->n_ids[L] * Geo<DIM>::MC + 255) / 256;
+            total += grids[L];
+        }
+        if (total > AGAL_MASS_NOALLOC_MAX_PARTIALS) {
+            char m[256];
+            std::snprintf(m, sizeof(m),
+                          "agal_mass_momentum_noalloc: %lld partial sums exceed the static scratch of %d "
+                          "(one per 256 active cells of each level); use agal_mass_momentum",
+                          total, AGAL_MASS_NOALLOC_MAX_PARTIALS);
+            return agal_set_err(c, AGAL_ERR_PARAM, m);
+        }
+        double *scratch = nullptr;
+        int rc = mass_scratch_on(c, &scratch);
+        if (rc) return rc;
+        double *res = scratch + 4 * (size_t)AGAL_MASS_NOALLOC_MAX_PARTIALS;
+        long long off = 0;
+        for (int L = 0; L < c->max_levels; L++) {
+            if (grids[L] == 0) continue;
+            MassArgs a;
+            a.ids = c->id_set + (long long)L * c->nmb;
+            a.n = c->n_ids[L];
+            a.f = c->F[c->cur[L]];
+            a.nbr_child = c->cblock_ID_nbr_child;
+            a.cmask = c->cells_ID_mask;
+            a.vol = std::ldexp(1.0, -L * DIM);
+            a.partial = scratch + 4 * off;
+            k_mass<DIM, Q, T><<<(unsigned)grids[L], 256, 0, c->stream>>>(a);
+            AGAL_CUDA(c, cudaGetLastError());
+            off += grids[L];
+        }
+        k_sum_partials<<<1, 32, 0, c->stream>>>(scratch, (int)total, res);
+        AGAL_CUDA(c, cudaGetLastError());
+        double h[4];
+        AGAL_CUDA(c, cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+        out[0] = h[0];
+        out[1] = h[1];
+        out[2] = h[2];
+        if (DIM == 3) out[3] = h[3];
+        return AGAL_OK;
+    }
+};
+
 }  // namespace agal
+
+extern "C" int agal_mass_momentum_noalloc(agal_ctx *c, double *out)
+{
+    if (!c || !out) return AGAL_ERR_PARAM;
+    return agal::dispatch<agal::RunMassNoAlloc>(c, out);
+}
 
 int agal_launch_step(agal_ctx *c, int L) { return agal::dispatch<agal::RunStep>(c, L, 0, true); }
 int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms)

@@ -172,6 +172,20 @@ int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
    Reads the macros of agal_refresh-free state (computes them itself). */
 int agal_mass_momentum(agal_ctx *ctx, double *out);
 
+/* Same sums as agal_mass_momentum, for callers that must not allocate device
+   memory (a memory-capped serving process, a pool that is fully reserved, a
+   code path between other libraries' allocations): the partial sums live in a
+   fixed static device array of AGAL_MASS_NOALLOC_MAX_PARTIALS x 4 doubles
+   (8 MiB), and no call allocates or frees.  One partial covers 256 active
+   cells of one level, so a mesh of more than 67,108,864 active cells (summed
+   per level, each level rounded up to 256) is rejected with AGAL_ERR_PARAM.
+   The first call on a device looks the array up (cudaGetSymbolAddress) with
+   that device current; make it before any stream capture.  The array is
+   shared by every context of the device: calls that overlap in time race
+   and must be serialised by the caller.  No reference counterpart. */
+#define AGAL_MASS_NOALLOC_MAX_PARTIALS 262144
+int agal_mass_momentum_noalloc(agal_ctx *ctx, double *out);
+
 /* Autotuner of the fused step kernel.  Variants: 1 = one cell per thread,
    2 = two cells per thread (one-shot grids), 3 = persistent pipeline with the
    cell-blocks staged in shared memory by TMA bulk copies.  Times each variant

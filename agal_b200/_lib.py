@@ -24,6 +24,7 @@ INTERP_LINEAR, INTERP_CUBIC = 0, 2
 STORE_FP32, STORE_FP64, STORE_FP16, STORE_BF16 = 0, 1, 2, 3
 BC_NONE, BC_LDC2D, BC_LDC3D, BC_FPSC2D, BC_FPSC3D = 0, 1, 2, 3, 4
 IC_REST, IC_UNIFORM = 0, 1
+REGION_NONE, REGION_BOUNDARY, REGION_BOX = 0, 1, 2
 INTERP_INTERFACE, INTERP_ADDED = 0, 1
 AVERAGE_INTERFACE, AVERAGE_BLOCK, AVERAGE_GRID = 0, 1, 2
 
@@ -56,6 +57,7 @@ class AgalParams(C.Structure):
                 [(k, C.c_char * 256) for k in STR_KEYS] +
                 [("velocity_set", C.c_int), ("collision", C.c_int), ("interp_order", C.c_int),
                  ("storage", C.c_int), ("bc_preset", C.c_int), ("ic_preset", C.c_int),
+                 ("region_preset", C.c_int),
                  ("u_ref", C.c_double), ("ic_noise", C.c_double), ("seed", C.c_uint64),
                  ("n_maxcblocks", C.c_int64), ("mem_frac", C.c_double), ("device", C.c_int)])
 

@@ -109,6 +109,7 @@ extern "C" int agal_params_default(agal_params *p)
     p->storage = AGAL_STORE_FP32;
     p->bc_preset = AGAL_BC_NONE;
     p->ic_preset = AGAL_IC_REST;
+    p->region_preset = AGAL_REGION_NONE;
     p->u_ref = 0.05;                       // custom.h literal
     p->ic_noise = 0.0;
     p->seed = 0;

@@ -64,6 +64,12 @@ extern "C" {
 /* initial-condition presets of the Cu_ComputeIC hook, inc/custom.h:50-60 */
 #define AGAL_IC_REST    0   /* rho = 1, u = 0                                   */
 #define AGAL_IC_UNIFORM 1   /* rho = 1, u = (u_ref, 0, 0) (+ seeded noise)      */
+/* near-wall refinement regions of the Cu_RefineRegion hook, inc/custom.h:17-42,
+   evaluated on a block's bounds (x + 1e-5, x + 4 dx_L - 1e-5) as
+   mesh_criterion.cu:28-50 passes them */
+#define AGAL_REGION_NONE     0   /* no block (the shipped hook returns false)     */
+#define AGAL_REGION_BOUNDARY 1   /* blocks on the domain boundary (onb == 1)      */
+#define AGAL_REGION_BOX      2   /* blocks inside [0.25, 0.75]^d (coordinates)    */
 
 /* interpolation / averaging modes, inc/mesh.h:58-62 */
 #define AGAL_INTERP_INTERFACE 0
@@ -115,6 +121,7 @@ typedef struct agal_params {
     int storage;          /* AGAL_STORE_*                        */
     int bc_preset;        /* AGAL_BC_*                           */
     int ic_preset;        /* AGAL_IC_*                           */
+    int region_preset;    /* AGAL_REGION_*                       */
     double u_ref;         /* velocity of the presets (custom.h hard-codes 0.05) */
     double ic_noise;      /* relative amplitude of seeded IC noise (0 = none)   */
     uint64_t seed;        /* seed of the IC noise                               */

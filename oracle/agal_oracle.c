@@ -624,6 +624,61 @@ int orc_refine_with_solution(orc_case *c)
     return orc_refine_coarsen(c);
 }
 
+/* Cu_RefineRegion presets on the block bounds of mesh_criterion.cu:28-33. */
+static int in_region(const orc_case *c, int b, float dxb)
+{
+    const int64_t nmb = c->nmb;
+    const float *fX = c->cblock_f_X;
+    switch (c->P.region_preset) {
+    case AGAL_REGION_BOUNDARY: return c->cblock_ID_onb[b] == 1;
+    case AGAL_REGION_BOX: {
+        for (int d = 0; d < c->dim; d++) {
+            const float lo = fX[b + d * nmb] + 1e-5f;
+            const float hi = fX[b + d * nmb] + dxb - 1e-5f;
+            if (!(lo >= 0.25f && hi <= 0.75f)) return 0;
+        }
+        return 1;
+    }
+    default: return 0;
+    }
+}
+
+static void mark_level(orc_case *c, int L, int uniform)
+{
+    /* Cu_ComputeRefCriteria_Uniform / _NearWall_Cases (mesh_criterion.cu:10-85). */
+    const int *ids = &c->id_set[(int64_t)L * c->nmb];
+    const float dxb = c->dxf[L] * 4.0f;
+    for (int k = 0; k < c->n_ids[L]; k++) {
+        const int b = ids[k];
+        if (c->cblock_ID_ref[b] != ORC_REF_UNREFINED) continue;
+        if (uniform || in_region(c, b, dxb)) c->cblock_ID_ref[b] = ORC_REF_MARK_REFINE;
+    }
+}
+
+int orc_refine_near_wall(orc_case *c)
+{
+    /* Mesh::M_Advance_RefineNearWall without geometry (mesh_advance.cu:54-122). */
+    const int ML = c->max_levels, MLW = c->P.MAX_LEVELS_WALL;
+    int rc;
+    for (int L = 0; L < c->L0; L++) {
+        mark_level(c, L, 1);
+        if ((rc = orc_refine_coarsen(c))) return rc;
+    }
+    for (int L = c->L0; L < MLW; L++) {
+        if (L < MLW - 1) mark_level(c, L, 0);
+        if (ML > 1 && L < MLW - 1 && (rc = orc_refine_coarsen(c))) return rc;
+        if ((rc = orc_set_ic(c, L))) return rc;
+    }
+    if (ML > 1) {
+        /* M_FreezeRefinedCells(0): Cu_FreezeRefined over id_max[MAX_LEVELS] (mesh_amr.cu:1888-1904). */
+        for (int b = 0; b < c->id_max[ML]; b++) {
+            if (c->cblock_ID_ref[b] == ORC_REF_REFINED) c->cblock_ID_ref[b] = ORC_REF_REFINED_PERM;
+            if (c->cblock_ID_ref[b] == ORC_REF_REFINED_WCHILD) c->cblock_ID_ref[b] = ORC_REF_REFINED_WCHILD_PERM;
+        }
+    }
+    return 0;
+}
+
 int orc_advance_n(orc_case *c, int n)
 {
     /* Loop body of Mesh::M_AdvanceLoop (mesh_advance.cu:421-463). */

@@ -59,6 +59,10 @@ int orc_ref_criteria(orc_case *c);
 int orc_refine_coarsen(orc_case *c);
 /* Mesh::M_Advance_RefineWithSolution (mesh_advance.cu:185-243). */
 int orc_refine_with_solution(orc_case *c);
+/* Mesh::M_Advance_RefineNearWall without geometry (mesh_advance.cu:54-122):
+   uniform refinement to N_LEVEL_START, Cu_RefineRegion marks (region_preset)
+   up to MAX_LEVELS_WALL, S_SetIC per level, then the refined blocks frozen. */
+int orc_refine_near_wall(orc_case *c);
 /* Solver_LBM::S_Advance (solver_lbm_advance.cu:31-174). */
 int orc_advance(orc_case *c, int L);
 /* n coarse steps of the M_AdvanceLoop body (mesh_advance.cu:421-463):

@@ -53,6 +53,7 @@ def lib() -> C.CDLL:
             ("orc_ref_criteria", C.c_int, [C.c_void_p]),
             ("orc_refine_coarsen", C.c_int, [C.c_void_p]),
             ("orc_refine_with_solution", C.c_int, [C.c_void_p]),
+            ("orc_refine_near_wall", C.c_int, [C.c_void_p]),
             ("orc_advance_n", C.c_int, [C.c_void_p, C.c_int]),
             ("orc_array_bytes", C.c_size_t, [C.c_void_p, C.c_int]),
             ("orc_dump", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
@@ -133,6 +134,9 @@ class OracleCase:
 
     def refine_with_solution(self):
         self._c(self._lib.orc_refine_with_solution(self._h))
+
+    def refine_near_wall(self):
+        self._c(self._lib.orc_refine_near_wall(self._h))
 
     def mass_momentum(self):
         out = (C.c_double * 4)()

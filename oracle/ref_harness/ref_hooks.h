@@ -20,12 +20,25 @@
 #define REF_IC 0
 #endif
 
+// Refinement region preset, set by the driver from the REF_REGION environment
+// variable: 0 none (the shipped hook), 1 blocks on the domain boundary,
+// 2 blocks inside [0.25, 0.75]^d.
+__device__ int g_ref_region = 0;
+
 template <typename ufloat_t>
 __device__ bool Cu_RefineRegion(const int L, const ufloat_t x, const ufloat_t y, const ufloat_t z,
                                 const ufloat_t xp, const ufloat_t yp, const ufloat_t zp, const int onb,
                                 const int nbr_1, const int nbr_2, const int nbr_3, const int nbr_4,
                                 const int nbr_5, const int nbr_6)
 {
+    if (g_ref_region == 1) return onb == 1;
+    if (g_ref_region == 2) {
+        bool in = x >= (ufloat_t)0.25 && xp <= (ufloat_t)0.75 && y >= (ufloat_t)0.25 && yp <= (ufloat_t)0.75;
+#if !defined(USED2Q9)
+        in = in && z >= (ufloat_t)0.25 && zp <= (ufloat_t)0.75;
+#endif
+        return in;
+    }
     return false;
 }
 

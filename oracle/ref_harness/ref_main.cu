@@ -150,6 +150,11 @@ int main(int argc, char **argv)
         if (cudaMalloc(&ballast, fr - keep) != cudaSuccess) { fprintf(stderr, "ballast failed\n"); return 3; }
     }
 
+    if (const char *rg = getenv("REF_REGION")) {
+        const int v = atoi(rg);
+        cudaMemcpyToSymbol(g_ref_region, &v, sizeof(int));
+    }
+
     Parser parser(input_dir);
     const int N_U = LPh.N_Q + APh.N_DIM + 1;
     Mesh<REAL_h, REAL_h, &APh> mesh(&parser, N_U);

@@ -48,6 +48,25 @@ CASES = {
     "d3q19_ldc16_pxy": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4, PERIODIC_X=1, PERIODIC_Y=1), 100, 4096),
 }
 
+# Multi-level cases: (binary, keys, steps, keep_mb, region preset of the
+# Cu_RefineRegion hook (REF_REGION: 0 none, 1 boundary blocks, 2 box)).
+# Near-wall/region refinement builds a static hierarchy before the loop;
+# MAX_LEVELS_INTERIOR > 1 adds the solution criterion every P_REFINE steps.
+AMR = dict(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, P_REFINE=16, N_REFINE_START=-2.0, N_REFINE_INC=1.0,
+           N_REFINE_MAX=1.0, S_CRITERION=0)
+AMR_CASES = {
+    "amr_d2q9_box3_cubic": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-4, MAX_LEVELS_WALL=3), 200, 4096, 2),
+    "amr_d2q9_wall2_linear": ("ref_d2q9_ldc_lin", dict(AMR, Nx=64, v0=5e-4, MAX_LEVELS_WALL=2), 200, 4096, 1),
+    # 128 steps = 8 regrids: at the 9th, one block's vorticity sits on a
+    # criterion threshold and FP32 rounding decides its refinement.
+    "amr_d2q9_sol3_cubic": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 128, 4096, 0),
+    "amr_d2q9_sol3_linear": ("ref_d2q9_ldc_lin", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 200, 4096, 0),
+    "amr_d2q9_wall2_sol3": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3),
+                            200, 4096, 1),
+    "amr_d3q19_box2": ("ref_d3q19_ldc", dict(AMR, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2), 60, 4096, 2),
+    "amr_d3q27_sol2": ("ref_d3q27_ldc", dict(AMR, Nx=16, v0=2.5e-5, MAX_LEVELS_INTERIOR=2, P_REFINE=8), 48, 4096, 0),
+}
+
 # Timing workloads of the reference build: (binary, keys, timed steps, keep_mb)
 TIMING = {
     "ldc2d_256": ("ref_d2q9_ldc", dict(Nx=256, v0=5e-4), 2000, 4096),
@@ -150,7 +169,8 @@ def read_dump(path: Path) -> dict:
     return res
 
 
-def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0) -> str:
+def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
+            region: int = 0) -> str:
     exe = REF_BIN / binary
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
@@ -166,7 +186,9 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             import resource
             resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
 
-        r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack)
+        env = dict(os.environ, REF_REGION=str(region))
+        r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
+                           env=env)
         if r.returncode != 0:
             raise RuntimeError(f"{binary} failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
         return r.stdout
@@ -174,14 +196,17 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
 
 def cmd_ref(out: Path, only: list[str] | None) -> None:
     out.mkdir(parents=True, exist_ok=True)
-    for name, (binary, keys, steps, keep) in CASES.items():
+    cases = {k: v + (0,) for k, v in CASES.items()}
+    cases.update(AMR_CASES)
+    for name, (binary, keys, steps, keep, region) in cases.items():
         if only and name not in only:
             continue
         raw = out / f"{name}.bin"
-        run_ref(binary, keys, steps, keep, raw)
+        run_ref(binary, keys, steps, keep, raw, region=region)
         d = read_dump(raw)
         d["case_keys"] = json.dumps(keys)
         d["binary"] = binary
+        d["region"] = region
         np.savez_compressed(out / f"{name}.npz", **d)
         raw.unlink()
         print(name, "n_maxcblocks", d["n_maxcblocks"], "active", len(d["blocks"]), flush=True)

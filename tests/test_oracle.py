@@ -98,11 +98,28 @@ def params_for_golden(g):
     # n_maxcblocks-1 .. n_coarse, popped from the end), so they do not depend
     # on the pool size: a pool just above the largest active ID reproduces the
     # reference's IDs without its multi-GB allocation.
-    nmb = int(g["blocks"].max()) + 1 + 64
+    # A multi-level case can hold more IDs in passing than at the end, so its
+    # pool covers the fully refined hierarchy.
+    ml = int(g["max_levels"])
+    nch = 4 if int(g["dim"]) == 2 else 8
+    n0 = int(g["n_ids"][0]) if ml == 1 else int(np.sum(g["level"][:, 0] == 0))
+    full = sum(n0 * nch ** L for L in range(ml))
+    nmb = max(int(g["blocks"].max()) + 1, full if ml > 1 else 0) + 64
+    interp = _lib.INTERP_LINEAR if (int(g["dim"]) == 3 or str(g["binary"]).endswith("_lin")) else _lib.INTERP_CUBIC
+    region = int(g["region"]) if "region" in g else 0
     kw = dict(velocity_set=vs, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, bc_preset=bc,
-              ic_preset=_lib.IC_REST, n_maxcblocks=nmb)
+              ic_preset=_lib.IC_REST, n_maxcblocks=nmb, interp_order=interp, region_preset=region)
     kw.update(keys)
     return ag.default_params(**kw), int(g["steps"])
+
+
+def run_like_reference(case, p, steps):
+    """The reference driver's sequence: IC, near-wall refinement when the
+    hierarchy has more than one level, then the M_AdvanceLoop body."""
+    case.set_ic(0)
+    if max(p.MAX_LEVELS_WALL, p.MAX_LEVELS_INTERIOR) > 1:
+        case.refine_near_wall()
+    case.advance_n(steps)
 
 
 def fp64_floor(g):
@@ -112,8 +129,7 @@ def fp64_floor(g):
     p, steps = params_for_golden(g)
     Q, dim, MC = int(g["Q"]), int(g["dim"]), int(g["MC"])
     o = OracleCase(p, p.n_maxcblocks, fp64=True)
-    o.set_ic(0)
-    o.advance_n(steps)
+    run_like_reference(o, p, steps)
     blocks = g["blocks"].astype(np.int64)
     F = o.dump(_lib.ARR_F).reshape(Q, p.n_maxcblocks, MC)[:, blocks, :].reshape(Q, -1)
     pb, c, _ = lattice(Q)
@@ -123,7 +139,7 @@ def fp64_floor(g):
     return rho64, np.stack(u64), rel_l2(np.stack(u_r), np.stack(u64)), rel_l2(rho_r, rho64)
 
 
-def compare_to_golden(g, dumpf, tol_rel_l2):
+def compare_to_golden(g, dumpf, tol_rel_l2, counts=None):
     """Integer arrays bit-exact; rho/u against the reference's own FP32 build.
 
     Two FP32 implementations that round differently cannot agree to better
@@ -135,6 +151,18 @@ def compare_to_golden(g, dumpf, tol_rel_l2):
     blocks = g["blocks"].astype(np.int64)
     dim, Q, Qmax, MC = int(g["dim"]), int(g["Q"]), int(g["Qmax"]), int(g["MC"])
     nmb = len(dumpf(_lib.ARR_CBLOCK_ID_ONB))
+    if counts is not None:
+        ml = int(g["max_levels"])
+        assert counts["n_ids"][:ml] == [int(v) for v in g["n_ids"][:ml]]
+        assert counts["id_max"][: ml + 1] == [int(v) for v in g["id_max"][: ml + 1]]
+        # top of the gap stack (recycled and lowest fresh IDs), as far as the
+        # smaller pool here reaches
+        gaps = dumpf(_lib.ARR_GAP_SET)[: counts["n_gaps"]]
+        tail = g["gaps_tail"]
+        k = 0
+        while k < min(len(tail), len(gaps)) and tail[len(tail) - 1 - k] < nmb - 64:
+            k += 1
+        assert (gaps[len(gaps) - k:] == tail[len(tail) - k:]).all()
     nbr = dumpf(_lib.ARR_CBLOCK_ID_NBR).reshape(Qmax, nmb)[:, blocks].T
     assert (nbr == g["nbr"]).all()
     ch = dumpf(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(Qmax, nmb)[:, blocks].T
@@ -170,6 +198,5 @@ def test_oracle_vs_reference_build(oracle_lib, name):
     g = load_golden(name)
     p, steps = params_for_golden(g)
     o = OracleCase(p, p.n_maxcblocks)
-    o.set_ic(0)
-    o.advance_n(steps)
-    compare_to_golden(g, o.dump, 1e-5)
+    run_like_reference(o, p, steps)
+    compare_to_golden(g, o.dump, 1e-5, o.counts())

@@ -133,6 +133,30 @@ class Case:
     def sync(self) -> None:
         self._c(self._lib.agal_sync(self._h))
 
+    # -- multi-level mesh ------------------------------------------------
+    def interpolate(self, L: int, var: int = _lib.INTERP_INTERFACE) -> None:
+        self._c(self._lib.agal_interpolate(self._h, L, var))
+
+    def average(self, L: int, var: int = _lib.AVERAGE_GRID) -> None:
+        self._c(self._lib.agal_average(self._h, L, var))
+
+    def ref_criteria(self) -> None:
+        self._c(self._lib.agal_ref_criteria(self._h))
+
+    def refine_coarsen(self) -> None:
+        self._c(self._lib.agal_refine_coarsen(self._h))
+
+    def refine_with_solution(self) -> None:
+        self._c(self._lib.agal_refine_with_solution(self._h))
+
+    def refine_near_wall(self) -> None:
+        self._c(self._lib.agal_refine_near_wall(self._h))
+
+    def refine_stats(self) -> dict:
+        it, nr, nc = C.c_longlong(), C.c_int(), C.c_int()
+        self._c(self._lib.agal_refine_stats(self._h, C.byref(it), C.byref(nr), C.byref(nc)))
+        return {"iter": it.value, "n_refined": nr.value, "n_coarsened": nc.value}
+
     STEP_VARIANTS = {1: "1 cell/thread", 2: "2 cells/thread", 3: "TMA-staged persistent pipeline"}
 
     def autotune(self, L: int = 0, reps: int = 5) -> dict:
@@ -193,8 +217,20 @@ class Mesh(Case):
         self.advance()
 
     def M_AdvanceLoop(self, n_iter: Optional[int] = None) -> None:
+        """mesh_advance.cu:381-466 without output: near-wall refinement, then
+        the coarse steps with solution-based refinement every P_REFINE."""
         n = self.params.N_ITER_TOTAL if n_iter is None else n_iter
+        self.M_Advance_RefineNearWall()
         self.advance_n(n, use_graph=True)
+
+    def M_Advance_RefineNearWall(self) -> None:
+        self.refine_near_wall()
+
+    def M_Advance_RefineWithSolution(self) -> None:
+        self.refine_with_solution()
+
+    def M_RefineAndCoarsenBlocks(self) -> None:
+        self.refine_coarsen()
 
 
 class Solver_LBM:
@@ -213,4 +249,16 @@ class Solver_LBM:
 
     def S_Advance(self, i_dev: int, L: int, tmp=None) -> int:
         self.mesh.advance(L)
+        return 0
+
+    def S_Interpolate(self, i_dev: int, L: int, var: int) -> int:
+        self.mesh.interpolate(L, var)
+        return 0
+
+    def S_Average(self, i_dev: int, L: int, var: int) -> int:
+        self.mesh.average(L, var)
+        return 0
+
+    def S_ComputeRefCriteria(self, i_dev: int, L: int, var: int) -> int:
+        self.mesh.ref_criteria()
         return 0

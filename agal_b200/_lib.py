@@ -86,6 +86,13 @@ PROTOS = [
     ("agal_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("agal_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     ("agal_set_tuning", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_interpolate", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("agal_average", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("agal_ref_criteria", C.c_int, [C.c_void_p]),
+    ("agal_refine_coarsen", C.c_int, [C.c_void_p]),
+    ("agal_refine_with_solution", C.c_int, [C.c_void_p]),
+    ("agal_refine_near_wall", C.c_int, [C.c_void_p]),
+    ("agal_refine_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
 ]
 
 _lib = None

@@ -1,0 +1,431 @@
+// Level-interface transfers and the solution-based refinement criterion.
+//
+//   k_interp     coarse-to-fine: the parent's cells (populations rescaled by
+//                tau_{L+1}/tau_L around their equilibrium) interpolated
+//                bilinearly/trilinearly or by tensor-product cubic Lagrange
+//                into the ghost cells of its children (INTERP_INTERFACE) or
+//                into every cell of newly added children (INTERP_ADDED).
+//                Cu_Interpolate_Linear / Cu_Interpolate_Cubic,
+//                solver_lbm_kernels_comm.cu:15-138, 406-640.
+//   k_average    fine-to-coarse: each parent cell the mean of the 2^d child
+//                cells under it, rescaled by tau_L/tau_{L+1}, where the child
+//                group's corner cell qualifies (Cu_Average, :174-347).
+//   k_criterion  velocity-gradient criterion per block (vorticity magnitude or
+//                Q, floor(log2)), block maximum, refine/coarsen marks
+//                (Cu_ComputeRefCriteria, solver_lbm_criterion.cu:440-592).
+//
+// The transfers compute each cell's macros from its populations with the
+// arithmetic of k_refresh, so they equal what the reference reads from the
+// macro rows its S_Interpolate / S_Average refresh just wrote.  One CTA per
+// parent block; NCH x M_CBLOCK threads (one per child cell).
+// Half-precision storage keeps weight offsets g = f - w: both transfers are
+// affine with weights summing to one, so they run on g directly, with the
+// equilibrium difference formed as a small quantity.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "ctx.h"
+#include "lattice.cuh"
+#include "storage.cuh"
+#include "step_common.cuh"
+#include "dispatch.cuh"
+
+namespace agal {
+
+// Macros of one cell with k_refresh's operation order; drho = rho - 1 in the
+// offset form (exact sum of the stored offsets), else rho.
+template <int DIM, int Q, typename T>
+__device__ __forceinline__ void cell_macros(const T *__restrict__ f, typename ST<T>::C &rho, typename ST<T>::C &drho,
+                                            typename ST<T>::C &u, typename ST<T>::C &v, typename ST<T>::C &w)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC;
+    C r = 0, d = 0, x = 0, y = 0, z = 0;
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const C g = ST<T>::dec(f[lat_pb(DIM, p) * MC]);
+        const C fp = g + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        r += fp;
+        d += g;
+        x += C(lat_c(DIM, 0, p)) * fp;
+        y += C(lat_c(DIM, 1, p)) * fp;
+        if (DIM == 3) z += C(lat_c(DIM, 2, p)) * fp;
+    }
+    rho = r;
+    drho = ST<T>::OFF ? d : r;
+    u = x / r;
+    v = y / r;
+    w = (DIM == 3) ? z / r : C(0);
+}
+
+// (feq_p - w_p) in the offset form, feq_p otherwise.
+template <int DIM, int Q, typename C, bool OFF>
+__device__ __forceinline__ C feq_stored(int p, C rho, C drho, C u, C v, C w)
+{
+    const C wp = C(lat_w(Q, p));
+    const C cu = C(lat_c(DIM, 0, p)) * u + C(lat_c(DIM, 1, p)) * v + C(lat_c(DIM, 2, p)) * w;
+    const C usq = u * u + v * v + w * w;
+    const C poly = C(3) * cu + C(4.5) * cu * cu - C(1.5) * usq;
+    if (OFF) return wp * (drho + rho * poly);
+    return wp * rho * (C(1) + poly);
+}
+
+// Lagrange weight of node a (nodes at 0, 1/3, 2/3, 1 of the parent block) at
+// child position m (centres at -1/12 + m/6).
+__host__ __device__ constexpr double lag_w(int a, int m)
+{
+    double x = -1.0 / 12.0 + m / 6.0, r = 1.0;
+    for (int k = 0; k < 4; k++)
+        if (k != a) r *= (x - k / 3.0) / (a / 3.0 - k / 3.0);
+    return r;
+}
+
+struct InterpArgs {
+    const int *ids;
+    int n;
+    const void *fpar;      // level L current buffer
+    void *fch;             // level L+1 current buffer
+    const int *nbr_child;  // row 0: first child
+    const int *bmask, *ref, *cmask;
+    double ratio;          // tau_{L+1} / tau_L in the compute type
+    int var;               // AGAL_INTERP_INTERFACE / AGAL_INTERP_ADDED
+};
+
+template <int DIM, int Q, typename T, bool CUBIC>
+__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const InterpArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
+    constexpr bool OFF = ST<T>::OFF;
+    __shared__ C sF[MC];
+    __shared__ C sW[4][8];
+    // Uniform per CTA: every early return below depends on blockIdx only.
+    const int b = a.ids[blockIdx.x];
+    if (b < 0) return;
+    const bool b1 = a.var == AGAL_INTERP_INTERFACE && a.bmask[b] == BLOCK_INTERFACE;
+    const bool b2 = a.var == AGAL_INTERP_ADDED && a.ref[b] == REF_MARK_REFINE;
+    if (!(b1 || b2)) return;
+    const int bc = a.nbr_child[b];
+    if (bc < 0) return;
+    const int tid = threadIdx.x;
+    if (CUBIC && tid < 32) sW[tid / 8][tid % 8] = C(lag_w(tid / 8, tid % 8));
+    const T *fp = static_cast<const T *>(a.fpar) + (long long)b * BLK;
+    T *fc = static_cast<T *>(a.fch);
+    C rho = 0, drho = 0, u = 0, v = 0, w = 0;
+    if (tid < MC) cell_macros<DIM, Q, T>(fp + tid, rho, drho, u, v, w);
+    const C ratio = C(a.ratio);
+    // Child cell of this thread.
+    const int ch = tid / MC, t = tid % MC;
+    const int ci = ch & 1, cj = (ch >> 1) & 1, ck = (ch >> 2) & 1;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const long long cell = (long long)(bc + ch) * BLK + t;
+    const bool write = a.var == AGAL_INTERP_ADDED || a.cmask[(long long)(bc + ch) * MC + t] == CELL_GHOST;
+    for (int p = 0; p < Q; p++) {
+        const int slot = lat_pb(DIM, p);
+        if (tid < MC) {
+            const C g = ST<T>::dec(fp[slot * MC + tid]);
+            const C e = feq_stored<DIM, Q, C, OFF>(p, rho, drho, u, v, w);
+            sF[tid] = e + (g - e) * ratio;
+        }
+        __syncthreads();
+        if (write) {
+            C val;
+            if (!CUBIC) {
+                const int s = 2 * ci + 8 * cj + 32 * ck;
+                const C x = C(-0.25) + C(0.5) * C(I), y = C(-0.25) + C(0.5) * C(J);
+                if (DIM == 2) {
+                    val = sF[s] + (sF[1 + s] - sF[s]) * x + (sF[4 + s] - sF[s]) * y +
+                          (sF[5 + s] - sF[4 + s] - sF[1 + s] + sF[s]) * x * y;
+                } else {
+                    const C z = C(-0.25) + C(0.5) * C(K);
+                    val = sF[s] + (sF[1 + s] - sF[s]) * x + (sF[4 + s] - sF[s]) * y + (sF[16 + s] - sF[s]) * z +
+                          (sF[5 + s] - sF[1 + s] - sF[4 + s] + sF[s]) * x * y +
+                          (sF[17 + s] - sF[1 + s] - sF[16 + s] + sF[s]) * x * z +
+                          (sF[20 + s] - sF[4 + s] - sF[16 + s] + sF[s]) * y * z +
+                          (sF[21 + s] + sF[1 + s] + sF[4 + s] + sF[16 + s] - sF[5 + s] - sF[17 + s] - sF[20 + s] -
+                           sF[s]) * x * y * z;
+                }
+            } else {
+                const int mx = I + 4 * ci, my = J + 4 * cj, mz = K + 4 * ck;
+                val = C(0);
+                if (DIM == 2) {
+#pragma unroll
+                    for (int bj = 0; bj < 4; bj++) {
+                        C row = C(0);
+#pragma unroll
+                        for (int ai = 0; ai < 4; ai++) row += sW[ai][mx] * sF[ai + 4 * bj];
+                        val += sW[bj][my] * row;
+                    }
+                } else {
+#pragma unroll
+                    for (int ck2 = 0; ck2 < 4; ck2++) {
+                        C pl = C(0);
+#pragma unroll
+                        for (int bj = 0; bj < 4; bj++) {
+                            C row = C(0);
+#pragma unroll
+                            for (int ai = 0; ai < 4; ai++) row += sW[ai][mx] * sF[ai + 4 * bj + 16 * ck2];
+                            pl += sW[bj][my] * row;
+                        }
+                        val += sW[ck2][mz] * pl;
+                    }
+                }
+            }
+            fc[cell + slot * MC] = ST<T>::enc(val);
+        }
+        __syncthreads();
+    }
+}
+
+struct AverageArgs {
+    const int *ids;
+    int n;
+    void *fpar;            // level L current buffer
+    const void *fch;       // level L+1 current buffer
+    const int *nbr_child, *bmask, *cmask;
+    double ratio;          // tau_L / tau_{L+1} in the compute type
+    int var;               // AGAL_AVERAGE_INTERFACE / _BLOCK / _GRID
+};
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const AverageArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, NCH = Geo<DIM>::NCH, BLK = Q * MC;
+    constexpr bool OFF = ST<T>::OFF;
+    __shared__ C sg[NCH * MC];
+    __shared__ int smask[NCH * MC];
+    const int b = a.ids[blockIdx.x];
+    if (b < 0) return;
+    const int bc = a.nbr_child[b];
+    if (!(bc > -1 && (a.var == AGAL_AVERAGE_GRID || a.bmask[b] == BLOCK_INTERFACE))) return;
+    const int tid = threadIdx.x;
+    const T *fc = static_cast<const T *>(a.fch) + (long long)bc * BLK;   // children are consecutive IDs
+    const int ch = tid / MC, t = tid % MC;
+    const T *own = fc + (long long)ch * BLK + t;
+    C rho, drho, u, v, w;
+    cell_macros<DIM, Q, T>(own, rho, drho, u, v, w);
+    int m = a.cmask[(long long)(bc + ch) * MC + t];
+    if (a.var > 0 && m < 2) m = 1;
+    smask[tid] = m;
+    const C ratio = C(a.ratio);
+    // Parent cell of this thread (tid < MC): its quadrant and the corner cell
+    // of the 2^d child cells under it.
+    const int I = tid & 3, J = (tid >> 2) & 3, K = (DIM == 3) ? ((tid >> 4) & 3) : 0;
+    const int qd = (I >= 2 ? 1 : 0) + (J >= 2 ? 2 : 0) + ((DIM == 3 && K >= 2) ? 4 : 0);
+    const int c0 = 2 * (I & 1) + 8 * (J & 1) + (DIM == 3 ? 32 * (K & 1) : 0);
+    T *fp = static_cast<T *>(a.fpar) + (long long)b * BLK + tid;
+    for (int p = 0; p < Q; p++) {
+        const int slot = lat_pb(DIM, p);
+        {
+            const C g = ST<T>::dec(own[slot * MC]);
+            const C e = feq_stored<DIM, Q, C, OFF>(p, rho, drho, u, v, w);
+            sg[tid] = e + (g - e) * ratio;
+        }
+        __syncthreads();
+        if (tid < MC && smask[qd * MC + c0] == 1) {
+            const C *s = sg + qd * MC + c0;
+            C val;
+            if (DIM == 2) val = C(0.25) * (s[0] + s[1] + s[4] + s[5]);
+            else val = C(0.125) * (s[0] + s[1] + s[4] + s[5] + s[16] + s[17] + s[20] + s[21]);
+            fp[slot * MC] = ST<T>::enc(val);
+        }
+        __syncthreads();
+    }
+}
+
+struct CriterionArgs {
+    int idm;
+    long long nmb, nmc;
+    const void *macro;     // [dim+1][n_maxcells] of the compute type
+    const int *cmask, *level, *nbr;
+    int *ref;
+    double dx;             // level-0 spacing (the reference passes dxf_vec[0])
+    int criterion;         // S_CRITERION: 0 vorticity magnitude, 1 Q
+    double nrs, nri, nrm;  // N_REFINE_START / _INC / _MAX
+    int mli;               // MAX_LEVELS_INTERIOR
+};
+
+// Fourth-order extrapolation to the one-cell halo (util_math.h:26-116).
+template <typename C>
+__device__ __forceinline__ C extrap4(C a, C b, C c, C d)
+{
+    return C(4) * a + C(-6) * b + C(4) * c + C(-1) * d;
+}
+
+template <int DIM>
+__device__ __forceinline__ int halo_ix(int i, int j, int k)
+{
+    return (i + 1) + 6 * (j + 1) + (DIM == 3 ? 36 * (k + 1) : 0);
+}
+
+template <int DIM, typename C>
+__global__ void __launch_bounds__(Geo<DIM>::MC) k_criterion(const CriterionArgs a)
+{
+    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, H = (DIM == 2) ? 36 : 216;
+    __shared__ C s[DIM][H];
+    __shared__ C sW[MC];
+    const int b = blockIdx.x;
+    if (a.ref[b] == REF_INACTIVE) return;   // uniform per CTA
+    const int t = threadIdx.x;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const C *m = static_cast<const C *>(a.macro);
+    const long long cell = (long long)b * MC + t;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) s[d][halo_ix<DIM>(I, J, K)] = m[(long long)(1 + d) * a.nmc + cell];
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        C *q = s[d];
+        if (I == 0) {
+            q[halo_ix<DIM>(-1, J, K)] = extrap4(q[halo_ix<DIM>(0, J, K)], q[halo_ix<DIM>(1, J, K)],
+                                                q[halo_ix<DIM>(2, J, K)], q[halo_ix<DIM>(3, J, K)]);
+            q[halo_ix<DIM>(4, J, K)] = extrap4(q[halo_ix<DIM>(3, J, K)], q[halo_ix<DIM>(2, J, K)],
+                                               q[halo_ix<DIM>(1, J, K)], q[halo_ix<DIM>(0, J, K)]);
+        }
+        if (J == 0) {
+            q[halo_ix<DIM>(I, -1, K)] = extrap4(q[halo_ix<DIM>(I, 0, K)], q[halo_ix<DIM>(I, 1, K)],
+                                                q[halo_ix<DIM>(I, 2, K)], q[halo_ix<DIM>(I, 3, K)]);
+            q[halo_ix<DIM>(I, 4, K)] = extrap4(q[halo_ix<DIM>(I, 3, K)], q[halo_ix<DIM>(I, 2, K)],
+                                               q[halo_ix<DIM>(I, 1, K)], q[halo_ix<DIM>(I, 0, K)]);
+        }
+        if (DIM == 3 && K == 0) {
+            q[halo_ix<DIM>(I, J, -1)] = extrap4(q[halo_ix<DIM>(I, J, 0)], q[halo_ix<DIM>(I, J, 1)],
+                                                q[halo_ix<DIM>(I, J, 2)], q[halo_ix<DIM>(I, J, 3)]);
+            q[halo_ix<DIM>(I, J, 4)] = extrap4(q[halo_ix<DIM>(I, J, 3)], q[halo_ix<DIM>(I, J, 2)],
+                                               q[halo_ix<DIM>(I, J, 1)], q[halo_ix<DIM>(I, J, 0)]);
+        }
+    }
+    __syncthreads();
+    C g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // g[component][axis]
+    const C dxL = C(a.dx);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const C *q = s[d];
+        const C ex = q[halo_ix<DIM>(I + 1, J, K)] - q[halo_ix<DIM>(I - 1, J, K)];
+        const C ey = q[halo_ix<DIM>(I, J + 1, K)] - q[halo_ix<DIM>(I, J - 1, K)];
+        if (DIM == 2) {
+            // the 2D kernel divides by the double 2.0*dx_L (criterion.cu:502-505)
+            g[d][0] = C((double)ex / (2.0 * (double)dxL));
+            g[d][1] = C((double)ey / (2.0 * (double)dxL));
+        } else {
+            const C ez = q[halo_ix<DIM>(I, J, K + 1)] - q[halo_ix<DIM>(I, J, K - 1)];
+            g[d][0] = ex / (C(2) * dxL);
+            g[d][1] = ey / (C(2) * dxL);
+            g[d][2] = ez / (C(2) * dxL);
+        }
+    }
+    const C uX = g[0][0], uY = g[0][1], uZ = g[0][2], vX = g[1][0], vY = g[1][1], vZ = g[1][2];
+    const C wX = g[2][0], wY = g[2][1], wZ = g[2][2];
+    C W = C(0);
+    if (a.criterion == 0) W = floor(log2(sqrt((wY - vZ) * (wY - vZ) + (uZ - wX) * (uZ - wX) + (vX - uY) * (vX - uY))));
+    if (a.criterion == 1)
+        W = floor(log2(fabs(C(0.5) * (uX * uX + vY * vY + wZ * wZ + C(2) * (uY * vX + uZ * wX + wY * vZ)))));
+    if (a.cmask[cell] == CELL_GHOST) W = C(0);
+    sW[t] = W;
+    __syncthreads();
+    for (int st = MC / 2; st > 0; st >>= 1) {
+        if (t < st) sW[t] = fmax(sW[t], sW[t + st]);
+        __syncthreads();
+    }
+    if (t == 0) {
+        C Wm = sW[0];
+        if (Wm > C(a.nrm)) Wm = C(a.nrm);
+        const int rk = a.ref[b], lk = a.level[b];
+        int Ld = a.mli - 1;
+        for (int p = 1; p <= a.mli - 1; p++)
+            if (Wm < C(a.nrs) - C(a.nri) * C(p)) Ld = (a.mli - 1) - p;
+        bool eligible = true;
+        for (int p = 0; p < QMAX; p++)
+            if (a.nbr[b + (long long)p * a.nmb] == N_SKIPID) eligible = false;
+        if (eligible && lk != a.mli - 1 && rk == REF_UNREFINED && Ld > lk) a.ref[b] = REF_MARK_REFINE;
+        if (rk == REF_REFINED && Ld < lk + 1) a.ref[b] = REF_MARK_COARSEN;
+    }
+}
+
+template <int DIM, int Q, typename T> struct RunInterp {
+    static int run(agal_ctx *c, int L, int var)
+    {
+        const int n = c->n_ids[L];
+        if (n <= 0) return AGAL_OK;
+        InterpArgs a;
+        a.ids = c->id_set + (long long)L * c->nmb;
+        a.n = n;
+        a.fpar = c->F[c->cur[L]];
+        a.fch = c->F[c->cur[L + 1]];
+        a.nbr_child = c->cblock_ID_nbr_child;
+        a.bmask = c->cblock_ID_mask;
+        a.ref = c->cblock_ID_ref;
+        a.cmask = c->cells_ID_mask;
+        a.ratio = c->tau[L + 1] / c->tau[L];
+        if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L + 1] / (float)c->tau[L]);
+        a.var = var;
+        constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
+        if (c->P.interp_order == AGAL_INTERP_CUBIC)
+            k_interp<DIM, Q, T, true><<<(unsigned)n, NT, 0, c->stream>>>(a);
+        else
+            k_interp<DIM, Q, T, false><<<(unsigned)n, NT, 0, c->stream>>>(a);
+        AGAL_CUDA(c, cudaGetLastError());
+        return AGAL_OK;
+    }
+};
+
+template <int DIM, int Q, typename T> struct RunAverage {
+    static int run(agal_ctx *c, int L, int var)
+    {
+        const int n = c->n_ids[L];
+        if (n <= 0) return AGAL_OK;
+        AverageArgs a;
+        a.ids = c->id_set + (long long)L * c->nmb;
+        a.n = n;
+        a.fpar = c->F[c->cur[L]];
+        a.fch = c->F[c->cur[L + 1]];
+        a.nbr_child = c->cblock_ID_nbr_child;
+        a.bmask = c->cblock_ID_mask;
+        a.cmask = c->cells_ID_mask;
+        a.ratio = c->tau[L] / c->tau[L + 1];
+        if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L] / (float)c->tau[L + 1]);
+        a.var = var;
+        constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
+        k_average<DIM, Q, T><<<(unsigned)n, NT, 0, c->stream>>>(a);
+        AGAL_CUDA(c, cudaGetLastError());
+        return AGAL_OK;
+    }
+};
+
+}  // namespace agal
+
+int agal_launch_interp(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunInterp>(c, L, var); }
+int agal_launch_average(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunAverage>(c, L, var); }
+
+int agal_launch_criterion(agal_ctx *c)
+{
+    const int idm = c->id_max[c->max_levels];
+    if (idm <= 0) return AGAL_OK;
+    agal::CriterionArgs a;
+    a.idm = idm;
+    a.nmb = c->nmb;
+    a.nmc = c->nmc;
+    a.macro = c->macro;
+    a.cmask = c->cells_ID_mask;
+    a.level = c->cblock_level;
+    a.nbr = c->cblock_ID_nbr;
+    a.ref = c->cblock_ID_ref;
+    a.dx = c->dxf[0];
+    a.criterion = c->P.S_CRITERION;
+    a.nrs = c->P.N_REFINE_START;
+    a.nri = c->P.N_REFINE_INC;
+    a.nrm = c->P.N_REFINE_MAX;
+    a.mli = c->P.MAX_LEVELS_INTERIOR;
+    const bool f64 = c->storage == AGAL_STORE_FP64;
+    if (c->dim == 2) {
+        if (f64) agal::k_criterion<2, double><<<(unsigned)idm, 16, 0, c->stream>>>(a);
+        else agal::k_criterion<2, float><<<(unsigned)idm, 16, 0, c->stream>>>(a);
+    } else {
+        if (f64) agal::k_criterion<3, double><<<(unsigned)idm, 64, 0, c->stream>>>(a);
+        else agal::k_criterion<3, float><<<(unsigned)idm, 64, 0, c->stream>>>(a);
+    }
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}

@@ -69,12 +69,28 @@ int fill(agal_ctx *c, T *p, long long n, T v)
 
 size_t compute_size(const agal_ctx *c) { return c->storage == AGAL_STORE_FP64 ? 8 : 4; }
 
-void release(agal_ctx *c)
+}  // namespace
+
+void agal_drop_graphs(agal_ctx *c)
 {
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+    for (int k = 0; k < 2; k++) {
+        if (c->ml_graph[k]) cudaGraphExecDestroy(c->ml_graph[k]);
+        c->ml_graph[k] = nullptr;
+        c->ml_graph_cur[k].clear();
+    }
+}
+
+namespace {
+
+void release(agal_ctx *c)
+{
+    agal_drop_graphs(c);
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
-                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta};
+                    c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
+                    c->amr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -159,7 +175,8 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     // Capacity: explicit, or from free memory like mesh_init.cu:155-169.
     const size_t per_block =
         (size_t)c->MC * (2 * c->Q * c->esize + (c->dim + 1) * compute_size(c) + sizeof(int)) +
-        sizeof(float) * c->dim + sizeof(int) * (2 * c->Qmax + 5 + c->max_levels);
+        sizeof(float) * c->dim + sizeof(int) * (2 * c->Qmax + 5 + c->max_levels) +
+        (c->max_levels > 1 ? 5 * sizeof(int) : 0);
     if (p->n_maxcblocks > 0) {
         c->nmb = p->n_maxcblocks;
     } else {
@@ -203,6 +220,17 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->red_out, sizeof(double) * 4);
     ALLOC(c->d_status, sizeof(int) * 4);
     ALLOC(c->meta, sizeof(int) * (size_t)(c->dim == 2 ? 12 : 28) * nmb);
+    if (c->max_levels > 1) {
+        const size_t na = agal_amr_scratch_ints(nmb);
+        ALLOC(c->amr, sizeof(int) * na);
+        c->amr_emap = c->amr;
+        c->amr_first = c->amr + nmb;
+        c->amr_a = c->amr + 2 * nmb;
+        c->amr_b = c->amr + 3 * nmb;
+        c->amr_snap = c->amr + 4 * nmb;
+        c->amr_parts = c->amr + 5 * nmb;
+        c->amr_small = c->amr + na - AGAL_AMR_SMALL;
+    }
 #undef ALLOC
     cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);
 
@@ -217,7 +245,8 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         // allocates them and fills only the live prefix); the refinement
         // pass reads slot 0 of an empty level as its id_max.
         (rc = fill<int>(c, c->id_set, c->max_levels * nmb, 0)) || (rc = fill<int>(c, c->gap_set, nmb, 0)) ||
-        (rc = fill<float>(c, c->cblock_f_X, c->dim * nmb, 0.0f))) {
+        (rc = fill<float>(c, c->cblock_f_X, c->dim * nmb, 0.0f)) ||
+        (c->amr && (rc = fill<int>(c, c->amr, 2 * nmb, -1)))) {
         std::string m = c->err;
         release(c);
         delete c;
@@ -334,7 +363,7 @@ extern "C" int agal_get_stream(const agal_ctx *c, void **stream)
 extern "C" int agal_autotune(agal_ctx *c, int L, int reps, float *ms, int *cells_per_thread)
 {
     if (!c || L < 0 || L >= c->max_levels || reps <= 0) return AGAL_ERR_PARAM;
-    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }   // launch shape changes
+    agal_drop_graphs(c);   // launch shape changes
     int rc = agal_launch_tune(c, L, reps, ms);
     if (rc) return rc;
     if (cells_per_thread) *cells_per_thread = c->step_cpt;
@@ -344,7 +373,7 @@ extern "C" int agal_autotune(agal_ctx *c, int L, int reps, float *ms, int *cells
 extern "C" int agal_set_tuning(agal_ctx *c, int cells_per_thread)
 {
     if (!c || cells_per_thread < 1 || cells_per_thread > AGAL_STEP_VARIANTS) return AGAL_ERR_PARAM;
-    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    agal_drop_graphs(c);
     int rc = agal_prepare_step(c);
     if (rc) return rc;
     c->step_cpt = cells_per_thread;
@@ -370,52 +399,218 @@ extern "C" int agal_mass_momentum(agal_ctx *c, double *out)
 }
 
 // ---------------------------------------------------------------------------
-// Advance (solver_lbm_advance.cu:31-174).  The single-level branch
-// (:239-251) is one fused kernel per step.
-static int advance_level(agal_ctx *c, int L)
+// Level-interface transfers with the refresh the reference's S_Interpolate /
+// S_Average perform first (solver_lbm_kernels_comm.cu:141-155, 351-370), so
+// the macro array ends up as the reference's macro rows do.
+extern "C" int agal_interpolate(agal_ctx *c, int L, int var)
 {
-    if (c->max_levels > 1 && c->max_levels != c->L0 + 1)
-        return agal_set_err(c, AGAL_ERR_UNSUPPORTED, "multi-level advance not built yet");
-    return agal_launch_step(c, L);
+    if (!c || L < 0 || L >= c->max_levels - 1) return AGAL_ERR_PARAM;
+    if (var != AGAL_INTERP_INTERFACE && var != AGAL_INTERP_ADDED) return AGAL_ERR_PARAM;
+    int rc = agal_launch_refresh(c, L);
+    return rc ? rc : agal_launch_interp(c, L, var);
+}
+
+extern "C" int agal_average(agal_ctx *c, int L, int var)
+{
+    if (!c || L < 0 || L >= c->max_levels - 1) return AGAL_ERR_PARAM;
+    if (var < AGAL_AVERAGE_INTERFACE || var > AGAL_AVERAGE_GRID) return AGAL_ERR_PARAM;
+    int rc = agal_launch_refresh(c, L + 1);
+    return rc ? rc : agal_launch_average(c, L, var);
+}
+
+extern "C" int agal_ref_criteria(agal_ctx *c)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    return agal_launch_criterion(c);
+}
+
+extern "C" int agal_refine_coarsen(agal_ctx *c)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    int rc = agal_refine_pass(c);
+    if (rc) return rc;
+    if (c->n_ref_last || c->n_coarse_last) agal_drop_graphs(c);   // launch sizes changed
+    return AGAL_OK;
+}
+
+// Mesh::M_Advance_RefineWithSolution (mesh_advance.cu:185-243).
+extern "C" int agal_refine_with_solution(agal_ctx *c)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    const int ML = c->max_levels;
+    int rc;
+    if (!(c->P.MAX_LEVELS_INTERIOR > 1 && c->P.N_PROBE_AVE == 0)) return AGAL_OK;
+    for (int L = ML - 2; L >= c->L0; L--)
+        if ((rc = agal_average(c, L, AGAL_AVERAGE_GRID))) return rc;
+    for (int L = c->L0; L < ML - 1; L++)
+        if ((rc = agal_interpolate(c, L, AGAL_INTERP_INTERFACE))) return rc;
+    if ((rc = agal_launch_criterion(c))) return rc;
+    return agal_refine_coarsen(c);
+}
+
+// Mesh::M_Advance_RefineNearWall without geometry (mesh_advance.cu:54-122).
+extern "C" int agal_refine_near_wall(agal_ctx *c)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    const int ML = c->max_levels, MLW = c->P.MAX_LEVELS_WALL;
+    int rc;
+    for (int L = 0; L < c->L0; L++) {
+        if ((rc = agal_mark_level(c, L, 1))) return rc;
+        if ((rc = agal_refine_coarsen(c))) return rc;
+    }
+    for (int L = c->L0; L < MLW; L++) {
+        if (L < MLW - 1 && (rc = agal_mark_level(c, L, 0))) return rc;
+        if (ML > 1 && L < MLW - 1 && (rc = agal_refine_coarsen(c))) return rc;
+        if ((rc = agal_launch_set_ic(c, L))) return rc;
+    }
+    if (ML > 1 && (rc = agal_freeze_refined(c))) return rc;
+    return AGAL_OK;
+}
+
+extern "C" int agal_refine_stats(const agal_ctx *c, long long *iter, int *n_refined, int *n_coarsened)
+{
+    if (!c) return AGAL_ERR_PARAM;
+    if (iter) *iter = c->iter;
+    if (n_refined) *n_refined = c->n_ref_last;
+    if (n_coarsened) *n_coarsened = c->n_coarse_last;
+    return AGAL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Advance (solver_lbm_advance.cu:31-174).  Each sub-step of a level is one
+// fused collide + boundary + stream kernel; each transfer between levels is
+// one kernel.
+static bool multi_level(const agal_ctx *c) { return c->max_levels > 1 && c->max_levels != c->L0 + 1; }
+
+static int avg_mode(const agal_ctx *c)
+{
+    // solver_lbm_init.cu:94-97
+    return (c->P.interp_order != AGAL_INTERP_LINEAR) ? AGAL_AVERAGE_BLOCK : AGAL_AVERAGE_INTERFACE;
+}
+
+static int advance_rec(agal_ctx *c, int L)
+{
+    const int ML = c->max_levels;
+    int rc;
+    if (!multi_level(c)) return agal_launch_step(c, L);   // :239-251
+    if (L == c->L0) {                                       // :39-58
+        if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
+        if ((rc = agal_launch_step(c, L))) return rc;
+        if ((rc = advance_rec(c, L + 1))) return rc;
+        return agal_launch_average(c, L, avg_mode(c));
+    }
+    if (L < ML - 1 && (rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;   // :96-99
+    if ((rc = agal_launch_step(c, L))) return rc;
+    if (L < ML - 1) {                                                                       // :106-111
+        if ((rc = advance_rec(c, L + 1))) return rc;
+        if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
+        if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
+    }
+    if ((rc = agal_launch_step(c, L))) return rc;                                           // :114-126
+    if (L < ML - 1) {                                                                       // :130-134
+        if ((rc = advance_rec(c, L + 1))) return rc;
+        if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
+    }
+    return AGAL_OK;
 }
 
 extern "C" int agal_advance(agal_ctx *c, int L)
 {
     if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;
-    return advance_level(c, L);
+    return advance_rec(c, L);
 }
 
+// One coarse step of M_Advance_Step (mesh_advance.cu:156-182): 2^N_LEVEL_START
+// sub-steps from the starting level.
+static int coarse_step(agal_ctx *c)
+{
+    const int mult = 1 << c->L0;
+    for (int j = 0; j < mult; j++) {
+        int rc = advance_rec(c, c->L0);
+        if (rc) return rc;
+    }
+    return AGAL_OK;
+}
+
+static int capture(agal_ctx *c, int steps, cudaGraphExec_t *out)
+{
+    std::vector<int> cur0 = c->cur;
+    cudaGraph_t g = nullptr;
+    AGAL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = AGAL_OK;
+    for (int i = 0; i < steps && rc == AGAL_OK; i++) rc = coarse_step(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->cur = cur0;   // the capture only recorded the launches
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGraphInstantiate");
+    return AGAL_OK;
+}
+
+// Buffer parity after `steps` coarse steps.  Per coarse step the starting
+// level L0 takes 2^L0 sub-steps and each finer level twice its parent's count
+// (multi-level), or only L0 is stepped (single level); levels stepped an odd
+// number of times flip.
+static void advance_parity(agal_ctx *c, int steps)
+{
+    for (int L = 0; L < c->max_levels; L++) {
+        long long k = 0;
+        if (multi_level(c)) {
+            if (L >= c->L0) k = (1LL << c->L0) << (L - c->L0);
+        } else if (L == c->L0) {
+            k = 1LL << c->L0;
+        }
+        if ((k * steps) & 1) c->cur[L] = 1 - c->cur[L];
+    }
+}
+
+// n coarse steps of the M_AdvanceLoop body (mesh_advance.cu:421-463): a coarse
+// step, then every P_REFINE steps the solution-based refinement.  use_graph
+// replays a captured coarse step (captured once per mesh and buffer parity).
 extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
 {
     if (!c || n < 0) return AGAL_ERR_PARAM;
-    if (!use_graph) {
-        for (int i = 0; i < n; i++) {
-            int rc = advance_level(c, c->L0);
-            if (rc) return rc;
+    int rc;
+    if (!multi_level(c)) {
+        if (!use_graph) {
+            for (int i = 0; i < n; i++)
+                if ((rc = coarse_step(c))) return rc;
+        } else if (n > 0) {
+            if (!c->graph_exec || c->graph_steps != n || c->graph_cur_in != c->cur) {
+                if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+                if ((rc = capture(c, n, &c->graph_exec))) return rc;
+                c->graph_steps = n;
+                c->graph_cur_in = c->cur;
+            }
+            AGAL_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+            advance_parity(c, n);
         }
+        c->iter += n;
         return AGAL_OK;
     }
-    // Capture n steps once; replay while the captured buffer parity matches.
-    if (!c->graph_exec || c->graph_steps != n || c->graph_cur_in != c->cur) {
-        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
-        std::vector<int> cur0 = c->cur;
-        cudaGraph_t g = nullptr;
-        AGAL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = AGAL_OK;
-        for (int i = 0; i < n && rc == AGAL_OK; i++) rc = advance_level(c, c->L0);
-        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-        c->cur = cur0;   // capture only recorded the launches
-        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-        if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaStreamEndCapture");
-        e = cudaGraphInstantiate(&c->graph_exec, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGraphInstantiate");
-        c->graph_steps = n;
-        c->graph_cur_in = cur0;
+    for (int s = 0; s < n; s++) {
+        if (!use_graph) {
+            if ((rc = coarse_step(c))) return rc;
+        } else {
+            int k = (c->ml_graph[0] && c->ml_graph_cur[0] == c->cur)   ? 0
+                    : (c->ml_graph[1] && c->ml_graph_cur[1] == c->cur) ? 1
+                                                                       : -1;
+            if (k < 0) {
+                k = c->ml_graph[0] ? 1 : 0;
+                if (c->ml_graph[k]) { cudaGraphExecDestroy(c->ml_graph[k]); c->ml_graph[k] = nullptr; }
+                if ((rc = capture(c, 1, &c->ml_graph[k]))) return rc;
+                c->ml_graph_cur[k] = c->cur;
+            }
+            AGAL_CUDA(c, cudaGraphLaunch(c->ml_graph[k], c->stream));
+            advance_parity(c, 1);
+        }
+        const long long i = c->iter;
+        if (c->P.P_REFINE > 0 && (i + 1) % c->P.P_REFINE == 0 && i > 0 && (rc = agal_refine_with_solution(c)))
+            return rc;
+        c->iter++;
     }
-    AGAL_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
-    for (int L = 0; L < c->max_levels; L++)
-        if (n & 1) c->cur[L] = 1 - c->cur[L];   // single-level: every level stepped n times
     return AGAL_OK;
 }
 

@@ -57,12 +57,25 @@ struct agal_ctx {
     int device = 0;
     // graph of n coarse steps (agal_advance_n)
     cudaGraphExec_t graph_exec = nullptr;
+    // multi-level: graphs of one coarse step, keyed on cur[] at entry (the
+    // coarse level's parity alternates, the finer levels' returns)
+    cudaGraphExec_t ml_graph[2] = {nullptr, nullptr};
+    std::vector<int> ml_graph_cur[2];
     int graph_steps = 0;
     std::vector<int> graph_cur_in;     // cur[] the graph was captured with
     int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
+    // refine/coarsen pass scratch (multi-level cases only), one allocation:
+    int *amr = nullptr;
+    int *amr_emap = nullptr;           // efficient map (mesh_amr.cu c_tmp_8), -1 = absent
+    int *amr_first = nullptr;          // first-child ID of each marked block, -1 = none
+    int *amr_a = nullptr, *amr_b = nullptr, *amr_snap = nullptr;   // compaction / snapshot buffers
+    int *amr_parts = nullptr;          // per-CTA partial counts of the compactions
+    int *amr_small = nullptr;          // small counters read back by the host
+    long long iter = 0;                // coarse steps taken (M_AdvanceLoop counter i)
+    int n_ref_last = 0, n_coarse_last = 0;   // marks acted on by the last refinement pass
     std::string err;
 };
 
@@ -87,3 +100,13 @@ int agal_prepare_step(agal_ctx *c);
 int agal_build_meta(agal_ctx *c);   // after any change of the block arrays
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);
+// Multi-level path (amr_kernels.cu, amr_pass.cu).
+int agal_launch_interp(agal_ctx *c, int L, int var);
+int agal_launch_average(agal_ctx *c, int L, int var);
+int agal_launch_criterion(agal_ctx *c);
+int agal_refine_pass(agal_ctx *c);          // Mesh::M_RefineAndCoarsenBlocks
+int agal_mark_level(agal_ctx *c, int L, int uniform);
+int agal_freeze_refined(agal_ctx *c);
+size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
+#define AGAL_AMR_SMALL 128
+void agal_drop_graphs(agal_ctx *c);         // after any change of the mesh or launch shapes

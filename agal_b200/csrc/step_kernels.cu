@@ -30,6 +30,7 @@
 #include "lattice.cuh"
 #include "storage.cuh"
 #include "step_common.cuh"
+#include "dispatch.cuh"
 
 namespace agal {
 
@@ -276,38 +277,6 @@ __global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child
     meta[g] = v;
 }
 
-// Dispatch on (velocity set, storage type).
-template <template <int, int, typename> class Fn, typename... Args>
-int dispatch(agal_ctx *c, Args... args)
-{
-    switch (c->Q) {
-    case 9:
-        switch (c->storage) {
-        case AGAL_STORE_FP32: return Fn<2, 9, float>::run(c, args...);
-        case AGAL_STORE_FP64: return Fn<2, 9, double>::run(c, args...);
-        case AGAL_STORE_FP16: return Fn<2, 9, __half>::run(c, args...);
-        case AGAL_STORE_BF16: return Fn<2, 9, __nv_bfloat16>::run(c, args...);
-        }
-        break;
-    case 19:
-        switch (c->storage) {
-        case AGAL_STORE_FP32: return Fn<3, 19, float>::run(c, args...);
-        case AGAL_STORE_FP64: return Fn<3, 19, double>::run(c, args...);
-        case AGAL_STORE_FP16: return Fn<3, 19, __half>::run(c, args...);
-        case AGAL_STORE_BF16: return Fn<3, 19, __nv_bfloat16>::run(c, args...);
-        }
-        break;
-    case 27:
-        switch (c->storage) {
-        case AGAL_STORE_FP32: return Fn<3, 27, float>::run(c, args...);
-        case AGAL_STORE_FP64: return Fn<3, 27, double>::run(c, args...);
-        case AGAL_STORE_FP16: return Fn<3, 27, __half>::run(c, args...);
-        case AGAL_STORE_BF16: return Fn<3, 27, __nv_bfloat16>::run(c, args...);
-        }
-        break;
-    }
-    return agal_set_err(c, AGAL_ERR_UNSUPPORTED, "velocity set / storage combination not built");
-}
 
 // TMA-staged persistent variant (step_tma.cu).
 template <int DIM, int Q, typename T>
@@ -339,7 +308,10 @@ template <int DIM, int Q, typename T> struct RunStep {
     static int run(agal_ctx *c, int L, int cpt = 0, bool flip = true)
     {
         const int n = c->n_ids[L];
-        if (n <= 0) return AGAL_OK;
+        if (n <= 0) {
+            if (flip) c->cur[L] = 1 - c->cur[L];   // an empty level keeps the parity bookkeeping
+            return AGAL_OK;
+        }
         StepArgs a;
         a.ids = c->id_set + (long long)L * c->nmb;
         a.n = n;

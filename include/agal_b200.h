@@ -165,9 +165,40 @@ int agal_refresh(agal_ctx *ctx, int L);
    level L and, recursively, of every finer level.  L = N_LEVEL_START is one
    coarse step. */
 int agal_advance(agal_ctx *ctx, int L);
-/* n coarse steps; with use_graph != 0 the steps are captured once into a CUDA
-   graph and replayed (same kernels, no per-step host work). */
+/* n coarse steps of the M_AdvanceLoop body (mesh_advance.cu:421-463): each a
+   2^N_LEVEL_START-fold S_Advance from N_LEVEL_START, then, on a multi-level
+   mesh, the solution-based refinement every P_REFINE steps (counted over the
+   context's life).  With use_graph != 0 a coarse step is captured once per
+   mesh and buffer parity into a CUDA graph and replayed (same kernels). */
 int agal_advance_n(agal_ctx *ctx, int n, int use_graph);
+
+/* ---- multi-level mesh ------------------------------------------------------ */
+/* Solver_LBM::S_Interpolate (solver_lbm_kernels_comm.cu:141-155, 642-658):
+   refresh the macros of level L, then interpolate from level L into the ghost
+   cells of its children (AGAL_INTERP_INTERFACE) or into every cell of the
+   children of blocks marked for refinement (AGAL_INTERP_ADDED). */
+int agal_interpolate(agal_ctx *ctx, int L, int var);
+/* Solver_LBM::S_Average (solver_lbm_kernels_comm.cu:351-370): refresh level
+   L+1, then average it into level L (AGAL_AVERAGE_INTERFACE/_BLOCK/_GRID). */
+int agal_average(agal_ctx *ctx, int L, int var);
+/* Solver_LBM::S_ComputeRefCriteria (solver_lbm_criterion.cu:595-613): marks
+   blocks for refinement/coarsening from the macros of the last refresh
+   (S_CRITERION, N_REFINE_START/_INC/_MAX, MAX_LEVELS_INTERIOR). */
+int agal_ref_criteria(agal_ctx *ctx);
+/* Mesh::M_RefineAndCoarsenBlocks (mesh_amr.cu:2162-2744): acts on the marks;
+   block IDs from the gap stack, ID sets, neighbour lists, masks rebuilt. */
+int agal_refine_coarsen(agal_ctx *ctx);
+/* Mesh::M_Advance_RefineWithSolution (mesh_advance.cu:185-243): grid
+   average, interface interpolation, criterion, refine/coarsen. */
+int agal_refine_with_solution(agal_ctx *ctx);
+/* Mesh::M_Advance_RefineNearWall (mesh_advance.cu:54-122) without geometry:
+   uniform refinement to N_LEVEL_START, Cu_RefineRegion marks (region_preset)
+   up to MAX_LEVELS_WALL with S_SetIC per level, refined blocks frozen. */
+int agal_refine_near_wall(agal_ctx *ctx);
+/* Coarse steps taken by agal_advance_n and the number of blocks refined /
+   coarsened by the last refine/coarsen pass (mesh_amr.cu:2714-2744 prints
+   them).  Pointers may be NULL. */
+int agal_refine_stats(const agal_ctx *ctx, long long *iter, int *n_refined, int *n_coarsened);
 
 /* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
    bytes must equal the size reported by agal_array_bytes. */

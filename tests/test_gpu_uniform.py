@@ -250,8 +250,11 @@ def test_refresh_macros():
     assert np.abs(M[1:] - np.stack(u)).max() < 1e-6
 
 
-@pytest.mark.skipif(not GOLDEN_CASES, reason="no reference dumps committed")
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+UNIFORM_CASES = [n for n in GOLDEN_CASES if not n.startswith("amr_")]
+
+
+@pytest.mark.skipif(not UNIFORM_CASES, reason="no reference dumps committed")
+@pytest.mark.parametrize("name", UNIFORM_CASES)
 def test_cuda_vs_reference_build(name):
     g = load_golden(name)
     p, steps = params_for_golden(g)

@@ -90,7 +90,7 @@ void release(agal_ctx *c)
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
-                    c->amr};
+                    c->amr, c->fix_count, c->fix_list};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -220,6 +220,8 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->red_out, sizeof(double) * 4);
     ALLOC(c->d_status, sizeof(int) * 4);
     ALLOC(c->meta, sizeof(int) * (size_t)(c->dim == 2 ? 12 : 28) * nmb);
+    ALLOC(c->fix_count, sizeof(int) * 4);
+    ALLOC(c->fix_list, sizeof(long long) * 2 * (size_t)AGAL_FIX_CAP);
     if (c->max_levels > 1) {
         const size_t na = agal_amr_scratch_ints(nmb);
         ALLOC(c->amr, sizeof(int) * na);
@@ -233,6 +235,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     }
 #undef ALLOC
     cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);
+    cudaMemsetAsync(c->fix_count, 0, sizeof(int) * 4, c->stream);
 
     // Reset values, mesh_init.cu:285-304.
     if ((rc = fill<int>(c, c->cells_ID_mask, nmc, CELL_INTERIOR)) ||
@@ -348,7 +351,8 @@ extern "C" int agal_sync(agal_ctx *c)
     AGAL_CUDA(c, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (st != 0) {
         cudaMemset(c->d_status, 0, sizeof(int));
-        return agal_set_err(c, st, "a device wait timed out (pipeline stalled)");
+        return agal_set_err(c, st, st == AGAL_ERR_TIMEOUT ? "a device wait timed out (pipeline stalled)"
+                                                          : "stream-guard fix-up list overflowed in a step");
     }
     return AGAL_OK;
 }

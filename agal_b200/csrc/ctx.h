@@ -67,6 +67,8 @@ struct agal_ctx {
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
+    int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
+    long long *fix_list = nullptr;
     // refine/coarsen pass scratch (multi-level cases only), one allocation:
     int *amr = nullptr;
     int *amr_emap = nullptr;           // efficient map (mesh_amr.cu c_tmp_8), -1 = absent
@@ -78,6 +80,9 @@ struct agal_ctx {
     int n_ref_last = 0, n_coarse_last = 0;   // marks acted on by the last refinement pass
     std::string err;
 };
+
+// Stream-guard fix-ups (refused swaps) one step of a context can hold.
+#define AGAL_FIX_CAP 65536
 
 // Step kernel variants: 1 and 2 cells per thread (one-shot grid), 3 the
 // TMA-staged persistent pipeline.

@@ -77,4 +77,11 @@ __host__ __device__ constexpr int nbr_cell(int dim, int I, int J, int K)
 }
 __host__ __device__ constexpr int center_slot(int dim) { return dim == 2 ? 4 : 13; }
 
+// Directions that own a swap pair in the in-place stream (kernels.cu:597, 769):
+// the stream visits p in this half set and swaps with pb(p) of the neighbour.
+__host__ __device__ constexpr bool lat_half(int dim, int p)
+{
+    return dim == 2 ? (p == 1 || (p + 1) % 3 == 0) : (p == 26 || ((p - 1) % 2 == 0 && p < 25));
+}
+
 }  // namespace agal

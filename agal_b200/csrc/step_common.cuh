@@ -40,6 +40,11 @@ struct StepArgs {
     double omega;
     double u_ref;
     int bc_preset;
+    // Links whose in-place swap the reference's guard would refuse (see
+    // push_cell): appended here, swapped back by k_stream_fixup.
+    int *fix_count;
+    long long *fix_list;   // [fix_cap][2] element offsets into fout
+    int fix_cap;
 };
 
 // Boundary hook presets (inc/custom.h:79-122); f is the full population.
@@ -179,6 +184,24 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
     const int sz[3] = {DIM == 3 ? (K > 0 ? 9 : 0) : 0, DIM == 3 ? 9 : 0, DIM == 3 ? (K < 3 ? 9 : 18) : 0};
     const int nz[3] = {16 * ((K + 3) & 3), 16 * K, 16 * ((K + 1) & 3)};
     T *__restrict__ own = fo + (long long)b * BLK + t;
+    // The reference streams in place: the owner x of a pair (p in the half
+    // set) swaps its f*_p with the neighbour y's f*_pb only if that value is
+    // positive (kernels.cu:620-628, the solid-cell guard f_pb > 0).  Here each
+    // cell pushes unconditionally; the cell on the non-owning side of an open
+    // link, which holds that value, records the link when it is not positive,
+    // and k_stream_fixup swaps the two pushed entries back, which is exactly
+    // the refused swap.  Non-positive populations are rare (strong
+    // over-relaxation near singular corners), so the list stays short.
+    auto guard = [&](int p, bool open, long long dst) {
+        if (p == 0 || lat_half(DIM, p) || !open) return;
+        const C full = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        if (full > C(0)) return;
+        const int k = atomicAdd(a.fix_count, 1);
+        if (k < a.fix_cap) {
+            a.fix_list[2 * k] = dst;
+            a.fix_list[2 * k + 1] = (long long)b * BLK + p * MC + t;
+        }
+    };
     if (!hook) {
         // No boundary hook on this block: closed links are plain bounce-back.
 #pragma unroll
@@ -188,8 +211,10 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
             const int nc = nx[cx] + ny[cy] + (DIM == 3 ? nz[cz] : 0);
             bool open = nb >= 0;
             if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
-            T *dst = open ? fo + ((long long)nb * BLK + lat_pb(DIM, p) * MC + nc) : own + p * MC;
+            const long long to = (long long)nb * BLK + lat_pb(DIM, p) * MC + nc;
+            T *dst = open ? fo + to : own + p * MC;
             *dst = ST<T>::enc(g[p]);
+            guard(p, open, to);
         }
     } else {
 #pragma unroll
@@ -200,7 +225,9 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
             bool open = nb >= 0;
             if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
             if (open) {
-                fo[(long long)nb * BLK + lat_pb(DIM, p) * MC + nc] = ST<T>::enc(g[p]);
+                const long long to = (long long)nb * BLK + lat_pb(DIM, p) * MC + nc;
+                fo[to] = ST<T>::enc(g[p]);
+                guard(p, true, to);
             } else {
                 C v = g[p];
                 if (nb != N_SKIPID) {   // domain boundary: Cu_ImposeBC hook (kernels.cu:791-792)

@@ -111,6 +111,13 @@ class Case:
         return {"n_ids": list(n_ids[: L + 1]), "id_max": list(id_max[: L + 1]), "n_gaps": n_gaps.value,
                 "n_maxcblocks": nmb.value, "max_levels": L}
 
+    def set_counts(self, n_ids, id_max, n_gaps: int) -> None:
+        """Restore n_ids / id_max / n_gaps after agal_load (restart)."""
+        ml = self.counts()["max_levels"]
+        a = (C.c_int * (ml + 1))(*[int(v) for v in n_ids[: ml + 1]])
+        b = (C.c_int * (ml + 1))(*[int(v) for v in id_max[: ml + 1]])
+        self._c(self._lib.agal_set_counts(self._h, a, b, int(n_gaps)))
+
     # -- solver entry points -------------------------------------------
     def set_ic(self, L: int = 0) -> None:
         self._c(self._lib.agal_set_ic(self._h, L))

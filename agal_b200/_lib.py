@@ -73,6 +73,7 @@ PROTOS = [
     ("agal_last_error", C.c_char_p, [C.c_void_p]),
     ("agal_get_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    ("agal_set_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
     ("agal_set_ic", C.c_int, [C.c_void_p, C.c_int]),
     ("agal_refresh", C.c_int, [C.c_void_p, C.c_int]),
     ("agal_advance", C.c_int, [C.c_void_p, C.c_int]),

@@ -341,6 +341,22 @@ extern "C" int agal_get_counts(const agal_ctx *c, int *n_ids, int *id_max, int *
     return AGAL_OK;
 }
 
+extern "C" int agal_set_counts(agal_ctx *c, const int *n_ids, const int *id_max, int n_gaps)
+{
+    if (!c || !n_ids || !id_max) return AGAL_ERR_PARAM;
+    for (int L = 0; L <= c->max_levels; L++)
+        if (n_ids[L] < 0 || n_ids[L] > c->nmb || id_max[L] > c->nmb)
+            return agal_set_err(c, AGAL_ERR_PARAM, "agal_set_counts: count beyond the block pool");
+    if (n_gaps < 0 || n_gaps > c->nmb) return agal_set_err(c, AGAL_ERR_PARAM, "agal_set_counts: n_gaps");
+    for (int L = 0; L <= c->max_levels; L++) {
+        c->n_ids[L] = n_ids[L];
+        c->id_max[L] = id_max[L];
+    }
+    c->n_gaps = n_gaps;
+    agal_drop_graphs(c);
+    return agal_build_meta(c);
+}
+
 extern "C" int agal_sync(agal_ctx *c)
 {
     if (!c) return AGAL_ERR_PARAM;

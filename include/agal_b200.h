@@ -156,6 +156,11 @@ const char *agal_last_error(const agal_ctx *ctx);
 /* Host mirrors: n_ids[MAX_LEVELS+1], id_max[MAX_LEVELS+1], n_gaps, capacity. */
 int agal_get_counts(const agal_ctx *ctx, int *n_ids, int *id_max, int *n_gaps,
                     int64_t *n_maxcblocks, int *max_levels);
+/* Restore the host mirrors after loading a mesh with agal_load, as the
+   restart reader does (mesh_restart.cu:111-121): n_ids[MAX_LEVELS+1],
+   id_max[MAX_LEVELS+1], n_gaps.  Rebuilds the step metadata of the loaded
+   blocks.  AGAL_ERR_PARAM if a count exceeds the pool. */
+int agal_set_counts(agal_ctx *ctx, const int *n_ids, const int *id_max, int n_gaps);
 
 /* Solver::S_SetIC (solver_lbm_kernels.cu:79-98). */
 int agal_set_ic(agal_ctx *ctx, int L);

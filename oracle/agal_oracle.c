@@ -213,6 +213,19 @@ int orc_get_counts(const orc_case *c, int *n_ids, int *id_max, int *n_gaps,
 
 #define DISPATCH(name, ...) (c->fp64 ? name##_f64(__VA_ARGS__) : name##_f32(__VA_ARGS__))
 
+int orc_set_counts(orc_case *c, const int *n_ids, const int *id_max, int n_gaps)
+{
+    /* Host counts of a restart (mesh_restart.cu:111-121). */
+    for (int L = 0; L <= c->max_levels; L++) {
+        if (n_ids[L] < 0 || n_ids[L] > c->nmb || id_max[L] > c->nmb) return AGAL_ERR_PARAM;
+        c->n_ids[L] = n_ids[L];
+        c->id_max[L] = id_max[L];
+    }
+    if (n_gaps < 0 || n_gaps > c->nmb) return AGAL_ERR_PARAM;
+    c->n_gaps = n_gaps;
+    return 0;
+}
+
 int orc_set_ic(orc_case *c, int L)
 {
     if (L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;

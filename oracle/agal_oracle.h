@@ -42,6 +42,9 @@ void orc_set_threads(int n);
 int orc_get_counts(const orc_case *c, int *n_ids, int *id_max, int *n_gaps,
                    int64_t *n_maxcblocks, int *max_levels);
 
+/* Restore n_ids[MAX_LEVELS+1], id_max[MAX_LEVELS+1] and n_gaps after
+   orc_load, as the restart reader does (mesh_restart.cu:111-121). */
+int orc_set_counts(orc_case *c, const int *n_ids, const int *id_max, int n_gaps);
 /* Solver_LBM::S_SetIC (solver_lbm_kernels.cu:15-98). */
 int orc_set_ic(orc_case *c, int L);
 /* Solver_LBM::S_RefreshVariables (solver_lbm_kernels.cu:112-175). */

@@ -42,6 +42,7 @@ def lib() -> C.CDLL:
             ("orc_set_threads", None, [C.c_int]),
             ("orc_get_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+            ("orc_set_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]),
             ("orc_set_ic", C.c_int, [C.c_void_p, C.c_int]),
             ("orc_refresh", C.c_int, [C.c_void_p, C.c_int]),
             ("orc_collide", C.c_int, [C.c_void_p, C.c_int]),
@@ -107,6 +108,12 @@ class OracleCase:
         L = ml.value
         return {"n_ids": list(n_ids[: L + 1]), "id_max": list(id_max[: L + 1]), "n_gaps": n_gaps.value,
                 "n_maxcblocks": nmb.value, "max_levels": L}
+
+    def set_counts(self, n_ids, id_max, n_gaps):
+        ml = self.counts()["max_levels"]
+        a = (C.c_int * (ml + 1))(*[int(v) for v in n_ids[: ml + 1]])
+        b = (C.c_int * (ml + 1))(*[int(v) for v in id_max[: ml + 1]])
+        self._c(self._lib.orc_set_counts(self._h, a, b, int(n_gaps)))
 
     def set_ic(self, L=0):
         self._c(self._lib.orc_set_ic(self._h, L))

@@ -166,8 +166,12 @@ int main(int argc, char **argv)
     // Loop body of M_AdvanceLoop (mesh_advance.cu:403-463) without output.
     const int iter_mult = (int)pow(2.0, (double)mesh.N_LEVEL_START);
     if (mesh.MAX_LEVELS > 1) mesh.M_Advance_RefineNearWall();
+    // REF_SKIP_LAST_REGRID=1 stops before the refinement of the last step, so
+    // the dump is the input of that refinement.
+    const bool skip_last = getenv("REF_SKIP_LAST_REGRID") && atoi(getenv("REF_SKIP_LAST_REGRID")) == 1;
     for (int i = 0; i < n_steps; i++) {
         mesh.M_Advance_Step(i, 0, iter_mult);
+        if (skip_last && i == n_steps - 1) break;
         if (mesh.MAX_LEVELS > 1 && (mesh.MAX_LEVELS != mesh.N_LEVEL_START + 1) && (i + 1) % mesh.P_REFINE == 0 && i > 0)
             mesh.M_Advance_RefineWithSolution(i, 0);
     }

@@ -57,14 +57,31 @@ AMR = dict(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, P_REFINE=16, N_REFINE_START
 AMR_CASES = {
     "amr_d2q9_box3_cubic": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-4, MAX_LEVELS_WALL=3), 200, 4096, 2),
     "amr_d2q9_wall2_linear": ("ref_d2q9_ldc_lin", dict(AMR, Nx=64, v0=5e-4, MAX_LEVELS_WALL=2), 200, 4096, 1),
-    # 128 steps = 8 regrids: at the 9th, one block's vorticity sits on a
-    # criterion threshold and FP32 rounding decides its refinement.
-    "amr_d2q9_sol3_cubic": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 128, 4096, 0),
+    # 112 steps = 7 regrids: at the 8th (step 128) one block's vorticity lies
+    # within FP32 rounding of a criterion threshold, so two FP32 trajectories
+    # may refine it differently; regrid_d2q9_cubic_s128 checks that regrid on
+    # identical inputs instead.
+    "amr_d2q9_sol3_cubic": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 112, 4096, 0),
     "amr_d2q9_sol3_linear": ("ref_d2q9_ldc_lin", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 200, 4096, 0),
     "amr_d2q9_wall2_sol3": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3),
                             200, 4096, 1),
     "amr_d3q19_box2": ("ref_d3q19_ldc", dict(AMR, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2), 60, 4096, 2),
     "amr_d3q27_sol2": ("ref_d3q27_ldc", dict(AMR, Nx=16, v0=2.5e-5, MAX_LEVELS_INTERIOR=2, P_REFINE=8), 48, 4096, 0),
+}
+
+# Regrid pairs: the reference state just before the refinement of the last
+# step (<name>_pre) and right after it (<name>_post).  Loading the first and
+# refining must give the second bit for bit: the criterion, marks and the
+# refine/coarsen pass judged on identical inputs, whatever FP32 rounding did to
+# the trajectory before.  (binary, keys, steps, keep_mb, region)
+REGRID_PAIRS = {
+    "regrid_d2q9_cubic_s128": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 128, 4096, 0),
+    "regrid_d2q9_cubic_s48": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 48, 4096, 0),
+    "regrid_d2q9_linear_s64": ("ref_d2q9_ldc_lin", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=3), 64, 4096, 0),
+    "regrid_d2q9_wall_s96": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3),
+                             96, 4096, 1),
+    "regrid_d3q19_s24": ("ref_d3q19_ldc", dict(AMR, Nx=16, v0=2.5e-5, MAX_LEVELS_INTERIOR=2, P_REFINE=8), 24, 4096, 0),
+    "regrid_d3q27_s40": ("ref_d3q27_ldc", dict(AMR, Nx=16, v0=2.5e-5, MAX_LEVELS_INTERIOR=2, P_REFINE=8), 40, 4096, 0),
 }
 
 # Timing workloads of the reference build: (binary, keys, timed steps, keep_mb)
@@ -170,7 +187,7 @@ def read_dump(path: Path) -> dict:
 
 
 def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
-            region: int = 0) -> str:
+            region: int = 0, skip_last_regrid: bool = False) -> str:
     exe = REF_BIN / binary
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
@@ -186,7 +203,7 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             import resource
             resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
 
-        env = dict(os.environ, REF_REGION=str(region))
+        env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0")
         r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
                            env=env)
         if r.returncode != 0:
@@ -196,13 +213,16 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
 
 def cmd_ref(out: Path, only: list[str] | None) -> None:
     out.mkdir(parents=True, exist_ok=True)
-    cases = {k: v + (0,) for k, v in CASES.items()}
-    cases.update(AMR_CASES)
-    for name, (binary, keys, steps, keep, region) in cases.items():
-        if only and name not in only:
+    cases = {k: v + (0, False) for k, v in CASES.items()}
+    cases.update({k: v + (False,) for k, v in AMR_CASES.items()})
+    for k, v in REGRID_PAIRS.items():
+        cases[k + "_pre"] = v + (True,)
+        cases[k + "_post"] = v + (False,)
+    for name, (binary, keys, steps, keep, region, skip) in cases.items():
+        if only and not any(name == o or name.startswith(o + "_") for o in only):
             continue
         raw = out / f"{name}.bin"
-        run_ref(binary, keys, steps, keep, raw, region=region)
+        run_ref(binary, keys, steps, keep, raw, region=region, skip_last_regrid=skip)
         d = read_dump(raw)
         d["case_keys"] = json.dumps(keys)
         d["binary"] = binary

@@ -11,7 +11,8 @@ import numpy as np
 import pytest
 
 from helpers import lattice, macros_from_F, rel_l2
-from test_oracle import GOLDEN_CASES, compare_to_golden, load_golden, params_for_golden, run_like_reference
+from test_oracle import (GOLDEN_CASES, REGRID_PAIRS, compare_to_golden, load_golden, params_for_golden,
+                         regrid_from_reference, run_like_reference)
 
 import agal_b200 as ag
 from agal_b200 import _lib
@@ -182,3 +183,14 @@ def test_cuda_amr_vs_reference_build(name):
         run_like_reference(c, p, steps)
         c.sync()
         compare_to_golden(g, c.dump, 1e-5, c.counts())
+
+
+@pytest.mark.skipif(not REGRID_PAIRS, reason="no reference regrid dumps committed")
+@pytest.mark.parametrize("name", REGRID_PAIRS)
+def test_cuda_regrid_vs_reference_build(name):
+    """The reference state before a refinement loaded into the CUDA library:
+    criterion, marks and refine/coarsen pass give the reference's state after
+    it bit for bit (integer arrays), on identical inputs."""
+    c = regrid_from_reference(lambda p, nmb: ag.Case(ag.default_params(**{
+        **{k: getattr(p, k) for k, _ in p._fields_}, "n_maxcblocks": nmb})), name)
+    c.close()

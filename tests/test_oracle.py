@@ -139,6 +139,82 @@ def fp64_floor(g):
     return rho64, np.stack(u64), rel_l2(np.stack(u_r), np.stack(u64)), rel_l2(rho_r, rho64)
 
 
+def compare_ints(g, dumpf, counts=None):
+    """Block and cell integer arrays of the dump's active blocks, the ID sets,
+    and (with counts) n_ids, id_max and the top of the gap stack: bit-exact."""
+    blocks = g["blocks"].astype(np.int64)
+    dim, Qmax, MC = int(g["dim"]), int(g["Qmax"]), int(g["MC"])
+    nmb = len(dumpf(_lib.ARR_CBLOCK_ID_ONB))
+    if counts is not None:
+        ml = int(g["max_levels"])
+        assert counts["n_ids"][:ml] == [int(v) for v in g["n_ids"][:ml]]
+        assert counts["id_max"][: ml + 1] == [int(v) for v in g["id_max"][: ml + 1]]
+        gaps = dumpf(_lib.ARR_GAP_SET)[: counts["n_gaps"]]
+        tail = g["gaps_tail"]
+        k = 0
+        while k < min(len(tail), len(gaps)) and tail[len(tail) - 1 - k] < nmb - 64:
+            k += 1
+        assert (gaps[len(gaps) - k:] == tail[len(tail) - k:]).all()
+    assert (dumpf(_lib.ARR_CBLOCK_ID_NBR).reshape(Qmax, nmb)[:, blocks].T == g["nbr"]).all()
+    assert (dumpf(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(Qmax, nmb)[:, blocks].T == g["nbr_child"]).all()
+    for arr, key in [(_lib.ARR_CBLOCK_ID_ONB, "onb"), (_lib.ARR_CBLOCK_ID_REF, "ref"),
+                     (_lib.ARR_CBLOCK_LEVEL, "level"), (_lib.ARR_CBLOCK_ID_MASK, "bmask")]:
+        assert (dumpf(arr)[blocks] == g[key][:, 0]).all(), key
+    assert (dumpf(_lib.ARR_CBLOCK_F_X).reshape(dim, nmb)[:, blocks].T == g["fX"]).all()
+    assert (dumpf(_lib.ARR_CELLS_ID_MASK).reshape(nmb, MC)[blocks] == g["cmask"]).all()
+    for L in range(int(g["max_levels"])):
+        n = int(g["n_ids"][L])
+        assert (dumpf(_lib.ARR_ID_SET).reshape(-1, nmb)[L, :n] == g[f"id_set_{L}"]).all()
+
+
+def load_reference_state(case, g, nmb):
+    """Load a reference dump (its active blocks) into an nmb-block pool of the
+    oracle or the CUDA library, with the counts of the restart reader.  Blocks
+    outside the dump take a fresh pool's values; the gap stack keeps the
+    dump's top (recycled and lowest fresh IDs, in stack order) over the
+    remaining free IDs of the smaller pool, in descending order."""
+    dim, Q, Qmax, MC, ML = (int(g[k]) for k in ("dim", "Q", "Qmax", "MC", "max_levels"))
+    blocks = g["blocks"].astype(np.int64)
+    cm = np.zeros((nmb, MC), np.int32)
+    cm[blocks] = g["cmask"]
+    fX = np.zeros((dim, nmb), np.float32)
+    fX[:, blocks] = g["fX"].T
+    arrs = {_lib.ARR_CELLS_ID_MASK: cm, _lib.ARR_CBLOCK_F_X: fX}
+    for arr, key, fill in [(_lib.ARR_CBLOCK_ID_MASK, "bmask", 0), (_lib.ARR_CBLOCK_ID_ONB, "onb", 0),
+                           (_lib.ARR_CBLOCK_ID_REF, "ref", 8), (_lib.ARR_CBLOCK_LEVEL, "level", 0)]:
+        a = np.full(nmb, fill, np.int32)
+        a[blocks] = g[key][:, 0]
+        arrs[arr] = a
+    for arr, key in [(_lib.ARR_CBLOCK_ID_NBR, "nbr"), (_lib.ARR_CBLOCK_ID_NBR_CHILD, "nbr_child")]:
+        a = np.full((Qmax, nmb), -999, np.int32)
+        a[:, blocks] = g[key].T
+        arrs[arr] = a
+    ids = np.zeros((ML, nmb), np.int32)
+    for L in range(ML):
+        v = g[f"id_set_{L}"]
+        ids[L, : len(v)] = v
+    arrs[_lib.ARR_ID_SET] = ids
+    tail = g["gaps_tail"]
+    top = []
+    for v in tail[::-1]:
+        if v >= nmb:
+            break
+        top.append(int(v))
+    top = top[::-1]
+    used = set(top) | set(blocks.tolist())
+    stack = [b for b in range(nmb - 1, -1, -1) if b not in used] + top
+    gaps = np.zeros(nmb, np.int32)
+    gaps[: len(stack)] = stack
+    arrs[_lib.ARR_GAP_SET] = gaps
+    F = np.zeros((Q, nmb * MC))
+    Fr = F.reshape(Q, nmb, MC)
+    Fr[:, blocks, :] = np.transpose(g["F"][:, :Q, :], (1, 0, 2))
+    arrs[_lib.ARR_F] = F
+    for k, a in arrs.items():
+        case.load(k, a.reshape(-1))
+    case.set_counts([int(v) for v in g["n_ids"]], [int(v) for v in g["id_max"]], len(stack))
+
+
 def compare_to_golden(g, dumpf, tol_rel_l2, counts=None):
     """Integer arrays bit-exact; rho/u against the reference's own FP32 build.
 
@@ -149,34 +225,9 @@ def compare_to_golden(g, dumpf, tol_rel_l2, counts=None):
     floor) of the reference, and no further from the FP64 result than
     1.5 x the reference's own distance."""
     blocks = g["blocks"].astype(np.int64)
-    dim, Q, Qmax, MC = int(g["dim"]), int(g["Q"]), int(g["Qmax"]), int(g["MC"])
+    dim, Q, MC = int(g["dim"]), int(g["Q"]), int(g["MC"])
     nmb = len(dumpf(_lib.ARR_CBLOCK_ID_ONB))
-    if counts is not None:
-        ml = int(g["max_levels"])
-        assert counts["n_ids"][:ml] == [int(v) for v in g["n_ids"][:ml]]
-        assert counts["id_max"][: ml + 1] == [int(v) for v in g["id_max"][: ml + 1]]
-        # top of the gap stack (recycled and lowest fresh IDs), as far as the
-        # smaller pool here reaches
-        gaps = dumpf(_lib.ARR_GAP_SET)[: counts["n_gaps"]]
-        tail = g["gaps_tail"]
-        k = 0
-        while k < min(len(tail), len(gaps)) and tail[len(tail) - 1 - k] < nmb - 64:
-            k += 1
-        assert (gaps[len(gaps) - k:] == tail[len(tail) - k:]).all()
-    nbr = dumpf(_lib.ARR_CBLOCK_ID_NBR).reshape(Qmax, nmb)[:, blocks].T
-    assert (nbr == g["nbr"]).all()
-    ch = dumpf(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(Qmax, nmb)[:, blocks].T
-    assert (ch == g["nbr_child"]).all()
-    for arr, key in [(_lib.ARR_CBLOCK_ID_ONB, "onb"), (_lib.ARR_CBLOCK_ID_REF, "ref"),
-                     (_lib.ARR_CBLOCK_LEVEL, "level"), (_lib.ARR_CBLOCK_ID_MASK, "bmask")]:
-        assert (dumpf(arr)[blocks] == g[key][:, 0]).all(), key
-    fX = dumpf(_lib.ARR_CBLOCK_F_X).reshape(dim, nmb)[:, blocks].T
-    assert (fX == g["fX"]).all()
-    cm = dumpf(_lib.ARR_CELLS_ID_MASK).reshape(nmb, MC)[blocks]
-    assert (cm == g["cmask"]).all()
-    for L in range(int(g["max_levels"])):
-        n = int(g["n_ids"][L])
-        assert (dumpf(_lib.ARR_ID_SET).reshape(-1, nmb)[L, :n] == g[f"id_set_{L}"]).all()
+    compare_ints(g, dumpf, counts)
     F = dumpf(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks, :].reshape(Q, -1)
     Fr = np.transpose(g["F"][:, :Q, :], (1, 0, 2)).reshape(Q, -1).astype(np.float64)
     pb, c, _ = lattice(Q)
@@ -191,8 +242,41 @@ def compare_to_golden(g, dumpf, tol_rel_l2, counts=None):
     return rel_l2(F, Fr)
 
 
-@pytest.mark.skipif(not GOLDEN_CASES, reason="no reference dumps committed")
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+REGRID_PAIRS = sorted(p.stem[: -len("_pre")] for p in GOLDEN.glob("regrid_*_pre.npz"))
+
+
+def regrid_from_reference(case_factory, name):
+    """Load the reference state before a refinement, refine, and compare with
+    the reference state after it: integer arrays bit-exact, populations (the
+    grid average and the data interpolated into new children) within 1e-6."""
+    pre, post = load_golden(name + "_pre"), load_golden(name + "_post")
+    p, _ = params_for_golden(post)
+    nmb = p.n_maxcblocks
+    case = case_factory(p, nmb)
+    load_reference_state(case, pre, nmb)
+    case.refine_with_solution()
+    counts = case.counts()
+    compare_ints(post, case.dump, counts)
+    blocks = post["blocks"].astype(np.int64)
+    Q, MC = int(post["Q"]), int(post["MC"])
+    F = case.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks, :]
+    Fr = np.transpose(post["F"][:, :Q, :], (1, 0, 2)).astype(np.float64)
+    assert np.abs(F - Fr).max() < 1e-6
+    return case
+
+
+@pytest.mark.skipif(not REGRID_PAIRS, reason="no reference regrid dumps committed")
+@pytest.mark.parametrize("name", REGRID_PAIRS)
+def test_oracle_regrid_vs_reference_build(oracle_lib, name):
+    from oracle.orc import OracleCase
+    regrid_from_reference(lambda p, nmb: OracleCase(p, nmb), name)
+
+
+GOLDEN_RUNS = [n for n in GOLDEN_CASES if not n.startswith("regrid_")]
+
+
+@pytest.mark.skipif(not GOLDEN_RUNS, reason="no reference dumps committed")
+@pytest.mark.parametrize("name", GOLDEN_RUNS)
 def test_oracle_vs_reference_build(oracle_lib, name):
     from oracle.orc import OracleCase
     g = load_golden(name)

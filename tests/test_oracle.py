@@ -248,7 +248,12 @@ REGRID_PAIRS = sorted(p.stem[: -len("_pre")] for p in GOLDEN.glob("regrid_*_pre.
 def regrid_from_reference(case_factory, name):
     """Load the reference state before a refinement, refine, and compare with
     the reference state after it: integer arrays bit-exact, populations (the
-    grid average and the data interpolated into new children) within 1e-6."""
+    grid average and the data interpolated into new children) within 1e-6
+    (linear interpolation) or 1e-4 (cubic).  The cubic bound is the
+    reference's own rounding: it evaluates the interpolant in FP32 from
+    monomial coefficients up to ~500 (util_interp.h), whose cancellation
+    leaves 1e-5..1e-4 absolute error; the oracle and the CUDA library
+    evaluate the same interpolant in the Lagrange form."""
     pre, post = load_golden(name + "_pre"), load_golden(name + "_post")
     p, _ = params_for_golden(post)
     nmb = p.n_maxcblocks
@@ -261,7 +266,8 @@ def regrid_from_reference(case_factory, name):
     Q, MC = int(post["Q"]), int(post["MC"])
     F = case.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks, :]
     Fr = np.transpose(post["F"][:, :Q, :], (1, 0, 2)).astype(np.float64)
-    assert np.abs(F - Fr).max() < 1e-6
+    tol = 1e-4 if p.interp_order == _lib.INTERP_CUBIC else 1e-6
+    assert np.abs(F - Fr).max() < tol
     return case
 
 

@@ -25,6 +25,7 @@ STORE_FP32, STORE_FP64, STORE_FP16, STORE_BF16 = 0, 1, 2, 3
 BC_NONE, BC_LDC2D, BC_LDC3D, BC_FPSC2D, BC_FPSC3D = 0, 1, 2, 3, 4
 IC_REST, IC_UNIFORM = 0, 1
 REGION_NONE, REGION_BOUNDARY, REGION_BOX = 0, 1, 2
+CRITERION_VORTICITY, CRITERION_Q, CRITERION_PERCENTILE = 0, 1, 2
 INTERP_INTERFACE, INTERP_ADDED = 0, 1
 AVERAGE_INTERFACE, AVERAGE_BLOCK, AVERAGE_GRID = 0, 1, 2
 
@@ -57,7 +58,7 @@ class AgalParams(C.Structure):
                 [(k, C.c_char * 256) for k in STR_KEYS] +
                 [("velocity_set", C.c_int), ("collision", C.c_int), ("interp_order", C.c_int),
                  ("storage", C.c_int), ("bc_preset", C.c_int), ("ic_preset", C.c_int),
-                 ("region_preset", C.c_int),
+                 ("region_preset", C.c_int), ("ref_pct_hi", C.c_double), ("ref_pct_lo", C.c_double),
                  ("u_ref", C.c_double), ("ic_noise", C.c_double), ("seed", C.c_uint64),
                  ("n_maxcblocks", C.c_int64), ("mem_frac", C.c_double), ("device", C.c_int)])
 

@@ -110,6 +110,8 @@ extern "C" int agal_params_default(agal_params *p)
     p->bc_preset = AGAL_BC_NONE;
     p->ic_preset = AGAL_IC_REST;
     p->region_preset = AGAL_REGION_NONE;
+    p->ref_pct_hi = 0.9;
+    p->ref_pct_lo = 0.5;
     p->u_ref = 0.05;                       // custom.h literal
     p->ic_noise = 0.0;
     p->seed = 0;

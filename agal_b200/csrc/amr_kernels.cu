@@ -344,6 +344,192 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_criterion(const CriterionArgs 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Percentile criterion (S_CRITERION = AGAL_CRITERION_PERCENTILE; no reference
+// counterpart).  k_wmax: maximum vorticity magnitude of each block over its
+// non-ghost cells at the block's own spacing, every operation explicitly
+// rounded in the order the oracle writes it.  The ref_pct_hi / ref_pct_lo
+// quantiles of the leaf blocks' values are then selected exactly on the
+// device by a radix select over the bits of the (non-negative, so
+// order-preserving) FP64 keys, 16 bits per pass, and k_pct_mark marks.
+__device__ __forceinline__ float r_sqrt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double r_sqrt(double a) { return __dsqrt_rn(a); }
+
+struct PctState {
+    unsigned long long prefix[2];   // key bits selected so far, per quantile
+    int k[2];                       // rank still sought within the prefix
+    int n;                          // leaf blocks in the population
+};
+
+struct WmaxArgs {
+    int idm;
+    long long nmc;
+    const void *macro;
+    const int *cmask, *level, *ref, *nbr_child;
+    double dx[16];                  // dx_L per level, in the compute type's value
+    double *wval;                   // [idm]: block maximum (-1 for inactive)
+    int *pop;                       // [idm]: 1 for a leaf block
+    PctState *st;
+};
+
+template <typename C>
+__device__ __forceinline__ C xpol4_rn(C a, C b, C c, C d)
+{
+    return r_add(r_add(r_add(r_mul(C(4), a), r_mul(C(-6), b)), r_mul(C(4), c)), r_mul(C(-1), d));
+}
+
+template <int DIM, typename C>
+__global__ void __launch_bounds__(Geo<DIM>::MC) k_wmax(const WmaxArgs a)
+{
+    constexpr int MC = Geo<DIM>::MC, H = (DIM == 2) ? 36 : 216;
+    __shared__ C s[DIM][H];
+    __shared__ C sW[MC];
+    const int b = blockIdx.x;
+    const int t = threadIdx.x;
+    if (a.ref[b] == REF_INACTIVE) {   // uniform per CTA
+        if (t == 0) {
+            a.wval[b] = -1.0;
+            a.pop[b] = 0;
+        }
+        return;
+    }
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const C *m = static_cast<const C *>(a.macro);
+    const long long cell = (long long)b * MC + t;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) s[d][halo_ix<DIM>(I, J, K)] = m[(long long)(1 + d) * a.nmc + cell];
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        C *q = s[d];
+        if (I == 0) {
+            q[halo_ix<DIM>(-1, J, K)] = xpol4_rn(q[halo_ix<DIM>(0, J, K)], q[halo_ix<DIM>(1, J, K)],
+                                                 q[halo_ix<DIM>(2, J, K)], q[halo_ix<DIM>(3, J, K)]);
+            q[halo_ix<DIM>(4, J, K)] = xpol4_rn(q[halo_ix<DIM>(3, J, K)], q[halo_ix<DIM>(2, J, K)],
+                                                q[halo_ix<DIM>(1, J, K)], q[halo_ix<DIM>(0, J, K)]);
+        }
+        if (J == 0) {
+            q[halo_ix<DIM>(I, -1, K)] = xpol4_rn(q[halo_ix<DIM>(I, 0, K)], q[halo_ix<DIM>(I, 1, K)],
+                                                 q[halo_ix<DIM>(I, 2, K)], q[halo_ix<DIM>(I, 3, K)]);
+            q[halo_ix<DIM>(I, 4, K)] = xpol4_rn(q[halo_ix<DIM>(I, 3, K)], q[halo_ix<DIM>(I, 2, K)],
+                                                q[halo_ix<DIM>(I, 1, K)], q[halo_ix<DIM>(I, 0, K)]);
+        }
+        if (DIM == 3 && K == 0) {
+            q[halo_ix<DIM>(I, J, -1)] = xpol4_rn(q[halo_ix<DIM>(I, J, 0)], q[halo_ix<DIM>(I, J, 1)],
+                                                 q[halo_ix<DIM>(I, J, 2)], q[halo_ix<DIM>(I, J, 3)]);
+            q[halo_ix<DIM>(I, J, 4)] = xpol4_rn(q[halo_ix<DIM>(I, J, 3)], q[halo_ix<DIM>(I, J, 2)],
+                                                q[halo_ix<DIM>(I, J, 1)], q[halo_ix<DIM>(I, J, 0)]);
+        }
+    }
+    __syncthreads();
+    const C h2 = r_mul(C(2), C(a.dx[a.level[b]]));
+    C g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const C *q = s[d];
+        g[d][0] = r_div(r_add(q[halo_ix<DIM>(I + 1, J, K)], -q[halo_ix<DIM>(I - 1, J, K)]), h2);
+        g[d][1] = r_div(r_add(q[halo_ix<DIM>(I, J + 1, K)], -q[halo_ix<DIM>(I, J - 1, K)]), h2);
+        if (DIM == 3) g[d][2] = r_div(r_add(q[halo_ix<DIM>(I, J, K + 1)], -q[halo_ix<DIM>(I, J, K - 1)]), h2);
+    }
+    C w;
+    if (DIM == 2) {
+        w = fabs(r_add(g[1][0], -g[0][1]));
+    } else {
+        const C wx = r_add(g[2][1], -g[1][2]), wy = r_add(g[0][2], -g[2][0]), wz = r_add(g[1][0], -g[0][1]);
+        w = r_sqrt(r_add(r_add(r_mul(wx, wx), r_mul(wy, wy)), r_mul(wz, wz)));
+    }
+    if (a.cmask[cell] == CELL_GHOST) w = C(0);
+    sW[t] = w;
+    __syncthreads();
+    for (int st = MC / 2; st > 0; st >>= 1) {
+        if (t < st) sW[t] = fmax(sW[t], sW[t + st]);
+        __syncthreads();
+    }
+    if (t == 0) {
+        const int leaf = a.nbr_child[b] < 0;
+        a.wval[b] = (double)sW[0];
+        a.pop[b] = leaf;
+        if (leaf) atomicAdd(&a.st->n, 1);
+    }
+}
+
+// One radix pass: histogram of the next 16 key bits of the population
+// elements that match each quantile's prefix.
+__global__ void k_pct_hist(const double *wval, const int *pop, int idm, const PctState *st, int pass, int *hist)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= idm || !pop[b]) return;
+    const unsigned long long key = (unsigned long long)__double_as_longlong(wval[b]);
+    const int sh = 48 - 16 * pass;
+    for (int r = 0; r < 2; r++) {
+        if (pass > 0 && (key >> (sh + 16)) != st->prefix[r]) continue;
+        atomicAdd(&hist[r * 65536 + (int)((key >> sh) & 0xFFFFull)], 1);
+    }
+}
+
+// Select the bin holding each quantile's rank (one CTA per quantile, 1024
+// threads x 64 bins), extend its prefix, and clear the histogram.
+__global__ void __launch_bounds__(1024) k_pct_pick(int *hist, PctState *st, int pass, double pct_hi, double pct_lo)
+{
+    __shared__ int s_warp[32];
+    const int r = blockIdx.x, t = threadIdx.x;
+    const int n = st->n;
+    if (n <= 0) return;   // uniform
+    int *h = hist + r * 65536;
+    const int k = (pass == 0) ? (int)floor((r == 0 ? pct_hi : pct_lo) * (double)(n - 1)) : st->k[r];
+    int sum = 0;
+    for (int i = 0; i < 64; i++) sum += h[t * 64 + i];
+    // exclusive scan of the per-thread sums
+    const int lane = t & 31, wid = t >> 5;
+    int x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int v = s_warp[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        s_warp[lane] = v;
+    }
+    __syncthreads();
+    int start = (wid ? s_warp[wid - 1] : 0) + x - sum;
+    if (start <= k && k < start + sum) {
+        for (int i = 0; i < 64; i++) {
+            const int c = h[t * 64 + i];
+            if (k < start + c) {
+                st->prefix[r] = (st->prefix[r] << 16) | (unsigned long long)(t * 64 + i);
+                st->k[r] = k - start;
+                break;
+            }
+            start += c;
+        }
+    }
+    __syncthreads();
+    for (int i = 0; i < 64; i++) h[t * 64 + i] = 0;
+}
+
+__global__ void k_pct_mark(const double *wval, const PctState *st, const int *nbr, long long nmb, int qmax,
+                           const int *level, int mli, int idm, int *ref)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= idm || st->n <= 0) return;
+    const int r = ref[b];
+    if (r == REF_INACTIVE) return;
+    const double thr_hi = __longlong_as_double((long long)st->prefix[0]);
+    const double thr_lo = __longlong_as_double((long long)st->prefix[1]);
+    bool eligible = true;
+    for (int p = 0; p < qmax; p++)
+        if (nbr[b + (long long)p * nmb] == N_SKIPID) eligible = false;
+    const double w = wval[b];
+    if (r == REF_UNREFINED && eligible && level[b] < mli - 1 && w > thr_hi) ref[b] = REF_MARK_REFINE;
+    if (r == REF_REFINED && w < thr_lo) ref[b] = REF_MARK_COARSEN;
+}
+
 template <int DIM, int Q, typename T> struct RunInterp {
     static int run(agal_ctx *c, int L, int var)
     {
@@ -399,10 +585,50 @@ template <int DIM, int Q, typename T> struct RunAverage {
 int agal_launch_interp(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunInterp>(c, L, var); }
 int agal_launch_average(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunAverage>(c, L, var); }
 
+static int launch_percentile(agal_ctx *c, int idm)
+{
+    if (!c->crit) return agal_set_err(c, AGAL_ERR_STATE, "percentile criterion needs MAX_LEVELS > 1");
+    double *wval = static_cast<double *>(c->crit);
+    int *hist = reinterpret_cast<int *>(wval + c->nmb);
+    agal::PctState *st = reinterpret_cast<agal::PctState *>(hist + 2 * 65536);
+    AGAL_CUDA(c, cudaMemsetAsync(st, 0, sizeof(agal::PctState), c->stream));
+    AGAL_CUDA(c, cudaMemsetAsync(hist, 0, sizeof(int) * 2 * 65536, c->stream));
+    agal::WmaxArgs a;
+    a.idm = idm;
+    a.nmc = c->nmc;
+    a.macro = c->macro;
+    a.cmask = c->cells_ID_mask;
+    a.level = c->cblock_level;
+    a.ref = c->cblock_ID_ref;
+    a.nbr_child = c->cblock_ID_nbr_child;
+    for (int L = 0; L < 16; L++) a.dx[L] = (L < c->max_levels) ? c->dxf[L] : 0.0;
+    a.wval = wval;
+    a.pop = c->amr_a;
+    a.st = st;
+    const bool f64 = c->storage == AGAL_STORE_FP64;
+    if (c->dim == 2) {
+        if (f64) agal::k_wmax<2, double><<<(unsigned)idm, 16, 0, c->stream>>>(a);
+        else agal::k_wmax<2, float><<<(unsigned)idm, 16, 0, c->stream>>>(a);
+    } else {
+        if (f64) agal::k_wmax<3, double><<<(unsigned)idm, 64, 0, c->stream>>>(a);
+        else agal::k_wmax<3, float><<<(unsigned)idm, 64, 0, c->stream>>>(a);
+    }
+    const unsigned g = (unsigned)((idm + 255) / 256);
+    for (int pass = 0; pass < 4; pass++) {
+        agal::k_pct_hist<<<g, 256, 0, c->stream>>>(wval, c->amr_a, idm, st, pass, hist);
+        agal::k_pct_pick<<<2, 1024, 0, c->stream>>>(hist, st, pass, c->P.ref_pct_hi, c->P.ref_pct_lo);
+    }
+    agal::k_pct_mark<<<g, 256, 0, c->stream>>>(wval, st, c->cblock_ID_nbr, c->nmb, c->Qmax, c->cblock_level,
+                                               c->P.MAX_LEVELS_INTERIOR, idm, c->cblock_ID_ref);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
 int agal_launch_criterion(agal_ctx *c)
 {
     const int idm = c->id_max[c->max_levels];
     if (idm <= 0) return AGAL_OK;
+    if (c->P.S_CRITERION == AGAL_CRITERION_PERCENTILE) return launch_percentile(c, idm);
     agal::CriterionArgs a;
     a.idm = idm;
     a.nmb = c->nmb;

@@ -90,7 +90,7 @@ void release(agal_ctx *c)
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
-                    c->amr, c->fix_count, c->fix_list};
+                    c->amr, c->fix_count, c->fix_list, c->crit};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -176,7 +176,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     const size_t per_block =
         (size_t)c->MC * (2 * c->Q * c->esize + (c->dim + 1) * compute_size(c) + sizeof(int)) +
         sizeof(float) * c->dim + sizeof(int) * (2 * c->Qmax + 5 + c->max_levels) +
-        (c->max_levels > 1 ? 5 * sizeof(int) : 0);
+        (c->max_levels > 1 ? 5 * sizeof(int) + sizeof(double) : 0);
     if (p->n_maxcblocks > 0) {
         c->nmb = p->n_maxcblocks;
     } else {
@@ -232,6 +232,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         c->amr_snap = c->amr + 4 * nmb;
         c->amr_parts = c->amr + 5 * nmb;
         c->amr_small = c->amr + na - AGAL_AMR_SMALL;
+        ALLOC(c->crit, sizeof(double) * nmb + sizeof(int) * 2 * 65536 + 256);
     }
 #undef ALLOC
     cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);

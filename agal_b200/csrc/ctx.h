@@ -76,6 +76,7 @@ struct agal_ctx {
     int *amr_a = nullptr, *amr_b = nullptr, *amr_snap = nullptr;   // compaction / snapshot buffers
     int *amr_parts = nullptr;          // per-CTA partial counts of the compactions
     int *amr_small = nullptr;          // small counters read back by the host
+    void *crit = nullptr;              // percentile criterion: block values, histograms, selection state
     long long iter = 0;                // coarse steps taken (M_AdvanceLoop counter i)
     int n_ref_last = 0, n_coarse_last = 0;   // marks acted on by the last refinement pass
     std::string err;

@@ -1,21 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the B200 octree-AMR lattice Boltzmann time step.
 
-One "step" is one coarse time step of the solver (Solver::S_Advance from
-N_LEVEL_START) on the workload named in the JSON line.  Metric: MLUPS
-(million lattice-cell updates per second, level-L leaf cells counted 2^(L-L0)
-times per coarse step as solver_lbm_advance.cu:74-89 counts them).
+One "step" is one coarse time step of the solver (Mesh::M_Advance_Step: the
+S_Advance recursion from N_LEVEL_START over every level, plus the
+solution-based refinement when its P_REFINE turn comes) on the workload named
+in the JSON line.  Metric: MLUPS, million lattice-cell updates per second,
+leaf cells of level L counted 2^(L-L0) times per coarse step as
+solver_lbm_advance.cu:74-89 counts them.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+Default workload: D2Q9 lid-driven cavity on a 128^2 base grid with up to 3
+levels, refined above the 90th and coarsened below the 50th percentile of the
+block vorticity every 64 coarse steps, Re = 1000, lid 0.05, FP16 weight-offset
+populations.  The multi-level hierarchy is developed by an untimed spin-up
+before the warm-up.  The same case in FP32 populations is timed beside it
+(`plain_fp32`).
+
 --impl b200 (default): the CUDA library.  Rank 0 prints one JSON line with
   value        device-timed MLUPS (CUDA events on the library's stream, L2
-               flushed between steps when the workload fits in L2)
+               flushed between steps when the state fits in L2)
   e2e          MLUPS through the public C ABI with host buffers: load the
-               initial populations from pinned host memory, K x (advance +
-               read back the FP64 mass/momentum), dump the final populations
-  roofline     the fused step kernel on a large case of the same physics
-               (inputs far larger than L2), algorithmic bytes 2*Q*s per cell
+               populations from pinned host memory, K x (coarse step + read
+               back the FP64 mass/momentum), dump the populations
+  roofline     the fused step kernel on a large single-level case of the same
+               physics and storage (inputs far larger than L2), algorithmic
+               bytes 2*Q*s per cell update
   cpu_baseline the CPU oracle (OpenMP restatement of the reference algorithm)
                on a bounded sample of the same workload, rank 0 only
 --impl reference: the reference's algorithm on the host cores (the CPU oracle
@@ -49,8 +59,20 @@ from agal_b200 import _lib  # noqa: E402
 
 L2_BYTES = 126 * 2 ** 20
 
+_AMR = dict(amr=True, levels=3, p_refine=64, Re=1000.0, bc=_lib.BC_LDC2D, velocity_set=_lib.D2Q9, Nx=128,
+            interp=_lib.INTERP_CUBIC, spinup=1280)
 # Workloads (synthetic: initialised at rest, nothing read from disk).
 WORKLOADS = {
+    "amr_ldc2d_128_fp16": dict(
+        _AMR, storage=_lib.STORE_FP16,
+        desc="D2Q9 BGK lid-driven cavity, 128^2 base in 4^2-cell blocks, up to 3 levels, percentile vorticity "
+             "criterion (refine > p90, coarsen < p50) every 64 coarse steps, Re=1000, lid 0.05, cubic "
+             "interpolation, FP16 weight-offset populations"),
+    "amr_ldc2d_128": dict(
+        _AMR, storage=_lib.STORE_FP32,
+        desc="D2Q9 BGK lid-driven cavity, 128^2 base in 4^2-cell blocks, up to 3 levels, percentile vorticity "
+             "criterion (refine > p90, coarsen < p50) every 64 coarse steps, Re=1000, lid 0.05, cubic "
+             "interpolation, FP32 populations"),
     "ldc2d_256": dict(
         desc="D2Q9 BGK lid-driven cavity 256x256, one level, Re=100, lid 0.05, FP32 populations",
         velocity_set=_lib.D2Q9, Nx=256, Re=100.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC2D),
@@ -60,6 +82,9 @@ WORKLOADS = {
     "ldc2d_4096": dict(
         desc="D2Q9 BGK lid-driven cavity 4096x4096, one level, Re=100, lid 0.05, FP32 populations",
         velocity_set=_lib.D2Q9, Nx=4096, Re=100.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC2D),
+    "ldc2d_4096_fp16": dict(
+        desc="D2Q9 BGK lid-driven cavity 4096x4096, one level, Re=100, lid 0.05, FP16 weight-offset populations",
+        velocity_set=_lib.D2Q9, Nx=4096, Re=100.0, storage=_lib.STORE_FP16, bc=_lib.BC_LDC2D),
     "ldc2d_8192": dict(
         desc="D2Q9 BGK lid-driven cavity 8192x8192, one level, Re=100, lid 0.05, FP32 populations",
         velocity_set=_lib.D2Q9, Nx=8192, Re=100.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC2D),
@@ -78,23 +103,59 @@ DIM_OF = {_lib.D2Q9: 2, _lib.D3Q19: 3, _lib.D3Q27: 3}
 ESIZE = {_lib.STORE_FP32: 4, _lib.STORE_FP64: 8, _lib.STORE_FP16: 2, _lib.STORE_BF16: 2}
 DTYPE_NAME = {_lib.STORE_FP32: "f32", _lib.STORE_FP64: "f64", _lib.STORE_FP16: "f16-offset(f32 math)",
               _lib.STORE_BF16: "bf16-offset(f32 math)"}
+ROOFLINE_FOR = {_lib.STORE_FP16: "ldc2d_8192_fp16", _lib.STORE_FP32: "ldc2d_8192"}
 
 
 def make_params(w: dict, device: int = -1):
     dim = DIM_OF[w["velocity_set"]]
     nb = (w["Nx"] // 4) ** dim
-    return ag.default_params(
-        velocity_set=w["velocity_set"], Nx=w["Nx"], MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1,
-        N_LEVEL_START=0, v0=0.05 / w["Re"], bc_preset=w["bc"], ic_preset=_lib.IC_REST,
-        storage=w["storage"], n_maxcblocks=nb, device=device)
+    kw = dict(velocity_set=w["velocity_set"], Nx=w["Nx"], MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1,
+              N_LEVEL_START=0, v0=0.05 / w["Re"], bc_preset=w["bc"], ic_preset=_lib.IC_REST,
+              storage=w["storage"], n_maxcblocks=nb, device=device)
+    if w.get("amr"):
+        nch = 2 ** dim
+        kw.update(MAX_LEVELS_INTERIOR=w["levels"], P_REFINE=w["p_refine"], S_CRITERION=_lib.CRITERION_PERCENTILE,
+                  ref_pct_hi=0.9, ref_pct_lo=0.5, interp_order=w["interp"],
+                  n_maxcblocks=sum(nb * nch ** L for L in range(w["levels"])) + 64)
+    return ag.default_params(**kw)
 
 
-def cells_per_step(w: dict) -> int:
-    return w["Nx"] ** DIM_OF[w["velocity_set"]]
+def leaf_cells(counts: dict, dim: int) -> int:
+    """Cell updates of one coarse step (solver_lbm_advance.cu:74-89): leaf
+    blocks of level L, counted 2^L times, times the cells per block."""
+    n = counts["n_ids"]
+    ml = counts["max_levels"]
+    nch, mc = 2 ** dim, 4 ** dim
+    cells = 0
+    for L in range(ml):
+        leaves = n[L] - (n[L + 1] // nch if L + 1 < ml else 0)
+        cells += (1 << L) * leaves
+    return cells * mc
 
 
-def state_bytes(w: dict) -> int:
-    return cells_per_step(w) * Q_OF[w["velocity_set"]] * ESIZE[w["storage"]]
+def state_bytes(case, w: dict) -> int:
+    c = case.counts()
+    return sum(c["n_ids"][: c["max_levels"]]) * 4 ** DIM_OF[w["velocity_set"]] * Q_OF[w["velocity_set"]] * \
+        ESIZE[w["storage"]]
+
+
+def launches_per_step(counts: dict, amr: bool) -> int:
+    """Kernels of one coarse step, from the structure of the level recursion:
+    level L takes 2^L sub-steps, each a fused step and its stream-guard
+    fix-up, and every non-empty level below the finest launches 2^L
+    interpolations and 2^L averagings."""
+    if not amr:
+        return 2
+    n, ml = counts["n_ids"], counts["max_levels"]
+    total = 0
+    for L in range(ml):
+        if n[L] == 0:
+            continue
+        mult = 1 << L
+        total += 2 * mult
+        if L < ml - 1:
+            total += 2 * mult
+    return total
 
 
 # ---------------------------------------------------------------------------
@@ -153,6 +214,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
+
+
 def measured_peak_hbm() -> tuple[float, str]:
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -176,21 +239,44 @@ def dram_traffic_per_launch(workload: str):
 
 
 # ---------------------------------------------------------------------------
-def time_steps(case, torch, n_steps: int, flush: bool) -> list[float]:
-    """Per-step device time (ms) with CUDA events on the library's stream."""
+def step_fn(case, w: dict):
+    """One coarse step: the captured multi-level step (with its regrid turn)
+    or the fused single-level step."""
+    if w.get("amr"):
+        return lambda: case.advance_n(1, use_graph=True)
+    return case.advance
+
+
+def time_steps(case, torch, w: dict, n_steps: int, flush: bool):
+    """Per-step device time (ms) with CUDA events on the library's stream,
+    and the cell updates of each step."""
     stream = torch.cuda.ExternalStream(case.stream_ptr())
     scratch = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda") if flush else None
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n_steps)]
+    step = step_fn(case, w)
+    dim = DIM_OF[w["velocity_set"]]
+    cells, launches = [], 0
     for i in range(n_steps):
         if flush:
             with torch.cuda.stream(stream):
                 scratch.add_(1.0)   # writes 252 MB > L2 between timed steps
+        cnt = case.counts()
+        cells.append(leaf_cells(cnt, dim))
+        launches += launches_per_step(cnt, w.get("amr", False))
         evs[i][0].record(stream)
-        case.advance()
+        step()
         evs[i][1].record(stream)
     case.sync()
     torch.cuda.synchronize()
-    return [a.elapsed_time(b) for a, b in evs]
+    return [a.elapsed_time(b) for a, b in evs], cells, launches
+
+
+def develop(case, w: dict):
+    """Initial state, then the untimed spin-up that builds the hierarchy."""
+    case.set_ic(0)
+    if w.get("amr"):
+        case.refine_near_wall()
+        case.advance_n(w["spinup"], use_graph=True)
 
 
 def run_cpu_oracle(w: dict, seconds: float, threads: int, max_steps: int | None = None) -> dict:
@@ -199,20 +285,29 @@ def run_cpu_oracle(w: dict, seconds: float, threads: int, max_steps: int | None 
     build()
     p = make_params(w)
     o = OracleCase(p, p.n_maxcblocks, fp64=(w["storage"] == _lib.STORE_FP64), threads=threads)
+    dim = DIM_OF[w["velocity_set"]]
     o.set_ic(0)
+    spin = 0
+    if w.get("amr"):
+        o.refine_near_wall()
+        spin = w["spinup"]
+        o.advance_n(spin)
     t0 = time.perf_counter()
     o.advance_n(2)
     per = (time.perf_counter() - t0) / 2
     n = max(1, int(seconds / max(per, 1e-9)))
     if max_steps:
         n = min(n, max_steps)
+    cells = 0
     t0 = time.perf_counter()
-    o.advance_n(n)
+    for _ in range(n):
+        cells += leaf_cells(o.counts(), dim)
+        o.advance_n(1)
     dt = time.perf_counter() - t0
     o.close()
-    mlups = cells_per_step(w) * n / dt / 1e6
-    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": f"{n} steps of {w['desc']} on {threads} host threads ({dt:.1f} s)"}
+    return {"value": cells / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{n} coarse steps of {w['desc']}" + (f" after a {spin}-step spin-up" if spin else "") +
+                      f", on {threads} host threads ({dt:.1f} s)"}
 
 
 def dist_setup():
@@ -222,14 +317,25 @@ def dist_setup():
     return ws, rank, local
 
 
+def regrid_launches(counts: dict) -> int:
+    """Kernels of one solution-based refinement, approximately: per parent
+    level a refresh and a grid average, a refresh and an interface
+    interpolation; the percentile criterion (block maxima, 4 x 2 selection
+    passes, marks); about 40 in the refine/coarsen pass."""
+    ml = counts["max_levels"]
+    return 4 * (ml - 1) + 10 + 40
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", default="ldc2d_256", choices=sorted(WORKLOADS))
-    ap.add_argument("--roofline-workload", default="ldc2d_8192", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="amr_ldc2d_128_fp16", choices=sorted(WORKLOADS))
+    ap.add_argument("--plain-workload", default="amr_ldc2d_128", choices=sorted(WORKLOADS),
+                    help="the same case in plain FP32, timed beside the headline workload")
+    ap.add_argument("--roofline-workload", default=None, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
@@ -242,10 +348,11 @@ def main(argv=None) -> int:
     if a.profile:
         pw = WORKLOADS[a.profile]
         with ag.Case(make_params(pw, device=0)) as pc:
-            pc.set_ic(0)
+            develop(pc, pw)
             pc.set_tuning(a.cpt)
+            step = step_fn(pc, pw)
             for _ in range(a.warmup + a.steps):
-                pc.advance()
+                step()
             pc.sync()
         print(f"profile run done: {a.profile}, {a.warmup}+{a.steps} steps")
         return 0
@@ -256,14 +363,22 @@ def main(argv=None) -> int:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": DTYPE_NAME[w["storage"]], "data": "synthetic (fluid at rest, lid-driven)"}
 
+    def config_of(wl: str, extra: dict) -> dict:
+        ww = WORKLOADS[wl]
+        cfg = {"workload": wl, "desc": ww["desc"]}
+        if ww.get("amr"):
+            cfg.update(base_grid=f"{ww['Nx']}^2", levels=ww["levels"], regrid_every=ww["p_refine"],
+                       spinup_steps=ww["spinup"])
+        cfg.update(extra)
+        return cfg
+
     if a.impl == "reference":
         # The reference algorithm on the host cores; other ranks idle.
         if rank != 0:
             return 0
         cb = run_cpu_oracle(w, seconds=1e9, threads=threads, max_steps=a.steps)
         line = dict(base, impl="reference", value=cb["value"], ms_per_step=None,
-                    config={"workload": a.workload, "desc": w["desc"], "cells": cells_per_step(w),
-                            "parallelism": "host OpenMP", "l2": "n/a (CPU)"},
+                    config=config_of(a.workload, {"parallelism": "host OpenMP", "l2": "n/a (CPU)"}),
                     cpu_baseline=cb, e2e={"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0})
         line["n_gpus"] = 0
@@ -288,40 +403,68 @@ def main(argv=None) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # --- device-timed steps -------------------------------------------------
-    p = make_params(w, device=local)
-    case = ag.Case(p)
-    case.set_ic(0)
-    tune = case.autotune(0, reps=10)
-    for _ in range(a.warmup):
-        case.advance()
-    case.sync()
-    flush = state_bytes(w) * 2 < L2_BYTES
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        per_step = time_steps(case, torch, a.steps, flush)
-    barrier()
-    t_ms = allmax(sum(per_step))
-    value = ws * cells_per_step(w) * a.steps / (t_ms * 1e-3) / 1e6
-    case.close()
+    def allsum(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def device_timed(wl: str, with_clocks: bool):
+        ww = WORKLOADS[wl]
+        case = ag.Case(make_params(ww, device=local))
+        develop(case, ww)
+        tune = case.autotune(0, reps=10)
+        step = step_fn(case, ww)
+        for _ in range(a.warmup):
+            step()
+        case.sync()
+        flush = state_bytes(case, ww) * 2 < L2_BYTES
+        barrier()
+        torch.cuda.synchronize()
+        it0 = case.refine_stats()["iter"]
+        if with_clocks:
+            with ClockSampler(local) as clk:
+                per_step, cells, launches = time_steps(case, torch, ww, a.steps, flush)
+            clocks = clk.summary()
+        else:
+            per_step, cells, launches = time_steps(case, torch, ww, a.steps, flush)
+            clocks = None
+        if ww.get("amr"):
+            p_ref = ww["p_refine"]
+            regrids = sum(1 for i in range(it0, it0 + a.steps) if (i + 1) % p_ref == 0 and i > 0)
+            launches += regrids * regrid_launches(case.counts())
+        counts = case.counts()
+        barrier()
+        t_ms = allmax(sum(per_step))
+        mlups = allsum(float(sum(cells))) / (t_ms * 1e-3) / 1e6
+        case.close()
+        return dict(value=mlups, ms_per_step=t_ms / a.steps, flush=flush, tune=tune, clocks=clocks,
+                    launches=launches, counts=counts, cells_per_step=float(np.mean(cells)))
+
+    # --- device-timed steps: headline workload, then the plain FP32 form -------
+    head = device_timed(a.workload, with_clocks=True)
+    plain = device_timed(a.plain_workload, with_clocks=False) if a.plain_workload != a.workload else None
 
     # --- end to end through the C ABI with host buffers ----------------------
-    p = make_params(w, device=local)
-    case = ag.Case(p)
-    case.set_ic(0)
-    case.set_tuning(tune["variant"])
+    case = ag.Case(make_params(w, device=local))
+    develop(case, w)
+    case.set_tuning(head["tune"]["variant"])
     f0 = case.dump(_lib.ARR_F)
     pinned = torch.from_numpy(f0).pin_memory()
     host_in = pinned.numpy()
     host_out = torch.empty_like(pinned).pin_memory().numpy()
     mm = (C.c_double * 4)()
     lib = _lib.lib()
+    dim = DIM_OF[w["velocity_set"]]
+    amr = bool(w.get("amr"))
+    e2e_cells = 0
     barrier()
     t0 = time.perf_counter()
     rc = lib.agal_load(case._h, _lib.ARR_F, host_in.ctypes.data_as(C.c_void_p), host_in.nbytes)
     for _ in range(a.steps):
-        rc |= lib.agal_advance(case._h, 0)
+        e2e_cells += leaf_cells(case.counts(), dim)
+        rc |= lib.agal_advance_n(case._h, 1, 1) if amr else lib.agal_advance(case._h, 0)
         rc |= lib.agal_mass_momentum(case._h, mm)   # D2H of the step's FP64 mass/momentum
     rc |= lib.agal_dump(case._h, _lib.ARR_F, host_out.ctypes.data_as(C.c_void_p), host_out.nbytes)
     e2e_s = time.perf_counter() - t0
@@ -329,31 +472,30 @@ def main(argv=None) -> int:
         raise RuntimeError("e2e run failed")
     e2e_s = allmax(e2e_s)
     case.close()
-    e2e = {"value": ws * cells_per_step(w) * a.steps / e2e_s / 1e6, "unit": "MLUPS",
+    e2e = {"value": allsum(float(e2e_cells)) / e2e_s / 1e6, "unit": "MLUPS",
            "h2d_bytes_per_step": int(host_in.nbytes / a.steps),
-           "d2h_bytes_per_step": int(host_out.nbytes / a.steps) + 8 * (DIM_OF[w["velocity_set"]] + 1)}
+           "d2h_bytes_per_step": int(host_out.nbytes / a.steps) + 8 * (dim + 1)}
 
     # --- roofline of the fused step kernel on a large case -------------------
-    rw = WORKLOADS[a.roofline_workload]
-    rp = make_params(rw, device=local)
-    rcase = ag.Case(rp)
+    rwl = a.roofline_workload or ROOFLINE_FOR.get(w["storage"], "ldc2d_8192")
+    rw = WORKLOADS[rwl]
+    rcase = ag.Case(make_params(rw, device=local))
     rcase.set_ic(0)
     rtune = rcase.autotune(0, reps=5)
     for _ in range(3):
         rcase.advance()
     rcase.sync()
-    rsteps = 20
-    rt = time_steps(rcase, torch, rsteps, flush=False)
+    rt, rcells, _ = time_steps(rcase, torch, rw, 20, flush=False)
     rcase.close()
     avg_ms = sum(rt) / len(rt)
-    alg_bytes = 2 * Q_OF[rw["velocity_set"]] * ESIZE[rw["storage"]] * cells_per_step(rw)
+    alg_bytes = 2 * Q_OF[rw["velocity_set"]] * ESIZE[rw["storage"]] * rcells[0]
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic = dram_traffic_per_launch(a.roofline_workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_kind, "kernel": "k_step (fused collide+BC+stream)",
-                "workload": a.roofline_workload, "algorithmic_bytes_per_launch": alg_bytes,
-                "avg_launch_ms": avg_ms, "autotune": rtune}
+                "traffic": dram_traffic_per_launch(rwl), "peak_source": peak_kind,
+                "kernel": "k_step (fused collide+BC+stream) + its stream-guard fix-up",
+                "workload": rwl, "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+                "autotune": rtune}
 
     # --- CPU baseline (rank 0 only) -------------------------------------------
     cpu = None
@@ -363,13 +505,18 @@ def main(argv=None) -> int:
     if ws > 1:
         dist.destroy_process_group()
     if rank == 0:
-        line = dict(base, value=value, ms_per_step=t_ms / a.steps,
-                    config={"workload": a.workload, "desc": w["desc"], "cells": cells_per_step(w),
-                            "parallelism": f"replicas x{ws}",
-                            "l2": "flushed between timed steps" if flush else "inputs larger than L2",
-                            "autotune": tune},
-                    e2e=e2e, roofline=roofline, cpu_baseline=cpu, clocks=clk.summary(),
-                    gpu_launches=a.steps)
+        extra = {"parallelism": f"replicas x{ws}",
+                 "l2": "flushed between timed steps" if head["flush"] else "inputs larger than L2",
+                 "autotune": head["tune"], "blocks_per_level": head["counts"]["n_ids"][:-1],
+                 "cell_updates_per_step": head["cells_per_step"]}
+        line = dict(base, value=head["value"], ms_per_step=head["ms_per_step"],
+                    config=config_of(a.workload, extra), e2e=e2e, roofline=roofline, cpu_baseline=cpu,
+                    clocks=head["clocks"], gpu_launches=head["launches"])
+        if plain is not None:
+            line["plain_fp32"] = {"workload": a.plain_workload, "value": plain["value"],
+                                  "ms_per_step": plain["ms_per_step"],
+                                  "blocks_per_level": plain["counts"]["n_ids"][:-1],
+                                  "ratio": head["value"] / plain["value"]}
         print(json.dumps(line), flush=True)
     return 0
 

@@ -71,6 +71,12 @@ extern "C" {
 #define AGAL_REGION_BOUNDARY 1   /* blocks on the domain boundary (onb == 1)      */
 #define AGAL_REGION_BOX      2   /* blocks inside [0.25, 0.75]^d (coordinates)    */
 
+/* S_CRITERION values: solver_lbm_criterion.cu:572-575 (0, 1) and the
+   percentile mode of this library (2) */
+#define AGAL_CRITERION_VORTICITY  0
+#define AGAL_CRITERION_Q          1
+#define AGAL_CRITERION_PERCENTILE 2
+
 /* interpolation / averaging modes, inc/mesh.h:58-62 */
 #define AGAL_INTERP_INTERFACE 0
 #define AGAL_INTERP_ADDED     1
@@ -122,6 +128,11 @@ typedef struct agal_params {
     int bc_preset;        /* AGAL_BC_*                           */
     int ic_preset;        /* AGAL_IC_*                           */
     int region_preset;    /* AGAL_REGION_*                       */
+    /* S_CRITERION = AGAL_CRITERION_PERCENTILE: leaf blocks whose maximum
+       vorticity magnitude lies above the ref_pct_hi quantile of all leaf
+       blocks are refined, refined blocks below the ref_pct_lo quantile
+       coarsened (no reference counterpart). */
+    double ref_pct_hi, ref_pct_lo;
     double u_ref;         /* velocity of the presets (custom.h hard-codes 0.05) */
     double ic_noise;      /* relative amplitude of seeded IC noise (0 = none)   */
     uint64_t seed;        /* seed of the IC noise                               */

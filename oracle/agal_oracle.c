@@ -282,6 +282,7 @@ int orc_average(orc_case *c, int L, int var)
 
 int orc_ref_criteria(orc_case *c)
 {
+    if (c->P.S_CRITERION == AGAL_CRITERION_PERCENTILE) return DISPATCH(ref_criteria_pct, c);
     return DISPATCH(ref_criteria, c);
 }
 

@@ -528,3 +528,116 @@ static int FN(ref_criteria)(orc_case *c)
     }
     return 0;
 }
+
+/* ---------------------------------------------------------------------------
+ * Percentile criterion (S_CRITERION = AGAL_CRITERION_PERCENTILE; the
+ * reference has no counterpart).  Per block the maximum vorticity magnitude
+ * over its non-ghost cells, from the macros of the last refresh, with the
+ * halo of solver_lbm_criterion.cu (fourth-order extrapolation) and central
+ * differences at the block's own spacing.  Every operation is written in the
+ * order the CUDA kernel rounds it (this file is compiled without
+ * contraction).  Leaf blocks above the ref_pct_hi quantile of all leaf
+ * blocks are refined, refined blocks below the ref_pct_lo quantile coarsened.
+ */
+static R FN(xpol4)(R a, R b, R c4, R d)
+{
+    return (((R)4 * a + (R)(-6) * b) + (R)4 * c4) + (R)(-1) * d;
+}
+
+static R FN(block_wmax)(const orc_case *c, int b, R dxL)
+{
+    const R *F = (const R *)c->F;
+    const int64_t nmc = c->nmc;
+    const int Q = c->Q, MC = c->MC, dim = c->dim;
+    R h[3][216];
+#define HX(i, j, k) (((i) + 1) + 6 * ((j) + 1) + (dim == 3 ? 36 * ((k) + 1) : 0))
+    for (int comp = 0; comp < dim; comp++) {
+        R *s = h[comp];
+        for (int t = 0; t < MC; t++) {
+            int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? t / 16 : 0;
+            s[HX(I, J, K)] = F[(int64_t)b * MC + t + (int64_t)(Q + 1 + comp) * nmc];
+        }
+        for (int t = 0; t < MC; t++) {
+            int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? t / 16 : 0;
+            if (I == 0) {
+                s[HX(-1, J, K)] = FN(xpol4)(s[HX(0, J, K)], s[HX(1, J, K)], s[HX(2, J, K)], s[HX(3, J, K)]);
+                s[HX(4, J, K)] = FN(xpol4)(s[HX(3, J, K)], s[HX(2, J, K)], s[HX(1, J, K)], s[HX(0, J, K)]);
+            }
+            if (J == 0) {
+                s[HX(I, -1, K)] = FN(xpol4)(s[HX(I, 0, K)], s[HX(I, 1, K)], s[HX(I, 2, K)], s[HX(I, 3, K)]);
+                s[HX(I, 4, K)] = FN(xpol4)(s[HX(I, 3, K)], s[HX(I, 2, K)], s[HX(I, 1, K)], s[HX(I, 0, K)]);
+            }
+            if (dim == 3 && K == 0) {
+                s[HX(I, J, -1)] = FN(xpol4)(s[HX(I, J, 0)], s[HX(I, J, 1)], s[HX(I, J, 2)], s[HX(I, J, 3)]);
+                s[HX(I, J, 4)] = FN(xpol4)(s[HX(I, J, 3)], s[HX(I, J, 2)], s[HX(I, J, 1)], s[HX(I, J, 0)]);
+            }
+        }
+    }
+    const R h2 = (R)2 * dxL;
+    R wmax = (R)0;
+    for (int t = 0; t < MC; t++) {
+        if (c->cells_ID_mask[(int64_t)b * MC + t] == ORC_CELL_GHOST) continue;
+        int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? t / 16 : 0;
+        R g[3][3] = {{0}};
+        for (int comp = 0; comp < dim; comp++) {
+            const R *s = h[comp];
+            g[comp][0] = (s[HX(I + 1, J, K)] - s[HX(I - 1, J, K)]) / h2;
+            g[comp][1] = (s[HX(I, J + 1, K)] - s[HX(I, J - 1, K)]) / h2;
+            if (dim == 3) g[comp][2] = (s[HX(I, J, K + 1)] - s[HX(I, J, K - 1)]) / h2;
+        }
+        R w;
+        if (dim == 2) {
+            w = (R)fabs((double)(g[1][0] - g[0][1]));
+        } else {
+            const R wx = g[2][1] - g[1][2], wy = g[0][2] - g[2][0], wz = g[1][0] - g[0][1];
+            const R ss = (wx * wx + wy * wy) + wz * wz;
+            w = (sizeof(R) == 4) ? (R)sqrtf((float)ss) : (R)sqrt((double)ss);
+        }
+        if (w > wmax) wmax = w;
+    }
+#undef HX
+    return wmax;
+}
+
+static int FN(cmp_r)(const void *a, const void *b)
+{
+    const R x = *(const R *)a, y = *(const R *)b;
+    return (x > y) - (x < y);
+}
+
+static int FN(ref_criteria_pct)(orc_case *c)
+{
+    const int64_t nmb = c->nmb;
+    const int idm = c->id_max[c->max_levels], Qmax = c->Qmax;
+    const int MLI = c->P.MAX_LEVELS_INTERIOR;
+    R *w = (R *)malloc(sizeof(R) * (size_t)(idm > 0 ? idm : 1));
+    R *pop = (R *)malloc(sizeof(R) * (size_t)(idm > 0 ? idm : 1));
+    if (!w || !pop) { free(w); free(pop); return AGAL_ERR_OOM; }
+    int n = 0;
+    for (int b = 0; b < idm; b++) {
+        w[b] = (R)-1;
+        if (c->cblock_ID_ref[b] == ORC_REF_INACTIVE) continue;
+        const int L = c->cblock_level[b];
+        const R dxL = c->fp64 ? (R)c->dxf_d[L] : (R)c->dxf[L];
+        w[b] = FN(block_wmax)(c, b, dxL);
+        if (c->cblock_ID_nbr_child[b] < 0) pop[n++] = w[b];
+    }
+    if (n > 0) {
+        qsort(pop, (size_t)n, sizeof(R), FN(cmp_r));
+        const R thr_hi = pop[(int)floor(c->P.ref_pct_hi * (double)(n - 1))];
+        const R thr_lo = pop[(int)floor(c->P.ref_pct_lo * (double)(n - 1))];
+        for (int b = 0; b < idm; b++) {
+            const int r = c->cblock_ID_ref[b];
+            if (r == ORC_REF_INACTIVE) continue;
+            int eligible = 1;
+            for (int p = 0; p < Qmax; p++)
+                if (c->cblock_ID_nbr[b + (int64_t)p * nmb] == ORC_N_SKIPID) eligible = 0;
+            if (r == ORC_REF_UNREFINED && eligible && c->cblock_level[b] < MLI - 1 && w[b] > thr_hi)
+                c->cblock_ID_ref[b] = ORC_REF_MARK_REFINE;
+            if (r == ORC_REF_REFINED && w[b] < thr_lo) c->cblock_ID_ref[b] = ORC_REF_MARK_COARSEN;
+        }
+    }
+    free(w);
+    free(pop);
+    return 0;
+}

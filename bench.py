@@ -342,11 +342,15 @@ def main(argv=None) -> int:
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
     ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3],
                     help="with --profile: step kernel variant (1, 2 cells per thread; 3 TMA pipeline)")
+    ap.add_argument("--spinup", type=int, default=None,
+                    help="with --profile: coarse steps of the untimed spin-up of a multi-level workload")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     w = WORKLOADS[a.workload]
     if a.profile:
-        pw = WORKLOADS[a.profile]
+        pw = dict(WORKLOADS[a.profile])
+        if a.spinup is not None and pw.get("amr"):
+            pw["spinup"] = a.spinup
         with ag.Case(make_params(pw, device=0)) as pc:
             develop(pc, pw)
             pc.set_tuning(a.cpt)

@@ -67,7 +67,7 @@ struct agal_ctx {
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
-    int *fix_count = nullptr;          // [0] stream-guard fix-ups of the running step, [1] finished CTAs (finish_step)
+    int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
     long long *fix_list = nullptr;
     // refine/coarsen pass scratch (multi-level cases only), one allocation:
     int *amr = nullptr;

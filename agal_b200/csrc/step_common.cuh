@@ -41,12 +41,10 @@ struct StepArgs {
     double u_ref;
     int bc_preset;
     // Links whose in-place swap the reference's guard would refuse (see
-    // push_cell): appended here, swapped back by the last CTA (finish_step).
+    // push_cell): appended here, swapped back by k_stream_fixup.
     int *fix_count;
     long long *fix_list;   // [fix_cap][2] element offsets into fout
     int fix_cap;
-    unsigned *fix_done;    // CTAs of this launch that have finished (ticket counter, starts at 0)
-    int *status;           // device status word (AGAL_ERR_STATE on a fix-up list overflow)
 };
 
 // Boundary hook presets (inc/custom.h:79-122); f is the full population.
@@ -191,7 +189,7 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
     // positive (kernels.cu:620-628, the solid-cell guard f_pb > 0).  Here each
     // cell pushes unconditionally; the cell on the non-owning side of an open
     // link, which holds that value, records the link when it is not positive,
-    // and finish_step swaps the two pushed entries back, which is exactly
+    // and k_stream_fixup swaps the two pushed entries back, which is exactly
     // the refused swap.  Non-positive populations are rare (strong
     // over-relaxation near singular corners), so the list stays short.
     auto guard = [&](int p, bool open, long long dst) {
@@ -241,41 +239,6 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
                 own[p * MC] = ST<T>::enc(v);
             }
         }
-    }
-}
-
-// End of a step launch, called by every thread of every CTA: the last CTA
-// to finish (completion ticket after a fence, so every other CTA's pushes
-// and list entries are visible) swaps back the pushed entries of the links
-// whose swap the reference's stream guard refuses, then resets the list and
-// the ticket for the next launch.  No CTA waits for another.
-template <typename T>
-__device__ __forceinline__ void finish_step(const StepArgs &a, T *fo)
-{
-    __shared__ int s_last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned t = atomicAdd(a.fix_done, 1u);
-        s_last = (t == gridDim.x * gridDim.y * gridDim.z - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const int n = atomicAdd(a.fix_count, 0);
-    const int m = n < a.fix_cap ? n : a.fix_cap;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        const long long x = __ldcg(&a.fix_list[2 * i]), y = __ldcg(&a.fix_list[2 * i + 1]);
-        const T vx = __ldcg(fo + x), vy = __ldcg(fo + y);
-        fo[x] = vy;
-        fo[y] = vx;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        if (n > a.fix_cap) atomicCAS(a.status, 0, AGAL_ERR_STATE);
-        *a.fix_count = 0;
-        *a.fix_done = 0u;
-        __threadfence();
     }
 }
 

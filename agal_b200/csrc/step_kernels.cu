@@ -65,20 +65,19 @@ k_step(const StepArgs a)
     }
     __syncthreads();
     const int fl = s_meta[lb][Meta<DIM>::FLAGS];
+    if (b < 0 || !(fl & META_ACTIVE)) return;
+
     T *__restrict__ fo = static_cast<T *>(a.fout);
-    if (b >= 0 && (fl & META_ACTIVE)) {
-        const int *nrow = s_meta[lb];
-        const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
+    const int *nrow = s_meta[lb];
+    const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
 #pragma unroll
-        for (int h = 0; h < CPT; h++) {
-            const int t = t0 + h * TPB;
-            if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;   // solid cells keep their guard
-            C ux, uy, uz;
-            bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], C(a.omega), ux, uy, uz);
-            push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
-        }
+    for (int h = 0; h < CPT; h++) {
+        const int t = t0 + h * TPB;
+        if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;   // solid cells keep their guard
+        C ux, uy, uz;
+        bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], C(a.omega), ux, uy, uz);
+        push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
     }
-    finish_step<T>(a, fo);
 }
 
 // ---------------------------------------------------------------------------
@@ -302,6 +301,28 @@ int launch_step(agal_ctx *c, const StepArgs &a, int n)
     return AGAL_OK;
 }
 
+// Swap back the pushed entries of every link whose swap the reference's
+// stream guard refuses (recorded by push_cell), then clear the list for the
+// next step.  One CTA; the list is usually empty.  A list longer than its
+// capacity leaves AGAL_ERR_STATE in the status word (reported by agal_sync).
+template <typename T>
+__global__ void __launch_bounds__(256) k_stream_fixup(T *fo, int *count, const long long *list, int cap, int *status)
+{
+    const int n = *count;
+    const int m = n < cap ? n : cap;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const long long x = list[2 * i], y = list[2 * i + 1];
+        const T vx = fo[x];
+        fo[x] = fo[y];
+        fo[y] = vx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n > cap) atomicCAS(status, 0, AGAL_ERR_STATE);
+        *count = 0;
+    }
+}
+
 template <int DIM, int Q, typename T> struct RunStep {
     // flip = false launches the kernel from the current buffer into the
     // other one without making it current (used by the autotuner: the step is
@@ -327,13 +348,14 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.fix_count = c->fix_count;
         a.fix_list = c->fix_list;
         a.fix_cap = AGAL_FIX_CAP;
-        a.fix_done = reinterpret_cast<unsigned *>(c->fix_count + 1);
-        a.status = c->d_status;
         if (cpt <= 0) cpt = c->step_cpt;
         const int rc = (cpt == 3)   ? launch_step_tma<DIM, Q, T>(c, a)
                        : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                                     : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
+        k_stream_fixup<T><<<1, 256, 0, c->stream>>>(static_cast<T *>(a.fout), c->fix_count, c->fix_list,
+                                                    AGAL_FIX_CAP, c->d_status);
+        AGAL_CUDA(c, cudaGetLastError());
         if (flip) c->cur[L] = 1 - c->cur[L];
         return AGAL_OK;
     }

@@ -219,7 +219,6 @@ k_step_tma(const StepArgs a, int *status)
             mbar_arrive(&empty[s]);
         }
     }
-    finish_step<T>(a, static_cast<T *>(a.fout));
 }
 
 // Kernel attributes and persistent grid size, set once per instantiation

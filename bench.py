@@ -141,18 +141,18 @@ def state_bytes(case, w: dict) -> int:
 
 def launches_per_step(counts: dict, amr: bool) -> int:
     """Kernels of one coarse step, from the structure of the level recursion:
-    level L takes 2^L sub-steps, each one fused step kernel, and every
-    non-empty level below the finest launches 2^L interpolations and 2^L
-    averagings."""
+    level L takes 2^L sub-steps, each a fused step and its stream-guard
+    fix-up, and every non-empty level below the finest launches 2^L
+    interpolations and 2^L averagings."""
     if not amr:
-        return 1
+        return 2
     n, ml = counts["n_ids"], counts["max_levels"]
     total = 0
     for L in range(ml):
         if n[L] == 0:
             continue
         mult = 1 << L
-        total += mult
+        total += 2 * mult
         if L < ml - 1:
             total += 2 * mult
     return total
@@ -497,7 +497,7 @@ def main(argv=None) -> int:
     peak, peak_kind = measured_peak_hbm()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": dram_traffic_per_launch(rwl), "peak_source": peak_kind,
-                "kernel": "k_step (fused collide + BC + stream, stream-guard fix-ups by its last CTA)",
+                "kernel": "k_step (fused collide+BC+stream) + its stream-guard fix-up",
                 "workload": rwl, "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "autotune": rtune}
 

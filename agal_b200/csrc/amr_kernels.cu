@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     constexpr bool OFF = ST<T>::OFF;
     __shared__ C sF[MC];
     __shared__ C sW[4][8];
+    pdl_wait();
     // Uniform per CTA: every early return below depends on blockIdx only.
     const int b = a.ids[blockIdx.x];
     if (b < 0) return;
@@ -196,6 +197,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     constexpr bool OFF = ST<T>::OFF;
     __shared__ C sg[NCH * MC];
     __shared__ int smask[NCH * MC];
+    pdl_wait();
     const int b = a.ids[blockIdx.x];
     if (b < 0) return;
     const int bc = a.nbr_child[b];
@@ -549,9 +551,9 @@ template <int DIM, int Q, typename T> struct RunInterp {
         a.var = var;
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
         if (c->P.interp_order == AGAL_INTERP_CUBIC)
-            k_interp<DIM, Q, T, true><<<(unsigned)n, NT, 0, c->stream>>>(a);
+            AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, true>, dim3((unsigned)n), dim3(NT), 0, c->stream, a));
         else
-            k_interp<DIM, Q, T, false><<<(unsigned)n, NT, 0, c->stream>>>(a);
+            AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, false>, dim3((unsigned)n), dim3(NT), 0, c->stream, a));
         AGAL_CUDA(c, cudaGetLastError());
         return AGAL_OK;
     }
@@ -574,7 +576,7 @@ template <int DIM, int Q, typename T> struct RunAverage {
         if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L] / (float)c->tau[L + 1]);
         a.var = var;
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
-        k_average<DIM, Q, T><<<(unsigned)n, NT, 0, c->stream>>>(a);
+        AGAL_CUDA(c, launch_pdl(k_average<DIM, Q, T>, dim3((unsigned)n), dim3(NT), 0, c->stream, a));
         AGAL_CUDA(c, cudaGetLastError());
         return AGAL_OK;
     }

@@ -116,7 +116,10 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     case AGAL_D3Q27: c->dim = 3; c->Q = 27; break;
     default: delete c; return agal_set_err(nullptr, AGAL_ERR_PARAM, "velocity_set");
     }
-    if (p->collision != AGAL_BGK) { delete c; return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "collision operator not built yet"); }
+    if (p->collision != AGAL_BGK && !(p->collision == AGAL_MRT && p->velocity_set == AGAL_D3Q19)) {
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "collision operator: BGK, or MRT with D3Q19");
+    }
     c->Qmax = (c->dim == 2) ? 9 : 27;
     c->MC = (c->dim == 2) ? 16 : 64;
     c->NCH = (c->dim == 2) ? 4 : 8;

@@ -17,6 +17,34 @@ static __device__ const int g_map2[9] = {7, 4, 8, 3, 0, 1, 6, 2, 5};
 static __device__ const int g_map3[27] = {20, 12, 26, 10, 6, 15, 24, 17, 21, 8, 4, 13, 2, 0,
                                    1, 14, 3, 7, 22, 18, 23, 16, 5, 9, 25, 11, 19};
 
+// Programmatic dependent launch.  A kernel launched with launch_pdl may start
+// while its predecessor on the stream is still draining; griddepcontrol.wait
+// blocks until that predecessor has completed and its writes are visible
+// (returns at once when there is none).  Every kernel launched this way calls
+// pdl_wait() before it touches memory, then lets its own successor launch.
+__device__ __forceinline__ void pdl_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...);
+}
+
 // Per-block step metadata row, rebuilt whenever the mesh changes
 // (agal_build_meta): the neighbour block in each lexicographic neighbour slot
 // S (the centre slot holds the block itself) and the step flags.  One
@@ -40,6 +68,8 @@ struct StepArgs {
     double omega;
     double u_ref;
     int bc_preset;
+    int mrt;               // D3Q19 multiple-relaxation-time collision instead of BGK
+    double s[5];           // MRT rates s1, s2, s3, s5, s6
     // Links whose in-place swap the reference's guard would refuse (see
     // push_cell): appended here, swapped back by k_stream_fixup.
     int *fix_count;
@@ -161,6 +191,135 @@ __device__ __forceinline__ void bgk_collide(C (&g)[Q], C omeg, C &ux, C &uy, C &
         g[p] = r_fma(g[p], omegp, r_add(even, odd));
         g[q] = r_fma(g[q], omegp, r_add(even, -odd));
     }
+}
+
+// D3Q19 multiple-relaxation-time collision (d'Humieres moment basis: rho, e,
+// eps, jx, qx, jy, qy, jz, qz, 3pxx, 3pixx, pww, piww, pxy, pyz, pxz, mx, my,
+// mz), with the equilibria of the reference's legacy MRT kernel
+// (solver_old/solver_lbm_collide_mrt_d3q19.cu:131-148; its e equilibrium is read
+// as 19 rho |u|^2).  Rates: s1 (e), s2 (eps), s3 (q), omega_L (3pxx, pww, pxy,
+// pyz, pxz), s5 (3pixx, piww), s6 (mx, my, mz); rho and j are conserved.
+// Entries of the basis, a polynomial in the direction vector:
+__host__ __device__ constexpr int mrt_m(int i, int p)
+{
+    const int x = lat_c(3, 0, p), y = lat_c(3, 1, p), z = lat_c(3, 2, p), c2 = x * x + y * y + z * z;
+    switch (i) {
+    case 0: return 1;
+    case 1: return 19 * c2 - 30;
+    case 2: return (21 * c2 * c2 - 53 * c2 + 24) / 2;
+    case 3: return x;
+    case 4: return (5 * c2 - 9) * x;
+    case 5: return y;
+    case 6: return (5 * c2 - 9) * y;
+    case 7: return z;
+    case 8: return (5 * c2 - 9) * z;
+    case 9: return 3 * x * x - c2;
+    case 10: return (3 * c2 - 5) * (3 * x * x - c2);
+    case 11: return y * y - z * z;
+    case 12: return (3 * c2 - 5) * (y * y - z * z);
+    case 13: return x * y;
+    case 14: return y * z;
+    case 15: return x * z;
+    case 16: return (y * y - z * z) * x;
+    case 17: return (z * z - x * x) * y;
+    default: return (x * x - y * y) * z;
+    }
+}
+// Squared norm of basis row i (the rows are orthogonal: M^-1 = M^T diag(1/n)).
+__host__ __device__ constexpr int mrt_n(int i)
+{
+    int s = 0;
+    for (int p = 0; p < 19; p++) s += mrt_m(i, p) * mrt_m(i, p);
+    return s;
+}
+
+// OFF: g holds weight offsets (rest moments of the weights, rho = 1, e = -11,
+// eps = 3, are carried implicitly).  The rates s = {s1, s2, s3, s5, s6}.
+template <typename C, bool OFF>
+__device__ __forceinline__ void mrt_collide(C (&g)[19], C omeg, const C (&s)[5], C &ux, C &uy, C &uz)
+{
+    C m[19];
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        C acc = C(0);
+#pragma unroll
+        for (int p = 0; p < 19; p++) {
+            const int k = mrt_m(i, p);
+            if (k == 1) acc = r_add(acc, g[p]);
+            else if (k == -1) acc = r_add(acc, -g[p]);
+            else if (k != 0) acc = r_fma(C(k), g[p], acc);
+        }
+        m[i] = acc;
+    }
+    const C drho = m[0];
+    const C rho = OFF ? r_add(C(1), drho) : drho;
+    const C inv = r_div(C(1), rho);
+    ux = r_mul(m[3], inv);
+    uy = r_mul(m[5], inv);
+    uz = r_mul(m[7], inv);
+    const C uu = r_mul(ux, ux), vv = r_mul(uy, uy), ww = r_mul(uz, uz);
+    const C usq = r_add(r_add(uu, vv), ww);
+    const C rusq = r_mul(rho, usq);
+    // deviations of the equilibria from the stored reference (rest moments in
+    // the offset form, zero otherwise)
+    const C dr = OFF ? drho : rho;
+    C eq[19];
+    eq[1] = r_fma(C(19), rusq, r_mul(C(-11), dr));
+    eq[2] = r_fma(C(-5.5), rusq, r_mul(C(3), dr));
+    eq[4] = r_mul(C(-2.0 / 3.0), m[3]);
+    eq[6] = r_mul(C(-2.0 / 3.0), m[5]);
+    eq[8] = r_mul(C(-2.0 / 3.0), m[7]);
+    const C pxx = r_mul(rho, r_add(r_mul(C(2), uu), -r_add(vv, ww)));
+    const C pww = r_mul(rho, r_add(vv, -ww));
+    eq[9] = pxx;
+    eq[10] = r_mul(C(-0.5), pxx);
+    eq[11] = pww;
+    eq[12] = r_mul(C(-0.5), pww);
+    eq[13] = r_mul(rho, r_mul(ux, uy));
+    eq[14] = r_mul(rho, r_mul(uy, uz));
+    eq[15] = r_mul(rho, r_mul(ux, uz));
+    auto relax = [&](int i, C rate, C e) { m[i] = r_add(m[i], -r_mul(rate, r_add(m[i], -e))); };
+    relax(1, s[0], eq[1]);
+    relax(2, s[1], eq[2]);
+    relax(4, s[2], eq[4]);
+    relax(6, s[2], eq[6]);
+    relax(8, s[2], eq[8]);
+    relax(9, omeg, eq[9]);
+    relax(10, s[3], eq[10]);
+    relax(11, omeg, eq[11]);
+    relax(12, s[3], eq[12]);
+    relax(13, omeg, eq[13]);
+    relax(14, omeg, eq[14]);
+    relax(15, omeg, eq[15]);
+    relax(16, s[4], C(0));
+    relax(17, s[4], C(0));
+    relax(18, s[4], C(0));
+#pragma unroll
+    for (int p = 0; p < 19; p++) {
+        C acc = C(0);
+#pragma unroll
+        for (int i = 0; i < 19; i++) {
+            const int k = mrt_m(i, p);
+            if (k != 0) acc = r_fma(C((double)k / (double)mrt_n(i)), m[i], acc);
+        }
+        g[p] = acc;
+    }
+}
+
+// BGK, or for D3Q19 with a.mrt the MRT collision (uniform per launch).
+template <int DIM, int Q, typename T>
+__device__ __forceinline__ void collide_cell(typename ST<T>::C (&g)[Q], const StepArgs &a, typename ST<T>::C &ux,
+                                             typename ST<T>::C &uy, typename ST<T>::C &uz)
+{
+    using C = typename ST<T>::C;
+    if constexpr (Q == 19) {
+        if (a.mrt) {
+            const C s[5] = {C(a.s[0]), C(a.s[1]), C(a.s[2]), C(a.s[3]), C(a.s[4])};
+            mrt_collide<C, ST<T>::OFF>(g, C(a.omega), s, ux, uy, uz);
+            return;
+        }
+    }
+    bgk_collide<DIM, Q, C, ST<T>::OFF>(g, C(a.omega), ux, uy, uz);
 }
 
 // Stream one collided cell (cell t of block b, populations g) into the

@@ -38,6 +38,7 @@ template <int DIM, int Q, typename T, int CPT, bool SOLID>
 __global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
 k_step(const StepArgs a)
 {
+    pdl_wait();
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
     constexpr int TPB = MC / CPT;          // threads per cell-block
@@ -75,7 +76,7 @@ k_step(const StepArgs a)
         const int t = t0 + h * TPB;
         if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;   // solid cells keep their guard
         C ux, uy, uz;
-        bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], C(a.omega), ux, uy, uz);
+        collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
         push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
     }
 }
@@ -294,9 +295,9 @@ int launch_step(agal_ctx *c, const StepArgs &a, int n)
     constexpr int BPC = 256 / (Geo<DIM>::MC / CPT);
     const unsigned grid = (unsigned)((n + BPC - 1) / BPC);
     if (c->geometry_init)
-        k_step<DIM, Q, T, CPT, true><<<grid, 256, 0, c->stream>>>(a);
+        AGAL_CUDA(c, launch_pdl(k_step<DIM, Q, T, CPT, true>, dim3(grid), dim3(256), 0, c->stream, a));
     else
-        k_step<DIM, Q, T, CPT, false><<<grid, 256, 0, c->stream>>>(a);
+        AGAL_CUDA(c, launch_pdl(k_step<DIM, Q, T, CPT, false>, dim3(grid), dim3(256), 0, c->stream, a));
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;
 }
@@ -308,6 +309,7 @@ int launch_step(agal_ctx *c, const StepArgs &a, int n)
 template <typename T>
 __global__ void __launch_bounds__(256) k_stream_fixup(T *fo, int *count, const long long *list, int cap, int *status)
 {
+    pdl_wait();
     const int n = *count;
     const int m = n < cap ? n : cap;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -345,6 +347,11 @@ template <int DIM, int Q, typename T> struct RunStep {
         if (sizeof(typename ST<T>::C) == 4) a.omega = (double)((float)c->dxf[L] / (float)c->tau[L]);
         a.u_ref = c->P.u_ref;
         a.bc_preset = c->P.bc_preset;
+        a.mrt = (Q == 19 && c->P.collision == AGAL_MRT) ? 1 : 0;
+        {
+            const double sv[5] = {c->P.s1, c->P.s2, c->P.s3, c->P.s5, c->P.s6};
+            for (int k = 0; k < 5; k++) a.s[k] = (sizeof(typename ST<T>::C) == 4) ? (double)(float)sv[k] : sv[k];
+        }
         a.fix_count = c->fix_count;
         a.fix_list = c->fix_list;
         a.fix_cap = AGAL_FIX_CAP;
@@ -353,8 +360,8 @@ template <int DIM, int Q, typename T> struct RunStep {
                        : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                                     : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
-        k_stream_fixup<T><<<1, 256, 0, c->stream>>>(static_cast<T *>(a.fout), c->fix_count, c->fix_list,
-                                                    AGAL_FIX_CAP, c->d_status);
+        AGAL_CUDA(c, launch_pdl(k_stream_fixup<T>, dim3(1), dim3(256), 0, c->stream, static_cast<T *>(a.fout),
+                                c->fix_count, c->fix_list, (int)AGAL_FIX_CAP, c->d_status));
         AGAL_CUDA(c, cudaGetLastError());
         if (flip) c->cur[L] = 1 - c->cur[L];
         return AGAL_OK;

@@ -212,7 +212,7 @@ k_step_tma(const StepArgs a, int *status)
 #pragma unroll
                 for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(pop[(size_t)lb * BLK + lat_pb(DIM, p) * MC + t]);
                 C ux, uy, uz;
-                bgk_collide<DIM, Q, C, ST<T>::OFF>(g, omeg, ux, uy, uz);
+                collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
                 const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
                 push_cell<DIM, Q, T, SOLID>(g, ux, uy, uz, b, t, row, hook, fo, a);
             }

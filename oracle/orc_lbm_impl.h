@@ -133,6 +133,77 @@ static int FN(refresh)(orc_case *c, int L)
     return 0;
 }
 
+/* D3Q19 MRT (no live kernel in the reference; the moment basis of the
+   legacy solver_old/solver_lbm_collide_mrt_d3q19.cu, whose inverse transform
+   is the transpose scaled by the row norms, with its equilibria :131-148 and
+   the e equilibrium read as 19 rho |u|^2).  Basis rows as polynomials of c. */
+static int FN(mrt_row)(int i, int cx, int cy, int cz)
+{
+    int c2 = cx * cx + cy * cy + cz * cz;
+    switch (i) {
+    case 0: return 1;
+    case 1: return 19 * c2 - 30;
+    case 2: return (21 * c2 * c2 - 53 * c2 + 24) / 2;
+    case 3: return cx;
+    case 4: return (5 * c2 - 9) * cx;
+    case 5: return cy;
+    case 6: return (5 * c2 - 9) * cy;
+    case 7: return cz;
+    case 8: return (5 * c2 - 9) * cz;
+    case 9: return 3 * cx * cx - c2;
+    case 10: return (3 * c2 - 5) * (3 * cx * cx - c2);
+    case 11: return cy * cy - cz * cz;
+    case 12: return (3 * c2 - 5) * (cy * cy - cz * cz);
+    case 13: return cx * cy;
+    case 14: return cy * cz;
+    case 15: return cx * cz;
+    case 16: return (cy * cy - cz * cz) * cx;
+    case 17: return (cz * cz - cx * cx) * cy;
+    default: return (cx * cx - cy * cy) * cz;
+    }
+}
+
+static void FN(mrt)(const orc_case *c, const R *f, R rho, R u, R v, R w, R omeg, R *out)
+{
+    R m[19];
+    int n[19];
+    for (int i = 0; i < 19; i++) {
+        R acc = 0;
+        n[i] = 0;
+        for (int p = 0; p < 19; p++) {
+            int k = FN(mrt_row)(i, c->cx[p], c->cy[p], c->cz[p]);
+            acc += (R)k * f[p];
+            n[i] += k * k;
+        }
+        m[i] = acc;
+    }
+    const R s1 = (R)c->P.s1, s2 = (R)c->P.s2, s3 = (R)c->P.s3, s5 = (R)c->P.s5, s6 = (R)c->P.s6;
+    const R usq = u * u + v * v + w * w;
+    R eq[19] = {0};
+    eq[1] = (R)(-11.0) * rho + (R)19.0 * rho * usq;
+    eq[2] = (R)3.0 * rho - (R)5.5 * rho * usq;
+    eq[4] = (R)(-2.0 / 3.0) * rho * u;
+    eq[6] = (R)(-2.0 / 3.0) * rho * v;
+    eq[8] = (R)(-2.0 / 3.0) * rho * w;
+    eq[9] = (R)2.0 * rho * u * u - rho * (v * v + w * w);
+    eq[10] = (R)(-0.5) * eq[9];
+    eq[11] = rho * (v * v - w * w);
+    eq[12] = (R)(-0.5) * eq[11];
+    eq[13] = rho * u * v;
+    eq[14] = rho * v * w;
+    eq[15] = rho * u * w;
+    const R rate[19] = {0, s1, s2, 0, s3, 0, s3, 0, s3, omeg, s5, omeg, s5, omeg, omeg, omeg, s6, s6, s6};
+    for (int i = 0; i < 19; i++) m[i] = m[i] - rate[i] * (m[i] - eq[i]);
+    for (int p = 0; p < 19; p++) {
+        R acc = 0;
+        for (int i = 0; i < 19; i++) {
+            int k = FN(mrt_row)(i, c->cx[p], c->cy[p], c->cz[p]);
+            if (k) acc += (R)((double)k / (double)n[i]) * m[i];
+        }
+        out[p] = acc;
+    }
+}
+
 static int FN(collide)(orc_case *c, int L)
 {
     /* Cu_Collide, solver_lbm_kernels.cu:206-289 */
@@ -170,6 +241,13 @@ static int FN(collide)(orc_case *c, int L)
             F[o + (int64_t)(Q + 1) * nmc] = u;
             F[o + (int64_t)(Q + 2) * nmc] = v;
             if (dim == 3) F[o + (int64_t)(Q + 3) * nmc] = w;
+            if (Q == 19 && c->P.collision == AGAL_MRT) {
+                R fn[19];
+                FN(mrt)(c, f_p, rho, u, v, w, omeg, fn);
+                for (int p = 0; p < Q; p++)
+                    if (valid_mask != ORC_CELL_SOLID) F[o + (int64_t)p * nmc] = fn[p];
+                continue;
+            }
             for (int p = 0; p < Q; p++) {
                 R cdotu = (R)c->cx[p] * u + (R)c->cy[p] * v + (R)c->cz[p] * w;
                 R fn = f_p[p] * omegp + ((R)c->w[p] * rho * ((R)1.0 + (R)3.0 * cdotu + (R)4.5 * cdotu * cdotu - (R)1.5 * udotu)) * omeg;

@@ -200,14 +200,14 @@ ALL_ARRAYS = INT_ARRAYS + (_lib.ARR_ID_SET, _lib.ARR_GAP_SET, _lib.ARR_F)
 
 
 @pytest.mark.parametrize("Q,N,storage", [(9, 32, _lib.STORE_FP32), (9, 32, _lib.STORE_FP64),
-                                         (19, 16, _lib.STORE_FP32), (27, 8, _lib.STORE_FP64)])
+                                         (19, 16, _lib.STORE_FP32), (27, 16, _lib.STORE_FP64)])
 def test_percentile_marks_bit_exact_on_identical_inputs(Q, N, storage):
     """The percentile criterion (block vorticity maxima, exact device
     quantile selection, marks) on the CUDA library and on the oracle, given
     the same populations and mesh: identical marks."""
     from oracle.orc import OracleCase
     p = amr_params(Q, N, storage=storage, S_CRITERION=_lib.CRITERION_PERCENTILE, P_REFINE=8,
-                   MAX_LEVELS_INTERIOR=3 if Q == 9 else 2, v0=5e-4)
+                   MAX_LEVELS_INTERIOR=3, v0=5e-4)
     with ag.Case(p) as c:
         run_like_reference(c, p, 12)   # one regrid done, the hierarchy still growing
         c.sync()

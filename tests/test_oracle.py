@@ -303,3 +303,18 @@ def test_oracle_percentile_criterion_refines_the_top_decile(oracle_lib):
     o.advance_n(16)
     n1 = o.counts()["n_ids"][1]
     assert n1 % 4 == 0 and 0 < n1 // 4 <= 26   # floor(0.9 * 255) = 229: 26 blocks strictly above
+
+
+def test_oracle_mrt_with_all_rates_omega_is_bgk(oracle_lib):
+    """The D3Q19 MRT moment basis, its inverse and the legacy equilibria are
+    consistent: with every rate equal to omega the collision is BGK."""
+    from oracle.orc import OracleCase
+    base = dict(velocity_set=_lib.D3Q19, Nx=8, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, v0=1.25e-4,
+                bc_preset=_lib.BC_LDC3D)
+    om = (1.0 / 8) / (1.25e-4 * 3 + 0.5 / 8)
+    a = OracleCase(ag.default_params(**base), 10, fp64=True)
+    b = OracleCase(ag.default_params(**base, collision=_lib.MRT, s1=om, s2=om, s3=om, s5=om, s6=om), 10, fp64=True)
+    for o in (a, b):
+        o.set_ic(0)
+        o.advance_n(30)
+    assert np.abs(a.dump(_lib.ARR_F) - b.dump(_lib.ARR_F)).max() < 1e-13

@@ -190,7 +190,6 @@ k_step_tma(const StepArgs a, int *status)
     } else {
         // ---------------- consumer warps ----------------
         T *__restrict__ fo = static_cast<T *>(a.fout);
-        const C omeg = C(a.omega);
         int k = 0;
         for (int chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x, ++k) {
             const int s = k % NS;

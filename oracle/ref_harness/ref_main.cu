@@ -156,8 +156,19 @@ int main(int argc, char **argv)
     }
 
     Parser parser(input_dir);
+    // REF_GEOM=1: import the STL named by G_FILENAME and bin it as main.cu:94-106
+    // does, then attach it to the mesh (mesh_init.cu:570-577).
+    const bool geom = getenv("REF_GEOM") && atoi(getenv("REF_GEOM")) == 1;
+    Geometry<REAL_h, REAL_h, &APh> *geometry = nullptr;
+    if (geom) {
+        geometry = new Geometry<REAL_h, REAL_h, &APh>(&parser);
+        geometry->G_ImportSTL_ASCII(geometry->G_FILENAME);
+        geometry->G_Init_Arrays_CoordsList_CPU();
+        geometry->G_InitBins(BinMake::GPU, 0);
+    }
     const int N_U = LPh.N_Q + APh.N_DIM + 1;
     Mesh<REAL_h, REAL_h, &APh> mesh(&parser, N_U);
+    if (geom) mesh.M_AddGeometry(geometry);
     Solver_LBM<REAL_h, REAL_h, &APh, &LPh> solver(&mesh);
     mesh.M_AddSolver(&solver);
     for (int L = 0; L < mesh.MAX_LEVELS; L++) solver.S_SetIC(0, L);
@@ -165,7 +176,45 @@ int main(int argc, char **argv)
 
     // Loop body of M_AdvanceLoop (mesh_advance.cu:403-463) without output.
     const int iter_mult = (int)pow(2.0, (double)mesh.N_LEVEL_START);
-    if (mesh.MAX_LEVELS > 1) mesh.M_Advance_RefineNearWall();
+    // With a geometry the near-wall pass also voxelizes a uniform grid
+    // (M_AdvanceLoop calls it unconditionally, mesh_advance.cu:395).
+    if (mesh.MAX_LEVELS > 1 || geom) mesh.M_Advance_RefineNearWall();
+    if (geom && n_steps > 0 && mesh.n_solidb > 0) {
+        // The wall kernels read the populations of the cell behind a
+        // boundary cell without checking that its block exists
+        // (solver_lbm_kernels.cu:808-815, 859-866; forces.cu:428-436).
+        // Refuse to step a case where any boundary cell of a wall block has
+        // a missing neighbour block along a lattice direction.
+        const long long nmb = mesh.n_maxcblocks;
+        const int dim = APh.N_DIM, Q = LPh.N_Q, MC = APh.M_CBLOCK, Qmax = APh.N_Q_max;
+        auto onb = d2h(mesh.c_cblock_ID_onb[0], (size_t)nmb);
+        auto onbs = d2h(mesh.c_cblock_ID_onb_solid[0], (size_t)nmb);
+        auto nbr = d2h(mesh.c_cblock_ID_nbr[0], (size_t)nmb * Qmax);
+        auto cm = d2h(mesh.c_cells_ID_mask[0], (size_t)mesh.n_maxcells);
+        long long bad = 0;
+        for (int L = 0; L < mesh.MAX_LEVELS; L++) {
+            auto ids = d2h(&mesh.c_id_set[0][(size_t)L * nmb], mesh.n_ids[0][L]);
+            for (int b : ids) {
+                if (onb[b] != 1 || onbs[b] < 0) continue;
+                for (int t = 0; t < MC; t++) {
+                    if (cm[(size_t)b * MC + t] != -6) continue;
+                    const int I = t % 4, J = (t / 4) % 4, K = dim == 3 ? t / 16 : 0;
+                    for (int p = 1; p < Q; p++) {
+                        const int Ip = I + V_CONN_ID_H[p], Jp = J + V_CONN_ID_H[p + 27];
+                        const int Kp = dim == 3 ? K + V_CONN_ID_H[p + 54] : 0;
+                        const int bx = Ip < 0 ? 0 : (Ip < 4 ? 1 : 2), by = Jp < 0 ? 0 : (Jp < 4 ? 1 : 2);
+                        const int bz = dim == 3 ? (Kp < 0 ? 0 : (Kp < 4 ? 1 : 2)) : 0;
+                        const int S = bx + 3 * by + 9 * bz;
+                        if (nbr[(size_t)b + (size_t)V_CONN_MAP_H[S] * nmb] < 0) bad++;
+                    }
+                }
+            }
+        }
+        if (bad) {
+            fprintf(stderr, "geometry guard: %lld boundary-cell links without a neighbour block\n", bad);
+            return 6;
+        }
+    }
     // REF_SKIP_LAST_REGRID=1 stops before the refinement of the last step, so
     // the dump is the input of that refinement.
     const bool skip_last = getenv("REF_SKIP_LAST_REGRID") && atoi(getenv("REF_SKIP_LAST_REGRID")) == 1;
@@ -218,6 +267,12 @@ int main(int argc, char **argv)
         auto lev = gather(mesh.c_cblock_level[0], nmb, 1, 1, d_blk, n_act);
         auto cm = gather(mesh.c_cells_ID_mask[0], nmc, 1, MC, d_blk, n_act);
         auto F = gather(mesh.c_cells_f_F[0], nmc, N_U, MC, d_blk, n_act);
+        std::vector<int> onb_s;
+        std::vector<REAL_h> Ff;
+        if (geom) {
+            if (mesh.n_solidb > 0) onb_s = gather(mesh.c_cblock_ID_onb_solid[0], nmb, 1, 1, d_blk, n_act);
+            Ff = gather(mesh.c_cblock_f_Ff[0], nmb, 6, 1, d_blk, n_act);
+        }
         cudaFree(d_blk);
         for (int i = 0; i < n_act; i++) {
             put(f, &fX[(size_t)i * dim], dim);
@@ -229,6 +284,56 @@ int main(int argc, char **argv)
             put(f, &lev[i], 1);
             put(f, &cm[(size_t)i * MC], MC);
             put(f, &F[(size_t)i * N_U * MC], (size_t)N_U * MC);
+        }
+        if (geom) {
+            // Geometry section: faces after import/refinement (SoA rows 0..8 of
+            // geom_f_face_X), the 3D bins of every bin level and the link
+            // bins (CSR: count, start, ids), the solid-boundary counts and
+            // map, the link lengths and the per-block MEA force partials.
+            fwrite("GEOM", 1, 4, f);
+            const long long nf = geometry->n_faces, nfa = geometry->n_faces_a;
+            put(f, &nf, 1);
+            for (int r = 0; r < 9; r++) put(f, &geometry->geom_f_face_X[(size_t)r * nfa], (size_t)nf);
+            auto *bins = geometry->bins;
+            const int nbl = bins->n_bin_levels;
+            put(f, &nbl, 1);
+            for (int L = 0; L < nbl; L++) {
+                const int dens = bins->n_bin_density[L], nb = bins->n_bins_3D[L];
+                long long ne = 0;
+                for (int k = 0; k < nb; k++) ne += bins->binned_face_ids_n_3D[L][k];
+                put(f, &dens, 1);
+                put(f, &nb, 1);
+                put(f, &ne, 1);
+                put(f, bins->binned_face_ids_n_3D[L], nb);
+                put(f, bins->binned_face_ids_N_3D[L], nb);
+                put(f, bins->binned_face_ids_3D[L], (size_t)ne);
+            }
+            const int mk = bins->make_links;
+            put(f, &mk, 1);
+            if (mk) {
+                const int lmd = bins->n_bin_level_MD, dens = bins->n_bin_density_MD, nb = bins->n_bins_MD;
+                long long ne = 0;
+                for (int k = 0; k < nb; k++) ne += bins->binned_face_ids_n_MD[k];
+                put(f, &lmd, 1);
+                put(f, &dens, 1);
+                put(f, &nb, 1);
+                put(f, &ne, 1);
+                put(f, bins->binned_face_ids_n_MD, nb);
+                put(f, bins->binned_face_ids_N_MD, nb);
+                put(f, bins->binned_face_ids_MD, (size_t)ne);
+            }
+            const long long sa = mesh.n_solida, sb = mesh.n_solidb, mcb = mesh.n_maxcells_b;
+            put(f, &sa, 1);
+            put(f, &sb, 1);
+            put(f, &mcb, 1);
+            if (sb > 0) put(f, onb_s.data(), onb_s.size());
+            long long nxb = (sb > 0 && mk) ? mcb * Qmax : 0;
+            put(f, &nxb, 1);
+            if (nxb) {
+                auto xb = d2h(mesh.c_cells_f_X_b[0], (size_t)nxb);
+                put(f, xb.data(), xb.size());
+            }
+            put(f, Ff.data(), Ff.size());
         }
         fclose(f);
     }

@@ -85,6 +85,30 @@ REGRID_PAIRS = {
     "regrid_d3q27_s40": ("ref_d3q27_ldc", dict(AMR, Nx=16, v0=2.5e-5, MAX_LEVELS_INTERIOR=2, P_REFINE=8), 40, 4096, 0),
 }
 
+# Geometry cases: a seeded icosphere (agal_b200.geometry.icosphere) written as
+# ASCII STL into the case's geometry/ folder, imported, binned and voxelized by
+# the reference (REF_GEOM=1), then flow past it with the custom.h FPSC-3D
+# preset.  The dump adds the faces, bins, link lengths and MEA partials.
+# (binary, keys, steps, keep_mb, sphere: subdivisions, radius, centre, seed)
+# The domain is the unit cube: the reference's ray filter and bin lookups
+# index cells as coordinate x N (geometry_bins_gpu.cu:203-206,
+# mesh_voxelizer_voxelize.cu:253-258), which is only right when every side
+# has length 1.
+GEO = dict(AMR, L_fy=1.0, L_fz=1.0, G_LOADTYPE=0, G_FILENAME="sphere.stl", G_BIN_DENSITY=8, G_BIN_LEVELS=3,
+           G_BIN_SPEC=2, G_BIN_APPROACH=1, G_BIN_MAKE_LINKS=1, G_NEAR_WALL_DISTANCE=0.05, G_VIS_TREE=0, G_PRINT=0,
+           P_REFINE=100000, S_FORCE_TYPE=0)
+GEOM_CASES = {
+    "geom_d3q19_wall3_bouzidi": ("ref_d3q19_fps", dict(GEO, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=3, MAX_LEVELS_INTERIOR=3,
+                                                       S_BC_TYPE=1, S_FORCE_ORDER=2), 24, 4096,
+                                 (3, 0.07, (0.45, 0.5, 0.5), 7)),
+    "geom_d3q27_wall2_bb": ("ref_d3q27_fps", dict(GEO, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=2,
+                                                  G_BIN_LEVELS=2, S_BC_TYPE=0, S_FORCE_ORDER=1), 16, 4096,
+                            (3, 0.1, (0.46, 0.49, 0.51), 11)),
+    "geom_d3q19_uniform": ("ref_d3q19_fps", dict(GEO, Nx=32, v0=1.25e-4, G_BIN_DENSITY=16, G_BIN_LEVELS=1,
+                                                 MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, S_BC_TYPE=1,
+                                                 S_FORCE_ORDER=2), 20, 4096, (3, 0.15, (0.47, 0.52, 0.49), 3)),
+}
+
 # Timing workloads of the reference build: (binary, keys, timed steps, keep_mb)
 TIMING = {
     "ldc2d_256": ("ref_d2q9_ldc", dict(Nx=256, v0=5e-4), 2000, 4096),
@@ -184,11 +208,42 @@ def read_dump(path: Path) -> dict:
     for k, _, _ in rec:
         res[k] = np.stack(out[k]) if out[k] else np.zeros((0,))
     res["F"] = res["F"].reshape(int(n_act), NU, int(MC))
+    if o < len(b) and b[o:o + 4] == b"GEOM":
+        o += 4
+        nf = int(take(np.int64, 1)[0])
+        res["faces_soa"] = take(np.float32, 9 * nf).reshape(9, nf)
+        nbl = int(take(np.int32, 1)[0])
+        res["n_bin_levels"] = nbl
+        for L in range(nbl):
+            dens, nb = (int(v) for v in take(np.int32, 2))
+            ne = int(take(np.int64, 1)[0])
+            res[f"bins_density_{L}"] = dens
+            res[f"bins_n_{L}"] = take(np.int32, nb)
+            res[f"bins_N_{L}"] = take(np.int32, nb)
+            res[f"bins_ids_{L}"] = take(np.int32, ne)
+        mk = int(take(np.int32, 1)[0])
+        res["make_links"] = mk
+        if mk:
+            lmd, dens, nb = (int(v) for v in take(np.int32, 3))
+            ne = int(take(np.int64, 1)[0])
+            res["bins_md_level"] = lmd
+            res["bins_md_density"] = dens
+            res["bins_md_n"] = take(np.int32, nb)
+            res["bins_md_N"] = take(np.int32, nb)
+            res["bins_md_ids"] = take(np.int32, ne)
+        sa, sb, mcb = (int(v) for v in take(np.int64, 3))
+        res["n_solida"], res["n_solidb"], res["n_maxcells_b"] = sa, sb, mcb
+        if sb > 0:
+            res["onb_solid"] = take(np.int32, int(n_act))
+        nxb = int(take(np.int64, 1)[0])
+        if nxb:
+            res["cells_f_X_b"] = take(np.float32, nxb).reshape(int(Qmax), mcb)
+        res["Ff"] = take(np.float32, 6 * int(n_act)).reshape(int(n_act), 6)
     return res
 
 
 def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
-            region: int = 0, skip_last_regrid: bool = False) -> str:
+            region: int = 0, skip_last_regrid: bool = False, sphere: tuple | None = None) -> str:
     exe = REF_BIN / binary
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
@@ -196,6 +251,11 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
         td = Path(td)
         (td / "out").mkdir()
         write_input(td, keys, td / "out")
+        if sphere is not None:
+            sys.path.insert(0, str(ROOT))
+            from agal_b200.geometry import icosphere, write_stl_ascii
+            (td / "geometry").mkdir()
+            write_stl_ascii(td / "geometry" / keys["G_FILENAME"], icosphere(*sphere))
         cmd = [str(exe), str(td) + "/", str(dump) if dump else "-", str(steps), str(keep_mb), str(n_timed)]
 
         def big_stack():
@@ -204,7 +264,8 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             import resource
             resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
 
-        env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0")
+        env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0",
+                   REF_GEOM="1" if sphere is not None else "0")
         r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
                            env=env)
         if r.returncode != 0:
@@ -214,20 +275,31 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
 
 def cmd_ref(out: Path, only: list[str] | None) -> None:
     out.mkdir(parents=True, exist_ok=True)
-    cases = {k: v + (0, False) for k, v in CASES.items()}
-    cases.update({k: v + (False,) for k, v in AMR_CASES.items()})
+    cases = {k: v + (0, False, None) for k, v in CASES.items()}
+    cases.update({k: v + (False, None) for k, v in AMR_CASES.items()})
     for k, v in REGRID_PAIRS.items():
-        cases[k + "_pre"] = v + (True,)
-        cases[k + "_post"] = v + (False,)
-    for name, (binary, keys, steps, keep, region, skip) in cases.items():
+        cases[k + "_pre"] = v + (True, None)
+        cases[k + "_post"] = v + (False, None)
+    for k, (binary, keys, steps, keep, sphere) in GEOM_CASES.items():
+        cases[k] = (binary, keys, steps, keep, 0, False, sphere)
+    # Multi-level geometry fixtures keep the populations of the wall blocks
+    # only (blocks with a solid-boundary slot); the uniform one keeps all.
+    wall_only_F = {"geom_d3q19_wall3_bouzidi", "geom_d3q27_wall2_bb"}
+    for name, (binary, keys, steps, keep, region, skip, sphere) in cases.items():
         if only and not any(name == o or name.startswith(o + "_") for o in only):
             continue
         raw = out / f"{name}.bin"
-        run_ref(binary, keys, steps, keep, raw, region=region, skip_last_regrid=skip)
+        run_ref(binary, keys, steps, keep, raw, region=region, skip_last_regrid=skip, sphere=sphere)
         d = read_dump(raw)
         d["case_keys"] = json.dumps(keys)
         d["binary"] = binary
         d["region"] = region
+        if sphere is not None:
+            d["sphere"] = json.dumps(sphere)
+            if name in wall_only_F:
+                keep_blk = d["onb_solid"] >= 0
+                d["F_blocks"] = np.nonzero(keep_blk)[0].astype(np.int32)
+                d["F"] = d["F"][keep_blk]
         np.savez_compressed(out / f"{name}.npz", **d)
         raw.unlink()
         print(name, "n_maxcblocks", d["n_maxcblocks"], "active", len(d["blocks"]), flush=True)

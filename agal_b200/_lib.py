@@ -32,6 +32,7 @@ AVERAGE_INTERFACE, AVERAGE_BLOCK, AVERAGE_GRID = 0, 1, 2
 ARR_F, ARR_MACROS, ARR_CELLS_ID_MASK, ARR_CBLOCK_F_X, ARR_CBLOCK_ID_MASK, ARR_CBLOCK_ID_NBR, \
     ARR_CBLOCK_ID_NBR_CHILD, ARR_CBLOCK_ID_ONB, ARR_CBLOCK_ID_REF, ARR_CBLOCK_LEVEL, ARR_ID_SET, \
     ARR_GAP_SET = range(12)
+ARR_CBLOCK_ID_ONB_SOLID, ARR_CELLS_F_X_B, ARR_CBLOCK_F_FF = 12, 13, 14
 
 INT_KEYS = ["MAX_LEVELS_WALL", "MAX_LEVELS_INTERIOR", "N_ITER_TOTAL", "N_LEVEL_START", "Nx", "N_RESTART",
             "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",

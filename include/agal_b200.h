@@ -97,6 +97,9 @@ extern "C" {
 #define AGAL_ARR_CBLOCK_LEVEL   9  /* int32 [n_maxcblocks]                    mesh.h:419                     */
 #define AGAL_ARR_ID_SET        10  /* int32 [MAX_LEVELS][n_maxcblocks]        mesh.h:428                     */
 #define AGAL_ARR_GAP_SET       11  /* int32 [n_maxcblocks] (first n_gaps valid) mesh.h:459                   */
+#define AGAL_ARR_CBLOCK_ID_ONB_SOLID 12 /* int32 [n_maxcblocks] wall-block slot, -1 = none  mesh.h:515      */
+#define AGAL_ARR_CELLS_F_X_B   13  /* float32 [N_Q_max][n_maxcells_b] link lengths, -1 = none   mesh.h:491   */
+#define AGAL_ARR_CBLOCK_F_FF   14  /* float64 [6][n_maxcblocks] MEA force partials per block   mesh.h:518    */
 
 /* ---- parameters: every input.txt key of inc/parser.h:62-144 ------------- */
 typedef struct agal_params {

@@ -179,6 +179,10 @@ orc_case *orc_create(const agal_params *p, int64_t n_maxcblocks, int fp64)
                 c->cblock_ID_onb[b] = onb;
                 c->cblock_ID_ref[b] = ORC_REF_UNREFINED;
             }
+    /* Voxelizer scratch and solid-boundary state (mesh_init.cu:241-286:
+       the upper half of cells_ID_mask starts INTERIOR; c_tmp_1/2 are -1
+       after M_ResetIntermediateAMRArraysV1, mesh_amr.cu:2077-2085). */
+    if (orc_geometry_alloc(c)) { orc_destroy(c); return NULL; }
     for (int L = 0; L <= ORC_MAXL; L++) { c->n_ids[L] = 0; c->id_max[L] = 0; }
     c->n_ids[0] = (int)n_coarse;
     c->id_max[0] = c->id_max[c->max_levels] = (int)n_coarse;
@@ -195,6 +199,7 @@ void orc_destroy(orc_case *c)
     free(c->cblock_ID_nbr); free(c->cblock_ID_nbr_child); free(c->cblock_ID_onb);
     free(c->cblock_ID_ref); free(c->cblock_level); free(c->id_set); free(c->gap_set);
     free(c->F); free(c->emap); free(c->first_child);
+    orc_geometry_free(c);
     free(c);
 }
 
@@ -292,12 +297,28 @@ static int avg_mode(const orc_case *c)
     return (c->P.interp_order != AGAL_INTERP_LINEAR) ? AGAL_AVERAGE_BLOCK : AGAL_AVERAGE_INTERFACE;
 }
 
-static int sub_step(orc_case *c, int L)
+static int sub_step_f(orc_case *c, int L, int forces)
 {
+    /* Collide, [MEA before the stream], BC, stream, [MEA after]
+       (solver_lbm_advance.cu:115-126, 141-148). */
     int rc;
     if ((rc = orc_collide(c, L))) return rc;
+    if (forces && (rc = DISPATCH(forces_mea, c, L, 0))) return rc;
     if ((rc = orc_impose_bc(c, L))) return rc;
-    return orc_stream(c, L);
+    if ((rc = orc_stream(c, L))) return rc;
+    if (forces && (rc = DISPATCH(forces_mea, c, L, 1))) return rc;
+    return 0;
+}
+
+static int sub_step(orc_case *c, int L) { return sub_step_f(c, L, 0); }
+
+int orc_forces(orc_case *c, double *out)
+{
+    /* Solver_LBM::S_ReportForces sums (solver_lbm_compute.cu:166-215):
+       out = {Fpx, Fmx, Fpy, Fmy, Fpz, Fmz}; the partials are then reset. */
+    DISPATCH(forces_sum, c, out);
+    memset(c->Ff, 0, (size_t)6 * c->nmb * (c->fp64 ? sizeof(double) : sizeof(float)));
+    return 0;
 }
 
 int orc_advance(orc_case *c, int L)
@@ -305,7 +326,8 @@ int orc_advance(orc_case *c, int L)
     /* Solver_LBM::S_Advance (solver_lbm_advance.cu:31-174). */
     const int ML = c->max_levels;
     int rc;
-    if (!(ML > 1 && ML != c->L0 + 1)) return sub_step(c, L);   /* :239-251 */
+    const int mea = c->P.S_FORCE_TYPE == 0;
+    if (!(ML > 1 && ML != c->L0 + 1)) return sub_step_f(c, L, mea);   /* :239-251 */
     if (L == c->L0) {                                           /* :39-58 */
         c->liter = 0;
         if ((rc = orc_interpolate(c, L, AGAL_INTERP_INTERFACE))) return rc;
@@ -321,7 +343,8 @@ int orc_advance(orc_case *c, int L)
         if ((rc = orc_average(c, L, avg_mode(c)))) return rc;
         if ((rc = orc_interpolate(c, L, AGAL_INTERP_INTERFACE))) return rc;
     }
-    if ((rc = sub_step(c, L))) return rc;                                               /* :114-126 */
+    /* :114-126: MEA on the last finest sub-step of the coarse step. */
+    if ((rc = sub_step_f(c, L, mea && L == ML - 1 && c->liter == (1 << (ML - 1)) - 1))) return rc;
     if (L == ML - 1) c->liter++;
     if (L < ML - 1) {                                                                   /* :130-134 */
         if ((rc = orc_advance(c, L + 1))) return rc;
@@ -671,8 +694,10 @@ static void mark_level(orc_case *c, int L, int uniform)
 
 int orc_refine_near_wall(orc_case *c)
 {
-    /* Mesh::M_Advance_RefineNearWall without geometry (mesh_advance.cu:54-122). */
+    /* Mesh::M_Advance_RefineNearWall (mesh_advance.cu:54-122), with the
+       voxelizer passes when a geometry is attached. */
     const int ML = c->max_levels, MLW = c->P.MAX_LEVELS_WALL;
+    const int geo = c->geometry_init;
     int rc;
     for (int L = 0; L < c->L0; L++) {
         mark_level(c, L, 1);
@@ -680,8 +705,18 @@ int orc_refine_near_wall(orc_case *c)
     }
     for (int L = c->L0; L < MLW; L++) {
         if (L < MLW - 1) mark_level(c, L, 0);
+        if (geo && (rc = orc_voxelize_s1(c, L))) return rc;
         if (ML > 1 && L < MLW - 1 && (rc = orc_refine_coarsen(c))) return rc;
+        if (geo && (rc = orc_update_solid_children(c, L))) return rc;
         if ((rc = orc_set_ic(c, L))) return rc;
+    }
+    if (geo) {
+        for (int L = c->L0; L < MLW; L++)
+            if ((rc = orc_voxelize_s2(c, L))) return rc;
+        if ((rc = orc_voxelize_s3(c))) return rc;
+        if (c->P.G_BIN_MAKE_LINKS)
+            for (int L = c->L0; L < MLW; L++)
+                if ((rc = orc_link_lengths(c, L))) return rc;
     }
     if (ML > 1) {
         /* M_FreezeRefinedCells(0): Cu_FreezeRefined over id_max[MAX_LEVELS] (mesh_amr.cu:1888-1904). */
@@ -729,6 +764,9 @@ size_t orc_array_bytes(const orc_case *c, int which)
     case AGAL_ARR_CBLOCK_ID_NBR:
     case AGAL_ARR_CBLOCK_ID_NBR_CHILD: return sizeof(int) * (size_t)c->Qmax * nmb;
     case AGAL_ARR_ID_SET: return sizeof(int) * (size_t)c->max_levels * nmb;
+    case AGAL_ARR_CBLOCK_ID_ONB_SOLID: return sizeof(int) * nmb;
+    case AGAL_ARR_CELLS_F_X_B: return c->X_b ? sizeof(float) * (size_t)c->Qmax * (size_t)c->n_maxcells_b : 0;
+    case AGAL_ARR_CBLOCK_F_FF: return sizeof(double) * 6 * nmb;
     default: return 0;
     }
 }
@@ -746,6 +784,8 @@ static const void *int_array(const orc_case *c, int which)
     case AGAL_ARR_CBLOCK_LEVEL: return c->cblock_level;
     case AGAL_ARR_ID_SET: return c->id_set;
     case AGAL_ARR_GAP_SET: return c->gap_set;
+    case AGAL_ARR_CBLOCK_ID_ONB_SOLID: return c->onb_solid;
+    case AGAL_ARR_CELLS_F_X_B: return c->X_b;
     default: return NULL;
     }
 }
@@ -754,6 +794,12 @@ int orc_dump(const orc_case *c, int which, void *buf, size_t bytes)
 {
     size_t need = orc_array_bytes(c, which);
     if (!need || bytes != need || !buf) return AGAL_ERR_PARAM;
+    if (which == AGAL_ARR_CBLOCK_F_FF) {
+        double *o = (double *)buf;
+        for (size_t i = 0; i < 6 * (size_t)c->nmb; i++)
+            o[i] = c->fp64 ? ((const double *)c->Ff)[i] : (double)((const float *)c->Ff)[i];
+        return 0;
+    }
     if (which == AGAL_ARR_F || which == AGAL_ARR_MACROS) {
         size_t off = (which == AGAL_ARR_F) ? 0 : (size_t)c->Q * (size_t)c->nmc;
         size_t n = need / sizeof(double);
@@ -770,6 +816,14 @@ int orc_load(orc_case *c, int which, const void *buf, size_t bytes)
 {
     size_t need = orc_array_bytes(c, which);
     if (!need || bytes != need || !buf) return AGAL_ERR_PARAM;
+    if (which == AGAL_ARR_CBLOCK_F_FF) {
+        const double *in = (const double *)buf;
+        for (size_t i = 0; i < 6 * (size_t)c->nmb; i++) {
+            if (c->fp64) ((double *)c->Ff)[i] = in[i];
+            else ((float *)c->Ff)[i] = (float)in[i];
+        }
+        return 0;
+    }
     if (which == AGAL_ARR_F || which == AGAL_ARR_MACROS) {
         size_t off = (which == AGAL_ARR_F) ? 0 : (size_t)c->Q * (size_t)c->nmc;
         size_t n = need / sizeof(double);

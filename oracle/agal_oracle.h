@@ -81,6 +81,27 @@ int orc_load(orc_case *c, int which, const void *buf, size_t bytes);
 /* FP64 mass and momentum over fluid cells of leaf blocks (all levels). */
 int orc_mass_momentum(orc_case *c, double *out);
 
+/* ---- geometry (3D) ------------------------------------------------------
+   faces: n_faces x 9 floats (v1x v1y v1z v2x v2y v2z v3x v3y v3z), as
+   imported (geometry_import.cu:11-83) and length-refined
+   (geometry_refine.cu:178-238).  Builds the bins of every bin level and, with
+   G_BIN_MAKE_LINKS, the link bins (Geometry::G_InitBins); attaches the
+   geometry to the mesh (Mesh::M_AddGeometry, mesh_init.cu:570-577), after
+   which orc_refine_near_wall voxelizes and orc_advance imposes the wall. */
+int orc_set_geometry(orc_case *c, const float *faces, int n_faces);
+/* level >= 0: voxelizer bins of that bin level; level = -1: link bins. */
+int orc_bins_info(const orc_case *c, int level, int *density, int *n_bins, int64_t *n_entries);
+int orc_bins_copy(const orc_case *c, int level, int *n, int *N, int *ids);
+int orc_voxelize_s1(orc_case *c, int L);          /* mesh_voxelizer.cu:34-156   */
+int orc_update_solid_children(orc_case *c, int L);/* mesh_voxelizer.cu:247-259  */
+int orc_voxelize_s2(orc_case *c, int L);          /* mesh_voxelizer.cu:158-189  */
+int orc_voxelize_s3(orc_case *c);                 /* mesh_voxelizer.cu:191-245  */
+int orc_link_lengths(orc_case *c, int L);         /* mesh_voxelizer.cu:261-294  */
+/* out = {n_faces, n_solida, n_solidb, n_maxcells_b} */
+int orc_geometry_counts(const orc_case *c, int64_t *out);
+/* MEA force sums {Fpx, Fmx, Fpy, Fmy, Fpz, Fmz}; resets the partials. */
+int orc_forces(orc_case *c, double *out);
+
 #ifdef __cplusplus
 }
 #endif

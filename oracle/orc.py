@@ -60,6 +60,17 @@ def lib() -> C.CDLL:
             ("orc_dump", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
             ("orc_load", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
             ("orc_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+            ("orc_set_geometry", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+            ("orc_bins_info", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int64)]),
+            ("orc_bins_copy", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+            ("orc_voxelize_s1", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_update_solid_children", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_voxelize_s2", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_voxelize_s3", C.c_int, [C.c_void_p]),
+            ("orc_link_lengths", C.c_int, [C.c_void_p, C.c_int]),
+            ("orc_geometry_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+            ("orc_forces", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
         ]
         for name, res, args in protos:
             fn = getattr(L, name)
@@ -150,8 +161,49 @@ class OracleCase:
         self._c(self._lib.orc_mass_momentum(self._h, out))
         return np.array(out[: self.dim + 1])
 
+    def set_geometry(self, faces):
+        """faces: (n, 3, 3) or (n, 9) float32, vertex coordinates per face."""
+        f = np.ascontiguousarray(np.asarray(faces, dtype=np.float32).reshape(-1, 9))
+        self._c(self._lib.orc_set_geometry(self._h, f.ctypes.data_as(C.c_void_p), int(f.shape[0])))
+
+    def bins(self, level):
+        """CSR bins (n, N, ids) of a voxelizer bin level, or of the link bins for level=-1."""
+        dens, nb, ne = C.c_int(), C.c_int(), C.c_int64()
+        self._c(self._lib.orc_bins_info(self._h, level, C.byref(dens), C.byref(nb), C.byref(ne)))
+        n = np.empty(nb.value, np.int32)
+        N = np.empty(nb.value, np.int32)
+        ids = np.empty(max(ne.value, 1), np.int32)
+        self._c(self._lib.orc_bins_copy(self._h, level, n.ctypes.data_as(C.c_void_p), N.ctypes.data_as(C.c_void_p),
+                                        ids.ctypes.data_as(C.c_void_p)))
+        return dens.value, n, N, ids[: ne.value]
+
+    def voxelize_s1(self, L):
+        self._c(self._lib.orc_voxelize_s1(self._h, L))
+
+    def update_solid_children(self, L):
+        self._c(self._lib.orc_update_solid_children(self._h, L))
+
+    def voxelize_s2(self, L):
+        self._c(self._lib.orc_voxelize_s2(self._h, L))
+
+    def voxelize_s3(self):
+        self._c(self._lib.orc_voxelize_s3(self._h))
+
+    def link_lengths(self, L):
+        self._c(self._lib.orc_link_lengths(self._h, L))
+
+    def geometry_counts(self):
+        out = (C.c_int64 * 4)()
+        self._c(self._lib.orc_geometry_counts(self._h, out))
+        return dict(n_faces=out[0], n_solida=out[1], n_solidb=out[2], n_maxcells_b=out[3])
+
+    def forces(self):
+        out = (C.c_double * 6)()
+        self._c(self._lib.orc_forces(self._h, out))
+        return np.array(out[:])
+
     def dump(self, which):
-        dt = np.float64 if which in (0, 1) else (np.float32 if which == 3 else np.int32)
+        dt = np.float64 if which in (0, 1, 14) else (np.float32 if which in (3, 13) else np.int32)
         n = self._lib.orc_array_bytes(self._h, which)
         out = np.empty(n // np.dtype(dt).itemsize, dtype=dt)
         self._c(self._lib.orc_dump(self._h, which, out.ctypes.data_as(C.c_void_p), out.nbytes))

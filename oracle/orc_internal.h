@@ -32,6 +32,22 @@
 #define ORC_BLOCK_SOLIDB (-1)
 #define ORC_BLOCK_SOLIDA (-2)
 #define ORC_BLOCK_SOLID (-3)
+/* Voxelizer cell states (inc/mesh.h:88-96) and the near-wall marking
+   states (mesh.h:45-46). */
+#define ORC_CELL_GUARD (-2)
+#define ORC_CELL_LL (-10)
+#define ORC_CELL_LR (-11)
+#define ORC_CELL_RL (-12)
+#define ORC_CELL_RR (-13)
+#define ORC_REF_INDET_E 11
+#define ORC_REF_INDET_O 12
+
+/* One CSR set of face bins (Bins::binned_face_ids_{n,N,}, geometry_bins.h:66-86). */
+typedef struct orc_bins {
+    int density, n_bins;
+    int64_t n_entries;
+    int *n, *N, *ids;
+} orc_bins;
 
 struct orc_case {
     agal_params P;
@@ -65,7 +81,23 @@ struct orc_case {
     int *first_child;        /* [nmb] scattered first-child IDs (c_tmp_2), -1 = none */
     long iter;               /* coarse steps taken (M_AdvanceLoop counter i) */
     int n_ref_last, n_coarse_last;  /* marks acted on by the last refinement pass */
+    /* Geometry (geometry.h, geometry_bins.h; mesh.h:304-307, 491-518). */
+    int n_faces;
+    float *faces;            /* [9][n_faces]: v1x v1y v1z v2x .. v3z */
+    int n_bin_levels, bin_level_md;
+    orc_bins bins[ORC_MAXL], bins_md;
+    int64_t n_solida, n_maxcells_b;
+    int n_solidb;
+    int *onb_solid;          /* [nmb] cblock_ID_onb_solid, -1 = none */
+    float *X_b;              /* [Qmax][n_maxcells_b] cells_f_X_b, -1 = no link */
+    int *tmp_1, *tmp_2;      /* [nmb] c_tmp_1 / c_tmp_2 scratch of the voxelizer */
+    int *cells_mask_hi;      /* [nmc] upper half of cells_ID_mask (mesh_init.cu:241) */
+    void *Ff;                /* [6][nmb] cblock_f_Ff, ufloat_t */
 };
+
+/* orc_geometry.c */
+int orc_geometry_alloc(orc_case *c);
+void orc_geometry_free(orc_case *c);
 
 static inline int orc_half(int dim, int p)
 {

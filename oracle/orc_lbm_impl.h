@@ -258,21 +258,44 @@ static int FN(collide)(orc_case *c, int L)
     return 0;
 }
 
+/* Interpolated bounce-back of one link (solver_lbm_kernels.cu:816-824):
+   f is the post-collision value leaving the boundary cell towards the wall,
+   f_m the one of the cell behind it, f_o the opposite population of the
+   boundary cell; dQ the link length in cell units. */
+static inline R FN(bouzidi)(R f, R f_m, R f_o, float dQf)
+{
+    const R dQ = (R)dQf;
+    if (dQf > 0 && dQf < 0.5f) return (R)2.0 * dQ * f + ((R)1.0 - (R)2.0 * dQ) * f_m;
+    if (dQf >= 0.5f) return ((R)1.0 / ((R)2.0 * dQ)) * f + (((R)2.0 * dQ - (R)1.0) / ((R)2.0 * dQ)) * f_o;
+    return f;
+}
+
 static int FN(impose_bc)(orc_case *c, int L)
 {
-    /* Cu_ImposeBC, solver_lbm_kernels.cu:693-887 (simple bounce-back hook path;
-       the interpolated bounce-back of S_BC_TYPE=1 needs link lengths). */
+    /* Cu_ImposeBC, solver_lbm_kernels.cu:693-887: the boundary hook on domain
+       faces, then with S_BC_TYPE=1 the interpolated bounce-back of boundary
+       cells of wall blocks, in the order p-hook, p-wall, pb-hook, pb-wall of
+       each pair.  The wall update reads the post-collision value of the
+       cell behind the boundary cell; the reference reads it while other
+       blocks rewrite their own pairs, so here every block reads the values
+       before this phase and the results are written afterwards. */
     R *F = (R *)c->F;
-    const int64_t nmc = c->nmc, nmb = c->nmb;
+    const int64_t nmc = c->nmc, nmb = c->nmb, ncb = c->n_maxcells_b;
     const int Q = c->Q, MC = c->MC, dim = c->dim, Qmax = c->Qmax;
     const int n = c->n_ids[L];
     const int *ids = &c->id_set[(int64_t)L * nmb];
-#pragma omp parallel for schedule(static)
+    const int wall = c->geometry_init && c->P.S_BC_TYPE > 0 && c->X_b;
+    R *out = (R *)malloc(sizeof(R) * (size_t)(n > 0 ? n : 1) * MC * Q);
+    if (!out) return AGAL_ERR_OOM;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
     for (int kap = 0; kap < n; kap++) {
         int b = ids[kap];
         if (c->cblock_ID_onb[b] != 1) continue;
+        const int bm = c->geometry_init ? c->onb_solid[b] : -1;
         int s_nbr[27];
         for (int S = 0; S < Qmax; S++) s_nbr[S] = c->cblock_ID_nbr[b + (int64_t)c->map[S] * nmb];
+        R *ob = &out[(int64_t)kap * MC * Q];
         for (int t = 0; t < MC; t++) {
             int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
             int64_t o = (int64_t)b * MC + t;
@@ -281,6 +304,8 @@ static int FN(impose_bc)(orc_case *c, int L)
             R u = F[o + (int64_t)(Q + 1) * nmc];
             R v = F[o + (int64_t)(Q + 2) * nmc];
             R w = (dim == 3) ? F[o + (int64_t)(Q + 3) * nmc] : (R)0.0;
+            const int bz = wall && valid_mask == ORC_CELL_BOUNDARY && bm > -1;
+            for (int p = 0; p < Q; p++) ob[p * MC + t] = F[o + (int64_t)p * nmc];
             for (int p = 1; p < Q; p++) {
                 if (!orc_half(dim, p)) continue;
                 int q = c->pb[p];
@@ -289,17 +314,127 @@ static int FN(impose_bc)(orc_case *c, int L)
                 int nb = s_nbr[orc_nbrslot(dim, I + c->cx[p], J + c->cy[p], K + c->cz[p])];
                 if (nb < 0 && nb != ORC_N_SKIPID)
                     f_p = FN(bc_hook)(c, nb, f_p, rho, u, v, w, (R)c->w[p], (R)c->cx[p], (R)c->cy[p], (R)c->cz[p]);
+                if (bz) {
+                    const int Ib = I + c->cx[q], Jb = J + c->cy[q], Kb = K + c->cz[q];
+                    const int nbh = s_nbr[orc_nbrslot(dim, Ib, Jb, Kb)];
+                    if (nbh < 0) { bad = 1; continue; }
+                    const R f_m = F[(int64_t)nbh * MC + orc_nbrcell(dim, Ib, Jb, Kb) + (int64_t)p * nmc];
+                    f_p = FN(bouzidi)(f_p, f_m, f_q, c->X_b[(int64_t)bm * MC + t + (int64_t)p * ncb]);
+                }
                 nb = s_nbr[orc_nbrslot(dim, I + c->cx[q], J + c->cy[q], K + c->cz[q])];
                 if (nb < 0 && nb != ORC_N_SKIPID)
                     f_q = FN(bc_hook)(c, nb, f_q, rho, u, v, w, (R)c->w[q], (R)c->cx[q], (R)c->cy[q], (R)c->cz[q]);
+                if (bz) {
+                    const int Ib = I + c->cx[p], Jb = J + c->cy[p], Kb = K + c->cz[p];
+                    const int nbh = s_nbr[orc_nbrslot(dim, Ib, Jb, Kb)];
+                    if (nbh < 0) { bad = 1; continue; }
+                    const R f_m = F[(int64_t)nbh * MC + orc_nbrcell(dim, Ib, Jb, Kb) + (int64_t)q * nmc];
+                    f_q = FN(bouzidi)(f_q, f_m, f_p, c->X_b[(int64_t)bm * MC + t + (int64_t)q * ncb]);
+                }
                 if (valid_mask != ORC_CELL_SOLID) {
-                    F[o + (int64_t)p * nmc] = f_p;
-                    F[o + (int64_t)q * nmc] = f_q;
+                    ob[p * MC + t] = f_p;
+                    ob[q * MC + t] = f_q;
                 }
             }
         }
     }
-    return 0;
+    for (int kap = 0; kap < n; kap++) {
+        int b = ids[kap];
+        if (c->cblock_ID_onb[b] != 1) continue;
+        const R *ob = &out[(int64_t)kap * MC * Q];
+        for (int p = 0; p < Q; p++)
+            for (int t = 0; t < MC; t++) F[(int64_t)b * MC + t + (int64_t)p * nmc] = ob[p * MC + t];
+    }
+    free(out);
+    /* A wall link whose cell behind has no block: the reference reads
+       outside its arrays there. */
+    return bad ? AGAL_ERR_STATE : 0;
+}
+
+/* Cu_ComputeForcesMEA (solver_lbm_kernels_forces.cu:324-537): momentum
+   exchange over the wall links of boundary cells, summed per block into
+   cblock_f_Ff (post = 0 stores, post = 1 adds). */
+static int FN(forces_mea)(orc_case *c, int L, int post)
+{
+    if (!c->geometry_init || !c->X_b || L != c->max_levels - 1 || c->n_ids[L] <= 0) return 0;
+    R *F = (R *)c->F;
+    R *Ff = (R *)c->Ff;
+    const int64_t nmc = c->nmc, nmb = c->nmb, ncb = c->n_maxcells_b;
+    const int Q = c->Q, MC = c->MC, dim = c->dim, Qmax = c->Qmax;
+    const int n = c->n_ids[L];
+    const int *ids = &c->id_set[(int64_t)L * nmb];
+    const R dxL = c->fp64 ? (R)c->dxf_d[L] : (R)c->dxf[L];
+    R dvL = (R)1.0;
+    for (int d = 0; d < dim; d++) dvL *= dxL;
+    const int order = c->P.S_FORCE_ORDER;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int kap = 0; kap < n; kap++) {
+        const int b = ids[kap];
+        const int bm = c->onb_solid[b];
+        if (bm < 0) continue;
+        int s_nbr[27];
+        for (int S = 0; S < Qmax; S++) s_nbr[S] = c->cblock_ID_nbr[b + (int64_t)c->map[S] * nmb];
+        R s[64][3];
+        for (int t = 0; t < MC; t++) {
+            s[t][0] = s[t][1] = s[t][2] = (R)0.0;
+            const int I = t % 4, J = (t / 4) % 4, K = (dim == 3) ? (t / 4) / 4 : 0;
+            const int64_t o = (int64_t)b * MC + t;
+            if (c->cells_ID_mask[o] != ORC_CELL_BOUNDARY) continue;
+            for (int p = 1; p < Q; p++) {
+                if (!orc_half(dim, p)) continue;
+                const int q = c->pb[p];
+                const R f_p = F[o + (int64_t)p * nmc];
+                const R f_q = F[o + (int64_t)q * nmc];
+                for (int side = 0; side < 2; side++) {
+                    const int a = side ? q : p;      /* link direction */
+                    const int e = side ? p : q;      /* towards the cell behind */
+                    const R f_a = side ? f_q : f_p;
+                    const float dist = c->X_b[(int64_t)bm * MC + t + (int64_t)a * ncb];
+                    if (!(dist > 0)) continue;
+                    const int Ib = I + c->cx[e], Jb = J + c->cy[e], Kb = K + c->cz[e];
+                    const int nbh = s_nbr[orc_nbrslot(dim, Ib, Jb, Kb)];
+                    if (nbh < 0) { bad = 1; continue; }
+                    const R f_m = F[(int64_t)nbh * MC + orc_nbrcell(dim, Ib, Jb, Kb) + (int64_t)a * nmc];
+                    const int ca[3] = {c->cx[a], c->cy[a], c->cz[a]};
+                    for (int d = 0; d < dim; d++) {
+                        if (order == 1) {
+                            s[t][d] += f_a * (R)ca[d];
+                        } else {
+                            /* 0.5 is a double literal there: the term is formed in double. */
+                            const double term = ((0.5 + (double)(R)dist) * (double)f_a + (0.5 - (double)(R)dist) * (double)f_m) * (double)ca[d];
+                            s[t][d] = (R)((double)s[t][d] + term);
+                        }
+                    }
+                }
+            }
+        }
+        for (int h = MC / 2; h > 0; h >>= 1)
+            for (int t = 0; t < h; t++)
+                for (int d = 0; d < dim; d++) s[t][d] = s[t][d] + s[t + h][d];
+        for (int d = 0; d < dim; d++) {
+            if (post == 0) {
+                Ff[b + (int64_t)(2 * d + 0) * nmb] = s[0][d] * dvL;
+                Ff[b + (int64_t)(2 * d + 1) * nmb] = (R)0.0;
+            } else {
+                Ff[b + (int64_t)(2 * d + 0) * nmb] += s[0][d] * dvL;
+            }
+        }
+    }
+    return bad ? AGAL_ERR_STATE : 0;
+}
+
+/* S_ReportForces sums (solver_lbm_compute.cu:166-201): the six rows of
+   cblock_f_Ff over block IDs below id_max[MAX_LEVELS], in double. */
+static void FN(forces_sum)(const orc_case *c, double *out)
+{
+    const R *Ff = (const R *)c->Ff;
+    const int n = c->id_max[c->max_levels];
+    for (int r = 0; r < 6; r++) {
+        double s = 0.0;
+        for (int b = 0; b < n; b++) s += (double)Ff[b + (int64_t)r * c->nmb];
+        out[r] = s;
+    }
 }
 
 static int FN(stream)(orc_case *c, int L)

@@ -193,8 +193,53 @@ class Case:
         self._c(self._lib.agal_mass_momentum_noalloc(self._h, out))
         return np.array(out[: self.dim + 1])
 
+    # -- geometry -------------------------------------------------------
+    def set_geometry(self, faces) -> None:
+        """Attach a triangle surface: faces (n, 3, 3) or (n, 9) float32 in
+        unit-length coordinates; builds the face bins on the device."""
+        f = np.ascontiguousarray(np.asarray(faces, dtype=np.float32).reshape(-1, 9))
+        self._c(self._lib.agal_set_geometry(self._h, f.ctypes.data_as(C.c_void_p), int(f.shape[0])))
+
+    def bins(self, level: int):
+        """(density, n, N, ids) of voxelizer bin level `level`, or of the link bins for level -1."""
+        dens, nb, ne = C.c_int(), C.c_int(), C.c_longlong()
+        self._c(self._lib.agal_bins_get(self._h, level, C.byref(dens), C.byref(nb), C.byref(ne), None, None, None))
+        n = np.empty(nb.value, np.int32)
+        N = np.empty(nb.value, np.int32)
+        ids = np.empty(max(ne.value, 1), np.int32)
+        self._c(self._lib.agal_bins_get(self._h, level, None, None, None, n.ctypes.data_as(C.c_void_p),
+                                        N.ctypes.data_as(C.c_void_p), ids.ctypes.data_as(C.c_void_p)))
+        return dens.value, n, N, ids[: ne.value]
+
+    def voxelize_s1(self, L: int) -> None:
+        self._c(self._lib.agal_voxelize_s1(self._h, L))
+
+    def update_solid_children(self, L: int) -> None:
+        self._c(self._lib.agal_update_solid_children(self._h, L))
+
+    def voxelize_s2(self, L: int) -> None:
+        self._c(self._lib.agal_voxelize_s2(self._h, L))
+
+    def voxelize_s3(self) -> None:
+        self._c(self._lib.agal_voxelize_s3(self._h))
+
+    def link_lengths(self, L: int) -> None:
+        self._c(self._lib.agal_link_lengths(self._h, L))
+
+    def geometry_counts(self) -> dict:
+        out = (C.c_longlong * 4)()
+        self._c(self._lib.agal_geometry_counts(self._h, out))
+        return dict(n_faces=out[0], n_solida=out[1], n_solidb=out[2], n_maxcells_b=out[3])
+
+    def forces(self) -> np.ndarray:
+        """MEA force sums {Fpx, Fmx, Fpy, Fmy, Fpz, Fmz} (FP64); resets the partials."""
+        out = (C.c_double * 6)()
+        self._c(self._lib.agal_forces(self._h, out))
+        return np.array(out[:])
+
     # -- arrays ---------------------------------------------------------
-    _DTYPES = {_lib.ARR_F: np.float64, _lib.ARR_MACROS: np.float64, _lib.ARR_CBLOCK_F_X: np.float32}
+    _DTYPES = {_lib.ARR_F: np.float64, _lib.ARR_MACROS: np.float64, _lib.ARR_CBLOCK_F_X: np.float32,
+               _lib.ARR_CELLS_F_X_B: np.float32, _lib.ARR_CBLOCK_F_FF: np.float64}
 
     def array_bytes(self, which: int) -> int:
         n = C.c_size_t()

@@ -96,6 +96,16 @@ PROTOS = [
     ("agal_refine_with_solution", C.c_int, [C.c_void_p]),
     ("agal_refine_near_wall", C.c_int, [C.c_void_p]),
     ("agal_refine_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("agal_set_geometry", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("agal_bins_get", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_longlong), C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("agal_voxelize_s1", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_update_solid_children", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_voxelize_s2", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_voxelize_s3", C.c_int, [C.c_void_p]),
+    ("agal_link_lengths", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_geometry_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("agal_forces", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
 ]
 
 _lib = None

@@ -39,14 +39,13 @@
 #include <vector>
 
 #include "ctx.h"
+#include "compact.cuh"
 #include "lattice.cuh"
 
 namespace agal {
 namespace {
 
-constexpr int SCAN_T = 512;
-constexpr int SCAN_I = 8;
-constexpr int SCAN_CHUNK = SCAN_T * SCAN_I;
+using cmp::SCAN_CHUNK;
 constexpr int NT = 256;   // threads per CTA of the per-block kernels
 
 // Small device counters (amr_small, AGAL_AMR_SMALL ints).
@@ -55,85 +54,6 @@ static_assert(S_NIDS + 17 <= AGAL_AMR_SMALL, "small counter layout");
 
 unsigned grid_for(long long n, int per = NT) { return (unsigned)((n + per - 1) / per); }
 
-// Exclusive CTA-wide scan of v (SCAN_T threads); *total receives the sum.
-__device__ __forceinline__ int cta_exscan(int v, int *s_warp, int *total)
-{
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-        int w = (lane < SCAN_T / 32) ? s_warp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < SCAN_T / 32) s_warp[lane] = w;
-    }
-    __syncthreads();
-    *total = s_warp[SCAN_T / 32 - 1];
-    return (wid ? s_warp[wid - 1] : 0) + x - v;
-}
-
-template <class F>
-__global__ void __launch_bounds__(SCAN_T) k_cmp_count(const F f, int n, int *parts)
-{
-    __shared__ int s_warp[SCAN_T / 32];
-    const long long base = (long long)blockIdx.x * SCAN_CHUNK + (long long)threadIdx.x * SCAN_I;
-    int cnt = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_I; k++) {
-        const long long i = base + k;
-        if (i < n && f.pred((int)i)) cnt++;
-    }
-    int total;
-    cta_exscan(cnt, s_warp, &total);
-    if (threadIdx.x == 0) parts[blockIdx.x] = total;
-}
-
-// Exclusive scan of the per-CTA counts in one CTA; total into *out.
-__global__ void __launch_bounds__(SCAN_T) k_cmp_scan(int *parts, int np, int *out)
-{
-    __shared__ int s_warp[SCAN_T / 32];
-    int carry = 0;
-    for (int base = 0; base < np; base += SCAN_T) {
-        const int i = base + threadIdx.x;
-        const int v = (i < np) ? parts[i] : 0;
-        int total;
-        const int ex = cta_exscan(v, s_warp, &total);
-        if (i < np) parts[i] = carry + ex;
-        carry += total;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = carry;
-}
-
-template <class F>
-__global__ void __launch_bounds__(SCAN_T) k_cmp_emit(const F f, int n, const int *parts)
-{
-    __shared__ int s_warp[SCAN_T / 32];
-    const long long base = (long long)blockIdx.x * SCAN_CHUNK + (long long)threadIdx.x * SCAN_I;
-    bool fl[SCAN_I];
-    int cnt = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_I; k++) {
-        const long long i = base + k;
-        fl[k] = i < n && f.pred((int)i);
-        cnt += fl[k];
-    }
-    int total;
-    int r = parts[blockIdx.x] + cta_exscan(cnt, s_warp, &total);
-#pragma unroll
-    for (int k = 0; k < SCAN_I; k++)
-        if (fl[k]) f.emit((int)(base + k), r++);
-}
-
 // Ordered compaction over [0, n): f.emit(i, rank) for every i with f.pred(i).
 // The predicate must not read what emit writes.  *count receives the count.
 template <class F>
@@ -141,11 +61,7 @@ int compact(agal_ctx *c, const F &f, int n, int *count)
 {
     *count = 0;
     if (n <= 0) return AGAL_OK;
-    const int np = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    k_cmp_count<F><<<np, SCAN_T, 0, c->stream>>>(f, n, c->amr_parts);
-    k_cmp_scan<<<1, SCAN_T, 0, c->stream>>>(c->amr_parts, np, c->amr_small + S_TOTAL);
-    k_cmp_emit<F><<<np, SCAN_T, 0, c->stream>>>(f, n, c->amr_parts);
-    AGAL_CUDA(c, cudaGetLastError());
+    AGAL_CUDA(c, cmp::compact_async(c->stream, c->amr_parts, c->amr_small + S_TOTAL, f, n));
     AGAL_CUDA(c, cudaMemcpyAsync(count, c->amr_small + S_TOTAL, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
     return AGAL_OK;

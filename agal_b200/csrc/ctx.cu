@@ -87,6 +87,7 @@ namespace {
 void release(agal_ctx *c)
 {
     agal_drop_graphs(c);
+    agal_geometry_release(c);
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
@@ -475,8 +476,11 @@ extern "C" int agal_refine_with_solution(agal_ctx *c)
 // Mesh::M_Advance_RefineNearWall without geometry (mesh_advance.cu:54-122).
 extern "C" int agal_refine_near_wall(agal_ctx *c)
 {
+    // Mesh::M_Advance_RefineNearWall (mesh_advance.cu:54-122), with the
+    // voxelizer passes when a geometry is attached.
     if (!c) return AGAL_ERR_PARAM;
     const int ML = c->max_levels, MLW = c->P.MAX_LEVELS_WALL;
+    const bool geo = c->geometry_init && c->faces;
     int rc;
     for (int L = 0; L < c->L0; L++) {
         if ((rc = agal_mark_level(c, L, 1))) return rc;
@@ -484,8 +488,20 @@ extern "C" int agal_refine_near_wall(agal_ctx *c)
     }
     for (int L = c->L0; L < MLW; L++) {
         if (L < MLW - 1 && (rc = agal_mark_level(c, L, 0))) return rc;
+        if (geo && (rc = agal_voxelize_s1(c, L))) return rc;
         if (ML > 1 && L < MLW - 1 && (rc = agal_refine_coarsen(c))) return rc;
+        if (geo && (rc = agal_update_solid_children(c, L))) return rc;
         if ((rc = agal_launch_set_ic(c, L))) return rc;
+    }
+    if (geo) {
+        for (int L = c->L0; L < MLW; L++)
+            if ((rc = agal_voxelize_s2(c, L))) return rc;
+        if ((rc = agal_voxelize_s3(c))) return rc;
+        if (c->P.G_BIN_MAKE_LINKS)
+            for (int L = c->L0; L < MLW; L++)
+                if ((rc = agal_link_lengths(c, L))) return rc;
+        // The wall flags of the step depend on the link lengths being present.
+        if ((rc = agal_build_meta(c))) return rc;
     }
     if (ML > 1 && (rc = agal_freeze_refined(c))) return rc;
     return AGAL_OK;
@@ -512,12 +528,25 @@ static int avg_mode(const agal_ctx *c)
     return (c->P.interp_order != AGAL_INTERP_LINEAR) ? AGAL_AVERAGE_BLOCK : AGAL_AVERAGE_INTERFACE;
 }
 
+// One sub-step of level L, with the MEA force passes around it when asked
+// (before the stream from the current buffer, after it from the new one).
+static int step_f(agal_ctx *c, int L, bool forces)
+{
+    int rc;
+    if (forces && (rc = agal_launch_forces(c, L, 0))) return rc;
+    if ((rc = agal_launch_step(c, L))) return rc;
+    if (forces && (rc = agal_launch_forces(c, L, 1))) return rc;
+    return AGAL_OK;
+}
+
 static int advance_rec(agal_ctx *c, int L)
 {
     const int ML = c->max_levels;
+    const bool mea = c->P.S_FORCE_TYPE == 0 && c->X_b;
     int rc;
-    if (!multi_level(c)) return agal_launch_step(c, L);   // :239-251
+    if (!multi_level(c)) return step_f(c, L, mea);          // :239-251
     if (L == c->L0) {                                       // :39-58
+        c->liter = 0;
         if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
         if ((rc = agal_launch_step(c, L))) return rc;
         if ((rc = advance_rec(c, L + 1))) return rc;
@@ -525,12 +554,15 @@ static int advance_rec(agal_ctx *c, int L)
     }
     if (L < ML - 1 && (rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;   // :96-99
     if ((rc = agal_launch_step(c, L))) return rc;
+    if (L == ML - 1) c->liter++;
     if (L < ML - 1) {                                                                       // :106-111
         if ((rc = advance_rec(c, L + 1))) return rc;
         if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
         if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
     }
-    if ((rc = agal_launch_step(c, L))) return rc;                                           // :114-126
+    // :114-126: the forces on the last finest sub-step of the coarse step.
+    if ((rc = step_f(c, L, mea && L == ML - 1 && c->liter == (1 << (ML - 1)) - 1))) return rc;
+    if (L == ML - 1) c->liter++;
     if (L < ML - 1) {                                                                       // :130-134
         if ((rc = advance_rec(c, L + 1))) return rc;
         if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
@@ -657,6 +689,18 @@ extern "C" int agal_array_bytes(const agal_ctx *c, int which, size_t *bytes)
     case AGAL_ARR_CBLOCK_ID_NBR:
     case AGAL_ARR_CBLOCK_ID_NBR_CHILD: *bytes = sizeof(int) * (size_t)c->Qmax * nmb; break;
     case AGAL_ARR_ID_SET: *bytes = sizeof(int) * (size_t)c->max_levels * nmb; break;
+    case AGAL_ARR_CBLOCK_ID_ONB_SOLID:
+        if (!c->onb_solid) return AGAL_ERR_PARAM;
+        *bytes = sizeof(int) * nmb;
+        break;
+    case AGAL_ARR_CELLS_F_X_B:
+        if (!c->X_b) return AGAL_ERR_PARAM;
+        *bytes = sizeof(float) * 27 * (size_t)c->n_maxcells_b;
+        break;
+    case AGAL_ARR_CBLOCK_F_FF:
+        if (!c->Ff) return AGAL_ERR_PARAM;
+        *bytes = sizeof(double) * 6 * nmb;
+        break;
     default: return AGAL_ERR_PARAM;
     }
     return AGAL_OK;
@@ -675,6 +719,8 @@ static void *int_array(agal_ctx *c, int which)
     case AGAL_ARR_CBLOCK_LEVEL: return c->cblock_level;
     case AGAL_ARR_ID_SET: return c->id_set;
     case AGAL_ARR_GAP_SET: return c->gap_set;
+    case AGAL_ARR_CBLOCK_ID_ONB_SOLID: return c->onb_solid;
+    case AGAL_ARR_CELLS_F_X_B: return c->X_b;
     default: return nullptr;
     }
 }
@@ -714,6 +760,18 @@ extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
     if (rc) return rc;
     if (!host_buf || bytes != need) return agal_set_err(c, AGAL_ERR_PARAM, "dump size mismatch");
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (which == AGAL_ARR_CBLOCK_F_FF) {
+        double *o = static_cast<double *>(host_buf);
+        const size_t n = 6 * (size_t)c->nmb;
+        if (c->storage == AGAL_STORE_FP64) {
+            AGAL_CUDA(c, cudaMemcpy(o, c->Ff, n * 8, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> t(n);
+            AGAL_CUDA(c, cudaMemcpy(t.data(), c->Ff, n * 4, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; i++) o[i] = t[i];
+        }
+        return AGAL_OK;
+    }
     if (which == AGAL_ARR_F) {
         const size_t n = (size_t)c->Q * c->nmc;
         std::vector<unsigned char> raw[2];
@@ -789,6 +847,7 @@ extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t by
         return AGAL_OK;
     }
     if (which == AGAL_ARR_MACROS) return agal_set_err(c, AGAL_ERR_PARAM, "macros are derived, not loaded");
+    if (which == AGAL_ARR_CBLOCK_F_FF) return agal_set_err(c, AGAL_ERR_PARAM, "force partials are derived, not loaded");
     AGAL_CUDA(c, cudaMemcpy(int_array(c, which), host_buf, need, cudaMemcpyHostToDevice));
     if ((rc = agal_build_meta(c))) return rc;
     if (which == AGAL_ARR_CELLS_ID_MASK) {

@@ -21,6 +21,14 @@
 
 #include "../../include/agal_b200.h"
 
+// One CSR set of face bins on the device (Bins::binned_face_ids_{n,N,},
+// geometry_bins.h:66-86): n = faces per bin, N = start, ids = face IDs.
+struct agal_bins_d {
+    int density = 0, n_bins = 0;
+    long long n_entries = 0;
+    int *n = nullptr, *N = nullptr, *ids = nullptr;
+};
+
 struct agal_ctx {
     agal_params P{};
     int dim = 2, Q = 9, Qmax = 9, MC = 16, NCH = 4;
@@ -79,6 +87,23 @@ struct agal_ctx {
     void *crit = nullptr;              // percentile criterion: block values, histograms, selection state
     long long iter = 0;                // coarse steps taken (M_AdvanceLoop counter i)
     int n_ref_last = 0, n_coarse_last = 0;   // marks acted on by the last refinement pass
+    // Geometry (geometry.cu): faces, bins, solid-boundary state, MEA partials.
+    int n_faces = 0;
+    float *faces = nullptr;            // [9][n_faces] v1x v1y v1z v2x .. v3z
+    int n_bin_levels = 0, bin_level_md = -1;
+    agal_bins_d bins[16], bins_md;
+    long long n_solida = 0, n_maxcells_b = 0;
+    int n_solidb = 0;
+    int *onb_solid = nullptr;          // [nmb] wall-block slot (cblock_ID_onb_solid), -1 = none
+    float *X_b = nullptr;              // [27][n_maxcells_b] link lengths (cells_f_X_b), -1 = none
+    int *vox_tmp = nullptr;            // [nmb] near-wall marking scratch (c_tmp_1), -1 at rest
+    unsigned long long *bnd_bits = nullptr;   // [nmb] boundary-cell flags of Voxelize_S2
+    void *Ff = nullptr;                // [6][nmb] MEA partials (cblock_f_Ff), compute type
+    int *geo_small = nullptr, *geo_parts = nullptr;   // counters / compaction partials
+    // Wall blocks (onb == 1 and a wall slot) per level for the interpolated
+    // bounce-back and the forces: wall_ids[wall_off[L] .. + wall_n[L]).
+    int *wall_ids = nullptr;
+    std::vector<int> wall_off, wall_n;
     std::string err;
 };
 
@@ -116,3 +141,9 @@ int agal_freeze_refined(agal_ctx *c);
 size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
 #define AGAL_AMR_SMALL 128
 void agal_drop_graphs(agal_ctx *c);         // after any change of the mesh or launch shapes
+// Geometry (geometry.cu, wall_kernels.cu).
+void agal_geometry_release(agal_ctx *c);
+int agal_build_wall_lists(agal_ctx *c);     // after the mesh or the wall slots change
+int agal_wall_active(const agal_ctx *c);    // interpolated bounce-back in force
+int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout);
+int agal_launch_forces(agal_ctx *c, int L, int post);

@@ -17,7 +17,8 @@ constexpr int N_SPECID = -998;   // cppspec.h:124
 // Reference enumerations (inc/mesh.h:34-105).
 constexpr int REF_UNREFINED = 0, REF_REFINED = 1, REF_REFINED_WCHILD = 2, REF_REFINED_PERM = 3,
               REF_MARK_REFINE = 4, REF_MARK_COARSEN = 5, REF_NEW = 6, REF_REMOVE = 7,
-              REF_INACTIVE = 8, REF_UNREFINED_VIO = 9, REF_REFINED_WCHILD_PERM = 10;
+              REF_INACTIVE = 8, REF_UNREFINED_VIO = 9, REF_REFINED_WCHILD_PERM = 10,
+              REF_INDET_E = 11, REF_INDET_O = 12;
 constexpr int CELL_INTERIOR = 0, CELL_INTERFACE = 1, CELL_GHOST = 2, CELL_SOLID = -1,
               CELL_GUARD = -2, CELL_BOUNDARY = -6;
 constexpr int BLOCK_REGULAR = 0, BLOCK_INTERFACE = 1, BLOCK_SOLIDB = -1, BLOCK_SOLIDA = -2,

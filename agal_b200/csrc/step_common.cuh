@@ -57,6 +57,7 @@ template <int DIM> struct Meta {
 };
 constexpr int META_ACTIVE = 1;   // collide/stream this block (kernels.cu:236)
 constexpr int META_ONB = 2;      // block touches a domain boundary (kernels.cu:736)
+constexpr int META_WALL = 4;     // wall block stepped by k_step_wall (interpolated bounce-back)
 
 struct StepArgs {
     const int *ids;

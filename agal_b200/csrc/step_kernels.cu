@@ -66,7 +66,7 @@ k_step(const StepArgs a)
     }
     __syncthreads();
     const int fl = s_meta[lb][Meta<DIM>::FLAGS];
-    if (b < 0 || !(fl & META_ACTIVE)) return;
+    if (b < 0 || !(fl & META_ACTIVE) || (fl & META_WALL)) return;
 
     T *__restrict__ fo = static_cast<T *>(a.fout);
     const int *nrow = s_meta[lb];
@@ -261,7 +261,7 @@ __global__ void k_sum_partials(const double *partial, int n, double *out)
 // flags of kernels.cu:236 (collide/stream) and :736 (boundary hook).
 template <int DIM>
 __global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child, const int *bmask,
-                             const int *onb, int *meta)
+                             const int *onb, const int *onb_solid, int *meta)
 {
     constexpr int W = Meta<DIM>::W, QMAX = Geo<DIM>::QMAX;
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,6 +274,7 @@ __global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child
     } else if (i == Meta<DIM>::FLAGS) {
         if (nbr_child[b] < 0 || bmask[b] != BLOCK_SOLID) v |= META_ACTIVE;
         if (onb[b] == 1) v |= META_ONB;
+        if (onb_solid && onb[b] == 1 && onb_solid[b] >= 0) v |= META_WALL;
     }
     meta[g] = v;
 }
@@ -360,6 +361,7 @@ template <int DIM, int Q, typename T> struct RunStep {
                        : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                                     : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
+        if (const int rw = agal_launch_wall_step(c, L, a.fin, a.fout)) return rw;
         AGAL_CUDA(c, launch_pdl(k_stream_fixup<T>, dim3(1), dim3(256), 0, c->stream, static_cast<T *>(a.fout),
                                 c->fix_count, c->fix_list, (int)AGAL_FIX_CAP, c->d_status));
         AGAL_CUDA(c, cudaGetLastError());
@@ -593,13 +595,16 @@ int agal_build_meta(agal_ctx *c)
 {
     const long long tot = c->nmb * (c->dim == 2 ? agal::Meta<2>::W : agal::Meta<3>::W);
     const unsigned grid = (unsigned)((tot + 255) / 256);
+    // Wall blocks leave the main step kernels only when k_step_wall takes them.
+    const int *wall = agal_wall_active(c) ? c->onb_solid : nullptr;
     if (c->dim == 2)
         agal::k_build_meta<2><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
-                                                           c->cblock_ID_mask, c->cblock_ID_onb, c->meta);
+                                                           c->cblock_ID_mask, c->cblock_ID_onb, wall, c->meta);
     else
         agal::k_build_meta<3><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
-                                                           c->cblock_ID_mask, c->cblock_ID_onb, c->meta);
+                                                           c->cblock_ID_mask, c->cblock_ID_onb, wall, c->meta);
     AGAL_CUDA(c, cudaGetLastError());
+    if (c->onb_solid) return agal_build_wall_lists(c);
     return AGAL_OK;
 }
 int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }

@@ -205,7 +205,7 @@ k_step_tma(const StepArgs a, int *status)
                 if (b < 0) continue;
                 const int *row = meta + lb * W;
                 const int fl = row[Meta<DIM>::FLAGS];
-                if (!(fl & META_ACTIVE)) continue;
+                if (!(fl & META_ACTIVE) || (fl & META_WALL)) continue;
                 if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;
                 C g[Q];
 #pragma unroll

@@ -1,0 +1,395 @@
+// Wall blocks of a geometry: the step with the interpolated bounce-back and
+// the momentum-exchange (MEA) forces.
+//
+// A wall block is a block on a boundary (cblock_ID_onb == 1) with a wall slot
+// (cblock_ID_onb_solid >= 0).  When S_BC_TYPE > 0 the main step kernels skip
+// them (META_WALL) and k_step_wall steps them instead: collide, then for each
+// direction pair (p, pb) the reference's order of Cu_ImposeBC
+// (solver_lbm_kernels.cu:769-876): boundary hook of p, interpolated
+// bounce-back of p, hook of pb, bounce-back of pb; then the push with the
+// stream guard.  The bounce-back needs the post-collision population of the
+// cell behind the boundary cell; the step reads the previous buffer only, so
+// that value is recomputed from it (one collision per link with 0 < q < 1/2).
+// The reference reads it while other blocks rewrite their own pairs; here
+// every block sees the values before the boundary phase.
+//
+// k_forces (Cu_ComputeForcesMEA, solver_lbm_kernels_forces.cu:324-537) sums
+// per wall block of the finest level the momentum carried along the wall
+// links of boundary cells, before the stream (post = 0, from the recomputed
+// post-collision populations) and after it (post = 1, from the new buffer),
+// into cblock_f_Ff; agal_forces reduces the partials in FP64.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "ctx.h"
+#include "dispatch.cuh"
+#include "step_common.cuh"
+
+namespace agal {
+namespace {
+
+struct WallArgs {
+    StepArgs s;
+    const int *wall;          // wall blocks of the level
+    const int *onb_solid;
+    const float *Xb;          // [27][ncb]
+    long long ncb;
+    int bc_type;
+    int *status;
+};
+
+template <int DIM, int Q, typename T>
+__device__ __forceinline__ typename ST<T>::C full_of(T v, int slot)
+{
+    using C = typename ST<T>::C;
+    return ST<T>::dec(v) + (ST<T>::OFF ? C(lat_w(Q, slot)) : C(0));
+}
+
+// Post-collision value of direction k at cell nc of block nb, as the
+// reference's collide kernel leaves it in slot k: collided for an active
+// block's fluid cell, the stored value otherwise (solid guard, inactive block).
+template <int DIM, int Q, typename T>
+__device__ typename ST<T>::C post_collision(const StepArgs &a, int nb, int nc, int k)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, W = Meta<DIM>::W;
+    const T *fin = static_cast<const T *>(a.fin) + (long long)nb * BLK + nc;
+    const bool active = (__ldg(&a.meta[(long long)nb * W + Meta<DIM>::FLAGS]) & META_ACTIVE) != 0;
+    if (!active || __ldg(&a.cmask[(long long)nb * MC + nc]) == CELL_SOLID) return full_of<DIM, Q, T>(fin[k * MC], k);
+    C g[Q];
+#pragma unroll
+    for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[lat_pb(DIM, p) * MC]);
+    C ux, uy, uz;
+    collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+    return g[k] + (ST<T>::OFF ? C(lat_w(Q, k)) : C(0));
+}
+
+// Interpolated bounce-back of one link (solver_lbm_kernels.cu:816-824).
+template <typename C>
+__device__ __forceinline__ C bouzidi(C f, C f_m, C f_o, float dQf)
+{
+    const C dQ = C(dQf);
+    const C two_q = r_mul(C(2), dQ);
+    if (dQf > 0.f && dQf < 0.5f) return r_add(r_mul(two_q, f), r_mul(r_add(C(1), -two_q), f_m));
+    return r_add(r_mul(r_div(C(1), two_q), f), r_mul(r_div(r_add(two_q, -C(1)), two_q), f_o));
+}
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
+{
+    pdl_wait();
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, W = Meta<DIM>::W;
+    const StepArgs &a = w.s;
+    __shared__ int s_meta[W];
+    const int b = w.wall[blockIdx.x];
+    const int t = threadIdx.x;
+    for (int i = t; i < W; i += MC) s_meta[i] = a.meta[(long long)b * W + i];
+    __syncthreads();
+    if (!(s_meta[Meta<DIM>::FLAGS] & META_ACTIVE)) return;
+    const int mask = a.cmask[(long long)b * MC + t];
+    if (mask == CELL_SOLID) return;   // solid cells keep their guard
+    const T *fin = static_cast<const T *>(a.fin) + (long long)b * BLK + t;
+    C g[Q];
+#pragma unroll
+    for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[lat_pb(DIM, p) * MC]);
+    C ux, uy, uz;
+    collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const int slot = w.onb_solid[b];
+    const bool wall = w.bc_type > 0 && mask == CELL_BOUNDARY && slot > -1;
+    const bool hook = a.bc_preset != AGAL_BC_NONE;
+    const int *nrow = s_meta;
+    auto nbr_at = [&](int p, int sgn, int &nc) {
+        const int Ip = I + sgn * lat_c(DIM, 0, p), Jp = J + sgn * lat_c(DIM, 1, p);
+        const int Kp = (DIM == 3) ? K + sgn * lat_c(DIM, 2, p) : 0;
+        nc = nbr_cell(DIM, Ip, Jp, Kp);
+        return nrow[nbr_slot(DIM, Ip, Jp, Kp)];
+    };
+    for (int p = 1; p < Q; p++) {
+        if (!lat_half(DIM, p)) continue;
+        const int q = lat_pb(DIM, p);
+        const C wp = C(lat_w(Q, p)), wq = C(lat_w(Q, q));
+        const C offp = ST<T>::OFF ? wp : C(0), offq = ST<T>::OFF ? wq : C(0);
+        C fp = g[p] + offp, fq = g[q] + offq;
+        int nc;
+        int nb = nbr_at(p, 1, nc);
+        if (hook && nb < 0 && nb != N_SKIPID)
+            fp = bc_hook<C>(a.bc_preset, nb, fp, ux, uy, uz, wp, lat_c(DIM, 0, p), lat_c(DIM, 1, p), lat_c(DIM, 2, p),
+                            C(a.u_ref));
+        if (wall) {
+            const float dQ = w.Xb[(long long)slot * MC + t + (long long)p * w.ncb];
+            if (dQ > 0.f) {
+                C fm = C(0);
+                if (dQ < 0.5f) {
+                    const int nbh = nbr_at(q, 1, nc);
+                    if (nbh < 0) atomicCAS(w.status, 0, AGAL_ERR_STATE);
+                    else fm = post_collision<DIM, Q, T>(a, nbh, nc, p);
+                }
+                fp = bouzidi<C>(fp, fm, fq, dQ);
+            }
+        }
+        nb = nbr_at(q, 1, nc);
+        if (hook && nb < 0 && nb != N_SKIPID)
+            fq = bc_hook<C>(a.bc_preset, nb, fq, ux, uy, uz, wq, lat_c(DIM, 0, q), lat_c(DIM, 1, q), lat_c(DIM, 2, q),
+                            C(a.u_ref));
+        if (wall) {
+            const float dQ = w.Xb[(long long)slot * MC + t + (long long)q * w.ncb];
+            if (dQ > 0.f) {
+                C fm = C(0);
+                if (dQ < 0.5f) {
+                    const int nbh = nbr_at(p, 1, nc);
+                    if (nbh < 0) atomicCAS(w.status, 0, AGAL_ERR_STATE);
+                    else fm = post_collision<DIM, Q, T>(a, nbh, nc, q);
+                }
+                fq = bouzidi<C>(fq, fm, fp, dQ);
+            }
+        }
+        g[p] = fp - offp;
+        g[q] = fq - offq;
+    }
+    T *__restrict__ fo = static_cast<T *>(a.fout);
+    push_cell<DIM, Q, T, true>(g, ux, uy, uz, b, t, nrow, false, fo, a);
+}
+
+struct ForceArgs {
+    StepArgs s;               // fin = the buffer read, meta, cmask, collision
+    const int *wall;
+    const int *onb_solid;
+    const float *Xb;
+    long long ncb, nmb;
+    double dv;
+    int order, post;
+    void *Ff;                 // [6][nmb] compute type
+    int *status;
+};
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::MC) k_forces(const ForceArgs fa)
+{
+    pdl_wait();
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, W = Meta<DIM>::W;
+    const StepArgs &a = fa.s;
+    __shared__ int s_meta[W];
+    __shared__ C s_F[3][MC];
+    const int b = fa.wall[blockIdx.x];
+    const int t = threadIdx.x;
+    for (int i = t; i < W; i += MC) s_meta[i] = a.meta[(long long)b * W + i];
+    __syncthreads();
+    const int slot = fa.onb_solid[b];
+    const int mask = a.cmask[(long long)b * MC + t];
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const T *fin = static_cast<const T *>(a.fin);
+    C s[3] = {C(0), C(0), C(0)};
+    if (mask == CELL_BOUNDARY && slot > -1) {
+        // Populations in slot order: post-collision before the stream (the
+        // cell's own collision), stored values after it.
+        C f[Q];
+        if (!fa.post) {
+            C g[Q];
+#pragma unroll
+            for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[(long long)b * BLK + lat_pb(DIM, p) * MC + t]);
+            C ux, uy, uz;
+            collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+#pragma unroll
+            for (int p = 0; p < Q; p++) f[p] = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        } else {
+#pragma unroll
+            for (int p = 0; p < Q; p++) f[p] = full_of<DIM, Q, T>(fin[(long long)b * BLK + p * MC + t], p);
+        }
+        for (int p = 1; p < Q; p++) {
+            if (!lat_half(DIM, p)) continue;
+            const int q = lat_pb(DIM, p);
+            for (int side = 0; side < 2; side++) {
+                const int ad = side ? q : p;   // link direction
+                const int e = side ? p : q;    // towards the cell behind
+                const float dist = fa.Xb[(long long)slot * MC + t + (long long)ad * fa.ncb];
+                if (!(dist > 0.f)) continue;
+                const int Ib = I + lat_c(DIM, 0, e), Jb = J + lat_c(DIM, 1, e);
+                const int Kb = (DIM == 3) ? K + lat_c(DIM, 2, e) : 0;
+                const int nbh = s_meta[nbr_slot(DIM, Ib, Jb, Kb)];
+                const int nc = nbr_cell(DIM, Ib, Jb, Kb);
+                if (nbh < 0) {
+                    atomicCAS(fa.status, 0, AGAL_ERR_STATE);
+                    continue;
+                }
+                const C fm = fa.post ? full_of<DIM, Q, T>(fin[(long long)nbh * BLK + ad * MC + nc], ad)
+                                     : post_collision<DIM, Q, T>(a, nbh, nc, ad);
+                const C fa_ = f[ad];
+                for (int d = 0; d < DIM; d++) {
+                    const int cd = lat_c(DIM, d, ad);
+                    if (fa.order == 1) {
+                        s[d] = r_add(s[d], r_mul(fa_, C(cd)));
+                    } else {
+                        // The reference's 0.5 is a double literal: the term is formed in double.
+                        const double qd = (double)(C)dist;
+                        const double term = __dmul_rn(__dadd_rn(__dmul_rn(__dadd_rn(0.5, qd), (double)fa_),
+                                                                __dmul_rn(__dadd_rn(0.5, -qd), (double)fm)),
+                                                      (double)cd);
+                        s[d] = (C)__dadd_rn((double)s[d], term);
+                    }
+                }
+            }
+        }
+    }
+    for (int d = 0; d < 3; d++) s_F[d][t] = s[d];
+    __syncthreads();
+    for (int h = MC / 2; h > 0; h >>= 1) {
+        if (t < h)
+            for (int d = 0; d < DIM; d++) s_F[d][t] = r_add(s_F[d][t], s_F[d][t + h]);
+        __syncthreads();
+    }
+    if (t == 0) {
+        C *Ff = static_cast<C *>(fa.Ff);
+        const C dv = C(fa.dv);
+        for (int d = 0; d < DIM; d++) {
+            const C v = r_mul(s_F[d][0], dv);
+            if (!fa.post) {
+                Ff[b + (2 * d + 0) * fa.nmb] = v;
+                Ff[b + (2 * d + 1) * fa.nmb] = C(0);
+            } else {
+                Ff[b + (2 * d + 0) * fa.nmb] = r_add(Ff[b + (2 * d + 0) * fa.nmb], v);
+            }
+        }
+    }
+}
+
+template <int DIM, int Q, typename T>
+StepArgs base_args(agal_ctx *c, int L, const void *fin, void *fout)
+{
+    StepArgs a{};
+    a.ids = c->id_set + (long long)L * c->nmb;
+    a.n = c->n_ids[L];
+    a.fin = fin;
+    a.fout = fout;
+    a.meta = c->meta;
+    a.cmask = c->cells_ID_mask;
+    a.omega = c->dxf[L] / c->tau[L];
+    if (sizeof(typename ST<T>::C) == 4) a.omega = (double)((float)c->dxf[L] / (float)c->tau[L]);
+    a.u_ref = c->P.u_ref;
+    a.bc_preset = c->P.bc_preset;
+    a.mrt = (Q == 19 && c->P.collision == AGAL_MRT) ? 1 : 0;
+    const double sv[5] = {c->P.s1, c->P.s2, c->P.s3, c->P.s5, c->P.s6};
+    for (int k = 0; k < 5; k++) a.s[k] = (sizeof(typename ST<T>::C) == 4) ? (double)(float)sv[k] : sv[k];
+    a.fix_count = c->fix_count;
+    a.fix_list = c->fix_list;
+    a.fix_cap = AGAL_FIX_CAP;
+    return a;
+}
+
+template <int DIM, int Q, typename T> struct RunWallStep {
+    static int run(agal_ctx *c, int L, const void *fin, void *fout)
+    {
+        if constexpr (DIM != 3) {
+            return AGAL_OK;
+        } else {
+            const int n = c->wall_n.empty() ? 0 : c->wall_n[L];
+            if (n <= 0) return AGAL_OK;
+            WallArgs w;
+            w.s = base_args<DIM, Q, T>(c, L, fin, fout);
+            w.wall = c->wall_ids + c->wall_off[L];
+            w.onb_solid = c->onb_solid;
+            w.Xb = c->X_b;
+            w.ncb = c->n_maxcells_b;
+            w.bc_type = c->P.S_BC_TYPE;
+            w.status = c->d_status;
+            AGAL_CUDA(c, launch_pdl(k_step_wall<DIM, Q, T>, dim3(n), dim3(Geo<DIM>::MC), 0, c->stream, w));
+            AGAL_CUDA(c, cudaGetLastError());
+            return AGAL_OK;
+        }
+    }
+};
+
+template <int DIM, int Q, typename T> struct RunForces {
+    static int run(agal_ctx *c, int L, int post)
+    {
+        if constexpr (DIM != 3) {
+            return AGAL_OK;
+        } else {
+            const int n = c->wall_n.empty() ? 0 : c->wall_n[L];
+            if (n <= 0 || !c->X_b || !c->Ff) return AGAL_OK;
+            ForceArgs fa;
+            fa.s = base_args<DIM, Q, T>(c, L, c->F[c->cur[L]], nullptr);
+            fa.wall = c->wall_ids + c->wall_off[L];
+            fa.onb_solid = c->onb_solid;
+            fa.Xb = c->X_b;
+            fa.ncb = c->n_maxcells_b;
+            fa.nmb = c->nmb;
+            // dvf_vec (solver_lbm_init.cu:21-27): dx_L^dim in ufloat_t.
+            double dv = 1.0;
+            for (int d = 0; d < DIM; d++) dv = (sizeof(typename ST<T>::C) == 4) ? (double)((float)dv * (float)c->dxf[L])
+                                                                                 : dv * c->dxf[L];
+            fa.dv = dv;
+            fa.order = c->P.S_FORCE_ORDER;
+            fa.post = post;
+            fa.Ff = c->Ff;
+            fa.status = c->d_status;
+            AGAL_CUDA(c, launch_pdl(k_forces<DIM, Q, T>, dim3(n), dim3(Geo<DIM>::MC), 0, c->stream, fa));
+            AGAL_CUDA(c, cudaGetLastError());
+            return AGAL_OK;
+        }
+    }
+};
+
+// S_ReportForces sums (solver_lbm_compute.cu:166-201): every row of the
+// partials over block IDs below id_max[MAX_LEVELS], in FP64, in one CTA.
+template <typename C>
+__global__ void __launch_bounds__(256) k_force_sums(const C *Ff, long long nmb, int n, double *out)
+{
+    __shared__ double s[256];
+    for (int r = 0; r < 6; r++) {
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < n; b += 256) acc += (double)Ff[b + r * nmb];
+        s[threadIdx.x] = acc;
+        __syncthreads();
+        for (int h = 128; h > 0; h >>= 1) {
+            if (threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[r] = s[0];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+}  // namespace agal
+
+int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout)
+{
+    if (!agal_wall_active(c)) return AGAL_OK;
+    return agal::dispatch<agal::RunWallStep>(c, L, fin, fout);
+}
+
+int agal_launch_forces(agal_ctx *c, int L, int post)
+{
+    if (!c->onb_solid || !c->X_b || c->P.S_FORCE_TYPE != 0) return AGAL_OK;
+    return agal::dispatch<agal::RunForces>(c, L, post);
+}
+
+extern "C" int agal_forces(agal_ctx *c, double *out)
+{
+    // Solver_LBM::S_ReportForces (solver_lbm_compute.cu:166-215): the sums
+    // {Fpx, Fmx, Fpy, Fmy, Fpz, Fmz} of the MEA partials in FP64, then the
+    // partials are reset.  The force is factor (Fp - Fm) with factor =
+    // 1 / dx of the finest level (S_FORCE_TYPE 0).
+    if (!c || !out) return AGAL_ERR_PARAM;
+    for (int r = 0; r < 6; r++) out[r] = 0.0;
+    if (!c->Ff) return AGAL_OK;
+    double *d_out = nullptr;
+    AGAL_CUDA(c, cudaMalloc(&d_out, sizeof(double) * 6));
+    const int n = c->id_max[c->max_levels];
+    if (c->storage == AGAL_STORE_FP64)
+        agal::k_force_sums<double><<<1, 256, 0, c->stream>>>(static_cast<const double *>(c->Ff), c->nmb, n, d_out);
+    else
+        agal::k_force_sums<float><<<1, 256, 0, c->stream>>>(static_cast<const float *>(c->Ff), c->nmb, n, d_out);
+    const size_t cs = (c->storage == AGAL_STORE_FP64) ? 8 : 4;
+    cudaError_t e = cudaMemcpyAsync(out, d_out, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->Ff, 0, cs * 6 * c->nmb, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return agal_cuda_check(c, e, "agal_forces");
+    return AGAL_OK;
+}

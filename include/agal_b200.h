@@ -219,6 +219,37 @@ int agal_refine_near_wall(agal_ctx *ctx);
    them).  Pointers may be NULL. */
 int agal_refine_stats(const agal_ctx *ctx, long long *iter, int *n_refined, int *n_coarsened);
 
+/* ---- Geometry (3D velocity sets) -------------------------------------------
+   agal_set_geometry: faces = n_faces x 9 floats (v1x v1y v1z v2x v2y v2z v3x
+   v3y v3z, unit-length domain coordinates), as Geometry imports and splits them
+   (geometry_import.cu:11-83, geometry_refine.cu:178-238).  Builds the
+   voxelizer bins of every bin level and, with G_BIN_MAKE_LINKS, the link bins
+   (Geometry::G_InitBins, geometry_bins.h:106-203; Bins::G_MakeBinsGPU and
+   _MD, geometry_bins_gpu.cu:587-1300), then attaches the geometry to the mesh
+   (Mesh::M_AddGeometry, mesh_init.cu:570-577): agal_refine_near_wall then
+   voxelizes and computes link lengths, and the step imposes the wall
+   (interpolated bounce-back with S_BC_TYPE 1) and sums MEA forces
+   (S_FORCE_TYPE 0).  The bin grid spans the unit cube, as the reference's
+   does (its cell and bin indexing assume L_c = L_fy = L_fz = 1); a face whose
+   bins fall outside it is refused (AGAL_ERR_PARAM). */
+int agal_set_geometry(agal_ctx *ctx, const float *faces, long long n_faces);
+/* CSR bins of voxelizer bin level `level`, or of the link bins for level -1
+   (binned_face_ids_n/N/ids).  Array pointers may be NULL (sizes first). */
+int agal_bins_get(agal_ctx *ctx, int level, int *density, int *n_bins, long long *n_entries, int *n, int *N,
+                  int *ids);
+int agal_voxelize_s1(agal_ctx *ctx, int L);          /* Mesh::M_Geometry_Voxelize_S1, mesh_voxelizer.cu:34-156  */
+int agal_update_solid_children(agal_ctx *ctx, int L);/* Mesh::M_UpdateSolidChildren, mesh_voxelizer.cu:247-259  */
+int agal_voxelize_s2(agal_ctx *ctx, int L);          /* Mesh::M_Geometry_Voxelize_S2, mesh_voxelizer.cu:158-189  */
+int agal_voxelize_s3(agal_ctx *ctx);                 /* Mesh::M_Geometry_Voxelize_S3, mesh_voxelizer.cu:191-245  */
+int agal_link_lengths(agal_ctx *ctx, int L);         /* Mesh::M_LinkLengthComputation, mesh_voxelizer.cu:261-294 */
+/* out = {n_faces, n_solida, n_solidb, n_maxcells_b} (mesh.h:304-307). */
+int agal_geometry_counts(const agal_ctx *ctx, long long *out);
+/* Solver_LBM::S_ReportForces (solver_lbm_compute.cu:166-215): out = {Fpx, Fmx,
+   Fpy, Fmy, Fpz, Fmz}, the FP64 sums of the per-block MEA partials over block
+   IDs below id_max[MAX_LEVELS]; the partials are reset.  The force is
+   (Fp - Fm) / dx of the finest level. */
+int agal_forces(agal_ctx *ctx, double *out);
+
 /* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
    bytes must equal the size reported by agal_array_bytes. */
 int agal_array_bytes(const agal_ctx *ctx, int which, size_t *bytes);

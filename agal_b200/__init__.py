@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import AgalError, AgalParams
 
-__all__ = ["Parser", "Case", "Mesh", "Solver_LBM", "AgalError", "AgalParams", "default_params"]
+__all__ = ["Parser", "Case", "Batch", "Mesh", "Solver_LBM", "AgalError", "AgalParams", "default_params"]
 
 
 def _check(rc: int, ctx: Optional[C.c_void_p] = None) -> None:
@@ -256,6 +256,54 @@ class Case:
         dt = self._DTYPES.get(which, np.int32)
         a = np.ascontiguousarray(arr, dtype=dt)
         self._c(self._lib.agal_load(self._h, which, a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+
+class Batch:
+    """Independent cases advanced together: one CUDA graph per coarse step with
+    one branch per case (agal_batch_*).  Each case ends where advancing it
+    alone would have left it."""
+
+    def __init__(self, cases):
+        self._lib = _lib.lib()
+        self.cases = list(cases)
+        arr = (C.c_void_p * len(self.cases))(*[c._h for c in self.cases])
+        h = C.c_void_p()
+        rc = self._lib.agal_batch_create(arr, len(self.cases), C.byref(h))
+        if rc != _lib.OK:
+            raise AgalError(rc, "agal_batch_create")
+        self._h = h
+
+    def _c(self, rc: int) -> None:
+        if rc != _lib.OK:
+            raise AgalError(rc, self._lib.agal_batch_last_error(self._h).decode())
+
+    def advance_n(self, n: int, use_graph: bool = True) -> None:
+        self._c(self._lib.agal_batch_advance_n(self._h, n, 1 if use_graph else 0))
+
+    def sync(self) -> None:
+        self._c(self._lib.agal_batch_sync(self._h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._c(self._lib.agal_batch_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.agal_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class Mesh(Case):

@@ -540,6 +540,12 @@ template <int DIM, int Q, typename T> struct RunInterp {
         InterpArgs a;
         a.ids = c->id_set + (long long)L * c->nmb;
         a.n = n;
+        // Interface interpolation touches the interface parents only.
+        if (var == AGAL_INTERP_INTERFACE && (int)c->iface_n.size() > L) {
+            a.ids = c->iface_ids + c->iface_off[L];
+            a.n = c->iface_n[L];
+            if (a.n <= 0) return AGAL_OK;
+        }
         a.fpar = c->F[c->cur[L]];
         a.fch = c->F[c->cur[L + 1]];
         a.nbr_child = c->cblock_ID_nbr_child;
@@ -551,9 +557,9 @@ template <int DIM, int Q, typename T> struct RunInterp {
         a.var = var;
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
         if (c->P.interp_order == AGAL_INTERP_CUBIC)
-            AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, true>, dim3((unsigned)n), dim3(NT), 0, c->stream, a));
+            AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, true>, dim3((unsigned)a.n), dim3(NT), 0, c->stream, a));
         else
-            AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, false>, dim3((unsigned)n), dim3(NT), 0, c->stream, a));
+            AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, false>, dim3((unsigned)a.n), dim3(NT), 0, c->stream, a));
         AGAL_CUDA(c, cudaGetLastError());
         return AGAL_OK;
     }
@@ -567,6 +573,12 @@ template <int DIM, int Q, typename T> struct RunAverage {
         AverageArgs a;
         a.ids = c->id_set + (long long)L * c->nmb;
         a.n = n;
+        // Interface and block averaging touch the interface parents only.
+        if (var != AGAL_AVERAGE_GRID && (int)c->iface_n.size() > L) {
+            a.ids = c->iface_ids + c->iface_off[L];
+            a.n = c->iface_n[L];
+            if (a.n <= 0) return AGAL_OK;
+        }
         a.fpar = c->F[c->cur[L]];
         a.fch = c->F[c->cur[L + 1]];
         a.nbr_child = c->cblock_ID_nbr_child;
@@ -576,7 +588,7 @@ template <int DIM, int Q, typename T> struct RunAverage {
         if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L] / (float)c->tau[L + 1]);
         a.var = var;
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
-        AGAL_CUDA(c, launch_pdl(k_average<DIM, Q, T>, dim3((unsigned)n), dim3(NT), 0, c->stream, a));
+        AGAL_CUDA(c, launch_pdl(k_average<DIM, Q, T>, dim3((unsigned)a.n), dim3(NT), 0, c->stream, a));
         AGAL_CUDA(c, cudaGetLastError());
         return AGAL_OK;
     }

@@ -462,6 +462,38 @@ int agal_mark_level(agal_ctx *c, int L, int uniform)
     return AGAL_OK;
 }
 
+namespace agal {
+namespace {
+struct IfaceList {   // interface parents of one level, in ID-set order
+    const int *ids, *bmask, *nch;
+    int *out;
+    __device__ bool pred(int k) const { const int b = ids[k]; return bmask[b] == BLOCK_INTERFACE && nch[b] > -1; }
+    __device__ void emit(int k, int r) const { out[r] = ids[k]; }
+};
+}  // namespace
+}  // namespace agal
+
+int agal_build_iface_lists(agal_ctx *c)
+{
+    c->iface_off.assign(c->max_levels, 0);
+    c->iface_n.assign(c->max_levels, 0);
+    if (!c->amr) return AGAL_OK;
+    if (!c->iface_ids) AGAL_CUDA(c, cudaMalloc(&c->iface_ids, sizeof(int) * c->nmb));
+    int off = 0;
+    for (int L = 0; L + 1 < c->max_levels; L++) {
+        c->iface_off[L] = off;
+        const int n = c->n_ids[L];
+        if (n <= 0) continue;
+        IfaceList f{c->id_set + (long long)L * c->nmb, c->cblock_ID_mask, c->cblock_ID_nbr_child, c->iface_ids + off};
+        int cnt = 0;
+        int rc = compact(c, f, n, &cnt);
+        if (rc) return rc;
+        c->iface_n[L] = cnt;
+        off += cnt;
+    }
+    return AGAL_OK;
+}
+
 int agal_freeze_refined(agal_ctx *c)
 {
     const int n = c->id_max[c->max_levels];

@@ -91,7 +91,7 @@ void release(agal_ctx *c)
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
-                    c->amr, c->fix_count, c->fix_list, c->crit};
+                    c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -180,7 +180,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     const size_t per_block =
         (size_t)c->MC * (2 * c->Q * c->esize + (c->dim + 1) * compute_size(c) + sizeof(int)) +
         sizeof(float) * c->dim + sizeof(int) * (2 * c->Qmax + 5 + c->max_levels) +
-        (c->max_levels > 1 ? 5 * sizeof(int) + sizeof(double) : 0);
+        (c->max_levels > 1 ? 7 * sizeof(int) + sizeof(double) : 0);
     if (p->n_maxcblocks > 0) {
         c->nmb = p->n_maxcblocks;
     } else {
@@ -578,7 +578,7 @@ extern "C" int agal_advance(agal_ctx *c, int L)
 
 // One coarse step of M_Advance_Step (mesh_advance.cu:156-182): 2^N_LEVEL_START
 // sub-steps from the starting level.
-static int coarse_step(agal_ctx *c)
+int agal_record_coarse_step(agal_ctx *c)
 {
     const int mult = 1 << c->L0;
     for (int j = 0; j < mult; j++) {
@@ -594,7 +594,7 @@ static int capture(agal_ctx *c, int steps, cudaGraphExec_t *out)
     cudaGraph_t g = nullptr;
     AGAL_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = AGAL_OK;
-    for (int i = 0; i < steps && rc == AGAL_OK; i++) rc = coarse_step(c);
+    for (int i = 0; i < steps && rc == AGAL_OK; i++) rc = agal_record_coarse_step(c);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     c->cur = cur0;   // the capture only recorded the launches
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -609,7 +609,7 @@ static int capture(agal_ctx *c, int steps, cudaGraphExec_t *out)
 // level L0 takes 2^L0 sub-steps and each finer level twice its parent's count
 // (multi-level), or only L0 is stepped (single level); levels stepped an odd
 // number of times flip.
-static void advance_parity(agal_ctx *c, int steps)
+void agal_advance_parity(agal_ctx *c, int steps)
 {
     for (int L = 0; L < c->max_levels; L++) {
         long long k = 0;
@@ -632,7 +632,7 @@ extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
     if (!multi_level(c)) {
         if (!use_graph) {
             for (int i = 0; i < n; i++)
-                if ((rc = coarse_step(c))) return rc;
+                if ((rc = agal_record_coarse_step(c))) return rc;
         } else if (n > 0) {
             if (!c->graph_exec || c->graph_steps != n || c->graph_cur_in != c->cur) {
                 if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
@@ -641,14 +641,14 @@ extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
                 c->graph_cur_in = c->cur;
             }
             AGAL_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
-            advance_parity(c, n);
+            agal_advance_parity(c, n);
         }
         c->iter += n;
         return AGAL_OK;
     }
     for (int s = 0; s < n; s++) {
         if (!use_graph) {
-            if ((rc = coarse_step(c))) return rc;
+            if ((rc = agal_record_coarse_step(c))) return rc;
         } else {
             int k = (c->ml_graph[0] && c->ml_graph_cur[0] == c->cur)   ? 0
                     : (c->ml_graph[1] && c->ml_graph_cur[1] == c->cur) ? 1
@@ -660,7 +660,7 @@ extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
                 c->ml_graph_cur[k] = c->cur;
             }
             AGAL_CUDA(c, cudaGraphLaunch(c->ml_graph[k], c->stream));
-            advance_parity(c, 1);
+            agal_advance_parity(c, 1);
         }
         const long long i = c->iter;
         if (c->P.P_REFINE > 0 && (i + 1) % c->P.P_REFINE == 0 && i > 0 && (rc = agal_refine_with_solution(c)))

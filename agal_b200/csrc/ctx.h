@@ -104,6 +104,11 @@ struct agal_ctx {
     // bounce-back and the forces: wall_ids[wall_off[L] .. + wall_n[L]).
     int *wall_ids = nullptr;
     std::vector<int> wall_off, wall_n;
+    // Interface parents per level (block mask INTERFACE with children), the
+    // only blocks the per-step interpolation and averaging touch:
+    // iface_ids[iface_off[L] .. + iface_n[L]), in ID-set order.
+    int *iface_ids = nullptr;
+    std::vector<int> iface_off, iface_n;
     std::string err;
 };
 
@@ -138,9 +143,14 @@ int agal_launch_criterion(agal_ctx *c);
 int agal_refine_pass(agal_ctx *c);          // Mesh::M_RefineAndCoarsenBlocks
 int agal_mark_level(agal_ctx *c, int L, int uniform);
 int agal_freeze_refined(agal_ctx *c);
+int agal_build_iface_lists(agal_ctx *c);    // after any mesh change (multi-level cases)
 size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
 #define AGAL_AMR_SMALL 128
 void agal_drop_graphs(agal_ctx *c);         // after any change of the mesh or launch shapes
+// One coarse step's launches on the context's stream (flips cur[] as it
+// records), and the buffer-parity bookkeeping of replaying `steps` of them.
+int agal_record_coarse_step(agal_ctx *c);
+void agal_advance_parity(agal_ctx *c, int steps);
 // Geometry (geometry.cu, wall_kernels.cu).
 void agal_geometry_release(agal_ctx *c);
 int agal_build_wall_lists(agal_ctx *c);     // after the mesh or the wall slots change

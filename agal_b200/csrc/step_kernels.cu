@@ -604,6 +604,8 @@ int agal_build_meta(agal_ctx *c)
         agal::k_build_meta<3><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
                                                            c->cblock_ID_mask, c->cblock_ID_onb, wall, c->meta);
     AGAL_CUDA(c, cudaGetLastError());
+    int rc;
+    if (c->amr && (rc = agal_build_iface_lists(c))) return rc;
     if (c->onb_solid) return agal_build_wall_lists(c);
     return AGAL_OK;
 }

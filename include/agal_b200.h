@@ -250,6 +250,21 @@ int agal_geometry_counts(const agal_ctx *ctx, long long *out);
    (Fp - Fm) / dx of the finest level. */
 int agal_forces(agal_ctx *ctx, double *out);
 
+/* ---- Batches of independent cases (no reference counterpart: AGAL runs one
+   case per process) ------------------------------------------------------------
+   agal_batch_advance_n advances every case of the batch by n coarse steps (each
+   with its own refinement every P_REFINE steps) as one CUDA graph per coarse
+   step whose branches are the cases, so small cases run concurrently.  Each
+   case ends exactly where agal_advance_n would have left it.  The contexts stay
+   owned by the caller and must outlive the batch; all on one device. */
+typedef struct agal_batch agal_batch;
+int agal_batch_create(agal_ctx *const *cases, int n_cases, agal_batch **out);
+int agal_batch_destroy(agal_batch *batch);
+int agal_batch_advance_n(agal_batch *batch, int n, int use_graph);
+int agal_batch_sync(agal_batch *batch);
+int agal_batch_get_stream(const agal_batch *batch, void **stream);
+const char *agal_batch_last_error(const agal_batch *batch);
+
 /* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
    bytes must equal the size reported by agal_array_bytes. */
 int agal_array_bytes(const agal_ctx *ctx, int which, size_t *bytes);

@@ -279,6 +279,129 @@ def develop(case, w: dict):
         case.advance_n(w["spinup"], use_graph=True)
 
 
+# ---------------------------------------------------------------------------
+# Batched workload: many independent D3Q19 cases advanced together
+# (agal_batch: one CUDA graph per coarse step, one branch per case) against
+# the same cases in FP32, one at a time.
+BATCH_SIZES = (32, 48, 64, 96)
+
+
+def batched_specs(n: int, seed: int) -> list[dict]:
+    """Seeded case list: base N^3 with N in {32, 48, 64, 96}, 1-3 levels, Re
+    log-uniform in [100, 1000] (on the unit domain length, v0 = 0.05/Re), half
+    lid-driven cavities (solution refinement, percentile criterion), half flow
+    past a seeded random ellipsoid (axes 8-24 cells, near-wall refinement,
+    interpolated bounce-back, MEA forces)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        s = dict(N=int(rng.choice(BATCH_SIZES)), levels=int(rng.integers(1, 4)),
+                 Re=float(np.exp(rng.uniform(np.log(100.0), np.log(1000.0)))),
+                 kind="cavity" if i % 2 == 0 else "ellipsoid")
+        if s["kind"] == "ellipsoid":
+            s["axes"] = [float(a) for a in rng.uniform(8.0, 24.0, size=3)]
+            s["centre"] = [float(x) for x in rng.uniform(0.42, 0.58, size=3)]
+            s["seed"] = int(rng.integers(1 << 30))
+        out.append(s)
+    return out
+
+
+def batched_case(s: dict, storage: int, device: int):
+    from agal_b200.geometry import icosphere
+    N, lv = s["N"], s["levels"]
+    nb = (N // 4) ** 3
+    kw = dict(velocity_set=_lib.D3Q19, Nx=N, v0=0.05 / s["Re"], storage=storage, device=device,
+              interp_order=_lib.INTERP_LINEAR, P_REFINE=32, S_CRITERION=_lib.CRITERION_PERCENTILE,
+              ref_pct_hi=0.9, ref_pct_lo=0.5, n_maxcblocks=nb if lv == 1 else 3 * nb + 2048)
+    if s["kind"] == "cavity":
+        kw.update(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=lv, bc_preset=_lib.BC_LDC3D, ic_preset=_lib.IC_REST)
+    else:
+        kw.update(MAX_LEVELS_WALL=lv, MAX_LEVELS_INTERIOR=1, bc_preset=_lib.BC_FPSC3D, ic_preset=_lib.IC_UNIFORM,
+                  u_ref=0.05, G_BIN_DENSITY=8, G_BIN_LEVELS=lv, G_BIN_SPEC=2, G_BIN_MAKE_LINKS=1,
+                  G_NEAR_WALL_DISTANCE=0.05, S_BC_TYPE=1, S_FORCE_TYPE=0, S_FORCE_ORDER=2)
+    case = ag.Case(ag.default_params(**kw))
+    if s["kind"] == "ellipsoid":
+        # Axes in cells of the base grid, at most half the base size, so that
+        # the body and its refinement band stay clear of the domain faces.
+        axes = np.minimum(np.asarray(s["axes"]), 0.5 * N)
+        f = icosphere(3, 1.0, (0.0, 0.0, 0.0), seed=s["seed"]).astype(np.float64)
+        f = f * (axes / (2.0 * N)) + np.asarray(s["centre"])
+        case.set_geometry(f.astype(np.float32))
+    case.set_ic(0)
+    case.refine_near_wall()
+    return case
+
+
+def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device: int) -> dict:
+    """Aggregate MLUPS of the batch (FP16 populations, batched graph) and of
+    the same cases in FP32 advanced one at a time; both after the same
+    spin-up, timed with CUDA events over `steps` coarse steps that hold no
+    regrid (P_REFINE = 32, spin-up past the first regrid)."""
+    specs = batched_specs(n_cases, seed)
+
+    def build(storage):
+        cases = [batched_case(s, storage, device) for s in specs]
+        tunes = [c.autotune(0, reps=3)["variant"] for c in cases]
+        return cases, tunes
+
+    def cells(cases):
+        return sum(leaf_cells(c.counts(), 3) for c in cases)
+
+    # batched, FP16
+    cases, tunes16 = build(_lib.STORE_FP16)
+    batch = ag.Batch(cases)
+    batch.advance_n(spinup)
+    batch.sync()
+    stream = torch.cuda.ExternalStream(batch.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    upd16 = cells(cases)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch.advance_n(steps)
+    e1.record(stream)
+    batch.sync()
+    t16 = e0.elapsed_time(e1)
+    levels16 = [c.counts()["n_ids"][:-1] for c in cases]
+    batch.close()
+    for c in cases:
+        c.close()
+    # one at a time, FP32
+    cases, tunes32 = build(_lib.STORE_FP32)
+    for c in cases:
+        c.advance_n(spinup)
+    t32 = 0.0
+    upd32 = cells(cases)
+    for c in cases:
+        c.sync()
+        st = torch.cuda.ExternalStream(c.stream_ptr())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        c.advance_n(steps)
+        b.record(st)
+        c.sync()
+        t32 += a.elapsed_time(b)
+    for c in cases:
+        c.close()
+    v16 = upd16 * steps / (t16 * 1e-3) / 1e6
+    v32 = upd32 * steps / (t32 * 1e-3) / 1e6
+    peak, kind = measured_peak_hbm()
+    gbs = upd16 * steps * 2 * 19 * 2 / (t16 * 1e-3) / 1e9
+    return {"workload": "batched_d3q19_64", "n_cases": n_cases, "seed": seed,
+            "desc": "independent D3Q19 BGK cases, base N^3 with N in {32,48,64,96}, 1-3 levels, Re log-uniform "
+                    "[100,1000], half lid-driven cavities with percentile solution refinement, half flow past "
+                    "a seeded ellipsoid (axes 8-24 cells) with near-wall refinement, interpolated bounce-back "
+                    "and MEA forces; refinement by the plain criterion (no learned predictor)",
+            "spinup_steps": spinup, "timed_steps": steps,
+            "value": v16, "unit": "MLUPS", "storage": "f16-offset", "ms_per_step": t16 / steps,
+            "cell_updates_per_step": upd16,
+            "one_at_a_time_fp32": {"value": v32, "ms_per_step": t32 / steps, "cell_updates_per_step": upd32},
+            "ratio_vs_one_at_a_time_fp32": v16 / v32,
+            "hbm": {"achieved_gbs": gbs, "peak": peak, "frac": gbs / peak, "peak_source": kind,
+                    "bytes_per_update": 2 * 19 * 2},
+            "autotune_variants": {"fp16": tunes16, "fp32": tunes32},
+            "blocks_per_level_fp16": levels16}
+
+
 def run_cpu_oracle(w: dict, seconds: float, threads: int, max_steps: int | None = None) -> dict:
     """Oracle (CPU restatement, OpenMP) MLUPS on a bounded sample of the workload."""
     from oracle.orc import OracleCase, build  # CPU baseline leg only
@@ -342,6 +465,9 @@ def main(argv=None) -> int:
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
     ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3],
                     help="with --profile: step kernel variant (1, 2 cells per thread; 3 TMA pipeline)")
+    ap.add_argument("--batched-cases", type=int, default=64,
+                    help="independent D3Q19 cases of the batched measurement (0 skips it)")
+    ap.add_argument("--batched-seed", type=int, default=2024)
     ap.add_argument("--spinup", type=int, default=None,
                     help="with --profile: coarse steps of the untimed spin-up of a multi-level workload")
     a = ap.parse_args(argv)
@@ -501,6 +627,11 @@ def main(argv=None) -> int:
                 "workload": rwl, "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "autotune": rtune}
 
+    # --- batched independent cases vs the same cases one at a time -----------
+    batched = None
+    if a.batched_cases > 0:
+        batched = run_batched(torch, a.batched_cases, a.batched_seed, spinup=40, steps=20, device=local)
+
     # --- CPU baseline (rank 0 only) -------------------------------------------
     cpu = None
     if rank == 0 and not a.no_cpu_baseline:
@@ -521,6 +652,8 @@ def main(argv=None) -> int:
                                   "ms_per_step": plain["ms_per_step"],
                                   "blocks_per_level": plain["counts"]["n_ids"][:-1],
                                   "ratio": head["value"] / plain["value"]}
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     return 0
 

@@ -106,6 +106,7 @@ PROTOS = [
     ("agal_link_lengths", C.c_int, [C.c_void_p, C.c_int]),
     ("agal_geometry_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("agal_forces", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("agal_learn_gemm_bf16", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
     ("agal_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("agal_batch_destroy", C.c_int, [C.c_void_p]),
     ("agal_batch_advance_n", C.c_int, [C.c_void_p, C.c_int, C.c_int]),

@@ -257,6 +257,12 @@ int agal_forces(agal_ctx *ctx, double *out);
    step whose branches are the cases, so small cases run concurrently.  Each
    case ends exactly where agal_advance_n would have left it.  The contexts stay
    owned by the caller and must outlive the batch; all on one device. */
+/* ---- Learned refinement predictor (no reference counterpart) ----------------
+   agal_learn_gemm_bf16: D[M x N] = A[M x K] . B[N x K]^T with BF16 inputs (bit
+   patterns) and FP32 accumulation on the tensor cores (tcgen05), host buffers;
+   N <= 32, K a multiple of 16.  The kernel behind the network's layers. */
+int agal_learn_gemm_bf16(const uint16_t *A, const uint16_t *B, float *D, int M, int N, int K);
+
 typedef struct agal_batch agal_batch;
 int agal_batch_create(agal_ctx *const *cases, int n_cases, agal_batch **out);
 int agal_batch_destroy(agal_batch *batch);

@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import AgalError, AgalParams
 
-__all__ = ["Parser", "Case", "Batch", "Mesh", "Solver_LBM", "AgalError", "AgalParams", "default_params"]
+__all__ = ["Parser", "Case", "Batch", "Learner", "Mesh", "Solver_LBM", "AgalError", "AgalParams", "default_params"]
 
 
 def _check(rc: int, ctx: Optional[C.c_void_p] = None) -> None:
@@ -291,6 +291,144 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.agal_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Learner:
+    """Learned refinement predictor (agal_learn_*): a 3-layer convolutional
+    network over each block's cells, trained on the GPU on snapshots that the
+    plain percentile criterion labels, and coupled with a case's
+    solution-based refinement."""
+
+    N_OUT = 2
+
+    def __init__(self, dim: int, seed: int = 0):
+        self._lib = _lib.lib()
+        h = C.c_void_p()
+        rc = self._lib.agal_learn_create(dim, seed, C.byref(h))
+        if rc != _lib.OK:
+            raise AgalError(rc, "agal_learn_create")
+        self._h = h
+        self.dim = dim
+        self.cells = 16 if dim == 2 else 64
+        self.taps = 9 if dim == 2 else 27
+        n = C.c_longlong()
+        self._c(self._lib.agal_learn_num_params(self._h, C.byref(n)))
+        self.num_params = n.value
+
+    def _c(self, rc: int) -> None:
+        if rc != _lib.OK:
+            raise AgalError(rc, self._lib.agal_learn_last_error(self._h).decode())
+
+    def shapes(self) -> dict:
+        """Parameter blocks in storage order: name -> (rows, columns)."""
+        T = self.taps
+        k1p = (8 * T + 15) // 16 * 16
+        return {"W1": (32, k1p), "b1": (32,), "W2": (32, 32 * T), "b2": (32,), "W3": (2, 32 * T), "b3": (2,)}
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.num_params, np.float32)
+        self._c(self._lib.agal_learn_get_params(self._h, out.ctypes.data_as(C.c_void_p), out.size))
+        return out
+
+    def set_params(self, w) -> None:
+        a = np.ascontiguousarray(w, dtype=np.float32)
+        self._c(self._lib.agal_learn_set_params(self._h, a.ctypes.data_as(C.c_void_p), a.size))
+
+    def record(self, case: Case) -> None:
+        self._c(self._lib.agal_learn_record(self._h, case._h))
+
+    def label(self, case: Case) -> None:
+        self._c(self._lib.agal_learn_label(self._h, case._h))
+
+    def counts(self) -> dict:
+        out = (C.c_longlong * 6)()
+        self._c(self._lib.agal_learn_counts(self._h, out))
+        keys = ("snapshots", "labelled", "regrids", "judged", "plain_refine", "missed")
+        return dict(zip(keys, list(out)))
+
+    def snapshot(self, k: int):
+        """(X [n*cells][8], labels [n][2], weights [n]) of snapshot k."""
+        n = C.c_int()
+        self._c(self._lib.agal_learn_snapshot(self._h, k, C.byref(n), None, None, None))
+        X = np.empty((n.value * self.cells, 8), np.float32)
+        Y = np.empty((n.value, 2), np.float32)
+        W = np.empty(n.value, np.float32)
+        self._c(self._lib.agal_learn_snapshot(self._h, k, C.byref(n), X.ctypes.data_as(C.c_void_p),
+                                              Y.ctypes.data_as(C.c_void_p), W.ctypes.data_as(C.c_void_p)))
+        return X, Y, W
+
+    def decisions(self, k: int) -> np.ndarray:
+        """The percentile rule's decisions [n][2] on snapshot k's own state."""
+        n = C.c_int()
+        self._c(self._lib.agal_learn_snapshot(self._h, k, C.byref(n), None, None, None))
+        out = np.zeros((n.value, 2), np.float32)
+        self._c(self._lib.agal_learn_snapshot_decisions(self._h, k, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def set_class_weights(self, refine: float, coarsen: float) -> None:
+        """Weights of the positive class (a mark) of the two outputs in the loss."""
+        self._c(self._lib.agal_learn_set_class_weights(self._h, refine, coarsen))
+
+    def balance_classes(self, first: int, last: int, cap: float = 50.0) -> tuple:
+        """Set the class weights to the ratio of unmarked to marked blocks over
+        the labelled snapshots [first, last), capped; returns them."""
+        pos = np.zeros(2)
+        tot = 0.0
+        for k in range(first, last):
+            _, Y, W = self.snapshot(k)
+            pos += (Y * W[:, None]).sum(axis=0)
+            tot += W.sum()
+        w = tuple(float(min(cap, max(1.0, (tot - p) / p))) if p > 0 else 1.0 for p in pos)
+        self.set_class_weights(*w)
+        return w
+
+    def gradients(self, k: int):
+        """(loss, gradient) of labelled snapshot k at the current weights."""
+        g = np.empty(self.num_params, np.float32)
+        loss = C.c_double()
+        self._c(self._lib.agal_learn_gradients(self._h, k, g.ctypes.data_as(C.c_void_p), g.size, C.byref(loss)))
+        return loss.value, g
+
+    def train(self, first: int, last: int, epochs: int, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = C.c_double()
+        self._c(self._lib.agal_learn_train(self._h, first, last, epochs, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def predict(self, k: int) -> np.ndarray:
+        n = C.c_int()
+        self._c(self._lib.agal_learn_snapshot(self._h, k, C.byref(n), None, None, None))
+        out = np.zeros((n.value, 2), np.float32)
+        self._c(self._lib.agal_learn_predict_snapshot(self._h, k, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def attach(self, case: Case, mode: int, judge_every: int = 4, threshold: float = 0.5) -> None:
+        """mode 1: collect labelled snapshots, 2: predict (judged), 0: detach."""
+        rc = self._lib.agal_learn_attach(case._h, self._h if mode else None, mode, judge_every, threshold)
+        if rc != _lib.OK:
+            raise AgalError(rc, "agal_learn_attach")
+        case._learner = self if mode else None
+        self._attached = [c for c in getattr(self, "_attached", []) if c is not case] + ([case] if mode else [])
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            for case in getattr(self, "_attached", []):   # the cases must not keep a dangling predictor
+                if getattr(case, "_h", None):
+                    self._lib.agal_learn_attach(case._h, None, 0, 1, 0.5)
+            self._attached = []
+            self._lib.agal_learn_destroy(self._h)
             self._h = None
 
     def __del__(self):

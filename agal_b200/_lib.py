@@ -25,7 +25,7 @@ STORE_FP32, STORE_FP64, STORE_FP16, STORE_BF16 = 0, 1, 2, 3
 BC_NONE, BC_LDC2D, BC_LDC3D, BC_FPSC2D, BC_FPSC3D = 0, 1, 2, 3, 4
 IC_REST, IC_UNIFORM = 0, 1
 REGION_NONE, REGION_BOUNDARY, REGION_BOX = 0, 1, 2
-CRITERION_VORTICITY, CRITERION_Q, CRITERION_PERCENTILE = 0, 1, 2
+CRITERION_VORTICITY, CRITERION_Q, CRITERION_PERCENTILE, CRITERION_LEARNED = 0, 1, 2, 3
 INTERP_INTERFACE, INTERP_ADDED = 0, 1
 AVERAGE_INTERFACE, AVERAGE_BLOCK, AVERAGE_GRID = 0, 1, 2
 
@@ -113,6 +113,23 @@ PROTOS = [
     ("agal_batch_sync", C.c_int, [C.c_void_p]),
     ("agal_batch_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("agal_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("agal_learn_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("agal_learn_destroy", C.c_int, [C.c_void_p]),
+    ("agal_learn_last_error", C.c_char_p, [C.c_void_p]),
+    ("agal_learn_num_params", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("agal_learn_get_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("agal_learn_set_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("agal_learn_record", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("agal_learn_label", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("agal_learn_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("agal_learn_snapshot", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("agal_learn_gradients", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong, C.POINTER(C.c_double)]),
+    ("agal_learn_train", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint64,
+                                   C.POINTER(C.c_double)]),
+    ("agal_learn_predict_snapshot", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("agal_learn_snapshot_decisions", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("agal_learn_set_class_weights", C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    ("agal_learn_attach", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double]),
 ]
 
 _lib = None

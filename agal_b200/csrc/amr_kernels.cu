@@ -532,6 +532,25 @@ __global__ void k_pct_mark(const double *wval, const PctState *st, const int *nb
     if (r == REF_REFINED && w < thr_lo) ref[b] = REF_MARK_COARSEN;
 }
 
+// The percentile rule's decisions for listed blocks (learned-predictor
+// labels): Y[j] = {leaf block value above the upper quantile, value below the
+// lower quantile}.  With lvl0, Wt[j] = 1 if block ids[j] is still active on
+// level lvl0[j], else 0 (and Y = 0).
+__global__ void k_pct_decide(const double *wval, const int *pop, const PctState *st, const int *ids,
+                             const int *lvl0, int n, const int *ref, const int *level, float *Y, float *Wt)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int b = ids[j];
+    const bool valid = ref[b] != REF_INACTIVE && (!lvl0 || level[b] == lvl0[j]) && st->n > 0;
+    const double thr_hi = __longlong_as_double((long long)st->prefix[0]);
+    const double thr_lo = __longlong_as_double((long long)st->prefix[1]);
+    const double w = wval[b];
+    Y[2 * j + 0] = (valid && pop[b] && w > thr_hi) ? 1.f : 0.f;
+    Y[2 * j + 1] = (valid && w < thr_lo) ? 1.f : 0.f;
+    if (Wt) Wt[j] = valid ? 1.f : 0.f;
+}
+
 template <int DIM, int Q, typename T> struct RunInterp {
     static int run(agal_ctx *c, int L, int var)
     {
@@ -599,7 +618,8 @@ template <int DIM, int Q, typename T> struct RunAverage {
 int agal_launch_interp(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunInterp>(c, L, var); }
 int agal_launch_average(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunAverage>(c, L, var); }
 
-static int launch_percentile(agal_ctx *c, int idm)
+// Block values and the two quantiles of the percentile rule (no marks).
+static int percentile_select(agal_ctx *c, int idm)
 {
     if (!c->crit) return agal_set_err(c, AGAL_ERR_STATE, "percentile criterion needs MAX_LEVELS > 1");
     double *wval = static_cast<double *>(c->crit);
@@ -632,8 +652,36 @@ static int launch_percentile(agal_ctx *c, int idm)
         agal::k_pct_hist<<<g, 256, 0, c->stream>>>(wval, c->amr_a, idm, st, pass, hist);
         agal::k_pct_pick<<<2, 1024, 0, c->stream>>>(hist, st, pass, c->P.ref_pct_hi, c->P.ref_pct_lo);
     }
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
+static int launch_percentile(agal_ctx *c, int idm)
+{
+    const int rc = percentile_select(c, idm);
+    if (rc) return rc;
+    double *wval = static_cast<double *>(c->crit);
+    agal::PctState *st = reinterpret_cast<agal::PctState *>(reinterpret_cast<int *>(wval + c->nmb) + 2 * 65536);
+    const unsigned g = (unsigned)((idm + 255) / 256);
     agal::k_pct_mark<<<g, 256, 0, c->stream>>>(wval, st, c->cblock_ID_nbr, c->nmb, c->Qmax, c->cblock_level,
                                                c->P.MAX_LEVELS_INTERIOR, idm, c->cblock_ID_ref);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
+int agal_percentile_decisions(agal_ctx *c, int select, const int *ids, const int *lvl0, int n, float *Y, float *Wt)
+{
+    if (!c->crit) return agal_set_err(c, AGAL_ERR_STATE, "percentile criterion needs MAX_LEVELS > 1");
+    const int idm = c->id_max[c->max_levels];
+    if (select && idm > 0) {
+        const int rc = percentile_select(c, idm);
+        if (rc) return rc;
+    }
+    if (n <= 0) return AGAL_OK;
+    double *wval = static_cast<double *>(c->crit);
+    agal::PctState *st = reinterpret_cast<agal::PctState *>(reinterpret_cast<int *>(wval + c->nmb) + 2 * 65536);
+    agal::k_pct_decide<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(wval, c->amr_a, st, ids, lvl0, n,
+                                                                           c->cblock_ID_ref, c->cblock_level, Y, Wt);
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;
 }
@@ -642,7 +690,9 @@ int agal_launch_criterion(agal_ctx *c)
 {
     const int idm = c->id_max[c->max_levels];
     if (idm <= 0) return AGAL_OK;
-    if (c->P.S_CRITERION == AGAL_CRITERION_PERCENTILE) return launch_percentile(c, idm);
+    // The learned mode's judge (and its stand-in without a network) is the percentile rule.
+    if (c->P.S_CRITERION == AGAL_CRITERION_PERCENTILE || c->P.S_CRITERION == AGAL_CRITERION_LEARNED)
+        return launch_percentile(c, idm);
     agal::CriterionArgs a;
     a.idm = idm;
     a.nmb = c->nmb;

@@ -180,7 +180,8 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     const size_t per_block =
         (size_t)c->MC * (2 * c->Q * c->esize + (c->dim + 1) * compute_size(c) + sizeof(int)) +
         sizeof(float) * c->dim + sizeof(int) * (2 * c->Qmax + 5 + c->max_levels) +
-        (c->max_levels > 1 ? 7 * sizeof(int) + sizeof(double) : 0);
+        (c->max_levels > 1 ? 7 * sizeof(int) + sizeof(double) : 0) +
+        (size_t)c->MC / 4 * 2 * sizeof(long long);   // stream-guard fix-up list
     if (p->n_maxcblocks > 0) {
         c->nmb = p->n_maxcblocks;
     } else {
@@ -225,7 +226,8 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->d_status, sizeof(int) * 4);
     ALLOC(c->meta, sizeof(int) * (size_t)(c->dim == 2 ? 12 : 28) * nmb);
     ALLOC(c->fix_count, sizeof(int) * 4);
-    ALLOC(c->fix_list, sizeof(long long) * 2 * (size_t)AGAL_FIX_CAP);
+    c->fix_cap = (int)std::min<long long>(std::max<long long>(nmc / 4, AGAL_FIX_CAP_MIN), 1LL << 26);
+    ALLOC(c->fix_list, sizeof(long long) * 2 * (size_t)c->fix_cap);
     if (c->max_levels > 1) {
         const size_t na = agal_amr_scratch_ints(nmb);
         ALLOC(c->amr, sizeof(int) * na);
@@ -469,8 +471,13 @@ extern "C" int agal_refine_with_solution(agal_ctx *c)
         if ((rc = agal_average(c, L, AGAL_AVERAGE_GRID))) return rc;
     for (int L = c->L0; L < ML - 1; L++)
         if ((rc = agal_interpolate(c, L, AGAL_INTERP_INTERFACE))) return rc;
-    if ((rc = agal_launch_criterion(c))) return rc;
-    return agal_refine_coarsen(c);
+    if (c->learner) {
+        if ((rc = agal_learn_marks(c))) return rc;
+    } else if ((rc = agal_launch_criterion(c))) {
+        return rc;
+    }
+    if ((rc = agal_refine_coarsen(c))) return rc;
+    return c->learner ? agal_learn_after_regrid(c) : AGAL_OK;
 }
 
 // Mesh::M_Advance_RefineNearWall without geometry (mesh_advance.cu:54-122).
@@ -779,9 +786,8 @@ extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
             raw[k].resize(n * c->esize);
             AGAL_CUDA(c, cudaMemcpy(raw[k].data(), c->F[k], n * c->esize, cudaMemcpyDeviceToHost));
         }
-        std::vector<int> wb, cm(c->nmc);
+        std::vector<int> wb;
         if ((rc = block_buffers(c, wb))) return rc;
-        AGAL_CUDA(c, cudaMemcpy(cm.data(), c->cells_ID_mask, sizeof(int) * c->nmc, cudaMemcpyDeviceToHost));
         // Device layout F[b][s][c] -> reference layout cells_f_F[s][b*MC + c].
         double *o = static_cast<double *>(host_buf);
         for (int s = 0; s < c->Q; s++) {
@@ -797,7 +803,6 @@ extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
                 case AGAL_STORE_FP16: decode<__half>(r, src, c->Q, p, &o[i]); break;
                 case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, src, c->Q, p, &o[i]); break;
                 }
-                if (cm[cell] == CELL_SOLID) o[i] = -1.0;
             }
         }
         return AGAL_OK;

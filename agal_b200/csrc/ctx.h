@@ -77,6 +77,7 @@ struct agal_ctx {
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
     int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
     long long *fix_list = nullptr;
+    int fix_cap = 0;
     // refine/coarsen pass scratch (multi-level cases only), one allocation:
     int *amr = nullptr;
     int *amr_emap = nullptr;           // efficient map (mesh_amr.cu c_tmp_8), -1 = absent
@@ -109,11 +110,16 @@ struct agal_ctx {
     // iface_ids[iface_off[L] .. + iface_n[L]), in ID-set order.
     int *iface_ids = nullptr;
     std::vector<int> iface_off, iface_n;
+    // Learned refinement predictor attached to this case (learn.cu).
+    struct agal_learn *learner = nullptr;
+    int learn_mode = 0;                // 1 = collect labelled snapshots, 2 = predict (judged)
     std::string err;
 };
 
-// Stream-guard fix-ups (refused swaps) one step of a context can hold.
-#define AGAL_FIX_CAP 65536
+// Stream-guard fix-ups (refused swaps) one step of a context can hold:
+// n_maxcells / 4, at least AGAL_FIX_CAP_MIN (every wall link of a geometry is
+// one refused swap per step).
+#define AGAL_FIX_CAP_MIN 65536
 
 // Step kernel variants: 1 and 2 cells per thread (one-shot grid), 3 the
 // TMA-staged persistent pipeline.
@@ -140,6 +146,10 @@ int agal_launch_mass(agal_ctx *c, double *out);
 int agal_launch_interp(agal_ctx *c, int L, int var);
 int agal_launch_average(agal_ctx *c, int L, int var);
 int agal_launch_criterion(agal_ctx *c);
+// Decisions of the percentile rule for listed blocks (k_pct_decide); select = 1
+// first computes the block values and quantiles on the current macros, 0
+// reuses those of the last criterion launch.
+int agal_percentile_decisions(agal_ctx *c, int select, const int *ids, const int *lvl0, int n, float *Y, float *Wt);
 int agal_refine_pass(agal_ctx *c);          // Mesh::M_RefineAndCoarsenBlocks
 int agal_mark_level(agal_ctx *c, int L, int uniform);
 int agal_freeze_refined(agal_ctx *c);
@@ -157,3 +167,6 @@ int agal_build_wall_lists(agal_ctx *c);     // after the mesh or the wall slots 
 int agal_wall_active(const agal_ctx *c);    // interpolated bounce-back in force
 int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout);
 int agal_launch_forces(agal_ctx *c, int L, int post);
+// Learned predictor hooks of the solution-based refinement (learn.cu).
+int agal_learn_marks(agal_ctx *c);          // instead of the criterion when a learner is attached
+int agal_learn_after_regrid(agal_ctx *c);   // after the refine/coarsen pass

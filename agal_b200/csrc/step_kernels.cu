@@ -66,15 +66,32 @@ k_step(const StepArgs a)
     }
     __syncthreads();
     const int fl = s_meta[lb][Meta<DIM>::FLAGS];
-    if (b < 0 || !(fl & META_ACTIVE) || (fl & META_WALL)) return;
+    if (b < 0 || (fl & META_WALL)) return;
 
     T *__restrict__ fo = static_cast<T *>(a.fout);
+    // The reference steps in place and leaves solid cells and inactive blocks
+    // (refined solid blocks) untouched, so whatever a grid average or an
+    // interpolation wrote there stays and feeds the next transfer: carry
+    // those cells into the output buffer unchanged.
+    auto carry = [&](int h) {
+#pragma unroll
+        for (int sl = 0; sl < Q; sl++) fo[(long long)b * BLK + sl * MC + t0 + h * TPB] = fin[sl * MC + h * TPB];
+    };
+    if (!(fl & META_ACTIVE)) {
+        if (SOLID)
+#pragma unroll
+            for (int h = 0; h < CPT; h++) carry(h);
+        return;
+    }
     const int *nrow = s_meta[lb];
     const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
 #pragma unroll
     for (int h = 0; h < CPT; h++) {
         const int t = t0 + h * TPB;
-        if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;   // solid cells keep their guard
+        if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) {
+            carry(h);
+            continue;
+        }
         C ux, uy, uz;
         collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
         push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
@@ -308,7 +325,7 @@ int launch_step(agal_ctx *c, const StepArgs &a, int n)
 // next step.  One CTA; the list is usually empty.  A list longer than its
 // capacity leaves AGAL_ERR_STATE in the status word (reported by agal_sync).
 template <typename T>
-__global__ void __launch_bounds__(256) k_stream_fixup(T *fo, int *count, const long long *list, int cap, int *status)
+__global__ void __launch_bounds__(1024) k_stream_fixup(T *fo, int *count, const long long *list, int cap, int *status)
 {
     pdl_wait();
     const int n = *count;
@@ -355,15 +372,15 @@ template <int DIM, int Q, typename T> struct RunStep {
         }
         a.fix_count = c->fix_count;
         a.fix_list = c->fix_list;
-        a.fix_cap = AGAL_FIX_CAP;
+        a.fix_cap = c->fix_cap;
         if (cpt <= 0) cpt = c->step_cpt;
         const int rc = (cpt == 3)   ? launch_step_tma<DIM, Q, T>(c, a)
                        : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                                     : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
         if (const int rw = agal_launch_wall_step(c, L, a.fin, a.fout)) return rw;
-        AGAL_CUDA(c, launch_pdl(k_stream_fixup<T>, dim3(1), dim3(256), 0, c->stream, static_cast<T *>(a.fout),
-                                c->fix_count, c->fix_list, (int)AGAL_FIX_CAP, c->d_status));
+        AGAL_CUDA(c, launch_pdl(k_stream_fixup<T>, dim3(1), dim3(1024), 0, c->stream, static_cast<T *>(a.fout),
+                                c->fix_count, c->fix_list, c->fix_cap, c->d_status));
         AGAL_CUDA(c, cudaGetLastError());
         if (flip) c->cur[L] = 1 - c->cur[L];
         return AGAL_OK;

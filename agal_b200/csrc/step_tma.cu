@@ -205,8 +205,16 @@ k_step_tma(const StepArgs a, int *status)
                 if (b < 0) continue;
                 const int *row = meta + lb * W;
                 const int fl = row[Meta<DIM>::FLAGS];
-                if (!(fl & META_ACTIVE) || (fl & META_WALL)) continue;
-                if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) continue;
+                if (fl & META_WALL) continue;
+                // Solid cells and inactive blocks are left untouched by the
+                // reference's in-place step: carry them over unchanged.
+                if (SOLID && (!(fl & META_ACTIVE) || __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID)) {
+#pragma unroll
+                    for (int sl = 0; sl < Q; sl++)
+                        fo[(long long)b * BLK + sl * MC + t] = pop[(size_t)lb * BLK + sl * MC + t];
+                    continue;
+                }
+                if (!(fl & META_ACTIVE)) continue;
                 C g[Q];
 #pragma unroll
                 for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(pop[(size_t)lb * BLK + lat_pb(DIM, p) * MC + t]);

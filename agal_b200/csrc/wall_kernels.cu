@@ -88,10 +88,15 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
     const int t = threadIdx.x;
     for (int i = t; i < W; i += MC) s_meta[i] = a.meta[(long long)b * W + i];
     __syncthreads();
-    if (!(s_meta[Meta<DIM>::FLAGS] & META_ACTIVE)) return;
     const int mask = a.cmask[(long long)b * MC + t];
-    if (mask == CELL_SOLID) return;   // solid cells keep their guard
     const T *fin = static_cast<const T *>(a.fin) + (long long)b * BLK + t;
+    if (!(s_meta[Meta<DIM>::FLAGS] & META_ACTIVE) || mask == CELL_SOLID) {
+        // untouched by the reference's in-place step: carried over unchanged
+        T *fo = static_cast<T *>(a.fout) + (long long)b * BLK + t;
+#pragma unroll
+        for (int sl = 0; sl < Q; sl++) fo[sl * MC] = fin[sl * MC];
+        return;
+    }
     C g[Q];
 #pragma unroll
     for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[lat_pb(DIM, p) * MC]);
@@ -276,7 +281,7 @@ StepArgs base_args(agal_ctx *c, int L, const void *fin, void *fout)
     for (int k = 0; k < 5; k++) a.s[k] = (sizeof(typename ST<T>::C) == 4) ? (double)(float)sv[k] : sv[k];
     a.fix_count = c->fix_count;
     a.fix_list = c->fix_list;
-    a.fix_cap = AGAL_FIX_CAP;
+    a.fix_cap = c->fix_cap;
     return a;
 }
 

@@ -76,6 +76,7 @@ extern "C" {
 #define AGAL_CRITERION_VORTICITY  0
 #define AGAL_CRITERION_Q          1
 #define AGAL_CRITERION_PERCENTILE 2
+#define AGAL_CRITERION_LEARNED    3   /* network predictions, percentile rule as the judge (agal_learn_attach) */
 
 /* interpolation / averaging modes, inc/mesh.h:58-62 */
 #define AGAL_INTERP_INTERFACE 0
@@ -262,6 +263,54 @@ int agal_forces(agal_ctx *ctx, double *out);
    patterns) and FP32 accumulation on the tensor cores (tcgen05), host buffers;
    N <= 32, K a multiple of 16.  The kernel behind the network's layers. */
 int agal_learn_gemm_bf16(const uint16_t *A, const uint16_t *B, float *D, int M, int N, int K);
+
+/* The predictor: per block of 4^d cells, 8 input channels ((rho-1)/U^2, u/U,
+   v/U, w/U, |curl u|/U, level/(ML-1), refined flag, 1), three 3^d
+   convolutions 8 -> 32 -> 32 -> 2 (ReLU between, zero padding at the block
+   faces), the last averaged over the block: logits of the percentile rule's
+   two decisions at the next regrid (a leaf block's value above the upper
+   quantile, a block's value below the lower one; the marks follow with the
+   rule's admissibility).  BF16 weights and activations, FP32 accumulation
+   (tcgen05), Adam on FP32 master weights.  Snapshots live on the device:
+   agal_learn_record stores the features of a case's current blocks and the
+   rule's decisions on that state, agal_learn_label labels the latest
+   unlabelled snapshot with the decisions of the rule's last run. */
+typedef struct agal_learn agal_learn;
+int agal_learn_create(int dim, unsigned long long seed, agal_learn **out);
+int agal_learn_destroy(agal_learn *m);
+const char *agal_learn_last_error(const agal_learn *m);
+int agal_learn_num_params(const agal_learn *m, long long *n);
+/* Parameters W1 [32][K1p], b1 [32], W2 [32][K2], b2 [32], W3 [2][K2], b3 [2];
+   K2 = 32 T, K1p = 16 ceil(8 T / 16), T = 3^d, column = tap * channels +
+   channel, tap = (dx+1) + 3 (dy+1) + 9 (dz+1); W1's padding columns are 0. */
+int agal_learn_get_params(agal_learn *m, float *out, long long n);
+int agal_learn_set_params(agal_learn *m, const float *in, long long n);
+int agal_learn_record(agal_learn *m, agal_ctx *ctx);
+int agal_learn_label(agal_learn *m, agal_ctx *ctx);
+/* {snapshots, labelled, regrids seen, judged regrids, plain refinement marks
+   at judged regrids, of those not predicted by the network} */
+int agal_learn_counts(const agal_learn *m, long long *out);
+/* Host copies of snapshot k: n blocks, X [n*4^d][8], labels [n][2], weights [n]. */
+int agal_learn_snapshot(agal_learn *m, int k, int *n_blocks, float *X, float *Y, float *Wt);
+/* The percentile rule's decisions [n][2] on snapshot k's own state. */
+int agal_learn_snapshot_decisions(agal_learn *m, int k, float *D);
+/* Weights of the positive class in the loss of the two outputs (refinement,
+   coarsening marks are rare): per block and output
+   wt (pw y softplus(-z) + (1 - y) softplus(z)); default 1, 1. */
+int agal_learn_set_class_weights(agal_learn *m, double refine, double coarsen);
+/* Mean binary cross entropy of snapshot k and its gradient w.r.t. the parameters. */
+int agal_learn_gradients(agal_learn *m, int k, float *grad, long long n, double *loss);
+/* Adam over labelled snapshots [first, last), `epochs` passes in seeded order. */
+int agal_learn_train(agal_learn *m, int first, int last, int epochs, double lr, unsigned long long seed, double *loss);
+/* Logits [n][2] of snapshot k's blocks. */
+int agal_learn_predict_snapshot(agal_learn *m, int k, float *out);
+/* Couple a predictor with a case's solution-based refinement: mode 1 collects
+   labelled snapshots (plain criterion), mode 2 predicts (the marks of a regrid
+   are the network's, made after the previous regrid, for probabilities above
+   `threshold`; every judge_every-th regrid the percentile rule also runs and
+   the refinements the network missed are counted and applied); mode 0
+   detaches.  The predictor must outlive the coupling. */
+int agal_learn_attach(agal_ctx *ctx, agal_learn *m, int mode, int judge_every, double threshold);
 
 typedef struct agal_batch agal_batch;
 int agal_batch_create(agal_ctx *const *cases, int n_cases, agal_batch **out);

@@ -116,6 +116,45 @@ def test_cuda_geometry_fp64_matches_oracle(name):
     c.close()
 
 
+@pytest.mark.parametrize("mli", [2, 3])
+def test_solution_refinement_with_geometry_fp64_matches_oracle(mli):
+    """Near-wall refinement around the sphere, then the percentile rule every
+    8 steps (grid average, interface interpolation, refine/coarsen pass with
+    wall blocks present): meshes, masks and wall slots bit-exact and
+    populations within 1e-11 of the FP64 oracle after four regrids."""
+    from oracle.orc import OracleCase
+    g = load("geom_d3q19_wall3_bouzidi")
+    p, _ = geom_params(g)
+    p.MAX_LEVELS_INTERIOR = mli
+    p.S_CRITERION = _lib.CRITERION_PERCENTILE
+    p.P_REFINE = 8
+    p.ref_pct_hi = 0.5
+    p.storage = _lib.STORE_FP64
+    p.n_maxcblocks = max(p.n_maxcblocks, 4096)
+    steps = 32
+    runs = []
+    for make in (lambda: ag.Case(p), lambda: OracleCase(p, p.n_maxcblocks, fp64=True)):
+        c = make()
+        c.set_geometry(faces_of(g))
+        c.set_ic(0)
+        c.refine_near_wall()
+        c.advance_n(steps)
+        runs.append(c)
+    c, o = runs
+    c.sync()
+    assert c.counts()["n_ids"] == o.counts()["n_ids"]
+    for k in INT_ARRAYS:
+        assert np.array_equal(c.dump(k), o.dump(k)), k
+    nmb, Q, MC = p.n_maxcblocks, int(g["Q"]), int(g["MC"])
+    ids = c.dump(_lib.ARR_ID_SET).reshape(-1, nmb)
+    cnt = c.counts()
+    blocks = np.sort(np.concatenate([ids[L, : cnt["n_ids"][L]] for L in range(cnt["max_levels"])])).astype(np.int64)
+    Fc = c.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks]
+    Fo = o.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks]
+    assert np.abs(Fc - Fo).max() < 1e-11
+    c.close()
+
+
 def test_wall_step_variants_and_graph_bit_identical():
     g = load("geom_d3q19_wall3_bouzidi")
     runs = []

@@ -422,6 +422,36 @@ class Learner:
         case._learner = self if mode else None
         self._attached = [c for c in getattr(self, "_attached", []) if c is not case] + ([case] if mode else [])
 
+    def set_thresholds(self, refine: float, coarsen: float) -> None:
+        """Probability thresholds of the two outputs in predict mode."""
+        self._c(self._lib.agal_learn_set_thresholds(self._h, refine, coarsen))
+
+    def calibrate_thresholds(self, first: int, last: int) -> tuple:
+        """Thresholds at which the network marks, over the labelled snapshots
+        [first, last), as many blocks as the labels do among the blocks a mark
+        can apply to (unrefined below the finest level for refinement, refined
+        for coarsening); returns them as probabilities (apply with
+        set_thresholds after attach).  Coarsening is never looser than
+        probability 1/2: a wrongly removed level costs accuracy, a wrongly
+        added one only time."""
+        zs, ys, cs = [], [], []
+        for k in range(first, last):
+            X, Y, W = self.snapshot(k)
+            Xb = X.reshape(len(W), self.cells, 8)[:, 0, :]
+            v = W > 0
+            zs.append(self.predict(k)[v])
+            ys.append(Y[v])
+            cs.append(np.stack([(Xb[v, 6] == 0) & (Xb[v, 5] < 1.0 - 1e-6), Xb[v, 6] == 1], axis=1))
+        z, y, cand = np.concatenate(zs), np.concatenate(ys), np.concatenate(cs)
+        out = []
+        for o in range(2):
+            zo = np.sort(z[cand[:, o], o])[::-1]
+            npos = int(y[cand[:, o], o].sum())
+            t = 0.0 if npos == 0 or npos >= len(zo) else float(zo[npos - 1: npos + 1].mean())
+            out.append(float(1.0 / (1.0 + np.exp(-t))))
+        out[1] = max(out[1], 0.5)
+        return tuple(min(max(x, 1e-6), 1 - 1e-6) for x in out)
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             for case in getattr(self, "_attached", []):   # the cases must not keep a dangling predictor

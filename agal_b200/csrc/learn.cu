@@ -4,8 +4,8 @@
 // counterpart: the reference has the plain vorticity / Q criterion only).
 //
 // Network, per block of P = 4^d cells, zero padding at the block faces:
-//   x0 [P x 8]  channels (rho - 1)/U^2, u/U, v/U, w/U, |curl u|/U, level/(ML-1),
-//               refined flag, 1            (U = the preset velocity u_ref)
+//   x0 [P x 8]  channels (rho - 1)/U^2, u/U, v/U, w/U, 2^L |curl u|/U (per
+//               coarse cell), level/(ML-1), refined flag, 1  (U = u_ref)
 //   h1 = relu(conv3^d(x0; 8 -> 32) + b1)
 //   h2 = relu(conv3^d(h1; 32 -> 32) + b2)
 //   z  = mean over cells of conv3^d(h2; 32 -> 2) + b3   (refine, coarsen logits)
@@ -122,7 +122,7 @@ __global__ void k_features(const FeatArgs a)
     o[1] = u;
     o[2] = v;
     o[3] = w;
-    o[4] = om;
+    o[4] = om * (float)(1 << L);   // per coarse cell, the units the percentile rule compares in
     o[5] = (float)L / (float)(a.ml > 1 ? a.ml - 1 : 1);
     o[6] = (a.ref[b] == REF_REFINED || a.ref[b] == REF_REFINED_WCHILD) ? 1.f : 0.f;
     o[7] = 1.f;
@@ -303,7 +303,8 @@ __global__ void k_gather_level(const int *ids, int n, const int *level, int *lvl
 // below MAX_LEVELS_INTERIOR-1, coarsening of refined blocks.
 // A block predicted at the previous regrid counts if it still sits on the
 // level it had then.  write = 0 only sets the refinement flags.
-__global__ void k_apply_marks(const int *ids, const int *lvl0, int n, const float *logits, float thr, int *ref,
+__global__ void k_apply_marks(const int *ids, const int *lvl0, int n, const float *logits, float thr_r, float thr_c,
+                              int *ref,
                               const int *nbr, long long nmb, int qmax, const int *level, int mli, int *flag,
                               int only_refine, int write)
 {
@@ -315,7 +316,7 @@ __global__ void k_apply_marks(const int *ids, const int *lvl0, int n, const floa
     bool eligible = true;
     for (int q = 0; q < qmax; q++)
         if (nbr[b + (long long)q * nmb] == N_SKIPID) eligible = false;
-    const bool up = same && logits[j * NO] > thr, down = same && logits[j * NO + 1] > thr;
+    const bool up = same && logits[j * NO] > thr_r, down = same && logits[j * NO + 1] > thr_c;
     if (flag) flag[j] = up ? 1 : 0;
     if (!write) return;
     if (r == REF_UNREFINED && eligible && level[b] < mli - 1 && up) ref[b] = REF_MARK_REFINE;
@@ -369,7 +370,7 @@ struct agal_learn {
     // solver coupling
     int judge_every = 4;
     long long regrids = 0, judged = 0, plain_refine = 0, missed = 0;
-    float thr = 0.f;                         // logit threshold (0 = probability 1/2)
+    float thr[NO] = {0.f, 0.f};              // logit thresholds of the two outputs (0 = probability 1/2)
     int pred_n = 0;                          // prediction made at the last regrid
     int *pred_ids = nullptr, *pred_lvl = nullptr;
     float *pred_X = nullptr, *pred_logits = nullptr;
@@ -890,8 +891,16 @@ extern "C" int agal_learn_attach(agal_ctx *c, agal_learn *m, int mode, int judge
     c->learner = m;
     c->learn_mode = mode;
     m->judge_every = judge_every;
-    m->thr = (float)std::log(threshold / (1.0 - threshold));
+    m->thr[0] = m->thr[1] = (float)std::log(threshold / (1.0 - threshold));
     m->pred_n = 0;
+    return AGAL_OK;
+}
+
+extern "C" int agal_learn_set_thresholds(agal_learn *m, double refine, double coarsen)
+{
+    if (!m || !(refine > 0.0 && refine < 1.0) || !(coarsen > 0.0 && coarsen < 1.0)) return AGAL_ERR_PARAM;
+    m->thr[0] = (float)std::log(refine / (1.0 - refine));
+    m->thr[1] = (float)std::log(coarsen / (1.0 - coarsen));
     return AGAL_OK;
 }
 
@@ -919,13 +928,13 @@ int agal_learn_marks(agal_ctx *c)
         // plain marks, whose coarsening marks stand)
         if (judge) AGAL_CUDA(c, cudaMemsetAsync(m->counts, 0, sizeof(int) * 4, c->stream));
         k_apply_marks<<<gridn(m->pred_n, 128), 128, 0, c->stream>>>(
-            m->pred_ids, m->pred_lvl, m->pred_n, m->pred_logits, m->thr, c->cblock_ID_ref, c->cblock_ID_nbr, c->nmb,
+            m->pred_ids, m->pred_lvl, m->pred_n, m->pred_logits, m->thr[0], m->thr[1], c->cblock_ID_ref, c->cblock_ID_nbr, c->nmb,
             c->Qmax, c->cblock_level, c->P.MAX_LEVELS_INTERIOR, m->flags, 0, 0);
         if (judge)
             k_judge<<<gridn(m->pred_n, 128), 128, 0, c->stream>>>(m->pred_ids, m->pred_n, m->flags, c->cblock_ID_ref,
                                                              m->counts);
         k_apply_marks<<<gridn(m->pred_n, 128), 128, 0, c->stream>>>(
-            m->pred_ids, m->pred_lvl, m->pred_n, m->pred_logits, m->thr, c->cblock_ID_ref, c->cblock_ID_nbr, c->nmb,
+            m->pred_ids, m->pred_lvl, m->pred_n, m->pred_logits, m->thr[0], m->thr[1], c->cblock_ID_ref, c->cblock_ID_nbr, c->nmb,
             c->Qmax, c->cblock_level, c->P.MAX_LEVELS_INTERIOR, nullptr, judge ? 1 : 0, 1);
         AGAL_CUDA(c, cudaGetLastError());
         if (judge) {

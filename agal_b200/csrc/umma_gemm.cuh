@@ -2,22 +2,26 @@
 //
 //   D[M x N] = A[M x K] . B[N x K]^T        (A, B row-major, K contiguous)
 //
-// One CTA of 128 threads per 128-row tile of D, N <= 32 (one 128 x 32 FP32
-// accumulator in tensor memory, 32 columns).  K is walked in chunks of KC:
-// the four warps copy the A and B chunks from global memory into shared
-// memory in the tensor core's no-swizzle K-major layout (8-row x 16-byte core
-// matrices; K-adjacent core matrices 128 B apart, 8-row groups KC x 2 B
-// apart), fence them into the async proxy, and one thread issues KC/16
-// tcgen05.mma (kind::f16, M = 128, N = 32, K = 16) and commits them to an
-// mbarrier.  After the last chunk each warp reads its 32 accumulator lanes
-// with tcgen05.ld and stores its rows of D.  Every mbarrier wait is bounded
-// (2 s of %globaltimer): on expiry the status word gets AGAL_ERR_TIMEOUT, the
-// tile is skipped, and the tensor memory is still freed.
+// One CTA of 128 threads per 128-row tile of D and K slice, N <= 32 (one
+// 128 x 32 FP32 accumulator in tensor memory, 32 columns).  K is walked in
+// chunks of KC through two shared-memory stages: the four warps copy chunk
+// k+1 of A and B with cp.async (16 bytes per copy, all in flight at once,
+// rows past M or N zero-filled) into the tensor core's no-swizzle K-major
+// layout (8-row x 16-byte core matrices; K-adjacent core matrices 128 B
+// apart, 8-row groups KC x 2 B apart) while the tensor core multiplies chunk
+// k; one thread issues KC/16 tcgen05.mma (kind::f16, M = 128, N = 32, K = 16)
+// per chunk and commits them to the stage's mbarrier, whose completion frees
+// the stage.  After the last chunk each warp reads its 32 accumulator lanes
+// with tcgen05.ld and stores (one K slice) or atomically adds (split K) its
+// rows of D.  Every mbarrier wait is bounded (2 s of %globaltimer): on expiry
+// the status word gets AGAL_ERR_TIMEOUT, the tile is skipped, and the tensor
+// memory is still freed.
 #pragma once
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "../../include/agal_b200.h"
@@ -29,7 +33,8 @@ constexpr int TM = 128;          // rows per CTA (tcgen05 M)
 constexpr int TN = 32;           // accumulator columns (tcgen05 N)
 constexpr int KC = 128;          // K elements per shared-memory chunk
 constexpr int THREADS = 128;
-constexpr size_t SMEM = (size_t)(TM + TN) * KC * 2;   // 40 KB
+constexpr size_t STAGE = (size_t)(TM + TN) * KC * 2;  // 40 KB
+constexpr size_t SMEM = 2 * STAGE;                     // two stages
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -93,17 +98,24 @@ __device__ __forceinline__ unsigned core_off(int r, int kg)
     return (unsigned)(((r >> 3) * (KC / 8) + kg) * 128 + (r & 7) * 16);
 }
 
+__device__ __forceinline__ void cp_async16(unsigned dst, const void *src, bool valid)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A,
                                                        const __nv_bfloat16 *__restrict__ B, float *__restrict__ D,
-                                                       int M, int N, int K, int ldd, int *status)
+                                                       int M, int N, int K, int ldd, int kslice, int *status)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *sA = smem;
-    unsigned char *sB = smem + (size_t)TM * KC * 2;
-    __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t s_taddr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * TM;
+    const int k_begin = blockIdx.y * kslice, k_end = min(K, k_begin + kslice);
+    const int nchunks = (k_end - k_begin + KC - 1) / KC;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
@@ -112,7 +124,8 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1) : "memory");
+        for (int s = 0; s < 2; s++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[s])), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -120,28 +133,45 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
     tc_fence_after();
     const uint32_t taddr = s_taddr;
 
-    bool ok = true;
-    int it = 0;
-    for (int kc = 0; kc < K; kc += KC, it++) {
-        const int kw = (K - kc < KC) ? (K - kc) : KC;   // multiple of 16
-        const int g8 = kw / 8;
+    // cp.async copies of chunk c into stage c & 1 (rows past M / N zero-filled)
+    auto load = [&](int c) {
+        unsigned char *sA = smem + (size_t)(c & 1) * STAGE;
+        unsigned char *sB = sA + (size_t)TM * KC * 2;
+        const int kc = k_begin + c * KC;
+        const int g8 = min(KC, k_end - kc) / 8;
         for (int i = tid; i < TM * g8; i += THREADS) {
             const int r = i / g8, kg = i % g8;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (m0 + r < M) v = *reinterpret_cast<const uint4 *>(A + (size_t)(m0 + r) * K + kc + kg * 8);
-            *reinterpret_cast<uint4 *>(sA + core_off(r, kg)) = v;
+            const bool ok = m0 + r < M;
+            cp_async16(smem_u32(sA + core_off(r, kg)), A + (size_t)(ok ? m0 + r : 0) * K + kc + kg * 8, ok);
         }
         for (int i = tid; i < TN * g8; i += THREADS) {
             const int r = i / g8, kg = i % g8;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (r < N) v = *reinterpret_cast<const uint4 *>(B + (size_t)r * K + kc + kg * 8);
-            *reinterpret_cast<uint4 *>(sB + core_off(r, kg)) = v;
+            const bool ok = r < N;
+            cp_async16(smem_u32(sB + core_off(r, kg)), B + (size_t)(ok ? r : 0) * K + kc + kg * 8, ok);
+        }
+        cp_async_commit();
+    };
+
+    bool ok = true;
+    if (nchunks > 0) load(0);
+    for (int it = 0; it < nchunks; it++) {
+        // the stage chunk it+1 goes to was read by the MMAs of chunk it-1
+        if (it >= 1) ok = mbar_wait_bounded(&mbar[(it - 1) & 1], (unsigned)(((it - 1) >> 1) & 1), status) && ok;
+        if (!__syncthreads_and(ok)) { ok = false; break; }
+        if (it + 1 < nchunks) {
+            load(it + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
+            const unsigned char *sA = smem + (size_t)(it & 1) * STAGE;
+            const unsigned char *sB = sA + (size_t)TM * KC * 2;
+            const int kw = min(KC, k_end - (k_begin + it * KC));   // multiple of 16
             for (int s = 0; s < kw / 16; s++) {
                 const uint64_t ad = smem_desc(sA + s * 256, 128, KC * 16);
                 const uint64_t bd = smem_desc(sB + s * 256, 128, KC * 16);
@@ -154,16 +184,17 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&mbar))
+                             smem_u32(&mbar[it & 1]))
                          : "memory");
         }
-        ok = mbar_wait_bounded(&mbar, (unsigned)(it & 1), status) && ok;
-        tc_fence_after();
-        __syncthreads();   // the chunk buffers are free again
-        if (!__syncthreads_and(ok)) { ok = false; break; }
     }
+    cp_async_wait<0>();   // nothing left in flight on an early exit
+    if (ok && nchunks > 0)
+        ok = mbar_wait_bounded(&mbar[(nchunks - 1) & 1], (unsigned)(((nchunks - 1) >> 1) & 1), status);
+    tc_fence_after();
+    ok = __syncthreads_and(ok);
 
-    if (ok) {
+    if (ok && nchunks > 0) {
         uint32_t v[32];
         const uint32_t src = taddr + ((uint32_t)(warp * 32) << 16);
         asm volatile(
@@ -177,10 +208,17 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
             : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int row = m0 + warp * 32 + lane;
-        if (row < M)
+        if (row < M) {
+            if (gridDim.y == 1) {
 #pragma unroll
-            for (int j = 0; j < TN; j++)
-                if (j < N) D[(size_t)row * ldd + j] = __uint_as_float(v[j]);
+                for (int j = 0; j < TN; j++)
+                    if (j < N) D[(size_t)row * ldd + j] = __uint_as_float(v[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < TN; j++)
+                    if (j < N) atomicAdd(&D[(size_t)row * ldd + j], __uint_as_float(v[j]));
+            }
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -188,13 +226,33 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(TN) : "memory");
 }
 
-// D = A . B^T for M rows (any), N <= 32, K a multiple of 16 (rows 16-byte aligned).
+// D = A . B^T for M rows (any), N <= 32, K a multiple of 16 (rows 16-byte
+// aligned).  A long K with few row tiles is split over CTAs (K slices of a
+// multiple of KC) whose partial tiles are added atomically into D, which is
+// zeroed first; that needs ldd == N (D contiguous).
 inline cudaError_t gemm_bf16(const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *D, int M, int N, int K, int ldd,
                              int *status, cudaStream_t s)
 {
     if (M <= 0) return cudaSuccess;
     if (N < 1 || N > TN || K <= 0 || K % 16) return cudaErrorInvalidValue;
-    k_gemm_bf16<<<(M + TM - 1) / TM, THREADS, SMEM, s>>>(A, B, D, M, N, K, ldd, status);
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+        const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr[dev] = true;
+    }
+    const int mt = (M + TM - 1) / TM;
+    int splits = 1;
+    if (ldd == N && mt < 148 && K > 4 * KC) splits = std::min((K + 4 * KC - 1) / (4 * KC), std::max(1, 296 / mt));
+    const int kslice = ((K + splits - 1) / splits + KC - 1) / KC * KC;
+    splits = (K + kslice - 1) / kslice;
+    if (splits > 1) {
+        const cudaError_t e = cudaMemsetAsync(D, 0, sizeof(float) * (size_t)M * ldd, s);
+        if (e != cudaSuccess) return e;
+    }
+    k_gemm_bf16<<<dim3((unsigned)mt, (unsigned)splits), THREADS, SMEM, s>>>(A, B, D, M, N, K, ldd, kslice, status);
     return cudaGetLastError();
 }
 

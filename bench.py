@@ -572,8 +572,58 @@ def main(argv=None) -> int:
         return dict(value=mlups, ms_per_step=t_ms / a.steps, flush=flush, tune=tune, clocks=clocks,
                     launches=launches, counts=counts, cells_per_step=float(np.mean(cells)))
 
+    def learned_timed(wl: str, wl_src: str):
+        """The workload with the learned predictor driving its refinement: the
+        network is trained on the GPU on snapshots of the plain FP32 run's
+        spin-up (labelled by the percentile rule), then predicts the marks of
+        every regrid of a fresh run, the rule judging every 4th regrid."""
+        ww, ws_ = WORKLOADS[wl], WORKLOADS[wl_src]
+        dim = DIM_OF[ww["velocity_set"]]
+        t0 = time.perf_counter()
+        src = ag.Case(make_params(ws_, device=local))
+        m = ag.Learner(dim, seed=7)
+        m.attach(src, 1)
+        develop(src, ws_)
+        src.sync()
+        nl = m.counts()["labelled"]
+        weights = m.balance_classes(0, nl)
+        loss = m.train(0, nl, 40, lr=2e-3, seed=7)
+        thr = m.calibrate_thresholds(0, nl)
+        m.attach(src, 0)
+        src.close()
+        train_s = time.perf_counter() - t0
+        case = ag.Case(make_params(ww, device=local))
+        m.attach(case, 2, judge_every=4)
+        m.set_thresholds(*thr)
+        develop(case, ww)
+        tune = case.autotune(0, reps=10)
+        step = step_fn(case, ww)
+        for _ in range(a.warmup):
+            step()
+        case.sync()
+        flush = state_bytes(case, ww) * 2 < L2_BYTES
+        c0 = m.counts()
+        barrier()
+        torch.cuda.synchronize()
+        per_step, cells, launches = time_steps(case, torch, ww, a.steps, flush)
+        c1 = m.counts()
+        counts = case.counts()
+        barrier()
+        t_ms = allmax(sum(per_step))
+        mlups = allsum(float(sum(cells))) / (t_ms * 1e-3) / 1e6
+        m.attach(case, 0)
+        case.close()
+        m.close()
+        return dict(workload=wl, value=mlups, ms_per_step=t_ms / a.steps, snapshots=nl, class_weights=weights,
+                    train_loss=loss, thresholds=thr, collect_and_train_s=train_s,
+                    regrids=c1["regrids"] - c0["regrids"], judged=c1["judged"] - c0["judged"],
+                    plain_refine_marks=c1["plain_refine"] - c0["plain_refine"],
+                    missed=c1["missed"] - c0["missed"], blocks_per_level=counts["n_ids"][:-1],
+                    cell_updates_per_step=float(np.mean(cells)), tune=tune)
+
     # --- device-timed steps: headline workload, then the plain FP32 form -------
     head = device_timed(a.workload, with_clocks=True)
+    learned = learned_timed(a.workload, a.plain_workload) if WORKLOADS[a.workload].get("amr") else None
     plain = device_timed(a.plain_workload, with_clocks=False) if a.plain_workload != a.workload else None
 
     # --- end to end through the C ABI with host buffers ----------------------
@@ -652,6 +702,12 @@ def main(argv=None) -> int:
                                   "ms_per_step": plain["ms_per_step"],
                                   "blocks_per_level": plain["counts"]["n_ids"][:-1],
                                   "ratio": head["value"] / plain["value"]}
+        if learned is not None:
+            mk = learned["plain_refine_marks"]
+            learned["missed_fraction"] = learned["missed"] / mk if mk > 0 else 0.0
+            if plain is not None:
+                learned["ratio_vs_plain_fp32"] = learned["value"] / plain["value"]
+            line["learned"] = learned
         if batched is not None:
             line["batched"] = batched
         print(json.dumps(line), flush=True)

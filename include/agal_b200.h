@@ -265,7 +265,7 @@ int agal_forces(agal_ctx *ctx, double *out);
 int agal_learn_gemm_bf16(const uint16_t *A, const uint16_t *B, float *D, int M, int N, int K);
 
 /* The predictor: per block of 4^d cells, 8 input channels ((rho-1)/U^2, u/U,
-   v/U, w/U, |curl u|/U, level/(ML-1), refined flag, 1), three 3^d
+   v/U, w/U, 2^L |curl u|/U, level/(ML-1), refined flag, 1), three 3^d
    convolutions 8 -> 32 -> 32 -> 2 (ReLU between, zero padding at the block
    faces), the last averaged over the block: logits of the percentile rule's
    two decisions at the next regrid (a leaf block's value above the upper
@@ -311,6 +311,9 @@ int agal_learn_predict_snapshot(agal_learn *m, int k, float *out);
    the refinements the network missed are counted and applied); mode 0
    detaches.  The predictor must outlive the coupling. */
 int agal_learn_attach(agal_ctx *ctx, agal_learn *m, int mode, int judge_every, double threshold);
+/* Separate probability thresholds of the refinement and coarsening outputs in
+   predict mode (after agal_learn_attach, which sets both to `threshold`). */
+int agal_learn_set_thresholds(agal_learn *m, double refine, double coarsen);
 
 typedef struct agal_batch agal_batch;
 int agal_batch_create(agal_ctx *const *cases, int n_cases, agal_batch **out);

@@ -120,6 +120,9 @@ struct agal_ctx {
 // n_maxcells / 4, at least AGAL_FIX_CAP_MIN (every wall link of a geometry is
 // one refused swap per step).
 #define AGAL_FIX_CAP_MIN 65536
+// Step launches over at most this many blocks apply their fix-ups in the
+// kernel's last CTA instead of a separate launch.
+#define AGAL_FUSED_FIXUP_BLOCKS 8192
 
 // Step kernel variants: 1 and 2 cells per thread (one-shot grid), 3 the
 // TMA-staged persistent pipeline.

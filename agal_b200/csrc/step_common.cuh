@@ -76,7 +76,43 @@ struct StepArgs {
     int *fix_count;
     long long *fix_list;   // [fix_cap][2] element offsets into fout
     int fix_cap;
+    // Non-null: the step kernel's last CTA applies the list itself (small
+    // grids, where the fence costs less than a separate launch).
+    int *fix_ticket;
+    int *status;
 };
+
+// The stream-guard fix-ups applied by the last CTA of the step kernel: every
+// thread fences its stores, the CTA takes a ticket, and the CTA holding the
+// last ticket swaps back the recorded pairs (the refused in-place swaps), then
+// resets the list and the ticket for the next launch.  Called by every thread
+// of every CTA.
+template <typename T>
+__device__ __forceinline__ void fused_fixup(const StepArgs &a)
+{
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(a.fix_ticket, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int n = atomicAdd(a.fix_count, 0);
+    const int m = n < a.fix_cap ? n : a.fix_cap;
+    T *fo = static_cast<T *>(a.fout);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const long long x = __ldcg(&a.fix_list[2 * i]), y = __ldcg(&a.fix_list[2 * i + 1]);
+        const T vx = __ldcg(&fo[x]), vy = __ldcg(&fo[y]);
+        fo[x] = vy;
+        fo[y] = vx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n > a.fix_cap) atomicCAS(a.status, 0, AGAL_ERR_STATE);
+        *a.fix_count = 0;
+        *a.fix_ticket = 0;
+    }
+}
 
 // Boundary hook presets (inc/custom.h:79-122); f is the full population.
 template <typename C>

@@ -66,36 +66,37 @@ k_step(const StepArgs a)
     }
     __syncthreads();
     const int fl = s_meta[lb][Meta<DIM>::FLAGS];
-    if (b < 0 || (fl & META_WALL)) return;
-
-    T *__restrict__ fo = static_cast<T *>(a.fout);
-    // The reference steps in place and leaves solid cells and inactive blocks
-    // (refined solid blocks) untouched, so whatever a grid average or an
-    // interpolation wrote there stays and feeds the next transfer: carry
-    // those cells into the output buffer unchanged.
-    auto carry = [&](int h) {
+    if (b >= 0 && !(fl & META_WALL)) {
+        T *__restrict__ fo = static_cast<T *>(a.fout);
+        // The reference steps in place and leaves solid cells and inactive
+        // blocks (refined solid blocks) untouched, so whatever a grid average
+        // or an interpolation wrote there stays and feeds the next transfer:
+        // carry those cells into the output buffer unchanged.
+        auto carry = [&](int h) {
 #pragma unroll
-        for (int sl = 0; sl < Q; sl++) fo[(long long)b * BLK + sl * MC + t0 + h * TPB] = fin[sl * MC + h * TPB];
-    };
-    if (!(fl & META_ACTIVE)) {
-        if (SOLID)
+            for (int sl = 0; sl < Q; sl++) fo[(long long)b * BLK + sl * MC + t0 + h * TPB] = fin[sl * MC + h * TPB];
+        };
+        if (!(fl & META_ACTIVE)) {
+            if (SOLID)
 #pragma unroll
-            for (int h = 0; h < CPT; h++) carry(h);
-        return;
-    }
-    const int *nrow = s_meta[lb];
-    const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
+                for (int h = 0; h < CPT; h++) carry(h);
+        } else {
+            const int *nrow = s_meta[lb];
+            const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
 #pragma unroll
-    for (int h = 0; h < CPT; h++) {
-        const int t = t0 + h * TPB;
-        if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) {
-            carry(h);
-            continue;
+            for (int h = 0; h < CPT; h++) {
+                const int t = t0 + h * TPB;
+                if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) {
+                    carry(h);
+                    continue;
+                }
+                C ux, uy, uz;
+                collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
+                push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
+            }
         }
-        C ux, uy, uz;
-        collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
-        push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
     }
+    if (a.fix_ticket) fused_fixup<T>(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -373,14 +374,22 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.fix_count = c->fix_count;
         a.fix_list = c->fix_list;
         a.fix_cap = c->fix_cap;
+        a.status = c->d_status;
         if (cpt <= 0) cpt = c->step_cpt;
+        // Small one-shot grids apply the fix-ups in their last CTA (saves a
+        // launch of a few µs per sub-step); large grids, the persistent
+        // variant and levels with a wall step use the separate kernel.
+        const bool wall = agal_wall_active(c) && (int)c->wall_n.size() > L && c->wall_n[L] > 0;
+        const bool fused = cpt != 3 && !wall && n <= AGAL_FUSED_FIXUP_BLOCKS;
+        a.fix_ticket = fused ? c->fix_count + 1 : nullptr;
         const int rc = (cpt == 3)   ? launch_step_tma<DIM, Q, T>(c, a)
                        : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                                     : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
         if (const int rw = agal_launch_wall_step(c, L, a.fin, a.fout)) return rw;
-        AGAL_CUDA(c, launch_pdl(k_stream_fixup<T>, dim3(1), dim3(1024), 0, c->stream, static_cast<T *>(a.fout),
-                                c->fix_count, c->fix_list, c->fix_cap, c->d_status));
+        if (!fused)
+            AGAL_CUDA(c, launch_pdl(k_stream_fixup<T>, dim3(1), dim3(1024), 0, c->stream, static_cast<T *>(a.fout),
+                                    c->fix_count, c->fix_list, c->fix_cap, c->d_status));
         AGAL_CUDA(c, cudaGetLastError());
         if (flip) c->cur[L] = 1 - c->cur[L];
         return AGAL_OK;

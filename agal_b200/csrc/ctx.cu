@@ -94,6 +94,9 @@ void release(agal_ctx *c)
                     c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -171,7 +174,11 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         return agal_set_err(nullptr, AGAL_ERR_CUDA, "cudaSetDevice failed");
     }
     if ((rc = cudaGetDevice(&c->device)) != cudaSuccess) { delete c; return agal_set_err(nullptr, AGAL_ERR_CUDA, "no CUDA device"); }
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        release(c);
         delete c;
         return agal_set_err(nullptr, AGAL_ERR_CUDA, "stream creation failed");
     }
@@ -546,6 +553,27 @@ static int step_f(agal_ctx *c, int L, bool forces)
     return AGAL_OK;
 }
 
+// The interface interpolation of level L beside the step of level L: the
+// interpolation reads F[cur[L]] and writes ghost cells of F[cur[L+1]], the
+// step reads F[cur[L]] and writes level L's other buffer, so they are
+// independent; the interpolation runs on the side stream, forked from and
+// joined back into the case's stream (two branches of the captured graph).
+static int interp_beside_step(agal_ctx *c, int L, bool forces)
+{
+    int rc;
+    AGAL_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    AGAL_CUDA(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    cudaStream_t main = c->stream;
+    c->stream = c->side;
+    rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE);
+    c->stream = main;
+    if (rc) return rc;
+    AGAL_CUDA(c, cudaEventRecord(c->ev_join, c->side));
+    if ((rc = step_f(c, L, forces))) return rc;
+    AGAL_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    return AGAL_OK;
+}
+
 static int advance_rec(agal_ctx *c, int L)
 {
     const int ML = c->max_levels;
@@ -554,21 +582,25 @@ static int advance_rec(agal_ctx *c, int L)
     if (!multi_level(c)) return step_f(c, L, mea);          // :239-251
     if (L == c->L0) {                                       // :39-58
         c->liter = 0;
-        if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
-        if ((rc = agal_launch_step(c, L))) return rc;
+        if ((rc = interp_beside_step(c, L, false))) return rc;
         if ((rc = advance_rec(c, L + 1))) return rc;
         return agal_launch_average(c, L, avg_mode(c));
     }
-    if (L < ML - 1 && (rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;   // :96-99
-    if ((rc = agal_launch_step(c, L))) return rc;
+    if (L < ML - 1) {                                                                       // :96-99
+        if ((rc = interp_beside_step(c, L, false))) return rc;
+    } else if ((rc = agal_launch_step(c, L))) {
+        return rc;
+    }
     if (L == ML - 1) c->liter++;
+    // :114-126: the forces on the last finest sub-step of the coarse step.
+    const bool f2 = mea && L == ML - 1 && c->liter == (1 << (ML - 1)) - 1;
     if (L < ML - 1) {                                                                       // :106-111
         if ((rc = advance_rec(c, L + 1))) return rc;
         if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
-        if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
+        if ((rc = interp_beside_step(c, L, f2))) return rc;
+    } else if ((rc = step_f(c, L, f2))) {
+        return rc;
     }
-    // :114-126: the forces on the last finest sub-step of the coarse step.
-    if ((rc = step_f(c, L, mea && L == ML - 1 && c->liter == (1 << (ML - 1)) - 1))) return rc;
     if (L == ML - 1) c->liter++;
     if (L < ML - 1) {                                                                       // :130-134
         if ((rc = advance_rec(c, L + 1))) return rc;

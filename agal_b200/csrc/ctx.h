@@ -62,6 +62,10 @@ struct agal_ctx {
     int red_len = 0;
     double *red_out = nullptr;
     cudaStream_t stream = nullptr;
+    // Side stream for the level interpolations that run beside the step of
+    // the same level (forked from and joined back into `stream`).
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int device = 0;
     // graph of n coarse steps (agal_advance_n)
     cudaGraphExec_t graph_exec = nullptr;

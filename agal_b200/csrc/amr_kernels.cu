@@ -100,8 +100,9 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     constexpr bool OFF = ST<T>::OFF;
     __shared__ C sF[MC];
     __shared__ C sW[4][8];
-    pdl_wait();
     // Uniform per CTA: every early return below depends on blockIdx only.
+    // The mesh arrays are read before the wait for the predecessor (no kernel
+    // that launches this one early writes them), the populations after it.
     const int b = a.ids[blockIdx.x];
     if (b < 0) return;
     const bool b1 = a.var == AGAL_INTERP_INTERFACE && a.bmask[b] == BLOCK_INTERFACE;
@@ -111,6 +112,8 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     if (bc < 0) return;
     const int tid = threadIdx.x;
     if (CUBIC && tid < 32) sW[tid / 8][tid % 8] = C(lag_w(tid / 8, tid % 8));
+    const bool ghost = a.cmask[(long long)(bc + tid / MC) * MC + tid % MC] == CELL_GHOST;
+    pdl_wait();
     const T *fp = static_cast<const T *>(a.fpar) + (long long)b * BLK;
     T *fc = static_cast<T *>(a.fch);
     C rho = 0, drho = 0, u = 0, v = 0, w = 0;
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     const int ci = ch & 1, cj = (ch >> 1) & 1, ck = (ch >> 2) & 1;
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     const long long cell = (long long)(bc + ch) * BLK + t;
-    const bool write = a.var == AGAL_INTERP_ADDED || a.cmask[(long long)(bc + ch) * MC + t] == CELL_GHOST;
+    const bool write = a.var == AGAL_INTERP_ADDED || ghost;
     for (int p = 0; p < Q; p++) {
         const int slot = lat_pb(DIM, p);
         if (tid < MC) {
@@ -197,7 +200,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     constexpr bool OFF = ST<T>::OFF;
     __shared__ C sg[NCH * MC];
     __shared__ int smask[NCH * MC];
-    pdl_wait();
+    // Mesh arrays before the wait for the predecessor, populations after it.
     const int b = a.ids[blockIdx.x];
     if (b < 0) return;
     const int bc = a.nbr_child[b];
@@ -206,9 +209,10 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     const T *fc = static_cast<const T *>(a.fch) + (long long)bc * BLK;   // children are consecutive IDs
     const int ch = tid / MC, t = tid % MC;
     const T *own = fc + (long long)ch * BLK + t;
+    int m = a.cmask[(long long)(bc + ch) * MC + t];
+    pdl_wait();
     C rho, drho, u, v, w;
     cell_macros<DIM, Q, T>(own, rho, drho, u, v, w);
-    int m = a.cmask[(long long)(bc + ch) * MC + t];
     if (a.var > 0 && m < 2) m = 1;
     smask[tid] = m;
     const C ratio = C(a.ratio);

@@ -38,7 +38,6 @@ template <int DIM, int Q, typename T, int CPT, bool SOLID>
 __global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
 k_step(const StepArgs a)
 {
-    pdl_wait();
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
     constexpr int TPB = MC / CPT;          // threads per cell-block
@@ -49,11 +48,14 @@ k_step(const StepArgs a)
     const int lb = tid / TPB, t0 = tid % TPB;
     const int kap = blockIdx.x * BPC + lb;
 
-    // Dependency depth 2: the block ID, then (populations | metadata row) in
-    // flight together before the one barrier.
+    // The block ID and its metadata row are written only by the mesh
+    // passes, never by a kernel that lets this one launch early, so they are
+    // read before the wait for the predecessor (the prologue of programmatic
+    // dependent launch); the populations after it.
     const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
     for (int i = t0; i < W; i += TPB) s_meta[lb][i] = (b >= 0) ? __ldg(&a.meta[(long long)b * W + i]) : 0;
     const T *__restrict__ fin = static_cast<const T *>(a.fin) + (long long)(b >= 0 ? b : 0) * BLK + t0;
+    pdl_wait();
 
     // Load: slot pb(p) holds f_p (offset form g_p for half storage).  Cell
     // h of this thread is t0 + h * TPB.

@@ -193,6 +193,20 @@ class Case:
         self._c(self._lib.agal_mass_momentum_noalloc(self._h, out))
         return np.array(out[: self.dim + 1])
 
+    # -- checkpoint / restart (the reference's restart.bin) -------------
+    def restart_save(self, path: str, iter: Optional[int] = None) -> None:
+        """Write restart.bin; iter = index of the last coarse step taken
+        (default: the library's own count - 1)."""
+        if iter is None:
+            iter = self.refine_stats()["iter"] - 1
+        self._c(self._lib.agal_restart_save(self._h, str(path).encode(), int(iter)))
+
+    def restart_load(self, path: str) -> int:
+        """Load a restart.bin; returns the coarse-step counter stored in it."""
+        it = C.c_int()
+        self._c(self._lib.agal_restart_load(self._h, str(path).encode(), C.byref(it)))
+        return it.value
+
     # -- geometry -------------------------------------------------------
     def set_geometry(self, faces) -> None:
         """Attach a triangle surface: faces (n, 3, 3) or (n, 9) float32 in
@@ -496,6 +510,16 @@ class Mesh(Case):
 
     def M_Advance_RefineWithSolution(self) -> None:
         self.refine_with_solution()
+
+    def M_Restart(self, var: int, iter: Optional[int] = None) -> int:
+        """mesh_restart.cu: var 0 saves <P_DIR_NAME>restart.bin, 1 loads it;
+        returns the stored loop index."""
+        path = self.params.P_DIR_NAME.decode() + "restart.bin"
+        if var == 0:
+            it = self.refine_stats()["iter"] - 1 if iter is None else iter
+            self.restart_save(path, it)
+            return it
+        return self.restart_load(path)
 
     def M_RefineAndCoarsenBlocks(self) -> None:
         self.refine_coarsen()

@@ -83,6 +83,8 @@ PROTOS = [
     ("agal_array_bytes", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]),
     ("agal_dump", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("agal_load", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    ("agal_restart_save", C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    ("agal_restart_load", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]),
     ("agal_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_mass_momentum_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_sync", C.c_int, [C.c_void_p]),

@@ -792,6 +792,66 @@ static int block_buffers(agal_ctx *c, std::vector<int> &which_buf)
     return AGAL_OK;
 }
 
+// Populations of blocks [0, nb) in the reference's slot-major layout
+// (out[s][b * MC + cell], absolute values), each block from its level's
+// current buffer; and the inverse, into both buffers.  Only the prefix of the
+// pool crosses PCIe (restart files hold blocks below id_max).
+int agal_read_blocks_F(agal_ctx *c, int nb, double *out)
+{
+    if (nb <= 0) return AGAL_OK;
+    AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)c->Q * c->MC * nb, ncell = (size_t)nb * c->MC;
+    std::vector<unsigned char> raw[2];
+    for (int k = 0; k < 2; k++) {
+        raw[k].resize(n * c->esize);
+        AGAL_CUDA(c, cudaMemcpy(raw[k].data(), c->F[k], n * c->esize, cudaMemcpyDeviceToHost));
+    }
+    std::vector<int> lev(nb), ref(nb);
+    AGAL_CUDA(c, cudaMemcpy(lev.data(), c->cblock_level, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+    AGAL_CUDA(c, cudaMemcpy(ref.data(), c->cblock_ID_ref, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < c->Q; s++) {
+        const int p = lat_pb(c->dim, s);
+        for (size_t cell = 0; cell < ncell; cell++) {
+            const size_t b = cell / c->MC;
+            const int L = (ref[b] != REF_INACTIVE && lev[b] >= 0 && lev[b] < c->max_levels) ? lev[b] : 0;
+            const auto &r = raw[c->cur[L]];
+            const size_t src = (b * c->Q + s) * c->MC + (cell % c->MC);
+            double *o = &out[(size_t)s * ncell + cell];
+            switch (c->storage) {
+            case AGAL_STORE_FP32: decode<float>(r, src, c->Q, p, o); break;
+            case AGAL_STORE_FP64: decode<double>(r, src, c->Q, p, o); break;
+            case AGAL_STORE_FP16: decode<__half>(r, src, c->Q, p, o); break;
+            case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, src, c->Q, p, o); break;
+            }
+        }
+    }
+    return AGAL_OK;
+}
+
+int agal_write_blocks_F(agal_ctx *c, int nb, const double *in)
+{
+    if (nb <= 0) return AGAL_OK;
+    AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    const size_t n = (size_t)c->Q * c->MC * nb, ncell = (size_t)nb * c->MC;
+    std::vector<unsigned char> raw(n * c->esize);
+    for (int s = 0; s < c->Q; s++) {
+        const int p = lat_pb(c->dim, s);
+        for (size_t cell = 0; cell < ncell; cell++) {
+            const size_t dst = ((cell / c->MC) * c->Q + s) * c->MC + (cell % c->MC);
+            const double v = in[(size_t)s * ncell + cell];
+            switch (c->storage) {
+            case AGAL_STORE_FP32: encode<float>(raw, dst, c->Q, p, v); break;
+            case AGAL_STORE_FP64: encode<double>(raw, dst, c->Q, p, v); break;
+            case AGAL_STORE_FP16: encode<__half>(raw, dst, c->Q, p, v); break;
+            case AGAL_STORE_BF16: encode<__nv_bfloat16>(raw, dst, c->Q, p, v); break;
+            }
+        }
+    }
+    for (int k = 0; k < 2; k++) AGAL_CUDA(c, cudaMemcpy(c->F[k], raw.data(), n * c->esize, cudaMemcpyHostToDevice));
+    agal_drop_graphs(c);
+    return AGAL_OK;
+}
+
 extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
 {
     size_t need = 0;

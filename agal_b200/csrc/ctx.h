@@ -168,6 +168,10 @@ void agal_drop_graphs(agal_ctx *c);         // after any change of the mesh or l
 // records), and the buffer-parity bookkeeping of replaying `steps` of them.
 int agal_record_coarse_step(agal_ctx *c);
 void agal_advance_parity(agal_ctx *c, int steps);
+// Populations of the first nb blocks in the reference's slot-major layout
+// (restart I/O without copying the whole pool).
+int agal_read_blocks_F(agal_ctx *c, int nb, double *out);
+int agal_write_blocks_F(agal_ctx *c, int nb, const double *in);
 // Geometry (geometry.cu, wall_kernels.cu).
 void agal_geometry_release(agal_ctx *c);
 int agal_build_wall_lists(agal_ctx *c);     // after the mesh or the wall slots change

@@ -326,6 +326,18 @@ const char *agal_batch_last_error(const agal_batch *batch);
 /* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
    bytes must equal the size reported by agal_array_bytes. */
 int agal_array_bytes(const agal_ctx *ctx, int which, size_t *bytes);
+/* Checkpoint / restart in the reference's restart.bin format
+   (Mesh::M_Restart SAVE / LOAD, mesh_restart.cu:45-225): the counts, ID sets,
+   gap stack, cell masks, block arrays and populations up to id_max, as floats
+   (doubles for FP64 storage).  Load adapts the gap stack to this context's
+   n_maxcblocks like the reference, restores the counts and the coarse-step
+   counter (`iter` is the M_AdvanceLoop index of the last step taken; the
+   loop resumes at iter + 1), and refuses a state beyond the
+   block pool (AGAL_ERR_OOM).  No velocity probes are kept: save writes none
+   and a zero running mean, load skips them.  Geometry arrays are not part of
+   the format. */
+int agal_restart_save(agal_ctx *ctx, const char *path, int iter);
+int agal_restart_load(agal_ctx *ctx, const char *path, int *iter);
 int agal_dump(agal_ctx *ctx, int which, void *host_buf, size_t bytes);
 int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
 

@@ -226,6 +226,14 @@ int main(int argc, char **argv)
     }
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) { fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); return 4; }
+    // REF_RESTART=1: the reference's own checkpoint of this state
+    // (M_RetrieveFromGPU, then M_Restart SAVE as at the end of M_AdvanceLoop,
+    // mesh_advance.cu:316-324) into <P_DIR_NAME>restart.bin.
+    if (getenv("REF_RESTART") && atoi(getenv("REF_RESTART")) == 1) {
+        mesh.M_RetrieveFromGPU();
+        int it = n_steps - 1;
+        mesh.M_Restart(0, V_MESH_RESTART_SAVE, &it);
+    }
 
     if (dump_file != "-") {
         const int dim = APh.N_DIM, Q = LPh.N_Q, Qmax = APh.N_Q_max, MC = APh.M_CBLOCK, ML = mesh.MAX_LEVELS;

@@ -22,6 +22,7 @@ the reference (KhodrJ/AGAL).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import re
@@ -243,7 +244,8 @@ def read_dump(path: Path) -> dict:
 
 
 def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
-            region: int = 0, skip_last_regrid: bool = False, sphere: tuple | None = None) -> str:
+            region: int = 0, skip_last_regrid: bool = False, sphere: tuple | None = None,
+            restart: Path | None = None) -> str:
     exe = REF_BIN / binary
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
@@ -265,11 +267,13 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
 
         env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0",
-                   REF_GEOM="1" if sphere is not None else "0")
+                   REF_GEOM="1" if sphere is not None else "0", REF_RESTART="1" if restart is not None else "0")
         r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
                            env=env)
         if r.returncode != 0:
             raise RuntimeError(f"{binary} failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
+        if restart is not None:
+            restart.write_bytes((td / "out" / "restart.bin").read_bytes())
         return r.stdout
 
 
@@ -305,6 +309,45 @@ def cmd_ref(out: Path, only: list[str] | None) -> None:
         print(name, "n_maxcblocks", d["n_maxcblocks"], "active", len(d["blocks"]), flush=True)
 
 
+# Restart fixture: the reference's own restart.bin of an AMR run (near-wall
+# and solution refinement), with a small memory allowance so that the block
+# pool, and with it the gap stack in the file, stays small; the harness dump
+# of the same state goes beside it.
+RESTART_CASES = {
+    "restart_d2q9_wall2_sol3": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3),
+                                200, 4096),
+}
+
+
+def cmd_restart(out: Path) -> None:
+    out.mkdir(parents=True, exist_ok=True)
+    for name, (binary, keys, steps, keep) in RESTART_CASES.items():
+        raw, rbin = out / f"{name}.bin", out / f"{name}.restart"
+        run_ref(binary, keys, steps, keep, raw, restart=rbin)
+        d = read_dump(raw)
+        d["case_keys"] = json.dumps(keys)
+        d["binary"] = binary
+        b = rbin.read_bytes()
+        # The gap stack (most of the file: the untouched part of the pool's
+        # descending ID list) is kept as first value + differences; the bytes
+        # before and after it verbatim; the file's SHA-256 checks the rebuild.
+        ml = int(d["max_levels"])
+        head = np.frombuffer(b, dtype=np.int32, count=2 * (ml + 1) + 5 + 2)
+        n_ids, n_gaps = head[1:ml + 2], int(head[ml + 2])
+        g0 = 4 * (2 * (ml + 1) + 5) + 8 + 4 * int(n_ids[:ml].sum())
+        gaps = np.frombuffer(b, dtype=np.int32, count=n_gaps, offset=g0)
+        d["restart_head"] = np.frombuffer(b[:g0], dtype=np.uint8)
+        d["restart_gap_first"] = np.int32(gaps[0] if n_gaps else 0)
+        d["restart_gap_diff"] = np.diff(gaps).astype(np.int32)
+        d["restart_n_gaps"] = n_gaps
+        d["restart_tail"] = np.frombuffer(b[g0 + 4 * n_gaps:], dtype=np.uint8)
+        d["restart_sha256"] = hashlib.sha256(b).hexdigest()
+        np.savez_compressed(out / f"{name}.npz", **d)
+        raw.unlink()
+        rbin.unlink()
+        print(name, "n_maxcblocks", d["n_maxcblocks"], "restart bytes", len(b), flush=True)
+
+
 def cmd_time(out: Path) -> None:
     out.mkdir(parents=True, exist_ok=True)
     res = {}
@@ -326,11 +369,15 @@ def main(argv=None) -> int:
     r.add_argument("--only", nargs="*")
     tm = sub.add_parser("time")
     tm.add_argument("--out", required=True)
+    rs = sub.add_parser("restart")
+    rs.add_argument("--out", default=str(HERE))
     a = ap.parse_args(argv)
     if a.cmd == "tables":
         cmd_tables(Path(a.ref))
     elif a.cmd == "ref":
         cmd_ref(Path(a.out).resolve(), a.only)
+    elif a.cmd == "restart":
+        cmd_restart(Path(a.out).resolve())
     else:
         cmd_time(Path(a.out).resolve())
     return 0

@@ -207,6 +207,27 @@ class Case:
         self._c(self._lib.agal_restart_load(self._h, str(path).encode(), C.byref(it)))
         return it.value
 
+    # -- headless uniform-grid output (out_direct.dat) -------------------
+    def uniform_dims(self) -> tuple:
+        d = (C.c_int * 3)()
+        self._c(self._lib.agal_uniform_dims(self._h, d))
+        return d[0], d[1], d[2]
+
+    def render_uniform(self) -> dict:
+        """rho, u, v, w, level, block ID on the output grid ([nz][ny][nx]) from
+        the current macros (refresh every level first)."""
+        nx, ny, nz = self.uniform_dims()
+        out = np.empty(6 * nx * ny * nz, np.float64)
+        self._c(self._lib.agal_uniform_render(self._h, out.ctypes.data_as(C.c_void_p), out.size))
+        f = out.reshape(6, nz, ny, nx)
+        return dict(zip(("rho", "u", "v", "w", "level", "block"), f))
+
+    def uniform_header(self, path: str) -> None:
+        self._c(self._lib.agal_uniform_header(self._h, str(path).encode()))
+
+    def uniform_frame(self, path: str, iter: int) -> None:
+        self._c(self._lib.agal_uniform_frame(self._h, str(path).encode(), int(iter)))
+
     # -- geometry -------------------------------------------------------
     def set_geometry(self, faces) -> None:
         """Attach a triangle surface: faces (n, 3, 3) or (n, 9) float32 in

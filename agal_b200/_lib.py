@@ -85,6 +85,10 @@ PROTOS = [
     ("agal_load", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("agal_restart_save", C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     ("agal_restart_load", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]),
+    ("agal_uniform_dims", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("agal_uniform_render", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("agal_uniform_header", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("agal_uniform_frame", C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     ("agal_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_mass_momentum_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_sync", C.c_int, [C.c_void_p]),

@@ -338,6 +338,22 @@ int agal_array_bytes(const agal_ctx *ctx, int which, size_t *bytes);
    the format. */
 int agal_restart_save(agal_ctx *ctx, const char *path, int iter);
 int agal_restart_load(agal_ctx *ctx, const char *path, int *iter);
+
+/* Headless uniform-grid output in the reference's out_direct.dat format
+   (header: mesh_init.cu:114-150; frames: Mesh::M_RenderAndPrint_Uniform,
+   mesh_print_uniform.cu:96-188).  The box is VOL_{I,J,K}_{MIN,MAX} (cells,
+   rounded down to root blocks) at the resolution of level N_PRINT_LEVELS-1;
+   each output cell takes the macros of the cell of the deepest block (up to
+   that level) covering it.  agal_uniform_header creates the file;
+   agal_uniform_frame prepares the state as M_Advance_PrintData does (grid
+   average, interface interpolation, refresh of every level) and appends
+   t = iter / Nx and the fields rho, u, v, w, level, block ID (doubles, x
+   fastest).  agal_uniform_render fills out[6][nz][ny][nx] from the current
+   macros without preparing; agal_uniform_dims gives {nx, ny, nz}. */
+int agal_uniform_dims(const agal_ctx *ctx, int *dims);
+int agal_uniform_render(agal_ctx *ctx, double *out, long long n);
+int agal_uniform_header(agal_ctx *ctx, const char *path);
+int agal_uniform_frame(agal_ctx *ctx, const char *path, int iter);
 int agal_dump(agal_ctx *ctx, int which, void *host_buf, size_t bytes);
 int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
 

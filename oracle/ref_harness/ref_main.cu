@@ -226,6 +226,21 @@ int main(int argc, char **argv)
     }
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) { fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err)); return 4; }
+    // REF_UNIFORM=1: one frame of the reference's uniform-grid output
+    // (M_Advance_PrintData, mesh_advance.cu:296-334: grid average, interface
+    // interpolation, refresh, M_RetrieveFromGPU, M_RenderAndPrint_Uniform)
+    // appended to <P_DIR_NAME>out_direct.dat, whose header M_Init wrote.
+    if (getenv("REF_UNIFORM") && atoi(getenv("REF_UNIFORM")) == 1) {
+        if (mesh.MAX_LEVELS > 1) {
+            for (int L = mesh.MAX_LEVELS - 2; L >= 0; L--) solver.S_Average(0, L, V_AVERAGE_GRID);
+            for (int L = 0; L < mesh.MAX_LEVELS - 1; L++) solver.S_Interpolate(0, L, V_INTERP_INTERFACE);
+        }
+        for (int L = 0; L < mesh.MAX_LEVELS; L++) solver.S_RefreshVariables(0, L);
+        cudaDeviceSynchronize();
+        mesh.M_RetrieveFromGPU();
+        mesh.M_RenderAndPrint_Uniform(0, n_steps);
+        mesh.output_file_direct->flush();
+    }
     // REF_RESTART=1: the reference's own checkpoint of this state
     // (M_RetrieveFromGPU, then M_Restart SAVE as at the end of M_AdvanceLoop,
     // mesh_advance.cu:316-324) into <P_DIR_NAME>restart.bin.

@@ -245,7 +245,7 @@ def read_dump(path: Path) -> dict:
 
 def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
             region: int = 0, skip_last_regrid: bool = False, sphere: tuple | None = None,
-            restart: Path | None = None) -> str:
+            restart: Path | None = None, uniform: Path | None = None) -> str:
     exe = REF_BIN / binary
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
@@ -267,13 +267,16 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
 
         env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0",
-                   REF_GEOM="1" if sphere is not None else "0", REF_RESTART="1" if restart is not None else "0")
+                   REF_GEOM="1" if sphere is not None else "0", REF_RESTART="1" if restart is not None else "0",
+                   REF_UNIFORM="1" if uniform is not None else "0")
         r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
                            env=env)
         if r.returncode != 0:
             raise RuntimeError(f"{binary} failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
         if restart is not None:
             restart.write_bytes((td / "out" / "restart.bin").read_bytes())
+        if uniform is not None:
+            uniform.write_bytes((td / "out" / "out_direct.dat").read_bytes())
         return r.stdout
 
 
@@ -314,16 +317,18 @@ def cmd_ref(out: Path, only: list[str] | None) -> None:
 # pool, and with it the gap stack in the file, stays small; the harness dump
 # of the same state goes beside it.
 RESTART_CASES = {
-    "restart_d2q9_wall2_sol3": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3),
-                                200, 4096),
+    "restart_d2q9_wall2_sol3": ("ref_d2q9_ldc", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3,
+                                                      N_PRINT_LEVELS=2, VOL_I_MIN=0, VOL_I_MAX=64, VOL_J_MIN=0,
+                                                      VOL_J_MAX=64, N_ITER_TOTAL=200, P_OUTPUT=100,
+                                                      N_OUTPUT_START=0), 200, 4096),
 }
 
 
 def cmd_restart(out: Path) -> None:
     out.mkdir(parents=True, exist_ok=True)
     for name, (binary, keys, steps, keep) in RESTART_CASES.items():
-        raw, rbin = out / f"{name}.bin", out / f"{name}.restart"
-        run_ref(binary, keys, steps, keep, raw, restart=rbin)
+        raw, rbin, ubin = out / f"{name}.bin", out / f"{name}.restart", out / f"{name}.uniform"
+        run_ref(binary, keys, steps, keep, raw, restart=rbin, uniform=ubin)
         d = read_dump(raw)
         d["case_keys"] = json.dumps(keys)
         d["binary"] = binary
@@ -342,9 +347,11 @@ def cmd_restart(out: Path) -> None:
         d["restart_n_gaps"] = n_gaps
         d["restart_tail"] = np.frombuffer(b[g0 + 4 * n_gaps:], dtype=np.uint8)
         d["restart_sha256"] = hashlib.sha256(b).hexdigest()
+        d["out_direct"] = np.frombuffer(ubin.read_bytes(), dtype=np.uint8)
         np.savez_compressed(out / f"{name}.npz", **d)
         raw.unlink()
         rbin.unlink()
+        ubin.unlink()
         print(name, "n_maxcblocks", d["n_maxcblocks"], "restart bytes", len(b), flush=True)
 
 

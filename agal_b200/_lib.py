@@ -103,6 +103,12 @@ PROTOS = [
     ("agal_refine_near_wall", C.c_int, [C.c_void_p]),
     ("agal_refine_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("agal_set_geometry", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("agal_geometry_read_stl", C.c_int, [C.c_char_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),
+    ("agal_geometry_read_text", C.c_int, [C.POINTER(AgalParams), C.c_char_p, C.c_void_p, C.c_longlong,
+                                          C.POINTER(C.c_longlong)]),
+    ("agal_geometry_refine_length", C.c_int, [C.POINTER(AgalParams), C.c_void_p, C.c_longlong,
+                                              C.POINTER(C.c_longlong)]),
+    ("agal_import_geometry", C.c_int, [C.c_void_p]),
     ("agal_bins_get", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_longlong), C.c_void_p, C.c_void_p, C.c_void_p]),
     ("agal_voxelize_s1", C.c_int, [C.c_void_p, C.c_int]),

@@ -113,3 +113,50 @@ def face_soa(faces: np.ndarray) -> np.ndarray:
     rows of the reference's geom_f_face_X (geometry_init.cu:139-149)."""
     f = np.asarray(faces, dtype=np.float32).reshape(-1, 9)
     return np.ascontiguousarray(f.T)
+
+
+# ---- the library's host-side import (the reference's import rules) --------
+def _call_faces(fn, *args):
+    import ctypes as C
+    from . import _lib
+    n = C.c_longlong()
+    rc = fn(*args, None, 0, C.byref(n))
+    if rc != _lib.OK:
+        raise _lib.AgalError(rc, fn.__name__)
+    out = np.zeros((n.value, 9), np.float32)
+    rc = fn(*args, out.ctypes.data_as(C.c_void_p), n.value, C.byref(n))
+    if rc != _lib.OK:
+        raise _lib.AgalError(rc, fn.__name__)
+    return out
+
+
+def import_stl(path) -> np.ndarray:
+    """ASCII STL read as the reference reads it (agal_geometry_read_stl): (n, 9) float32."""
+    from . import _lib
+    return _call_faces(_lib.lib().agal_geometry_read_stl, str(path).encode())
+
+
+def import_text(params, path) -> np.ndarray:
+    """The primitives of a geometry.txt (agal_geometry_read_text): (n, 9) float32."""
+    import ctypes as C
+    from . import _lib
+    return _call_faces(_lib.lib().agal_geometry_read_text, C.byref(params), str(path).encode())
+
+
+def refine_length(params, faces) -> np.ndarray:
+    """Faces split as G_RefineFaces_Length splits them (agal_geometry_refine_length)."""
+    import ctypes as C
+    from . import _lib
+    f = np.ascontiguousarray(faces, np.float32).reshape(-1, 9)
+    n = C.c_longlong(len(f))
+    L = _lib.lib()
+    buf = f.copy()
+    rc = L.agal_geometry_refine_length(C.byref(params), buf.ctypes.data_as(C.c_void_p), len(buf), C.byref(n))
+    if rc == _lib.ERR_PARAM and n.value > len(buf):
+        buf = np.zeros((n.value, 9), np.float32)
+        buf[: len(f)] = f
+        n = C.c_longlong(len(f))
+        rc = L.agal_geometry_refine_length(C.byref(params), buf.ctypes.data_as(C.c_void_p), len(buf), C.byref(n))
+    if rc != _lib.OK:
+        raise _lib.AgalError(rc, "agal_geometry_refine_length")
+    return buf[: n.value]

@@ -234,6 +234,25 @@ int agal_refine_stats(const agal_ctx *ctx, long long *iter, int *n_refined, int 
    does (its cell and bin indexing assume L_c = L_fy = L_fz = 1); a face whose
    bins fall outside it is refused (AGAL_ERR_PARAM). */
 int agal_set_geometry(agal_ctx *ctx, const float *faces, long long n_faces);
+/* Geometry import on the host, no device needed (faces n x 9 floats; with
+   faces NULL only *n is set; AGAL_ERR_PARAM if cap is too small, *n then
+   holding the size needed):
+   agal_geometry_read_stl   - ASCII STL as G_ImportSTL_ASCII (geometry_import.cu:11-83),
+                              degenerate facets dropped;
+   agal_geometry_read_text  - the primitives of a geometry.txt
+                              (G_ImportBoundariesFromTextFile + G_Convert_IndexListsToCoordList,
+                              geometry_add.cu:539-666): BOX, PRISM, SPHERE; the 2D shapes
+                              and NACA profiles give AGAL_ERR_UNSUPPORTED;
+   agal_geometry_refine_length - G_RefineFaces_Length (geometry_refine.cu): faces longer than
+                              0.95 G_BIN_SPEC min(L) / (2^(G_BIN_LEVELS-1) G_BIN_DENSITY)
+                              split at the edge midpoints, in place;
+   agal_import_geometry     - main.cu:94-101 for a context: G_LOADTYPE 0 reads
+                              I_DIR_NAME/geometry/G_FILENAME, 1 reads I_DIR_NAME/geometry.txt,
+                              then the length refinement and agal_set_geometry. */
+int agal_geometry_read_stl(const char *path, float *faces, long long cap, long long *n);
+int agal_geometry_read_text(const agal_params *p, const char *path, float *faces, long long cap, long long *n);
+int agal_geometry_refine_length(const agal_params *p, float *faces, long long cap, long long *n);
+int agal_import_geometry(agal_ctx *ctx);
 /* CSR bins of voxelizer bin level `level`, or of the link bins for level -1
    (binned_face_ids_n/N/ids).  Array pointers may be NULL (sizes first). */
 int agal_bins_get(agal_ctx *ctx, int level, int *density, int *n_bins, long long *n_entries, int *n, int *N,

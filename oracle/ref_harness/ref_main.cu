@@ -162,7 +162,13 @@ int main(int argc, char **argv)
     Geometry<REAL_h, REAL_h, &APh> *geometry = nullptr;
     if (geom) {
         geometry = new Geometry<REAL_h, REAL_h, &APh>(&parser);
-        geometry->G_ImportSTL_ASCII(geometry->G_FILENAME);
+        // main.cu:95-101: STL, or the primitives of geometry.txt
+        if (geometry->G_LOADTYPE == static_cast<int>(LoadType::STL)) {
+            geometry->G_ImportSTL_ASCII(geometry->G_FILENAME);
+        } else {
+            geometry->G_ImportBoundariesFromTextFile();
+            geometry->G_Convert_IndexListsToCoordList();
+        }
         geometry->G_Init_Arrays_CoordsList_CPU();
         geometry->G_InitBins(BinMake::GPU, 0);
     }

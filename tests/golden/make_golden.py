@@ -245,7 +245,7 @@ def read_dump(path: Path) -> dict:
 
 def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
             region: int = 0, skip_last_regrid: bool = False, sphere: tuple | None = None,
-            restart: Path | None = None, uniform: Path | None = None) -> str:
+            restart: Path | None = None, uniform: Path | None = None, geometry_txt: str | None = None) -> str:
     exe = REF_BIN / binary
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
@@ -258,6 +258,8 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             from agal_b200.geometry import icosphere, write_stl_ascii
             (td / "geometry").mkdir()
             write_stl_ascii(td / "geometry" / keys["G_FILENAME"], icosphere(*sphere))
+        if geometry_txt is not None:
+            (td / "geometry.txt").write_text(geometry_txt)
         cmd = [str(exe), str(td) + "/", str(dump) if dump else "-", str(steps), str(keep_mb), str(n_timed)]
 
         def big_stack():
@@ -267,7 +269,7 @@ def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None
             resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
 
         env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0",
-                   REF_GEOM="1" if sphere is not None else "0", REF_RESTART="1" if restart is not None else "0",
+                   REF_GEOM="1" if (sphere is not None or geometry_txt is not None) else "0", REF_RESTART="1" if restart is not None else "0",
                    REF_UNIFORM="1" if uniform is not None else "0")
         r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
                            env=env)
@@ -355,6 +357,37 @@ def cmd_restart(out: Path) -> None:
         print(name, "n_maxcblocks", d["n_maxcblocks"], "restart bytes", len(b), flush=True)
 
 
+# Face import fixtures: the reference's face list after its import and the
+# splitting of long faces (G_Init_Arrays_CoordsList_CPU) for a coarse STL
+# icosphere whose faces get split, and for the primitives of a geometry.txt.
+FACE_CASES = {
+    "faces_stl_split": (dict(GEO, Nx=16, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, G_BIN_LEVELS=1, G_BIN_DENSITY=16),
+                        (1, 0.3, (0.5, 0.5, 0.5), 5), None),
+    "faces_text_primitives": (dict(GEO, Nx=16, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, G_BIN_LEVELS=1,
+                                   G_BIN_DENSITY=8, G_LOADTYPE=1),
+                              None, "PRISM CORNER 0.2 0.35 0.3 0.45 0.25 0.4\n"
+                                    "PRISM CENTER 0.7 0.6 0.5 0.1 0.15 0.2\n"
+                                    "SPHERE 9 13 0.5 0.3 0.6 0.12\nEND\n"),
+}
+
+
+def cmd_faces(out: Path) -> None:
+    out.mkdir(parents=True, exist_ok=True)
+    for name, (keys, sphere, txt) in FACE_CASES.items():
+        raw = out / f"{name}.bin"
+        run_ref("ref_d3q19_fps", keys, 1, 4096, raw, sphere=sphere, geometry_txt=txt)
+        d = read_dump(raw)
+        keep = {k: d[k] for k in ("faces_soa",) if k in d}
+        keep["case_keys"] = json.dumps(keys)
+        if sphere is not None:
+            keep["sphere"] = json.dumps(sphere)
+        if txt is not None:
+            keep["geometry_txt"] = txt
+        np.savez_compressed(out / f"{name}.npz", **keep)
+        raw.unlink()
+        print(name, "faces", keep["faces_soa"].shape, flush=True)
+
+
 def cmd_time(out: Path) -> None:
     out.mkdir(parents=True, exist_ok=True)
     res = {}
@@ -378,6 +411,8 @@ def main(argv=None) -> int:
     tm.add_argument("--out", required=True)
     rs = sub.add_parser("restart")
     rs.add_argument("--out", default=str(HERE))
+    fc = sub.add_parser("faces")
+    fc.add_argument("--out", default=str(HERE))
     a = ap.parse_args(argv)
     if a.cmd == "tables":
         cmd_tables(Path(a.ref))
@@ -385,6 +420,8 @@ def main(argv=None) -> int:
         cmd_ref(Path(a.out).resolve(), a.only)
     elif a.cmd == "restart":
         cmd_restart(Path(a.out).resolve())
+    elif a.cmd == "faces":
+        cmd_faces(Path(a.out).resolve())
     else:
         cmd_time(Path(a.out).resolve())
     return 0

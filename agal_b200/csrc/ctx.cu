@@ -233,6 +233,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->d_status, sizeof(int) * 4);
     ALLOC(c->meta, sizeof(int) * (size_t)(c->dim == 2 ? 12 : 28) * nmb);
     ALLOC(c->fix_count, sizeof(int) * 4);
+    if (p->S_FORCE_TYPE == 1) ALLOC(c->Ff, (p->storage == AGAL_STORE_FP64 ? 8 : 4) * 6 * (size_t)nmb);   // CV partials
     c->fix_cap = (int)std::min<long long>(std::max<long long>(nmc / 4, AGAL_FIX_CAP_MIN), 1LL << 26);
     ALLOC(c->fix_list, sizeof(long long) * 2 * (size_t)c->fix_cap);
     if (c->max_levels > 1) {
@@ -272,6 +273,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     cudaMemsetAsync(c->F[0], 0, c->esize * (size_t)c->Q * nmc, c->stream);
     cudaMemsetAsync(c->F[1], 0, c->esize * (size_t)c->Q * nmc, c->stream);
     cudaMemsetAsync(c->macro, 0, compute_size(c) * (size_t)(c->dim + 1) * nmc, c->stream);
+    if (c->Ff) cudaMemsetAsync(c->Ff, 0, compute_size(c) * 6 * (size_t)nmb, c->stream);
 
     // Root grid (mesh_init.cu:354-516), built on the host and copied in.
     std::vector<int> nbr((size_t)c->Qmax * n_coarse), onb(n_coarse), ref(n_coarse, REF_UNREFINED);
@@ -579,12 +581,31 @@ static int advance_rec(agal_ctx *c, int L)
     const int ML = c->max_levels;
     const bool mea = c->P.S_FORCE_TYPE == 0 && c->X_b;
     int rc;
-    if (!multi_level(c)) return step_f(c, L, mea);          // :239-251
-    if (L == c->L0) {                                       // :39-58
+    const bool cv = c->P.S_FORCE_TYPE == 1;
+    if (!multi_level(c)) {                                  // :136-151
+        if (cv && (rc = agal_launch_forces_cv(c, L, 0))) return rc;
+        if ((rc = step_f(c, L, mea))) return rc;
+        return cv ? agal_launch_forces_cv(c, L, 1) : AGAL_OK;
+    }
+    if (L == c->L0) {                                       // :39-70
         c->liter = 0;
+        if (cv)
+            for (int K = c->L0; K < ML; K++)
+                if ((rc = agal_launch_forces_cv(c, K, 0))) return rc;
         if ((rc = interp_beside_step(c, L, false))) return rc;
         if ((rc = advance_rec(c, L + 1))) return rc;
-        return agal_launch_average(c, L, avg_mode(c));
+        if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
+        if (cv) {
+            // the control volume sees every level consistent: grid average,
+            // interface interpolation, then the post-step pass
+            for (int K = ML - 2; K >= c->L0; K--)
+                if ((rc = agal_launch_average(c, K, AGAL_AVERAGE_GRID))) return rc;
+            for (int K = c->L0; K < ML - 1; K++)
+                if ((rc = agal_launch_interp(c, K, AGAL_INTERP_INTERFACE))) return rc;
+            for (int K = c->L0; K < ML; K++)
+                if ((rc = agal_launch_forces_cv(c, K, 1))) return rc;
+        }
+        return AGAL_OK;
     }
     if (L < ML - 1) {                                                                       // :96-99
         if ((rc = interp_beside_step(c, L, false))) return rc;

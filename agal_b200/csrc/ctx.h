@@ -178,6 +178,7 @@ int agal_build_wall_lists(agal_ctx *c);     // after the mesh or the wall slots 
 int agal_wall_active(const agal_ctx *c);    // interpolated bounce-back in force
 int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout);
 int agal_launch_forces(agal_ctx *c, int L, int post);
+int agal_launch_forces_cv(agal_ctx *c, int L, int post);   // S_FORCE_TYPE 1
 // Learned predictor hooks of the solution-based refinement (learn.cu).
 int agal_learn_marks(agal_ctx *c);          // instead of the criterion when a learner is attached
 int agal_learn_after_regrid(agal_ctx *c);   // after the refine/coarsen pass

@@ -339,6 +339,160 @@ template <int DIM, int Q, typename T> struct RunForces {
     }
 };
 
+// Control-volume forces (S_FORCE_TYPE 1; Cu_ComputeForcesCV,
+// solver_lbm_kernels_forces.cu:13-245): per block of level L, over the cells
+// whose centre lies strictly inside the box S_FORCEVOLUME_* and that are not
+// solid, the momentum of the leaf blocks before the step (row 2d) and after it
+// (row 2d+1), and, on the root level only, the momentum leaving through the
+// box's surface: before the step the BGK post-collision value at the root
+// level's relaxation rate of each direction that points out of the box, after
+// it the population arriving from outside.  Block sums by a tree reduction,
+// times dx_L^d; the pre-step pass writes the rows, the post-step pass adds.
+struct CvArgs {
+    const int *ids;
+    int n;
+    const void *f;            // level L's current buffer
+    const int *cmask, *nbr_child;
+    const float *fX;          // block lower corners [d][nmb]
+    long long nmb;
+    double dx, dv, omega0;    // dx_L, dx_L^d, dx_0 / tau_0 in the compute type
+    int root, post;
+    double box[6];            // xm, xM, ym, yM, zm, zM
+    void *Ff;                 // [6][nmb] compute type
+};
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::MC) k_forces_cv(const CvArgs a)
+{
+    pdl_wait();
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
+    __shared__ C sP[3][MC], sM[3][MC];
+    const int b = a.ids[blockIdx.x];
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int d = 0; d < 3; d++) sP[d][t] = sM[d][t] = C(0);
+    const int mask = a.cmask[(long long)b * MC + t];
+    const bool leaf = a.nbr_child[b] < 0;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    const C dx = C(a.dx);
+    const C x = C(a.fX[b]) + dx * (C(0.5) + C(I));
+    const C y = C(a.fX[a.nmb + b]) + dx * (C(0.5) + C(J));
+    const C z = DIM == 3 ? C(a.fX[2 * a.nmb + b]) + dx * (C(0.5) + C(K)) : C(0);
+    auto inside = [&](C px, C py, C pz) {
+        const bool in2 = px > C(a.box[0]) && px < C(a.box[1]) && py > C(a.box[2]) && py < C(a.box[3]);
+        return DIM == 2 ? in2 : (in2 && pz > C(a.box[4]) && pz < C(a.box[5]));
+    };
+    const bool pv = inside(x, y, z) && mask != CELL_SOLID;
+    const T *fin = static_cast<const T *>(a.f) + (long long)b * BLK + t;
+    C f[Q];
+    C rho = 0, ru = 0, rv = 0, rw = 0;
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const C v = ST<T>::dec(fin[lat_pb(DIM, p) * MC]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        rho += v;
+        ru += v * C(lat_c(DIM, 0, p));
+        rv += v * C(lat_c(DIM, 1, p));
+        if (DIM == 3) rw += v * C(lat_c(DIM, 2, p));
+        f[p] = v;
+    }
+    if (pv && leaf) {
+        C(*s)[MC] = a.post ? sM : sP;
+        s[0][t] += ru;
+        s[1][t] += rv;
+        if (DIM == 3) s[2][t] += rw;
+    }
+    if (a.root) {
+        const C om = C(a.omega0), omp = C(1) - om;
+        if (!a.post) {
+            ru = ru / rho;
+            rv = rv / rho;
+            rw = rw / rho;
+        }
+#pragma unroll
+        for (int p = 1; p < Q; p++) {
+            C v = f[p];
+            // direction of the population leaving (pre-step) or arriving (post-step)
+            const int q = a.post ? lat_pb(DIM, p) : p;
+            if (!a.post) {
+                const C uu = ru * ru + rv * rv + rw * rw;
+                const C cu = C(lat_c(DIM, 0, p)) * ru + C(lat_c(DIM, 1, p)) * rv + C(lat_c(DIM, 2, p)) * rw;
+                v = v * omp + (C(lat_w(Q, p)) * rho * (C(1) + C(3) * cu + C(4.5) * cu * cu - C(1.5) * uu)) * om;
+            }
+            const bool ps = !inside(x + C(lat_c(DIM, 0, q)) * dx, y + C(lat_c(DIM, 1, q)) * dx,
+                                    z + C(lat_c(DIM, 2, q)) * dx);
+            if (ps && pv) {
+                sM[0][t] += v * C(lat_c(DIM, 0, q));
+                sM[1][t] += v * C(lat_c(DIM, 1, q));
+                if (DIM == 3) sM[2][t] += v * C(lat_c(DIM, 2, q));
+            }
+        }
+    }
+    __syncthreads();
+    for (int st = MC / 2; st > 0; st >>= 1) {
+        if (t < st)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                sP[d][t] = sP[d][t] + sP[d][t + st];
+                sM[d][t] = sM[d][t] + sM[d][t + st];
+            }
+        __syncthreads();
+    }
+    if (t == 0) {
+        C *F = static_cast<C *>(a.Ff);
+        const C dv = C(a.dv);
+        for (int d = 0; d < DIM; d++) {
+            C *fp = F + b + (long long)(2 * d) * a.nmb, *fm = F + b + (long long)(2 * d + 1) * a.nmb;
+            if (!a.post) {
+                *fp = sP[d][0] * dv;
+                *fm = sM[d][0] * dv;
+            } else {
+                *fp += sP[d][0] * dv;
+                *fm += sM[d][0] * dv;
+            }
+        }
+    }
+}
+
+template <int DIM, int Q, typename T> struct RunForcesCv {
+    static int run(agal_ctx *c, int L, int post)
+    {
+        const int n = c->n_ids[L];
+        if (n <= 0 || !c->Ff) return AGAL_OK;
+        using Cc = typename ST<T>::C;
+        const bool f32 = sizeof(Cc) == 4;
+        CvArgs a{};
+        a.ids = c->id_set + (long long)L * c->nmb;
+        a.n = n;
+        a.f = c->F[c->cur[L]];
+        a.cmask = c->cells_ID_mask;
+        a.nbr_child = c->cblock_ID_nbr_child;
+        a.fX = c->cblock_f_X;
+        a.nmb = c->nmb;
+        a.dx = c->dxf[L];
+        double dv = 1.0;
+        for (int d = 0; d < DIM; d++) dv = f32 ? (double)((float)dv * (float)c->dxf[L]) : dv * c->dxf[L];
+        a.dv = dv;
+        a.omega0 = f32 ? (double)((float)c->dxf[c->L0] / (float)c->tau[c->L0]) : c->dxf[c->L0] / c->tau[c->L0];
+        a.root = L == c->L0;
+        a.post = post;
+        // The box snapped to root-block boundaries, 4 int(b Nxi / 4) dx_0
+        // (solver_lbm_init.cu:36-41), stored in the compute type.
+        const agal_params &P = c->P;
+        const double box[6] = {P.S_FORCEVOLUME_Xm, P.S_FORCEVOLUME_XM, P.S_FORCEVOLUME_Ym,
+                               P.S_FORCEVOLUME_YM, P.S_FORCEVOLUME_Zm, P.S_FORCEVOLUME_ZM};
+        const int nxi[3] = {c->Nx, c->Ny, c->Nz};
+        for (int k = 0; k < 6; k++) {
+            const double v = 4.0 * (double)(int)(box[k] * (double)(nxi[k / 2] / 4)) * c->dxf[0];
+            a.box[k] = f32 ? (double)(float)v : v;
+        }
+        a.Ff = c->Ff;
+        AGAL_CUDA(c, launch_pdl(k_forces_cv<DIM, Q, T>, dim3(n), dim3(Geo<DIM>::MC), 0, c->stream, a));
+        AGAL_CUDA(c, cudaGetLastError());
+        return AGAL_OK;
+    }
+};
+
 // S_ReportForces sums (solver_lbm_compute.cu:166-201): every row of the
 // partials over block IDs below id_max[MAX_LEVELS], in FP64, in one CTA.
 template <typename C>
@@ -366,6 +520,12 @@ int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout)
 {
     if (!agal_wall_active(c)) return AGAL_OK;
     return agal::dispatch<agal::RunWallStep>(c, L, fin, fout);
+}
+
+int agal_launch_forces_cv(agal_ctx *c, int L, int post)
+{
+    if (c->P.S_FORCE_TYPE != 1) return AGAL_OK;
+    return agal::dispatch<agal::RunForcesCv>(c, L, post);
 }
 
 int agal_launch_forces(agal_ctx *c, int L, int post)

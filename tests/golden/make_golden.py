@@ -105,6 +105,11 @@ GEOM_CASES = {
     "geom_d3q27_wall2_bb": ("ref_d3q27_fps", dict(GEO, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=2,
                                                   G_BIN_LEVELS=2, S_BC_TYPE=0, S_FORCE_ORDER=1), 16, 4096,
                             (3, 0.1, (0.46, 0.49, 0.51), 11)),
+    "geom_d3q19_cv": ("ref_d3q19_fps", dict(GEO, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=3, MAX_LEVELS_INTERIOR=3,
+                                            S_BC_TYPE=1, S_FORCE_TYPE=1, S_FORCEVOLUME_Xm=0.28,
+                                            S_FORCEVOLUME_XM=0.66, S_FORCEVOLUME_Ym=0.31, S_FORCEVOLUME_YM=0.69,
+                                            S_FORCEVOLUME_Zm=0.3, S_FORCEVOLUME_ZM=0.7), 16, 4096,
+                      (3, 0.07, (0.45, 0.5, 0.5), 7)),
     "geom_d3q19_uniform": ("ref_d3q19_fps", dict(GEO, Nx=32, v0=1.25e-4, G_BIN_DENSITY=16, G_BIN_LEVELS=1,
                                                  MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, S_BC_TYPE=1,
                                                  S_FORCE_ORDER=2), 20, 4096, (3, 0.15, (0.47, 0.52, 0.49), 3)),
@@ -293,7 +298,7 @@ def cmd_ref(out: Path, only: list[str] | None) -> None:
         cases[k] = (binary, keys, steps, keep, 0, False, sphere)
     # Multi-level geometry fixtures keep the populations of the wall blocks
     # only (blocks with a solid-boundary slot); the uniform one keeps all.
-    wall_only_F = {"geom_d3q19_wall3_bouzidi", "geom_d3q27_wall2_bb"}
+    wall_only_F = {"geom_d3q19_wall3_bouzidi", "geom_d3q27_wall2_bb", "geom_d3q19_cv"}
     for name, (binary, keys, steps, keep, region, skip, sphere) in cases.items():
         if only and not any(name == o or name.startswith(o + "_") for o in only):
             continue

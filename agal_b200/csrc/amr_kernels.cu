@@ -96,9 +96,14 @@ template <int DIM, int Q, typename T, bool CUBIC>
 __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const InterpArgs a)
 {
     using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, NT = Geo<DIM>::NCH * Geo<DIM>::MC;
     constexpr bool OFF = ST<T>::OFF;
-    __shared__ C sF[MC];
+    // The parent's populations as stored, its cells' macros, and the rescaled
+    // values of every direction: staged once, so that the per-direction
+    // interpolation below needs no barrier.
+    __shared__ T sRaw[BLK];
+    __shared__ C sMac[5][MC];
+    __shared__ C sF[Q][MC];
     __shared__ C sW[4][8];
     // Uniform per CTA: every early return below depends on blockIdx only.
     // The mesh arrays are read before the wait for the predecessor (no kernel
@@ -115,70 +120,77 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     const bool ghost = a.cmask[(long long)(bc + tid / MC) * MC + tid % MC] == CELL_GHOST;
     pdl_wait();
     const T *fp = static_cast<const T *>(a.fpar) + (long long)b * BLK;
-    T *fc = static_cast<T *>(a.fch);
-    C rho = 0, drho = 0, u = 0, v = 0, w = 0;
-    if (tid < MC) cell_macros<DIM, Q, T>(fp + tid, rho, drho, u, v, w);
+    for (int i = tid; i < BLK; i += NT) sRaw[i] = fp[i];
+    __syncthreads();
+    if (tid < MC) {
+        C rho, drho, u, v, w;
+        cell_macros<DIM, Q, T>(sRaw + tid, rho, drho, u, v, w);
+        sMac[0][tid] = rho;
+        sMac[1][tid] = drho;
+        sMac[2][tid] = u;
+        sMac[3][tid] = v;
+        sMac[4][tid] = w;
+    }
+    __syncthreads();
     const C ratio = C(a.ratio);
+    for (int i = tid; i < BLK; i += NT) {
+        const int p = i / MC, cl = i % MC;
+        const C g = ST<T>::dec(sRaw[lat_pb(DIM, p) * MC + cl]);
+        const C e = feq_stored<DIM, Q, C, OFF>(p, sMac[0][cl], sMac[1][cl], sMac[2][cl], sMac[3][cl], sMac[4][cl]);
+        sF[p][cl] = e + (g - e) * ratio;
+    }
+    __syncthreads();
+    if (!(a.var == AGAL_INTERP_ADDED || ghost)) return;
     // Child cell of this thread.
+    T *fc = static_cast<T *>(a.fch);
     const int ch = tid / MC, t = tid % MC;
     const int ci = ch & 1, cj = (ch >> 1) & 1, ck = (ch >> 2) & 1;
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     const long long cell = (long long)(bc + ch) * BLK + t;
-    const bool write = a.var == AGAL_INTERP_ADDED || ghost;
+#pragma unroll 1
     for (int p = 0; p < Q; p++) {
-        const int slot = lat_pb(DIM, p);
-        if (tid < MC) {
-            const C g = ST<T>::dec(fp[slot * MC + tid]);
-            const C e = feq_stored<DIM, Q, C, OFF>(p, rho, drho, u, v, w);
-            sF[tid] = e + (g - e) * ratio;
-        }
-        __syncthreads();
-        if (write) {
-            C val;
-            if (!CUBIC) {
-                const int s = 2 * ci + 8 * cj + 32 * ck;
-                const C x = C(-0.25) + C(0.5) * C(I), y = C(-0.25) + C(0.5) * C(J);
-                if (DIM == 2) {
-                    val = sF[s] + (sF[1 + s] - sF[s]) * x + (sF[4 + s] - sF[s]) * y +
-                          (sF[5 + s] - sF[4 + s] - sF[1 + s] + sF[s]) * x * y;
-                } else {
-                    const C z = C(-0.25) + C(0.5) * C(K);
-                    val = sF[s] + (sF[1 + s] - sF[s]) * x + (sF[4 + s] - sF[s]) * y + (sF[16 + s] - sF[s]) * z +
-                          (sF[5 + s] - sF[1 + s] - sF[4 + s] + sF[s]) * x * y +
-                          (sF[17 + s] - sF[1 + s] - sF[16 + s] + sF[s]) * x * z +
-                          (sF[20 + s] - sF[4 + s] - sF[16 + s] + sF[s]) * y * z +
-                          (sF[21 + s] + sF[1 + s] + sF[4 + s] + sF[16 + s] - sF[5 + s] - sF[17 + s] - sF[20 + s] -
-                           sF[s]) * x * y * z;
+        const C *F = sF[p];
+        C val;
+        if (!CUBIC) {
+            const int s = 2 * ci + 8 * cj + 32 * ck;
+            const C x = C(-0.25) + C(0.5) * C(I), y = C(-0.25) + C(0.5) * C(J);
+            if (DIM == 2) {
+                val = F[s] + (F[1 + s] - F[s]) * x + (F[4 + s] - F[s]) * y + (F[5 + s] - F[4 + s] - F[1 + s] + F[s]) * x * y;
+            } else {
+                const C z = C(-0.25) + C(0.5) * C(K);
+                val = F[s] + (F[1 + s] - F[s]) * x + (F[4 + s] - F[s]) * y + (F[16 + s] - F[s]) * z +
+                      (F[5 + s] - F[1 + s] - F[4 + s] + F[s]) * x * y +
+                      (F[17 + s] - F[1 + s] - F[16 + s] + F[s]) * x * z +
+                      (F[20 + s] - F[4 + s] - F[16 + s] + F[s]) * y * z +
+                      (F[21 + s] + F[1 + s] + F[4 + s] + F[16 + s] - F[5 + s] - F[17 + s] - F[20 + s] - F[s]) * x * y * z;
+            }
+        } else {
+            const int mx = I + 4 * ci, my = J + 4 * cj, mz = K + 4 * ck;
+            val = C(0);
+            if (DIM == 2) {
+#pragma unroll
+                for (int bj = 0; bj < 4; bj++) {
+                    C row = C(0);
+#pragma unroll
+                    for (int ai = 0; ai < 4; ai++) row += sW[ai][mx] * F[ai + 4 * bj];
+                    val += sW[bj][my] * row;
                 }
             } else {
-                const int mx = I + 4 * ci, my = J + 4 * cj, mz = K + 4 * ck;
-                val = C(0);
-                if (DIM == 2) {
+#pragma unroll
+                for (int ck2 = 0; ck2 < 4; ck2++) {
+                    C pl = C(0);
 #pragma unroll
                     for (int bj = 0; bj < 4; bj++) {
                         C row = C(0);
 #pragma unroll
-                        for (int ai = 0; ai < 4; ai++) row += sW[ai][mx] * sF[ai + 4 * bj];
-                        val += sW[bj][my] * row;
+                        for (int ai = 0; ai < 4; ai++) row += sW[ai][mx] * F[ai + 4 * bj + 16 * ck2];
+                        pl += sW[bj][my] * row;
                     }
-                } else {
-#pragma unroll
-                    for (int ck2 = 0; ck2 < 4; ck2++) {
-                        C pl = C(0);
-#pragma unroll
-                        for (int bj = 0; bj < 4; bj++) {
-                            C row = C(0);
-#pragma unroll
-                            for (int ai = 0; ai < 4; ai++) row += sW[ai][mx] * sF[ai + 4 * bj + 16 * ck2];
-                            pl += sW[bj][my] * row;
-                        }
-                        val += sW[ck2][mz] * pl;
-                    }
+                    val += sW[ck2][mz] * pl;
                 }
             }
-            fc[cell + slot * MC] = ST<T>::enc(val);
         }
-        __syncthreads();
+        fc[cell + lat_pb(DIM, p) * MC] = ST<T>::enc(val);
     }
 }
 
@@ -198,7 +210,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, NCH = Geo<DIM>::NCH, BLK = Q * MC;
     constexpr bool OFF = ST<T>::OFF;
-    __shared__ C sg[NCH * MC];
+    __shared__ C sg[2][NCH * MC];   // double-buffered: one barrier per direction
     __shared__ int smask[NCH * MC];
     // Mesh arrays before the wait for the predecessor, populations after it.
     const int b = a.ids[blockIdx.x];
@@ -224,20 +236,22 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     T *fp = static_cast<T *>(a.fpar) + (long long)b * BLK + tid;
     for (int p = 0; p < Q; p++) {
         const int slot = lat_pb(DIM, p);
+        C *buf = sg[p & 1];
         {
             const C g = ST<T>::dec(own[slot * MC]);
             const C e = feq_stored<DIM, Q, C, OFF>(p, rho, drho, u, v, w);
-            sg[tid] = e + (g - e) * ratio;
+            buf[tid] = e + (g - e) * ratio;
         }
+        // the buffer written here was last read two directions ago, before
+        // the previous barrier
         __syncthreads();
         if (tid < MC && smask[qd * MC + c0] == 1) {
-            const C *s = sg + qd * MC + c0;
+            const C *s = buf + qd * MC + c0;
             C val;
             if (DIM == 2) val = C(0.25) * (s[0] + s[1] + s[4] + s[5]);
             else val = C(0.125) * (s[0] + s[1] + s[4] + s[5] + s[16] + s[17] + s[20] + s[21]);
             fp[slot * MC] = ST<T>::enc(val);
         }
-        __syncthreads();
     }
 }
 

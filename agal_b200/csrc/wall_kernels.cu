@@ -88,20 +88,38 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
     const int t = threadIdx.x;
     for (int i = t; i < W; i += MC) s_meta[i] = a.meta[(long long)b * W + i];
     __syncthreads();
+    // Post-collision values of this block's cells (full populations), the
+    // f_m the interpolated bounce-back reads from the cell behind a link when
+    // that cell is in the same block; other blocks' cells are recomputed.
+    __shared__ C sPost[Q][MC];
     const int mask = a.cmask[(long long)b * MC + t];
     const T *fin = static_cast<const T *>(a.fin) + (long long)b * BLK + t;
-    if (!(s_meta[Meta<DIM>::FLAGS] & META_ACTIVE) || mask == CELL_SOLID) {
+    if (!(s_meta[Meta<DIM>::FLAGS] & META_ACTIVE)) {   // uniform per CTA
         // untouched by the reference's in-place step: carried over unchanged
         T *fo = static_cast<T *>(a.fout) + (long long)b * BLK + t;
 #pragma unroll
         for (int sl = 0; sl < Q; sl++) fo[sl * MC] = fin[sl * MC];
         return;
     }
+    const bool solid = mask == CELL_SOLID;
     C g[Q];
 #pragma unroll
     for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[lat_pb(DIM, p) * MC]);
-    C ux, uy, uz;
-    collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+    C ux = C(0), uy = C(0), uz = C(0);
+    if (!solid) collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+#pragma unroll
+    for (int p = 0; p < Q; p++) sPost[p][t] = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+    __syncthreads();
+    if (solid) {
+        // untouched by the reference's in-place step: carried over unchanged
+        T *fo = static_cast<T *>(a.fout) + (long long)b * BLK + t;
+#pragma unroll
+        for (int sl = 0; sl < Q; sl++) fo[sl * MC] = fin[sl * MC];
+        return;
+    }
+    auto post = [&](int nbh, int nc, int k) {
+        return nbh == b ? sPost[k][nc] : post_collision<DIM, Q, T>(a, nbh, nc, k);
+    };
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     const int slot = w.onb_solid[b];
     const bool wall = w.bc_type > 0 && mask == CELL_BOUNDARY && slot > -1;
@@ -131,7 +149,7 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
                 if (dQ < 0.5f) {
                     const int nbh = nbr_at(q, 1, nc);
                     if (nbh < 0) atomicCAS(w.status, 0, AGAL_ERR_STATE);
-                    else fm = post_collision<DIM, Q, T>(a, nbh, nc, p);
+                    else fm = post(nbh, nc, p);
                 }
                 fp = bouzidi<C>(fp, fm, fq, dQ);
             }
@@ -147,7 +165,7 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
                 if (dQ < 0.5f) {
                     const int nbh = nbr_at(p, 1, nc);
                     if (nbh < 0) atomicCAS(w.status, 0, AGAL_ERR_STATE);
-                    else fm = post_collision<DIM, Q, T>(a, nbh, nc, q);
+                    else fm = post(nbh, nc, q);
                 }
                 fq = bouzidi<C>(fq, fm, fp, dQ);
             }
@@ -189,18 +207,28 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_forces(const ForceArgs fa)
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     const T *fin = static_cast<const T *>(a.fin);
     C s[3] = {C(0), C(0), C(0)};
+    // Before the stream: every cell's post-collision values (stored values for
+    // solid cells and inactive blocks) in shared memory, read for the cells
+    // behind the links inside this block; other blocks' cells are recomputed.
+    __shared__ C sPost[Q][MC];
+    if (!fa.post) {
+        const bool collide = (s_meta[Meta<DIM>::FLAGS] & META_ACTIVE) && mask != CELL_SOLID;
+        C g[Q];
+#pragma unroll
+        for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[(long long)b * BLK + lat_pb(DIM, p) * MC + t]);
+        C ux, uy, uz;
+        if (collide) collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+#pragma unroll
+        for (int p = 0; p < Q; p++) sPost[p][t] = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        __syncthreads();
+    }
     if (mask == CELL_BOUNDARY && slot > -1) {
         // Populations in slot order: post-collision before the stream (the
         // cell's own collision), stored values after it.
         C f[Q];
         if (!fa.post) {
-            C g[Q];
 #pragma unroll
-            for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[(long long)b * BLK + lat_pb(DIM, p) * MC + t]);
-            C ux, uy, uz;
-            collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
-#pragma unroll
-            for (int p = 0; p < Q; p++) f[p] = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+            for (int p = 0; p < Q; p++) f[p] = sPost[p][t];
         } else {
 #pragma unroll
             for (int p = 0; p < Q; p++) f[p] = full_of<DIM, Q, T>(fin[(long long)b * BLK + p * MC + t], p);
@@ -222,7 +250,7 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_forces(const ForceArgs fa)
                     continue;
                 }
                 const C fm = fa.post ? full_of<DIM, Q, T>(fin[(long long)nbh * BLK + ad * MC + nc], ad)
-                                     : post_collision<DIM, Q, T>(a, nbh, nc, ad);
+                                     : (nbh == b ? sPost[ad][nc] : post_collision<DIM, Q, T>(a, nbh, nc, ad));
                 const C fa_ = f[ad];
                 for (int d = 0; d < DIM; d++) {
                     const int cd = lat_c(DIM, d, ad);

@@ -39,64 +39,66 @@ __global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
 k_step(const StepArgs a)
 {
     using C = typename ST<T>::C;
-    constexpr int MC = Geo<DIM>::MC, QMAX = Geo<DIM>::QMAX, BLK = Q * MC;
-    constexpr int TPB = MC / CPT;          // threads per cell-block
-    constexpr int BPC = 256 / TPB;         // cell-blocks per CTA
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
+    constexpr int NB = 256 / MC;           // cell-blocks per CTA and round
     constexpr int W = Meta<DIM>::W;
-    __shared__ int s_meta[BPC][W];
+    __shared__ int s_meta[CPT * NB][W];
     const int tid = threadIdx.x;
-    const int lb = tid / TPB, t0 = tid % TPB;
-    const int kap = blockIdx.x * BPC + lb;
+    const int lb = tid / MC, t = tid % MC;
 
-    // The block ID and its metadata row are written only by the mesh
+    // Round h of this thread is cell t of the CTA's cell-block h * NB + lb:
+    // with several rounds a thread holds the same cell of several blocks, so
+    // that every warp-wide load and push still covers whole rows of a block.
+    // The block IDs and their metadata rows are written only by the mesh
     // passes, never by a kernel that lets this one launch early, so they are
     // read before the wait for the predecessor (the prologue of programmatic
     // dependent launch); the populations after it.
-    const int b = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
-    for (int i = t0; i < W; i += TPB) s_meta[lb][i] = (b >= 0) ? __ldg(&a.meta[(long long)b * W + i]) : 0;
-    const T *__restrict__ fin = static_cast<const T *>(a.fin) + (long long)(b >= 0 ? b : 0) * BLK + t0;
+    int b[CPT];
+#pragma unroll
+    for (int h = 0; h < CPT; h++) {
+        const int kap = (blockIdx.x * CPT + h) * NB + lb;
+        b[h] = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
+        for (int i = t; i < W; i += MC)
+            s_meta[h * NB + lb][i] = (b[h] >= 0) ? __ldg(&a.meta[(long long)b[h] * W + i]) : 0;
+    }
+    const T *__restrict__ f0 = static_cast<const T *>(a.fin) + t;
     pdl_wait();
 
-    // Load: slot pb(p) holds f_p (offset form g_p for half storage).  Cell
-    // h of this thread is t0 + h * TPB.
+    // Load: slot pb(p) holds f_p (offset form g_p for half storage).
     C g[CPT][Q];
-    if (b >= 0) {
 #pragma unroll
-        for (int h = 0; h < CPT; h++)
+    for (int h = 0; h < CPT; h++)
+        if (b[h] >= 0)
 #pragma unroll
-            for (int p = 0; p < Q; p++) g[h][p] = ST<T>::dec(__ldg(fin + lat_pb(DIM, p) * MC + h * TPB));
-    }
+            for (int p = 0; p < Q; p++) g[h][p] = ST<T>::dec(__ldg(f0 + (long long)b[h] * BLK + lat_pb(DIM, p) * MC));
     __syncthreads();
-    const int fl = s_meta[lb][Meta<DIM>::FLAGS];
-    if (b >= 0 && !(fl & META_WALL)) {
-        T *__restrict__ fo = static_cast<T *>(a.fout);
+    T *__restrict__ fo = static_cast<T *>(a.fout);
+#pragma unroll
+    for (int h = 0; h < CPT; h++) {
+        const int *nrow = s_meta[h * NB + lb];
+        const int fl = nrow[Meta<DIM>::FLAGS];
+        if (b[h] < 0 || (fl & META_WALL)) continue;
         // The reference steps in place and leaves solid cells and inactive
         // blocks (refined solid blocks) untouched, so whatever a grid average
         // or an interpolation wrote there stays and feeds the next transfer:
         // carry those cells into the output buffer unchanged.
-        auto carry = [&](int h) {
+        const long long base = (long long)b[h] * BLK + t;
+        auto carry = [&]() {
 #pragma unroll
-            for (int sl = 0; sl < Q; sl++) fo[(long long)b * BLK + sl * MC + t0 + h * TPB] = fin[sl * MC + h * TPB];
+            for (int sl = 0; sl < Q; sl++) fo[base + sl * MC] = f0[base - t + sl * MC];
         };
         if (!(fl & META_ACTIVE)) {
-            if (SOLID)
-#pragma unroll
-                for (int h = 0; h < CPT; h++) carry(h);
-        } else {
-            const int *nrow = s_meta[lb];
-            const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
-#pragma unroll
-            for (int h = 0; h < CPT; h++) {
-                const int t = t0 + h * TPB;
-                if (SOLID && __ldg(&a.cmask[(long long)b * MC + t]) == CELL_SOLID) {
-                    carry(h);
-                    continue;
-                }
-                C ux, uy, uz;
-                collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
-                push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b, t, nrow, hook, fo, a);
-            }
+            if (SOLID) carry();
+            continue;
         }
+        if (SOLID && __ldg(&a.cmask[(long long)b[h] * MC + t]) == CELL_SOLID) {
+            carry();
+            continue;
+        }
+        const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
+        C ux, uy, uz;
+        collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
+        push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b[h], t, nrow, hook, fo, a);
     }
     if (a.fix_ticket) fused_fixup<T>(a);
 }

@@ -91,7 +91,7 @@ void release(agal_ctx *c)
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
-                    c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids};
+                    c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids, c->nu_sgs};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -123,6 +123,13 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     if (p->collision != AGAL_BGK && !(p->collision == AGAL_MRT && p->velocity_set == AGAL_D3Q19)) {
         delete c;
         return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "collision operator: BGK, or MRT with D3Q19");
+    }
+    if (p->S_LES < 0 || p->S_LES > 3) { delete c; return agal_set_err(nullptr, AGAL_ERR_PARAM, "S_LES: 0..3"); }
+    if (p->S_LES > 0 && (p->collision != AGAL_BGK || std::max(p->MAX_LEVELS_WALL, p->MAX_LEVELS_INTERIOR) != 1 ||
+                         p->S_BC_TYPE != 0)) {
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED,
+                            "S_LES: built for BGK on one-level meshes without interpolated bounce-back");
     }
     c->Qmax = (c->dim == 2) ? 9 : 27;
     c->MC = (c->dim == 2) ? 16 : 64;
@@ -233,6 +240,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     ALLOC(c->d_status, sizeof(int) * 4);
     ALLOC(c->meta, sizeof(int) * (size_t)(c->dim == 2 ? 12 : 28) * nmb);
     ALLOC(c->fix_count, sizeof(int) * 4);
+    if (p->S_LES > 0) ALLOC(c->nu_sgs, (p->storage == AGAL_STORE_FP64 ? 8 : 4) * (size_t)nmb * c->MC);   // eddy viscosity
     if (p->S_FORCE_TYPE == 1) ALLOC(c->Ff, (p->storage == AGAL_STORE_FP64 ? 8 : 4) * 6 * (size_t)nmb);   // CV partials
     c->fix_cap = (int)std::min<long long>(std::max<long long>(nmc / 4, AGAL_FIX_CAP_MIN), 1LL << 26);
     ALLOC(c->fix_list, sizeof(long long) * 2 * (size_t)c->fix_cap);

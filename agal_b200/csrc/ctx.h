@@ -103,6 +103,7 @@ struct agal_ctx {
     float *X_b = nullptr;              // [27][n_maxcells_b] link lengths (cells_f_X_b), -1 = none
     int *vox_tmp = nullptr;            // [nmb] near-wall marking scratch (c_tmp_1), -1 at rest
     unsigned long long *bnd_bits = nullptr;   // [nmb] boundary-cell flags of Voxelize_S2
+    void *nu_sgs = nullptr;            // [nmb][MC] LES eddy viscosity (S_LES > 0), compute type
     void *Ff = nullptr;                // [6][nmb] MEA partials (cblock_f_Ff), compute type
     int *geo_small = nullptr, *geo_parts = nullptr;   // counters / compaction partials
     // Wall blocks (onb == 1 and a wall slot) per level for the interpolated

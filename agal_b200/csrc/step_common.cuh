@@ -80,6 +80,11 @@ struct StepArgs {
     // grids, where the fence costs less than a separate launch).
     int *fix_ticket;
     int *status;
+    // LES (S_LES > 0): eddy viscosity per cell of the pool (compute type);
+    // the cell relaxes with omega = dx / (3 (nu + nu_SGS) + dx / 2)
+    // (Cu_CollideLES, solver_lbm_kernels.cu:352-355).  Null otherwise.
+    const void *nu_sgs;
+    double nu, dxL;
 };
 
 // The stream-guard fix-ups applied by the last CTA of the step kernel: every

@@ -97,7 +97,14 @@ k_step(const StepArgs a)
         }
         const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
         C ux, uy, uz;
-        collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
+        if (a.nu_sgs) {
+            const C nus = static_cast<const C *>(a.nu_sgs)[(long long)b[h] * MC + t];
+            const C dx = C(a.dxL);
+            const C tau = r_fma(C(3), r_add(C(a.nu), nus), r_mul(C(0.5), dx));
+            bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], r_div(dx, tau), ux, uy, uz);
+        } else {
+            collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
+        }
         push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b[h], t, nrow, hook, fo, a);
     }
     if (a.fix_ticket) fused_fixup<T>(a);
@@ -215,6 +222,132 @@ __global__ void k_refresh(const MacroArgs a)
     m[a.nmc + cell] = u;
     m[2 * a.nmc + cell] = v;
     if (DIM == 3) m[3 * a.nmc + cell] = w;
+}
+
+// ---------------------------------------------------------------------------
+// Eddy viscosity of the LES models (Cu_ComputeEddyViscosity,
+// solver_lbm_kernels_les.cu:460-600): per block, the velocity of the current
+// populations (the reference refreshes its macros right before, one-level
+// meshes), a one-cell halo extrapolated from the block itself with the
+// fourth-order rule 4 d1 - 6 d2 + 4 d3 - d4 (util_math.h:28-110), central
+// differences (d+ - d-) / (2 dx), then the model (les.cu:13-250).
+template <typename C>
+__device__ __forceinline__ C les_model(int model, int dim, C dx, C ux, C uy, C uz, C vx, C vy, C vz, C wx, C wy,
+                                       C wz)
+{
+    const C dx2 = r_mul(dx, dx);
+    // strain rate S = (grad u + grad u^T) / 2 and its squared norm
+    const C Sxy = r_mul(C(0.5), r_add(uy, vx)), Sxz = r_mul(C(0.5), r_add(uz, wx)),
+            Syz = r_mul(C(0.5), r_add(vz, wy));
+    C F2 = r_add(r_add(r_mul(ux, ux), r_mul(C(2), r_mul(Sxy, Sxy))), r_mul(vy, vy));
+    if (dim == 3)
+        F2 = r_add(r_add(r_add(F2, r_mul(C(2), r_mul(Sxz, Sxz))), r_mul(C(2), r_mul(Syz, Syz))), r_mul(wz, wz));
+    if (model == 1) {   // Smagorinsky, C_s = 0.1
+        return F2 > C(0) ? r_mul(r_mul(C(0.1 * 0.1), dx2), sqrt(r_mul(C(2), F2))) : C(0);
+    }
+    if (model == 2) {   // WALE, C_w = 0.325
+        // g = grad u . grad u, its traceless symmetric part Sd
+        const C gxx = r_add(r_add(r_mul(ux, ux), r_mul(uy, vx)), r_mul(uz, wx));
+        const C gxy = r_add(r_add(r_mul(ux, uy), r_mul(uy, vy)), r_mul(uz, wy));
+        const C gxz = r_add(r_add(r_mul(ux, uz), r_mul(uy, vz)), r_mul(uz, wz));
+        const C gyx = r_add(r_add(r_mul(vx, ux), r_mul(vy, vx)), r_mul(vz, wx));
+        const C gyy = r_add(r_add(r_mul(vx, uy), r_mul(vy, vy)), r_mul(vz, wy));
+        const C gyz = r_add(r_add(r_mul(vx, uz), r_mul(vy, vz)), r_mul(vz, wz));
+        const C gzx = r_add(r_add(r_mul(wx, ux), r_mul(wy, vx)), r_mul(wz, wx));
+        const C gzy = r_add(r_add(r_mul(wx, uy), r_mul(wy, vy)), r_mul(wz, wy));
+        const C gzz = r_add(r_add(r_mul(wx, uz), r_mul(wy, vz)), r_mul(wz, wz));
+        const C gkk = dim == 3 ? r_add(r_add(gxx, gyy), gzz) : r_add(gxx, gyy);
+        const C third = r_mul(C(1.0 / 3.0), gkk);
+        const C Dxx = r_add(gxx, -third), Dyy = r_add(gyy, -third), Dzz = r_add(gzz, -third);
+        const C Dxy = r_mul(C(0.5), r_add(gxy, gyx)), Dxz = r_mul(C(0.5), r_add(gxz, gzx)),
+                Dyz = r_mul(C(0.5), r_add(gyz, gzy));
+        C F1 = r_add(r_add(r_mul(Dxx, Dxx), r_mul(C(2), r_mul(Dxy, Dxy))), r_mul(Dyy, Dyy));
+        if (dim == 3)
+            F1 = r_add(r_add(r_add(F1, r_mul(C(2), r_mul(Dxz, Dxz))), r_mul(C(2), r_mul(Dyz, Dyz))), r_mul(Dzz, Dzz));
+        if (!(F1 > C(0) && F2 > C(0))) return C(0);
+        const C num = r_mul(r_mul(C(0.325 * 0.325), dx2), r_mul(F1, sqrt(F1)));
+        const C den = r_add(r_mul(r_mul(F2, F2), sqrt(F2)), r_mul(F1, sqrt(sqrt(F1))));
+        return r_div(num, den);
+    }
+    // Vreman, c = 2.5 * 0.17^2: B = grad u^T grad u
+    const C Bxx = r_add(r_add(r_mul(ux, ux), r_mul(uy, uy)), r_mul(uz, uz));
+    const C Bxy = r_add(r_add(r_mul(ux, vx), r_mul(uy, vy)), r_mul(uz, vz));
+    const C Bxz = r_add(r_add(r_mul(ux, wx), r_mul(uy, wy)), r_mul(uz, wz));
+    const C Byy = r_add(r_add(r_mul(vx, vx), r_mul(vy, vy)), r_mul(vz, vz));
+    const C Byz = r_add(r_add(r_mul(vx, wx), r_mul(vy, wy)), r_mul(vz, wz));
+    const C Bzz = r_add(r_add(r_mul(wx, wx), r_mul(wy, wy)), r_mul(wz, wz));
+    C Bb = r_add(r_mul(Bxx, Byy), -r_mul(Bxy, Bxy));
+    if (dim == 3)
+        Bb = r_add(r_add(r_add(Bb, r_add(r_mul(Bxx, Bzz), -r_mul(Bxz, Bxz))), r_mul(Byy, Bzz)), -r_mul(Byz, Byz));
+    C aa = r_add(r_add(r_mul(ux, ux), r_mul(vx, vx)), r_add(r_mul(uy, uy), r_mul(vy, vy)));
+    if (dim == 3)
+        aa = r_add(aa, r_add(r_add(r_add(r_mul(wx, wx), r_mul(wy, wy)), r_add(r_mul(uz, uz), r_mul(vz, vz))),
+                             r_mul(wz, wz)));
+    if (!(aa > C(0))) return C(0);
+    Bb = r_div(Bb, aa);
+    return Bb > C(0) ? r_mul(r_mul(C(0.17 * 0.17 * 2.5), dx2), sqrt(Bb)) : C(0);
+}
+
+struct EddyArgs {
+    const int *ids;
+    int n;
+    const void *f;
+    void *nu_sgs;
+    double dx;
+    int model;
+};
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::MC) k_eddy(const EddyArgs a)
+{
+    using C = typename ST<T>::C;
+    constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
+    constexpr int H = 6, HV = (DIM == 3) ? H * H * H : H * H;   // block plus a one-cell halo
+    __shared__ C s[3][HV];
+    const int b = a.ids[blockIdx.x];
+    const int t = threadIdx.x;
+    const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
+    auto at = [&](int i, int j, int k) { return (i + 1) + H * (j + 1) + (DIM == 3 ? H * H * (k + 1) : 0); };
+    const T *f = static_cast<const T *>(a.f) + (long long)b * BLK + t;
+    C rho = 0, m[3] = {0, 0, 0};
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const C fp = ST<T>::dec(f[lat_pb(DIM, p) * MC]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+        rho += fp;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) m[d] += C(lat_c(DIM, d, p)) * fp;
+    }
+    for (int d = 0; d < 3; d++) s[d][at(I, J, K)] = d < DIM ? m[d] / rho : C(0);
+    __syncthreads();
+    auto ext = [](C d1, C d2, C d3, C d4) {
+        return r_add(r_add(r_add(r_mul(C(4), d1), r_mul(C(-6), d2)), r_mul(C(4), d3)), -d4);
+    };
+    for (int d = 0; d < DIM; d++) {
+        C *u = s[d];
+        if (I == 0) {
+            u[at(-1, J, K)] = ext(u[at(0, J, K)], u[at(1, J, K)], u[at(2, J, K)], u[at(3, J, K)]);
+            u[at(4, J, K)] = ext(u[at(3, J, K)], u[at(2, J, K)], u[at(1, J, K)], u[at(0, J, K)]);
+        }
+        if (J == 0) {
+            u[at(I, -1, K)] = ext(u[at(I, 0, K)], u[at(I, 1, K)], u[at(I, 2, K)], u[at(I, 3, K)]);
+            u[at(I, 4, K)] = ext(u[at(I, 3, K)], u[at(I, 2, K)], u[at(I, 1, K)], u[at(I, 0, K)]);
+        }
+        if (DIM == 3 && K == 0) {
+            u[at(I, J, -1)] = ext(u[at(I, J, 0)], u[at(I, J, 1)], u[at(I, J, 2)], u[at(I, J, 3)]);
+            u[at(I, J, 4)] = ext(u[at(I, J, 3)], u[at(I, J, 2)], u[at(I, J, 1)], u[at(I, J, 0)]);
+        }
+    }
+    __syncthreads();
+    const C dx = C(a.dx), two_dx = r_mul(C(2), dx);
+    C gr[3][3] = {};   // gr[component][axis]
+    for (int d = 0; d < DIM; d++) {
+        gr[d][0] = r_div(r_add(s[d][at(I + 1, J, K)], -s[d][at(I - 1, J, K)]), two_dx);
+        gr[d][1] = r_div(r_add(s[d][at(I, J + 1, K)], -s[d][at(I, J - 1, K)]), two_dx);
+        if (DIM == 3) gr[d][2] = r_div(r_add(s[d][at(I, J, K + 1)], -s[d][at(I, J, K - 1)]), two_dx);
+    }
+    static_cast<C *>(a.nu_sgs)[(long long)b * MC + t] =
+        les_model<C>(a.model, DIM, dx, gr[0][0], gr[0][1], gr[0][2], gr[1][0], gr[1][1], gr[1][2], gr[2][0],
+                     gr[2][1], gr[2][2]);
 }
 
 // ---------------------------------------------------------------------------
@@ -386,6 +519,17 @@ template <int DIM, int Q, typename T> struct RunStep {
         const bool wall = agal_wall_active(c) && (int)c->wall_n.size() > L && c->wall_n[L] > 0;
         const bool fused = cpt != 3 && !wall && n <= AGAL_FUSED_FIXUP_BLOCKS;
         a.fix_ticket = fused ? c->fix_count + 1 : nullptr;
+        a.nu_sgs = c->nu_sgs;
+        a.nu = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->P.v0 : c->P.v0;
+        a.dxL = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->dxf[L] : c->dxf[L];
+        if (c->nu_sgs) {
+            // The eddy viscosity of the current populations; the persistent
+            // variant has no per-cell relaxation rate, so LES steps one-shot.
+            if (cpt == 3) cpt = 1;
+            EddyArgs e{a.ids, n, a.fin, c->nu_sgs, a.dxL, c->P.S_LES};
+            k_eddy<DIM, Q, T><<<n, Geo<DIM>::MC, 0, c->stream>>>(e);
+            AGAL_CUDA(c, cudaGetLastError());
+        }
         const int rc = (cpt == 3)   ? launch_step_tma<DIM, Q, T>(c, a)
                        : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                                     : launch_step<DIM, Q, T, 1>(c, a, n);

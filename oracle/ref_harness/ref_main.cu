@@ -78,15 +78,18 @@ constexpr ArgsPack AP3D_H = ArgsPack(3, 128, 1, 1, 1, 24, 2048);
 #ifndef REF_INTERP3D
 #define REF_INTERP3D InterpOrder::Linear
 #endif
+#ifndef REF_LES
+#define REF_LES LESModel::None
+#endif
 #if defined(USED2Q9)
 constexpr ArgsPack APh = AP2D_H;
-constexpr LBMPack LPh = LBMPack(&AP2D_H, VelocitySet::D2Q9, CollisionOperator::BGK, REF_INTERP2D, LESModel::None);
+constexpr LBMPack LPh = LBMPack(&AP2D_H, VelocitySet::D2Q9, CollisionOperator::BGK, REF_INTERP2D, REF_LES);
 #elif defined(USED3Q19)
 constexpr ArgsPack APh = AP3D_H;
-constexpr LBMPack LPh = LBMPack(&AP3D_H, VelocitySet::D3Q19, CollisionOperator::BGK, REF_INTERP3D, LESModel::None);
+constexpr LBMPack LPh = LBMPack(&AP3D_H, VelocitySet::D3Q19, CollisionOperator::BGK, REF_INTERP3D, REF_LES);
 #else
 constexpr ArgsPack APh = AP3D_H;
-constexpr LBMPack LPh = LBMPack(&AP3D_H, VelocitySet::D3Q27, CollisionOperator::BGK, REF_INTERP3D, LESModel::None);
+constexpr LBMPack LPh = LBMPack(&AP3D_H, VelocitySet::D3Q27, CollisionOperator::BGK, REF_INTERP3D, REF_LES);
 #endif
 typedef float REAL_h;
 
@@ -172,7 +175,9 @@ int main(int argc, char **argv)
         geometry->G_Init_Arrays_CoordsList_CPU();
         geometry->G_InitBins(BinMake::GPU, 0);
     }
-    const int N_U = LPh.N_Q + APh.N_DIM + 1;
+    // With an LES model the field also holds the eddy viscosity in row
+    // N_Q + 4 (solver_lbm_kernels_les.cu:591; main.cu:109's commented size).
+    const int N_U = LPh.N_Q + APh.N_DIM + 1 + (LPh.LM != LESModel::None ? 1 : 0);
     Mesh<REAL_h, REAL_h, &APh> mesh(&parser, N_U);
     if (geom) mesh.M_AddGeometry(geometry);
     Solver_LBM<REAL_h, REAL_h, &APh, &LPh> solver(&mesh);

@@ -47,6 +47,10 @@ CASES = {
     "d3q19_ldc16_re400": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4), 200, 4096),
     "d3q27_ldc16_re200": ("ref_d3q27_ldc", dict(Nx=16, v0=2.5e-4), 200, 4096),
     "d3q19_ldc16_pxy": ("ref_d3q19_ldc", dict(Nx=16, v0=1.25e-4, PERIODIC_X=1, PERIODIC_Y=1), 100, 4096),
+    # LES (one level): the field carries the eddy viscosity in row Q + 4.
+    "les_d3q19_ldc16_smag": ("ref_d3q19_ldc_smag", dict(Nx=16, v0=1.25e-4), 200, 4096),
+    "les_d3q19_ldc16_wale": ("ref_d3q19_ldc_wale", dict(Nx=16, v0=1.25e-4), 200, 4096),
+    "les_d3q19_ldc16_vreman": ("ref_d3q19_ldc_vreman", dict(Nx=16, v0=1.25e-4), 200, 4096),
 }
 
 # Multi-level cases: (binary, keys, steps, keep_mb, region preset of the
@@ -175,8 +179,12 @@ def write_input(d: Path, keys: dict, out_dir: Path) -> None:
     (d / "input.txt").write_text("\n".join(lines) + "\n")
 
 
-def read_dump(path: Path) -> dict:
-    """Parse an AGALREF1 dump written by oracle/ref_harness/ref_main.cu."""
+LES_BINARIES = ("ref_d3q19_ldc_smag", "ref_d3q19_ldc_wale", "ref_d3q19_ldc_vreman")
+
+
+def read_dump(path: Path, les: bool = False) -> dict:
+    """Parse an AGALREF1 dump written by oracle/ref_harness/ref_main.cu (an LES
+    build's field has one more row, the eddy viscosity)."""
     b = path.read_bytes()
     if b[:8] != b"AGALREF1":
         raise ValueError("bad magic")
@@ -198,7 +206,7 @@ def read_dump(path: Path) -> dict:
     gaps_tail = take(np.int32, int(n_gap_keep))
     n_act = take(np.int32, 1)[0]
     blocks = take(np.int32, int(n_act))
-    NU = Q + dim + 1
+    NU = Q + dim + 1 + (1 if les else 0)
     rec = [("fX", np.float32, dim), ("bmask", np.int32, 1), ("nbr", np.int32, Qmax), ("nbr_child", np.int32, Qmax),
            ("onb", np.int32, 1), ("ref", np.int32, 1), ("level", np.int32, 1), ("cmask", np.int32, MC),
            ("F", np.float32, NU * MC)]
@@ -304,7 +312,7 @@ def cmd_ref(out: Path, only: list[str] | None) -> None:
             continue
         raw = out / f"{name}.bin"
         run_ref(binary, keys, steps, keep, raw, region=region, skip_last_regrid=skip, sphere=sphere)
-        d = read_dump(raw)
+        d = read_dump(raw, les=binary in LES_BINARIES)
         d["case_keys"] = json.dumps(keys)
         d["binary"] = binary
         d["region"] = region

@@ -250,7 +250,7 @@ def test_refresh_macros():
     assert np.abs(M[1:] - np.stack(u)).max() < 1e-6
 
 
-UNIFORM_CASES = [n for n in GOLDEN_CASES if not n.startswith(("amr_", "regrid_", "geom_", "restart_", "faces_"))]
+UNIFORM_CASES = [n for n in GOLDEN_CASES if not n.startswith(("amr_", "regrid_", "geom_", "restart_", "faces_", "les_"))]
 
 
 @pytest.mark.skipif(not UNIFORM_CASES, reason="no reference dumps committed")

@@ -278,7 +278,7 @@ def test_oracle_regrid_vs_reference_build(oracle_lib, name):
     regrid_from_reference(lambda p, nmb: OracleCase(p, nmb), name)
 
 
-GOLDEN_RUNS = [n for n in GOLDEN_CASES if not n.startswith(("regrid_", "geom_", "restart_", "faces_"))]
+GOLDEN_RUNS = [n for n in GOLDEN_CASES if not n.startswith(("regrid_", "geom_", "restart_", "faces_", "les_"))]
 
 
 @pytest.mark.skipif(not GOLDEN_RUNS, reason="no reference dumps committed")

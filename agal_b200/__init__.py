@@ -164,14 +164,17 @@ class Case:
         self._c(self._lib.agal_refine_stats(self._h, C.byref(it), C.byref(nr), C.byref(nc)))
         return {"iter": it.value, "n_refined": nr.value, "n_coarsened": nc.value}
 
-    STEP_VARIANTS = {1: "1 cell/thread", 2: "2 cells/thread", 3: "TMA-staged persistent pipeline"}
+    STEP_VARIANTS = {1: "1 cell/thread", 2: "2 cells/thread", 3: "TMA-staged persistent pipeline",
+                     4: "1 row of 4 cells/thread, vector loads and stores",
+                     5: "root-level tile of 8x8 blocks per CTA, gathered whole-block stores (2D)"}
 
     def autotune(self, L: int = 0, reps: int = 5) -> dict:
         """Pick the step kernel variant by timing each one (state unchanged)."""
-        ms = (C.c_float * 3)()
+        n = len(self.STEP_VARIANTS)
+        ms = (C.c_float * n)()
         v = C.c_int()
         self._c(self._lib.agal_autotune(self._h, L, reps, ms, C.byref(v)))
-        return {"variant": v.value, "name": self.STEP_VARIANTS[v.value], "ms": [ms[0], ms[1], ms[2]]}
+        return {"variant": v.value, "name": self.STEP_VARIANTS[v.value], "ms": [ms[i] for i in range(n)]}
 
     def set_tuning(self, variant: int) -> None:
         self._c(self._lib.agal_set_tuning(self._h, variant))

@@ -91,7 +91,8 @@ void release(agal_ctx *c)
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
-                    c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids, c->nu_sgs};
+                    c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids, c->nu_sgs, c->blk_solid,
+                    c->tiles};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -975,12 +976,11 @@ extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t by
     if (which == AGAL_ARR_MACROS) return agal_set_err(c, AGAL_ERR_PARAM, "macros are derived, not loaded");
     if (which == AGAL_ARR_CBLOCK_F_FF) return agal_set_err(c, AGAL_ERR_PARAM, "force partials are derived, not loaded");
     AGAL_CUDA(c, cudaMemcpy(int_array(c, which), host_buf, need, cudaMemcpyHostToDevice));
-    if ((rc = agal_build_meta(c))) return rc;
     if (which == AGAL_ARR_CELLS_ID_MASK) {
         // Geometry present when any cell is solid.
         std::vector<int> cm(c->nmc);
         std::memcpy(cm.data(), host_buf, need);
         c->geometry_init = std::any_of(cm.begin(), cm.end(), [](int v) { return v == CELL_SOLID; }) ? 1 : 0;
     }
-    return AGAL_OK;
+    return agal_build_meta(c);
 }

@@ -79,6 +79,9 @@ struct agal_ctx {
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
+    int *blk_solid = nullptr;          // [nmb] 1 = the block holds a solid cell (geometry cases)
+    int *tiles = nullptr;              // root-level tile table of the 2D tile step (step_tile.cu)
+    int n_tiles = 0;                   // 0 = the tile step is not available
     int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
     long long *fix_list = nullptr;
     int fix_cap = 0;
@@ -130,8 +133,10 @@ struct agal_ctx {
 #define AGAL_FUSED_FIXUP_BLOCKS 8192
 
 // Step kernel variants: 1 and 2 cells per thread (one-shot grid), 3 the
-// TMA-staged persistent pipeline.
-#define AGAL_STEP_VARIANTS 3
+// TMA-staged persistent pipeline, 4 one x-row of four cells per thread with
+// vector loads and stores (step_row.cu), 5 the root-level tile step of 2D
+// cases (step_tile.cu; other levels and cases run variant 4 in its place).
+#define AGAL_STEP_VARIANTS 5
 
 // Error helpers shared by the translation units.
 int agal_set_err(agal_ctx *c, int code, const std::string &msg);
@@ -148,6 +153,7 @@ int agal_launch_step(agal_ctx *c, int L);
 int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms);
 int agal_prepare_step(agal_ctx *c);
 int agal_build_meta(agal_ctx *c);   // after any change of the block arrays
+int agal_build_tiles(agal_ctx *c);  // root-level tile table (agal_build_meta calls it)
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);
 // Multi-level path (amr_kernels.cu, amr_pass.cu).

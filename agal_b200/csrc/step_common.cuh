@@ -58,6 +58,7 @@ template <int DIM> struct Meta {
 constexpr int META_ACTIVE = 1;   // collide/stream this block (kernels.cu:236)
 constexpr int META_ONB = 2;      // block touches a domain boundary (kernels.cu:736)
 constexpr int META_WALL = 4;     // wall block stepped by k_step_wall (interpolated bounce-back)
+constexpr int META_NEARSOLID = 8;   // a solid cell in this block or a neighbour (geometry cases)
 
 struct StepArgs {
     const int *ids;
@@ -119,7 +120,22 @@ __device__ __forceinline__ void fused_fixup(const StepArgs &a)
     }
 }
 
+// Explicitly rounded arithmetic (never contracted or reordered by the
+// compiler), so that every kernel variant that inlines the collision performs
+// the same operation sequence and produces bit-identical populations.
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float r_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float r_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double r_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double r_div(double a, double b) { return __ddiv_rn(a, b); }
+
 // Boundary hook presets (inc/custom.h:79-122); f is the full population.
+// Every operation is rounded as written (the order of the C++ expressions
+// of the presets, no fused multiply-add), so the bounced value is the same in
+// every kernel that inlines the hook.
 template <typename C>
 __device__ __forceinline__ C bc_hook(int preset, int nb, C f, C u, C v, C w, C wp, int cx, int cy, int cz, C U)
 {
@@ -134,11 +150,12 @@ __device__ __forceinline__ C bc_hook(int preset, int nb, C f, C u, C v, C w, C w
         break;
     default: break;
     }
-    if (inflow) return f - C(2) * wp * (C(3) * (C(cx) * U));
+    if (inflow) return r_add(f, -r_mul(r_mul(C(2), wp), r_mul(C(3), r_mul(C(cx), U))));
     if (outflow) {
-        C cu = C(cx) * u + C(cy) * v + C(cz) * w;
-        C e = C(1) + C(4.5) * cu * cu - C(1.5) * (u * u + v * v + w * w);
-        return -f + C(2) * wp * e;
+        const C cu = r_add(r_add(r_mul(C(cx), u), r_mul(C(cy), v)), r_mul(C(cz), w));
+        const C uu = r_add(r_add(r_mul(u, u), r_mul(v, v)), r_mul(w, w));
+        const C e = r_add(r_add(C(1), r_mul(r_mul(C(4.5), cu), cu)), -r_mul(C(1.5), uu));
+        return r_add(-f, r_mul(r_mul(C(2), wp), e));
     }
     return f;
 }
@@ -149,18 +166,6 @@ template <int DIM, int Q, typename T, int CPT> struct StepOcc {
     static constexpr int words = CPT * Q * (sizeof(typename ST<T>::C) == 8 ? 2 : 1);   // registers for g[][]
     static constexpr int value = words <= 9 ? 6 : words <= 19 ? 4 : words <= 27 ? 3 : words <= 38 ? 2 : 1;
 };
-
-// Explicitly rounded arithmetic (never contracted or reordered by the
-// compiler), so that every kernel variant that inlines the collision performs
-// the same operation sequence and produces bit-identical populations.
-__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float r_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ float r_div(float a, float b) { return __fdiv_rn(a, b); }
-__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double r_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
-__device__ __forceinline__ double r_div(double a, double b) { return __ddiv_rn(a, b); }
 
 // sum_p c_p g_p along one axis for lattice directions with c in {-1, 0, 1}.
 template <int DIM, int Q, int AXIS, typename C>

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "ctx.h"
@@ -416,7 +417,7 @@ __global__ void k_sum_partials(const double *partial, int n, double *out)
 // flags of kernels.cu:236 (collide/stream) and :736 (boundary hook).
 template <int DIM>
 __global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child, const int *bmask,
-                             const int *onb, const int *onb_solid, int *meta)
+                             const int *onb, const int *onb_solid, const int *blk_solid, int *meta)
 {
     constexpr int W = Meta<DIM>::W, QMAX = Geo<DIM>::QMAX;
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -430,8 +431,30 @@ __global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child
         if (nbr_child[b] < 0 || bmask[b] != BLOCK_SOLID) v |= META_ACTIVE;
         if (onb[b] == 1) v |= META_ONB;
         if (onb_solid && onb[b] == 1 && onb_solid[b] >= 0) v |= META_WALL;
+        if (blk_solid) {
+            // A solid cell in the block or in a block of its neighbourhood:
+            // the row-mapped step tests solid neighbours cell by cell there.
+            bool near = blk_solid[b] != 0;
+            for (int k = 0; k < QMAX && !near; k++) {
+                const int nb = nbr[b + (long long)k * nmb];
+                near = nb >= 0 && nb < nmb && blk_solid[nb] != 0;
+            }
+            if (near) v |= META_NEARSOLID;
+        }
     }
     meta[g] = v;
+}
+
+// 1 per block holding a solid cell (any block of the pool).
+template <int DIM>
+__global__ void k_block_solid(long long nmb, const int *cmask, int *blk_solid)
+{
+    constexpr int MC = Geo<DIM>::MC;
+    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nmb) return;
+    int s = 0;
+    for (int t = 0; t < MC; t++) s |= (cmask[b * MC + t] == CELL_SOLID);
+    blk_solid[b] = s;
 }
 
 
@@ -457,6 +480,21 @@ int launch_step(agal_ctx *c, const StepArgs &a, int n)
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;
 }
+
+// Row-mapped variant (step_row.cu); built for FP32 and the half types (FP64
+// contexts run variant 1 for it).
+template <int DIM, int Q, typename T>
+int launch_step_row(agal_ctx *c, const StepArgs &a, int n);
+template <int DIM, int Q, typename T>
+int launch_row_or_cell(agal_ctx *c, const StepArgs &a, int n)
+{
+    if constexpr (std::is_same<T, double>::value) return launch_step<DIM, Q, T, 1>(c, a, n);
+    else return launch_step_row<DIM, Q, T>(c, a, n);
+}
+// Root-level tile step of 2D cases (step_tile.cu); AGAL_ERR_UNSUPPORTED when
+// the case or level has no tile table.
+template <int DIM, int Q, typename T>
+int launch_step_tile(agal_ctx *c, const StepArgs &a, int L);
 
 // Swap back the pushed entries of every link whose swap the reference's
 // stream guard refuses (recorded by push_cell), then clear the list for the
@@ -513,26 +551,41 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.fix_cap = c->fix_cap;
         a.status = c->d_status;
         if (cpt <= 0) cpt = c->step_cpt;
+        // The tile step covers the root level of 2D cases; elsewhere the row
+        // variant takes its place.
+        const bool tile = cpt == 5 && !std::is_same<T, double>::value && L == c->L0 && c->n_tiles > 0 && !c->nu_sgs;
+        if (cpt == 5 && !tile) cpt = 4;
         // Small one-shot grids apply the fix-ups in their last CTA (saves a
         // launch of a few µs per sub-step); large grids, the persistent
-        // variant and levels with a wall step use the separate kernel.
+        // variant and levels with a wall step use the separate kernel.  The
+        // tile step resolves refused swaps itself (no list).
         const bool wall = agal_wall_active(c) && (int)c->wall_n.size() > L && c->wall_n[L] > 0;
-        const bool fused = cpt != 3 && !wall && n <= AGAL_FUSED_FIXUP_BLOCKS;
+        const bool fused = cpt != 3 && !tile && !wall && n <= AGAL_FUSED_FIXUP_BLOCKS;
         a.fix_ticket = fused ? c->fix_count + 1 : nullptr;
         a.nu_sgs = c->nu_sgs;
         a.nu = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->P.v0 : c->P.v0;
         a.dxL = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->dxf[L] : c->dxf[L];
         if (c->nu_sgs) {
             // The eddy viscosity of the current populations; the persistent
-            // variant has no per-cell relaxation rate, so LES steps one-shot.
-            if (cpt == 3) cpt = 1;
+            // and row-mapped variants have no per-cell relaxation rate, so
+            // LES steps one cell per thread.
+            if (cpt >= 3) cpt = 1;
             EddyArgs e{a.ids, n, a.fin, c->nu_sgs, a.dxL, c->P.S_LES};
             k_eddy<DIM, Q, T><<<n, Geo<DIM>::MC, 0, c->stream>>>(e);
             AGAL_CUDA(c, cudaGetLastError());
         }
-        const int rc = (cpt == 3)   ? launch_step_tma<DIM, Q, T>(c, a)
-                       : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
-                                    : launch_step<DIM, Q, T, 1>(c, a, n);
+        int rc = AGAL_OK;
+        if (tile) {
+            rc = launch_step_tile<DIM, Q, T>(c, a, L);
+            if (rc == AGAL_ERR_UNSUPPORTED) return agal_set_err(c, rc, "tile step not available");
+            if (rc) return rc;
+            if (flip) c->cur[L] = 1 - c->cur[L];
+            return AGAL_OK;
+        }
+        rc = (cpt == 4)   ? launch_row_or_cell<DIM, Q, T>(c, a, n)
+             : (cpt == 3) ? launch_step_tma<DIM, Q, T>(c, a)
+             : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
+                          : launch_step<DIM, Q, T, 1>(c, a, n);
         if (rc) return rc;
         if (const int rw = agal_launch_wall_step(c, L, a.fin, a.fout)) return rw;
         if (!fused)
@@ -545,8 +598,9 @@ template <int DIM, int Q, typename T> struct RunStep {
 };
 
 // Autotuner of the step kernel: times every variant (1: one cell per thread,
-// 2: two cells per thread, 3: TMA-staged persistent pipeline) on level L's
-// current state, writing only the scratch buffer.
+// 2: two cells per thread, 3: TMA-staged persistent pipeline, 4: one row of
+// four cells per thread, 5: root-level tile step) on level L's current
+// state, writing only the scratch buffer.
 template <int DIM, int Q, typename T> struct RunTune {
     static int run(agal_ctx *c, int L, int reps, float *ms_out)
     {
@@ -771,14 +825,23 @@ int agal_build_meta(agal_ctx *c)
     const unsigned grid = (unsigned)((tot + 255) / 256);
     // Wall blocks leave the main step kernels only when k_step_wall takes them.
     const int *wall = agal_wall_active(c) ? c->onb_solid : nullptr;
+    const int *bs = nullptr;
+    if (c->geometry_init) {
+        if (!c->blk_solid) AGAL_CUDA(c, cudaMalloc(&c->blk_solid, sizeof(int) * (size_t)c->nmb));
+        const unsigned gb = (unsigned)((c->nmb + 255) / 256);
+        if (c->dim == 2) agal::k_block_solid<2><<<gb, 256, 0, c->stream>>>(c->nmb, c->cells_ID_mask, c->blk_solid);
+        else agal::k_block_solid<3><<<gb, 256, 0, c->stream>>>(c->nmb, c->cells_ID_mask, c->blk_solid);
+        bs = c->blk_solid;
+    }
     if (c->dim == 2)
         agal::k_build_meta<2><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
-                                                           c->cblock_ID_mask, c->cblock_ID_onb, wall, c->meta);
+                                                           c->cblock_ID_mask, c->cblock_ID_onb, wall, bs, c->meta);
     else
         agal::k_build_meta<3><<<grid, 256, 0, c->stream>>>(c->nmb, c->cblock_ID_nbr, c->cblock_ID_nbr_child,
-                                                           c->cblock_ID_mask, c->cblock_ID_onb, wall, c->meta);
+                                                           c->cblock_ID_mask, c->cblock_ID_onb, wall, bs, c->meta);
     AGAL_CUDA(c, cudaGetLastError());
     int rc;
+    if ((rc = agal_build_tiles(c))) return rc;
     if (c->amr && (rc = agal_build_iface_lists(c))) return rc;
     if (c->onb_solid) return agal_build_wall_lists(c);
     return AGAL_OK;

@@ -94,6 +94,9 @@ WORKLOADS = {
     "ldc3d19_384": dict(
         desc="D3Q19 BGK lid-driven cavity 384^3, one level, Re=400, lid 0.05, FP32 populations",
         velocity_set=_lib.D3Q19, Nx=384, Re=400.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC3D),
+    "ldc3d19_384_fp16": dict(
+        desc="D3Q19 BGK lid-driven cavity 384^3, one level, Re=400, lid 0.05, FP16 weight-offset populations",
+        velocity_set=_lib.D3Q19, Nx=384, Re=400.0, storage=_lib.STORE_FP16, bc=_lib.BC_LDC3D),
     "ldc3d27_256": dict(
         desc="D3Q27 BGK lid-driven cavity 256^3, one level, Re=200, lid 0.05, FP32 populations",
         velocity_set=_lib.D3Q27, Nx=256, Re=200.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC3D),
@@ -463,8 +466,9 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
-    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3],
-                    help="with --profile: step kernel variant (1, 2 cells per thread; 3 TMA pipeline)")
+    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3, 4, 5],
+                    help="with --profile: step kernel variant (1, 2 cells per thread; 3 TMA pipeline; "
+                         "4 one row of four cells per thread; 5 root-level tiles, 2D)")
     ap.add_argument("--batched-cases", type=int, default=64,
                     help="independent D3Q19 cases of the batched measurement (0 skips it)")
     ap.add_argument("--batched-seed", type=int, default=2024)

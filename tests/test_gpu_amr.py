@@ -241,3 +241,31 @@ def test_percentile_refinement_fp64_matches_oracle(Q, N, steps):
         run_like_reference(c, p, steps)
         c.sync()
         compare_states(c, o, p, 1e-11)
+
+
+@pytest.mark.parametrize("Q,N,storage,kw", [
+    (9, 32, _lib.STORE_FP16, dict(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=3, S_CRITERION=_lib.CRITERION_PERCENTILE)),
+    (9, 32, _lib.STORE_FP32, dict(MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=3, region_preset=_lib.REGION_BOUNDARY)),
+    (19, 16, _lib.STORE_FP16, dict(MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=1, region_preset=_lib.REGION_BOX)),
+    (27, 8, _lib.STORE_BF16, dict(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=2, S_CRITERION=_lib.CRITERION_PERCENTILE)),
+])
+def test_row_variant_bit_identical_on_multilevel_runs(Q, N, storage, kw):
+    """The row-mapped step (variant 4) through interface blocks with missing
+    same-level neighbours, the boundary hook and regrids, and the root-level
+    tile step (variant 5, 2D): the same populations and mesh as one cell per
+    thread, bit for bit."""
+    p = amr_params(Q, N, storage=storage, **kw)
+    out = []
+    for v in (1, 4, 5):
+        with ag.Case(p) as c:
+            c.set_ic(0)
+            c.set_tuning(v)
+            c.refine_near_wall()
+            c.advance_n(48, use_graph=True)
+            c.sync()
+            out.append((c.dump(_lib.ARR_F), c.dump(_lib.ARR_ID_SET), c.counts()["n_ids"]))
+    assert max(out[0][2][1:]) > 0
+    for o in out[1:]:
+        assert out[0][2] == o[2]
+        assert np.array_equal(out[0][1], o[1])
+        assert np.array_equal(out[0][0], o[0])

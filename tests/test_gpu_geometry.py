@@ -189,10 +189,13 @@ def test_solution_refinement_with_geometry_fp64_matches_oracle(mli):
     c.close()
 
 
-def test_wall_step_variants_and_graph_bit_identical():
-    g = load("geom_d3q19_wall3_bouzidi")
+@pytest.mark.parametrize("name", ["geom_d3q19_wall3_bouzidi", "geom_d3q27_wall2_bb"])
+def test_wall_step_variants_and_graph_bit_identical(name):
+    """Interpolated bounce-back (wall step) and plain bounce-back through the
+    solid cells (the row variant's per-cell path next to solid cells)."""
+    g = load(name)
     runs = []
-    for variant, graph in [(1, True), (2, True), (3, True), (1, False)]:
+    for variant, graph in [(1, True), (2, True), (3, True), (4, True), (5, True), (1, False)]:
         c, p = run_case(g, variant=variant, use_graph=graph, steps=8)
         runs.append((c.dump(_lib.ARR_F), c.dump(_lib.ARR_CBLOCK_F_FF)))
         c.close()

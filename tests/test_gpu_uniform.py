@@ -157,27 +157,28 @@ def test_graph_replay_bit_identical():
 @pytest.mark.parametrize("Q,storage", [(9, _lib.STORE_FP32), (19, _lib.STORE_FP16), (27, _lib.STORE_FP32),
                                        (9, _lib.STORE_FP64)])
 def test_step_variants_bit_identical_and_autotune_pure(Q, storage):
-    """The three step kernels (1 and 2 cells per thread, TMA-staged
-    pipeline) do the same arithmetic per cell, so their results agree bit for
-    bit; autotuning leaves the state untouched."""
+    """The five step kernels (1 and 2 cells per thread, TMA-staged
+    pipeline, one row of four cells per thread, root-level tiles) do the same
+    arithmetic per cell, so their results agree bit for bit; autotuning leaves
+    the state untouched."""
     N = 32 if Q == 9 else 12
     p = ldc_params(Q, N, storage=storage)
     out = []
-    for v in (1, 2, 3):
+    for v in (1, 2, 3, 4, 5):
         with ag.Case(p) as c:
             c.set_ic(0)
             c.set_tuning(v)
             c.advance_n(17, use_graph=False)
             c.sync()
             out.append(c.dump(_lib.ARR_F))
-    assert np.array_equal(out[0], out[1])
-    assert np.array_equal(out[0], out[2])
+    for o in out[1:]:
+        assert np.array_equal(out[0], o)
     with ag.Case(p) as c:
         c.set_ic(0)
         c.advance_n(5, use_graph=False)
         before = c.dump(_lib.ARR_F)
         r = c.autotune(0, reps=3)
-        assert r["variant"] in (1, 2, 3) and min(r["ms"]) > 0
+        assert r["variant"] in (1, 2, 3, 4, 5) and min(r["ms"]) > 0
         c.sync()
         assert np.array_equal(c.dump(_lib.ARR_F), before)   # tuning does not advance the state
 
@@ -279,3 +280,53 @@ def test_large_grid_properties():
         m1 = c.mass_momentum()
     assert abs(m1[0] - m0[0]) < 1e-6 * m0[0]
     assert np.abs(m1[1:]).max() < 1e-6 * m0[0]
+
+
+@pytest.mark.parametrize("storage,extra", [
+    (_lib.STORE_FP16, dict(PERIODIC_X=1, PERIODIC_Y=1, bc_preset=_lib.BC_NONE, ic_preset=_lib.IC_UNIFORM,
+                           ic_noise=0.3, seed=11)),
+    (_lib.STORE_FP32, dict(PERIODIC_X=1, bc_preset=_lib.BC_NONE, ic_preset=_lib.IC_UNIFORM, ic_noise=0.2,
+                           seed=5)),
+    (_lib.STORE_BF16, dict()),
+    (_lib.STORE_FP32, dict(Ny_factor=2)),
+])
+def test_tile_step_bit_identical(storage, extra):
+    """The root-level tile step (variant 5): fully periodic tiles (the
+    select-free gather), a periodic channel with closed y walls, and lid-driven
+    cavities (closed links, the lid hook) give the populations of one cell per
+    thread bit for bit, with graph replay."""
+    extra = dict(extra)
+    ny = extra.pop("Ny_factor", 1)
+    p = ldc_params(9, 64, storage=storage, extra=extra)
+    if ny != 1:
+        p.L_fy = float(ny)
+        p.n_maxcblocks = 16 * 16 * ny
+    out = []
+    for v in (1, 5):
+        with ag.Case(p) as c:
+            c.set_ic(0)
+            c.set_tuning(v)
+            c.advance_n(40, use_graph=True)
+            c.sync()
+            out.append(c.dump(_lib.ARR_F))
+    assert np.array_equal(out[0], out[1])
+
+
+def test_tile_step_refused_swaps_bit_identical():
+    """A lid-driven cavity driven hard enough (tau near 1/2, lid 0.3) that
+    populations go non-positive at the lid corners: the reference's stream
+    guard refuses those swaps.  The tile step decides them locally and must
+    match the push variants' fix-up list bit for bit."""
+    p = ldc_params(9, 64, extra=dict(v0=1e-7, u_ref=0.3))
+    out, neg = [], 0
+    for v in (1, 5):
+        with ag.Case(p) as c:
+            c.set_ic(0)
+            c.set_tuning(v)
+            for _ in range(6):
+                c.advance_n(5, use_graph=False)
+                F = c.dump(_lib.ARR_F)
+                neg += int((F.reshape(9, -1) <= 0).sum())
+            out.append(F)
+    assert neg > 0, "the case did not produce a non-positive population"
+    assert np.array_equal(out[0], out[1])

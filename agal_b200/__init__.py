@@ -190,6 +190,26 @@ class Case:
         self._c(self._lib.agal_mass_momentum(self._h, out))
         return np.array(out[: self.dim + 1])
 
+    def mass_momentum_async(self, out: np.ndarray) -> None:
+        """Enqueue mass_momentum into out[0:4] (float64, ideally pinned);
+        valid after sync()."""
+        if out.dtype != np.float64 or out.size < 4 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of at least 4 values")
+        self._c(self._lib.agal_mass_momentum_async(self._h, out.ctypes.data_as(C.c_void_p)))
+
+    def render_prepared(self) -> dict:
+        """The uniform-grid fields after M_Advance_PrintData's preparation
+        (grid averages, interface interpolations, macros of every level), as
+        agal_uniform_frame writes them."""
+        ml = self.counts()["max_levels"]
+        for L in range(ml - 2, -1, -1):
+            self.average(L, _lib.AVERAGE_GRID)
+        for L in range(ml - 1):
+            self.interpolate(L, _lib.INTERP_INTERFACE)
+        for L in range(ml):
+            self.refresh(L)
+        return self.render_uniform()
+
     def mass_momentum_noalloc(self) -> np.ndarray:
         """mass_momentum with a fixed static device scratch (allocates nothing)."""
         out = (C.c_double * 4)()

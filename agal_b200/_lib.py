@@ -91,6 +91,7 @@ PROTOS = [
     ("agal_uniform_frame", C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     ("agal_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_mass_momentum_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("agal_mass_momentum_async", C.c_int, [C.c_void_p, C.c_void_p]),
     ("agal_sync", C.c_int, [C.c_void_p]),
     ("agal_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("agal_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),

@@ -92,7 +92,7 @@ void release(agal_ctx *c)
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
                     c->cblock_level, c->id_set, c->gap_set, c->red, c->red_out, c->d_status, c->meta,
                     c->amr, c->fix_count, c->fix_list, c->crit, c->iface_ids, c->nu_sgs, c->blk_solid,
-                    c->tiles};
+                    c->tiles, c->xfer};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -441,6 +441,12 @@ extern "C" int agal_mass_momentum(agal_ctx *c, double *out)
 {
     if (!c || !out) return AGAL_ERR_PARAM;
     return agal_launch_mass(c, out);
+}
+
+extern "C" int agal_mass_momentum_async(agal_ctx *c, double *out)
+{
+    if (!c || !out) return AGAL_ERR_PARAM;
+    return agal_launch_mass_async(c, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -794,34 +800,6 @@ static void *int_array(agal_ctx *c, int which)
     }
 }
 
-template <typename T>
-static void decode(const std::vector<unsigned char> &raw, size_t i, int Q, int p, double *o)
-{
-    const T v = reinterpret_cast<const T *>(raw.data())[i];
-    *o = (double)ST<T>::dec(v) + (ST<T>::OFF ? lat_w(Q, p) : 0.0);
-}
-
-template <typename T>
-static void encode(std::vector<unsigned char> &raw, size_t i, int Q, int p, double v)
-{
-    using C = typename ST<T>::C;
-    reinterpret_cast<T *>(raw.data())[i] = ST<T>::enc((C)(v - (ST<T>::OFF ? lat_w(Q, p) : 0.0)));
-}
-
-// Buffer index each block's populations currently live in.
-static int block_buffers(agal_ctx *c, std::vector<int> &which_buf)
-{
-    std::vector<int> lev(c->nmb), ref(c->nmb);
-    AGAL_CUDA(c, cudaMemcpy(lev.data(), c->cblock_level, sizeof(int) * c->nmb, cudaMemcpyDeviceToHost));
-    AGAL_CUDA(c, cudaMemcpy(ref.data(), c->cblock_ID_ref, sizeof(int) * c->nmb, cudaMemcpyDeviceToHost));
-    which_buf.resize(c->nmb);
-    for (long long b = 0; b < c->nmb; b++) {
-        const int L = (ref[b] != REF_INACTIVE && lev[b] >= 0 && lev[b] < c->max_levels) ? lev[b] : 0;
-        which_buf[b] = c->cur[L];
-    }
-    return AGAL_OK;
-}
-
 // Populations of blocks [0, nb) in the reference's slot-major layout
 // (out[s][b * MC + cell], absolute values), each block from its level's
 // current buffer; and the inverse, into both buffers.  Only the prefix of the
@@ -830,56 +808,16 @@ int agal_read_blocks_F(agal_ctx *c, int nb, double *out)
 {
     if (nb <= 0) return AGAL_OK;
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
-    const size_t n = (size_t)c->Q * c->MC * nb, ncell = (size_t)nb * c->MC;
-    std::vector<unsigned char> raw[2];
-    for (int k = 0; k < 2; k++) {
-        raw[k].resize(n * c->esize);
-        AGAL_CUDA(c, cudaMemcpy(raw[k].data(), c->F[k], n * c->esize, cudaMemcpyDeviceToHost));
-    }
-    std::vector<int> lev(nb), ref(nb);
-    AGAL_CUDA(c, cudaMemcpy(lev.data(), c->cblock_level, sizeof(int) * nb, cudaMemcpyDeviceToHost));
-    AGAL_CUDA(c, cudaMemcpy(ref.data(), c->cblock_ID_ref, sizeof(int) * nb, cudaMemcpyDeviceToHost));
-    for (int s = 0; s < c->Q; s++) {
-        const int p = lat_pb(c->dim, s);
-        for (size_t cell = 0; cell < ncell; cell++) {
-            const size_t b = cell / c->MC;
-            const int L = (ref[b] != REF_INACTIVE && lev[b] >= 0 && lev[b] < c->max_levels) ? lev[b] : 0;
-            const auto &r = raw[c->cur[L]];
-            const size_t src = (b * c->Q + s) * c->MC + (cell % c->MC);
-            double *o = &out[(size_t)s * ncell + cell];
-            switch (c->storage) {
-            case AGAL_STORE_FP32: decode<float>(r, src, c->Q, p, o); break;
-            case AGAL_STORE_FP64: decode<double>(r, src, c->Q, p, o); break;
-            case AGAL_STORE_FP16: decode<__half>(r, src, c->Q, p, o); break;
-            case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, src, c->Q, p, o); break;
-            }
-        }
-    }
-    return AGAL_OK;
+    return agal_f_to_host(c, nb, (long long)nb * c->MC, out);
 }
 
 int agal_write_blocks_F(agal_ctx *c, int nb, const double *in)
 {
     if (nb <= 0) return AGAL_OK;
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
-    const size_t n = (size_t)c->Q * c->MC * nb, ncell = (size_t)nb * c->MC;
-    std::vector<unsigned char> raw(n * c->esize);
-    for (int s = 0; s < c->Q; s++) {
-        const int p = lat_pb(c->dim, s);
-        for (size_t cell = 0; cell < ncell; cell++) {
-            const size_t dst = ((cell / c->MC) * c->Q + s) * c->MC + (cell % c->MC);
-            const double v = in[(size_t)s * ncell + cell];
-            switch (c->storage) {
-            case AGAL_STORE_FP32: encode<float>(raw, dst, c->Q, p, v); break;
-            case AGAL_STORE_FP64: encode<double>(raw, dst, c->Q, p, v); break;
-            case AGAL_STORE_FP16: encode<__half>(raw, dst, c->Q, p, v); break;
-            case AGAL_STORE_BF16: encode<__nv_bfloat16>(raw, dst, c->Q, p, v); break;
-            }
-        }
-    }
-    for (int k = 0; k < 2; k++) AGAL_CUDA(c, cudaMemcpy(c->F[k], raw.data(), n * c->esize, cudaMemcpyHostToDevice));
+    int rc = agal_f_from_host(c, nb, (long long)nb * c->MC, in);
     agal_drop_graphs(c);
-    return AGAL_OK;
+    return rc;
 }
 
 extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
@@ -902,32 +840,9 @@ extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
         return AGAL_OK;
     }
     if (which == AGAL_ARR_F) {
-        const size_t n = (size_t)c->Q * c->nmc;
-        std::vector<unsigned char> raw[2];
-        for (int k = 0; k < 2; k++) {
-            raw[k].resize(n * c->esize);
-            AGAL_CUDA(c, cudaMemcpy(raw[k].data(), c->F[k], n * c->esize, cudaMemcpyDeviceToHost));
-        }
-        std::vector<int> wb;
-        if ((rc = block_buffers(c, wb))) return rc;
-        // Device layout F[b][s][c] -> reference layout cells_f_F[s][b*MC + c].
-        double *o = static_cast<double *>(host_buf);
-        for (int s = 0; s < c->Q; s++) {
-            const int p = lat_pb(c->dim, s);   // slot s holds f_p, w_p == w_s
-            for (long long cell = 0; cell < c->nmc; cell++) {
-                const size_t i = (size_t)s * c->nmc + cell;
-                const long long b = cell / c->MC;
-                const size_t src = ((size_t)b * c->Q + s) * c->MC + (cell % c->MC);
-                const auto &r = raw[wb[b]];
-                switch (c->storage) {
-                case AGAL_STORE_FP32: decode<float>(r, src, c->Q, p, &o[i]); break;
-                case AGAL_STORE_FP64: decode<double>(r, src, c->Q, p, &o[i]); break;
-                case AGAL_STORE_FP16: decode<__half>(r, src, c->Q, p, &o[i]); break;
-                case AGAL_STORE_BF16: decode<__nv_bfloat16>(r, src, c->Q, p, &o[i]); break;
-                }
-            }
-        }
-        return AGAL_OK;
+        // Device layout F[b][s][c] -> reference layout cells_f_F[s][b*MC + c],
+        // converted on the device.
+        return agal_f_to_host(c, c->nmb, c->nmc, static_cast<double *>(host_buf));
     }
     if (which == AGAL_ARR_MACROS) {
         const size_t n = (size_t)(c->dim + 1) * c->nmc;
@@ -953,25 +868,8 @@ extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t by
     if (!host_buf || bytes != need) return agal_set_err(c, AGAL_ERR_PARAM, "load size mismatch");
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
     if (which == AGAL_ARR_F) {
-        // The same values go to both buffers.
-        const size_t n = (size_t)c->Q * c->nmc;
-        std::vector<unsigned char> raw(n * c->esize);
-        const double *in = static_cast<const double *>(host_buf);
-        for (int s = 0; s < c->Q; s++) {
-            const int p = lat_pb(c->dim, s);
-            for (long long cell = 0; cell < c->nmc; cell++) {
-                const size_t i = (size_t)s * c->nmc + cell;
-                const size_t dst = ((size_t)(cell / c->MC) * c->Q + s) * c->MC + (cell % c->MC);
-                switch (c->storage) {
-                case AGAL_STORE_FP32: encode<float>(raw, dst, c->Q, p, in[i]); break;
-                case AGAL_STORE_FP64: encode<double>(raw, dst, c->Q, p, in[i]); break;
-                case AGAL_STORE_FP16: encode<__half>(raw, dst, c->Q, p, in[i]); break;
-                case AGAL_STORE_BF16: encode<__nv_bfloat16>(raw, dst, c->Q, p, in[i]); break;
-                }
-            }
-        }
-        for (int k = 0; k < 2; k++) AGAL_CUDA(c, cudaMemcpy(c->F[k], raw.data(), raw.size(), cudaMemcpyHostToDevice));
-        return AGAL_OK;
+        // The same values go to both buffers, converted on the device.
+        return agal_f_from_host(c, c->nmb, c->nmc, static_cast<const double *>(host_buf));
     }
     if (which == AGAL_ARR_MACROS) return agal_set_err(c, AGAL_ERR_PARAM, "macros are derived, not loaded");
     if (which == AGAL_ARR_CBLOCK_F_FF) return agal_set_err(c, AGAL_ERR_PARAM, "force partials are derived, not loaded");

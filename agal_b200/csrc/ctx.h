@@ -82,6 +82,7 @@ struct agal_ctx {
     int *blk_solid = nullptr;          // [nmb] 1 = the block holds a solid cell (geometry cases)
     int *tiles = nullptr;              // root-level tile table of the 2D tile step (step_tile.cu)
     int n_tiles = 0;                   // 0 = the tile step is not available
+    void *xfer = nullptr;              // 64 MiB FP64 staging of the population dumps and loads (xfer.cu)
     int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
     long long *fix_list = nullptr;
     int fix_cap = 0;
@@ -156,6 +157,9 @@ int agal_build_meta(agal_ctx *c);   // after any change of the block arrays
 int agal_build_tiles(agal_ctx *c);  // root-level tile table (agal_build_meta calls it)
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);
+// Enqueue the FP64 sums and their copy into host memory (pinned for a truly
+// asynchronous copy); the values are valid once the stream has reached it.
+int agal_launch_mass_async(agal_ctx *c, double *host_out);
 // Multi-level path (amr_kernels.cu, amr_pass.cu).
 int agal_launch_interp(agal_ctx *c, int L, int var);
 int agal_launch_average(agal_ctx *c, int L, int var);
@@ -179,6 +183,10 @@ void agal_advance_parity(agal_ctx *c, int steps);
 // (restart I/O without copying the whole pool).
 int agal_read_blocks_F(agal_ctx *c, int nb, double *out);
 int agal_write_blocks_F(agal_ctx *c, int nb, const double *in);
+// Device-side conversions behind them (xfer.cu): blocks [0, nb) to / from
+// host[s * pitch + b * M_CBLOCK + c] (FP64, absolute values).
+int agal_f_to_host(agal_ctx *c, long long nb, long long pitch, double *host);
+int agal_f_from_host(agal_ctx *c, long long nb, long long pitch, const double *host);
 // Geometry (geometry.cu, wall_kernels.cu).
 void agal_geometry_release(agal_ctx *c);
 int agal_build_wall_lists(agal_ctx *c);     // after the mesh or the wall slots change

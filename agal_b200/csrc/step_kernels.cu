@@ -401,14 +401,21 @@ __global__ void __launch_bounds__(256) k_mass(const MassArgs a)
     if (threadIdx.x < 4) a.partial[blockIdx.x * 4 + threadIdx.x] = s[threadIdx.x][0];
 }
 
-__global__ void k_sum_partials(const double *partial, int n, double *out)
+// One CTA per component (gridDim.x = 4): strided partial sums, then a
+// fixed-shape tree, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(256) k_sum_partials(const double *partial, int n, double *out)
 {
-    // One thread per component, fixed summation order.
-    const int k = threadIdx.x;
-    if (k >= 4) return;
+    __shared__ double s[256];
+    const int k = blockIdx.x;
     double acc = 0.0;
-    for (int i = 0; i < n; i++) acc += partial[i * 4 + k];
-    out[k] = acc;
+    for (int i = threadIdx.x; i < n; i += 256) acc += partial[(long long)i * 4 + k];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = 128; st > 0; st >>= 1) {
+        if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = s[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -676,7 +683,8 @@ template <int DIM, int Q, typename T> struct RunRefresh {
 };
 
 template <int DIM, int Q, typename T> struct RunMass {
-    static int run(agal_ctx *c, double *out)
+    // Enqueue the sums and the copy of the four results to host_out.
+    static int run(agal_ctx *c, double *host_out)
     {
         // Partials of all levels, laid out level after level.
         long long total = 0;
@@ -706,15 +714,13 @@ template <int DIM, int Q, typename T> struct RunMass {
             AGAL_CUDA(c, cudaGetLastError());
             off += grids[L];
         }
-        k_sum_partials<<<1, 32, 0, c->stream>>>(c->red, (int)total, c->red_out);
-        AGAL_CUDA(c, cudaGetLastError());
-        double h[4];
-        AGAL_CUDA(c, cudaMemcpyAsync(h, c->red_out, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-        AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
-        out[0] = h[0];
-        out[1] = h[1];
-        out[2] = h[2];
-        if (DIM == 3) out[3] = h[3];
+        if (total == 0) {
+            AGAL_CUDA(c, cudaMemsetAsync(c->red_out, 0, 4 * sizeof(double), c->stream));
+        } else {
+            k_sum_partials<<<4, 256, 0, c->stream>>>(c->red, (int)total, c->red_out);
+            AGAL_CUDA(c, cudaGetLastError());
+        }
+        AGAL_CUDA(c, cudaMemcpyAsync(host_out, c->red_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         return AGAL_OK;
     }
 };
@@ -790,8 +796,12 @@ template <int DIM, int Q, typename T> struct RunMassNoAlloc {
             AGAL_CUDA(c, cudaGetLastError());
             off += grids[L];
         }
-        k_sum_partials<<<1, 32, 0, c->stream>>>(scratch, (int)total, res);
-        AGAL_CUDA(c, cudaGetLastError());
+        if (total == 0) {
+            AGAL_CUDA(c, cudaMemsetAsync(res, 0, 4 * sizeof(double), c->stream));
+        } else {
+            k_sum_partials<<<4, 256, 0, c->stream>>>(scratch, (int)total, res);
+            AGAL_CUDA(c, cudaGetLastError());
+        }
         double h[4];
         AGAL_CUDA(c, cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
         AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -848,4 +858,13 @@ int agal_build_meta(agal_ctx *c)
 }
 int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }
 int agal_launch_refresh(agal_ctx *c, int L) { return agal::dispatch<agal::RunRefresh>(c, L); }
-int agal_launch_mass(agal_ctx *c, double *out) { return agal::dispatch<agal::RunMass>(c, out); }
+int agal_launch_mass_async(agal_ctx *c, double *host_out) { return agal::dispatch<agal::RunMass>(c, host_out); }
+int agal_launch_mass(agal_ctx *c, double *out)
+{
+    double h[4];
+    int rc = agal_launch_mass_async(c, h);
+    if (rc) return rc;
+    AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < c->dim + 1; k++) out[k] = h[k];
+    return AGAL_OK;
+}

@@ -1,35 +1,41 @@
 #!/usr/bin/env python
 """Benchmark of the B200 octree-AMR lattice Boltzmann time step.
 
-One "step" is one coarse time step of the solver (Mesh::M_Advance_Step: the
-S_Advance recursion from N_LEVEL_START over every level, plus the
-solution-based refinement when its P_REFINE turn comes) on the workload named
-in the JSON line.  Metric: MLUPS, million lattice-cell updates per second,
-leaf cells of level L counted 2^(L-L0) times per coarse step as
-solver_lbm_advance.cu:74-89 counts them.
-
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Default workload: D2Q9 lid-driven cavity on a 128^2 base grid with up to 3
-levels, refined above the 90th and coarsened below the 50th percentile of the
-block vorticity every 64 coarse steps, Re = 1000, lid 0.05, FP16 weight-offset
-populations.  The multi-level hierarchy is developed by an untimed spin-up
-before the warm-up.  The same case in FP32 populations is timed beside it
-(`plain_fp32`).
+Workload (the headline configuration): D2Q9 lid-driven cavity on a 128^2
+base grid in 4^2-cell blocks, up to 3 levels, refined above the 90th and
+coarsened below the 50th percentile of the block vorticity every 64 coarse
+steps, Re = 1000, lid 0.05, cubic interpolation, FP16 weight-offset
+populations.  Seeded synthetic input: the fluid starts at rest and the
+hierarchy develops in an untimed 1280-coarse-step spin-up.
+
+One "step" is one regrid period: P_REFINE = 64 coarse steps
+(Mesh::M_Advance_Step, the S_Advance recursion over every level) followed by
+the solution-based refinement of the 64th (M_Advance_RefineWithSolution), so
+every timed step holds exactly one regrid.  Metric: MLUPS, million lattice
+cell updates per second, leaf cells of level L counted 2^L times per coarse
+step as solver_lbm_advance.cu:74-89 counts them.
 
 --impl b200 (default): the CUDA library.  Rank 0 prints one JSON line with
-  value        device-timed MLUPS (CUDA events on the library's stream, L2
-               flushed between steps when the state fits in L2)
-  e2e          MLUPS through the public C ABI with host buffers: load the
-               populations from pinned host memory, K x (coarse step + read
-               back the FP64 mass/momentum), dump the populations
+  value        device-timed MLUPS (CUDA events on the library's stream; the
+               state is L2-resident, so L2 is flushed before every timed step)
+  e2e          the same steps through the public C ABI with host buffers:
+               the populations loaded from pinned host memory, K x (period +
+               an asynchronous FP64 mass/momentum read back into pinned
+               memory), the populations dumped; timed by wall clock
+  plain_fp32   the same case in FP32 populations; learned: the FP16 case with
+               the learned refinement predictor driving the regrids
   roofline     the fused step kernel on a large single-level case of the same
-               physics and storage (inputs far larger than L2), algorithmic
-               bytes 2*Q*s per cell update
+               physics (FP16 and FP32), algorithmic bytes 2*Q*s per update
+  error_vs_fp64  rho and u of FP32 and FP16 runs of the headline case against
+               an FP64 run of this library after --error-steps coarse steps
   cpu_baseline the CPU oracle (OpenMP restatement of the reference algorithm)
                on a bounded sample of the same workload, rank 0 only
---impl reference: the reference's algorithm on the host cores (the CPU oracle
-  port; the reference has no CPU implementation of its own), rank 0 only.
+--impl reference: the reference algorithm on the host cores (the CPU oracle
+  port; the reference has no CPU implementation of its own), rank 0 only,
+  plus the reference's own CUDA build (oracle/_ref) timed on this GPU where
+  it was built.  Loads nothing of the agal_b200 native library.
 
 Multi-GPU: one process per GPU under torchrun; every rank runs an
 independent replica of the workload (a single case does not shard), so the
@@ -73,6 +79,11 @@ WORKLOADS = {
         desc="D2Q9 BGK lid-driven cavity, 128^2 base in 4^2-cell blocks, up to 3 levels, percentile vorticity "
              "criterion (refine > p90, coarsen < p50) every 64 coarse steps, Re=1000, lid 0.05, cubic "
              "interpolation, FP32 populations"),
+    "amr_ldc2d_128_log2": dict(
+        _AMR, storage=_lib.STORE_FP32, criterion=_lib.CRITERION_VORTICITY, refine_start=-2.0,
+        desc="D2Q9 BGK lid-driven cavity, 128^2 base in 4^2-cell blocks, up to 3 levels, the reference's own "
+             "criterion (floor(log2 |vorticity|) against N_REFINE_START -2, N_REFINE_INC 1, N_REFINE_MAX 1) every "
+             "64 coarse steps, Re=1000, lid 0.05, cubic interpolation, FP32 populations"),
     "ldc2d_256": dict(
         desc="D2Q9 BGK lid-driven cavity 256x256, one level, Re=100, lid 0.05, FP32 populations",
         velocity_set=_lib.D2Q9, Nx=256, Re=100.0, storage=_lib.STORE_FP32, bc=_lib.BC_LDC2D),
@@ -109,7 +120,10 @@ DTYPE_NAME = {_lib.STORE_FP32: "f32", _lib.STORE_FP64: "f64", _lib.STORE_FP16: "
 ROOFLINE_FOR = {_lib.STORE_FP16: "ldc2d_8192_fp16", _lib.STORE_FP32: "ldc2d_8192"}
 
 
-def make_params(w: dict, device: int = -1):
+def make_params(w: dict, device: int = -1, defaults=None, **extra):
+    """agal_params of a workload; `defaults` builds the parameter structure
+    (the library's agal_params_default, or the oracle's restatement where the
+    CUDA library must not be loaded)."""
     dim = DIM_OF[w["velocity_set"]]
     nb = (w["Nx"] // 4) ** dim
     kw = dict(velocity_set=w["velocity_set"], Nx=w["Nx"], MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1,
@@ -120,7 +134,11 @@ def make_params(w: dict, device: int = -1):
         kw.update(MAX_LEVELS_INTERIOR=w["levels"], P_REFINE=w["p_refine"], S_CRITERION=_lib.CRITERION_PERCENTILE,
                   ref_pct_hi=0.9, ref_pct_lo=0.5, interp_order=w["interp"],
                   n_maxcblocks=sum(nb * nch ** L for L in range(w["levels"])) + 64)
-    return ag.default_params(**kw)
+        if w.get("criterion") is not None:
+            kw.update(S_CRITERION=w["criterion"], N_REFINE_START=w["refine_start"], N_REFINE_INC=1.0,
+                      N_REFINE_MAX=1.0)
+    kw.update(extra)
+    return (defaults or ag.default_params)(**kw)
 
 
 def leaf_cells(counts: dict, dim: int) -> int:
@@ -242,30 +260,40 @@ def dram_traffic_per_launch(workload: str):
 
 
 # ---------------------------------------------------------------------------
+def coarse_per_step(w: dict) -> int:
+    """Coarse steps in one bench step: a whole regrid period for multi-level
+    workloads, one for single-level ones."""
+    return w["p_refine"] if w.get("amr") else 1
+
+
 def step_fn(case, w: dict):
-    """One coarse step: the captured multi-level step (with its regrid turn)
-    or the fused single-level step."""
+    """One bench step: a captured regrid period (its 64th coarse step ends
+    with the refinement) or one fused single-level step."""
     if w.get("amr"):
-        return lambda: case.advance_n(1, use_graph=True)
+        n = coarse_per_step(w)
+        return lambda: case.advance_n(n, use_graph=True)
     return case.advance
 
 
 def time_steps(case, torch, w: dict, n_steps: int, flush: bool):
     """Per-step device time (ms) with CUDA events on the library's stream,
-    and the cell updates of each step."""
+    the cell updates and the library kernel launches of each step."""
     stream = torch.cuda.ExternalStream(case.stream_ptr())
     scratch = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda") if flush else None
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n_steps)]
     step = step_fn(case, w)
     dim = DIM_OF[w["velocity_set"]]
+    k = coarse_per_step(w)
     cells, launches = [], 0
     for i in range(n_steps):
         if flush:
             with torch.cuda.stream(stream):
                 scratch.add_(1.0)   # writes 252 MB > L2 between timed steps
-        cnt = case.counts()
-        cells.append(leaf_cells(cnt, dim))
-        launches += launches_per_step(cnt, w.get("amr", False))
+        cnt = case.counts()   # the mesh holds for the whole period (regrid at its end)
+        cells.append(k * leaf_cells(cnt, dim))
+        launches += k * launches_per_step(cnt, w.get("amr", False))
+        if w.get("amr"):
+            launches += regrid_launches(cnt)
         evs[i][0].record(stream)
         step()
         evs[i][1].record(stream)
@@ -275,11 +303,13 @@ def time_steps(case, torch, w: dict, n_steps: int, flush: bool):
 
 
 def develop(case, w: dict):
-    """Initial state, then the untimed spin-up that builds the hierarchy."""
+    """Initial state, then the untimed spin-up that builds the hierarchy (a
+    whole number of regrid periods, so that bench steps start on a period)."""
     case.set_ic(0)
     if w.get("amr"):
         case.refine_near_wall()
         case.advance_n(w["spinup"], use_graph=True)
+        assert case.refine_stats()["iter"] % w["p_refine"] == 0
 
 
 # ---------------------------------------------------------------------------
@@ -406,10 +436,12 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
 
 
 def run_cpu_oracle(w: dict, seconds: float, threads: int, max_steps: int | None = None) -> dict:
-    """Oracle (CPU restatement, OpenMP) MLUPS on a bounded sample of the workload."""
-    from oracle.orc import OracleCase, build  # CPU baseline leg only
+    """Oracle (CPU restatement, OpenMP) MLUPS on a bounded sample of the
+    workload, after the same spin-up; parameters from the oracle's own
+    defaults, so no native code of agal_b200 is loaded here."""
+    from oracle.orc import OracleCase, build, default_params  # CPU baseline / reference arm only
     build()
-    p = make_params(w)
+    p = make_params(w, defaults=default_params)
     o = OracleCase(p, p.n_maxcblocks, fp64=(w["storage"] == _lib.STORE_FP64), threads=threads)
     dim = DIM_OF[w["velocity_set"]]
     o.set_ic(0)
@@ -436,6 +468,36 @@ def run_cpu_oracle(w: dict, seconds: float, threads: int, max_steps: int | None 
                       f", on {threads} host threads ({dt:.1f} s)"}
 
 
+def reference_cuda(timeout_s: float = 600.0) -> dict:
+    """The reference's own CUDA build (oracle/_ref, compiled from its sources by
+    `make -C oracle ref`) timed on this GPU with CUDA events around its
+    M_Advance_Step loop (oracle/ref_harness/ref_main.cu; the reference
+    synchronises after every kernel, solver_lbm_advance.cu:72-89): the
+    single-level 256^2 cavity (Re 100) and the 3-level 128^2 cavity with its own
+    log2 vorticity criterion (Re 1000, regrid every 64 steps, 1280-step
+    spin-up; the timed steps hold no regrid, as the harness times them)."""
+    from oracle.ref_run import REF_BIN, run_ref   # reference arm only
+    out = {"source": "oracle/_ref/ref_d2q9_ldc (the reference's sources, nvcc sm_100a)"}
+    if not (REF_BIN / "ref_d2q9_ldc").exists():
+        out["unavailable"] = "oracle/_ref/ref_d2q9_ldc was not built (no reference tree where build() ran)"
+        return out
+    w2 = WORKLOADS["amr_ldc2d_128_log2"]
+    runs = {
+        "ldc2d_256": (dict(Nx=256, v0=5e-4), 3, 2000),
+        "amr_ldc2d_128_log2": (dict(Nx=128, v0=0.05 / w2["Re"], MAX_LEVELS_INTERIOR=w2["levels"],
+                                    P_REFINE=w2["p_refine"], S_CRITERION=0, N_REFINE_START=w2["refine_start"],
+                                    N_REFINE_INC=1.0, N_REFINE_MAX=1.0), w2["spinup"], 1280),
+    }
+    for name, (keys, spin, timed) in runs.items():
+        try:
+            txt = run_ref("ref_d2q9_ldc", keys, spin, 4096, None, n_timed=timed)
+            line = [ln for ln in txt.splitlines() if ln.startswith('{"ref_timing"')]
+            out[name] = json.loads(line[-1]) if line else {"error": txt[-300:]}
+        except Exception as e:   # noqa: BLE001 - reported, not fatal
+            out[name] = {"error": str(e)[-300:]}
+    return out
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -452,11 +514,47 @@ def regrid_launches(counts: dict) -> int:
     return 4 * (ml - 1) + 10 + 40
 
 
+def error_vs_fp64(wl: str, steps: int, device: int) -> dict:
+    """rho and u of the workload in FP32 and in FP16 weight-offset storage
+    against the same case in FP64 after `steps` coarse steps (regrids
+    included), all runs of this library.  The meshes may differ (each run
+    refines on its own solution), so the fields are compared on the uniform
+    grid of the finest level over the whole domain, prepared as the
+    reference's M_Advance_PrintData prepares its output: relative L2 norms
+    over every cell."""
+    ww = dict(WORKLOADS[wl])
+    fields = {}
+    for name, st in (("fp64", _lib.STORE_FP64), ("fp32", _lib.STORE_FP32), ("fp16", _lib.STORE_FP16)):
+        w = dict(ww, storage=st)
+        p = make_params(w, device=device, N_PRINT_LEVELS=w["levels"], VOL_I_MIN=0, VOL_I_MAX=w["Nx"],
+                        VOL_J_MIN=0, VOL_J_MAX=w["Nx"])
+        with ag.Case(p) as c:
+            c.set_ic(0)
+            c.refine_near_wall()
+            c.advance_n(steps, use_graph=True)
+            c.sync()
+            fields[name] = (c.render_prepared(), c.counts()["n_ids"][: w["levels"]])
+    ref, ref_blocks = fields["fp64"]
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    out = {"workload": wl, "coarse_steps": steps, "grid": "uniform, finest level, whole domain",
+           "blocks_per_level_fp64": ref_blocks}
+    for name in ("fp32", "fp16"):
+        f, blocks = fields[name]
+        u = np.stack([f["u"], f["v"]])
+        uref = np.stack([ref["u"], ref["v"]])
+        out[name] = {"rho_rel_l2": rel(f["rho"], ref["rho"]), "u_rel_l2": rel(u, uref),
+                     "blocks_per_level": blocks}
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=30, help="timed steps (regrid periods of the AMR workload)")
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", default="amr_ldc2d_128_fp16", choices=sorted(WORKLOADS))
     ap.add_argument("--plain-workload", default="amr_ldc2d_128", choices=sorted(WORKLOADS),
@@ -464,6 +562,8 @@ def main(argv=None) -> int:
     ap.add_argument("--roofline-workload", default=None, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--error-steps", type=int, default=20000,
+                    help="coarse steps of the FP32/FP16-vs-FP64 error runs (0 skips them)")
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
     ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3, 4, 5],
@@ -492,7 +592,9 @@ def main(argv=None) -> int:
         return 0
     ws, rank, local = dist_setup()
     threads = os.cpu_count() or 1
-    base = {"metric": "MLUPS (lattice cell updates per second / 1e6), one coarse time step per step",
+    per = coarse_per_step(w)
+    base = {"metric": "MLUPS (lattice cell updates per second / 1e6); one step = one regrid period of "
+                      f"{per} coarse time steps including its refinement",
             "unit": "MLUPS", "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": DTYPE_NAME[w["storage"]], "data": "synthetic (fluid at rest, lid-driven)"}
@@ -502,20 +604,23 @@ def main(argv=None) -> int:
         cfg = {"workload": wl, "desc": ww["desc"]}
         if ww.get("amr"):
             cfg.update(base_grid=f"{ww['Nx']}^2", levels=ww["levels"], regrid_every=ww["p_refine"],
-                       spinup_steps=ww["spinup"])
+                       coarse_steps_per_step=coarse_per_step(ww), spinup_steps=ww["spinup"])
         cfg.update(extra)
         return cfg
 
     if a.impl == "reference":
-        # The reference algorithm on the host cores; other ranks idle.
+        # The reference algorithm on the host cores, plus the reference's own
+        # CUDA build; other ranks idle.  Nothing of agal_b200's native code.
         if rank != 0:
             return 0
-        cb = run_cpu_oracle(w, seconds=1e9, threads=threads, max_steps=a.steps)
+        steps = a.steps * per
+        cb = run_cpu_oracle(w, seconds=1e9, threads=threads, max_steps=steps)
         line = dict(base, impl="reference", value=cb["value"], ms_per_step=None,
                     config=config_of(a.workload, {"parallelism": "host OpenMP", "l2": "n/a (CPU)"}),
                     cpu_baseline=cb, e2e={"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0})
         line["n_gpus"] = 0
+        line["reference_cuda"] = reference_cuda()
         print(json.dumps(line), flush=True)
         return 0
 
@@ -544,48 +649,48 @@ def main(argv=None) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    def device_timed(wl: str, with_clocks: bool):
+    def device_timed(wl: str, with_clocks: bool, steps: int):
         ww = WORKLOADS[wl]
         case = ag.Case(make_params(ww, device=local))
         develop(case, ww)
         tune = case.autotune(0, reps=10)
         step = step_fn(case, ww)
+        flush = state_bytes(case, ww) * 2 < L2_BYTES
+        clk = ClockSampler(local) if with_clocks else None
+        if clk:
+            clk.__enter__()
+            time.sleep(1.0)   # nvidia-smi is sampling before the warm-up starts
         for _ in range(a.warmup):
             step()
         case.sync()
-        flush = state_bytes(case, ww) * 2 < L2_BYTES
         barrier()
         torch.cuda.synchronize()
-        it0 = case.refine_stats()["iter"]
-        if with_clocks:
-            with ClockSampler(local) as clk:
-                per_step, cells, launches = time_steps(case, torch, ww, a.steps, flush)
+        it0 = case.refine_stats()
+        per_step, cells, launches = time_steps(case, torch, ww, steps, flush)
+        it1 = case.refine_stats()
+        clocks = None
+        if clk:
+            clk.__exit__(None, None, None)
             clocks = clk.summary()
-        else:
-            per_step, cells, launches = time_steps(case, torch, ww, a.steps, flush)
-            clocks = None
-        if ww.get("amr"):
-            p_ref = ww["p_refine"]
-            regrids = sum(1 for i in range(it0, it0 + a.steps) if (i + 1) % p_ref == 0 and i > 0)
-            launches += regrids * regrid_launches(case.counts())
         counts = case.counts()
         barrier()
         t_ms = allmax(sum(per_step))
         mlups = allsum(float(sum(cells))) / (t_ms * 1e-3) / 1e6
         case.close()
-        return dict(value=mlups, ms_per_step=t_ms / a.steps, flush=flush, tune=tune, clocks=clocks,
-                    launches=launches, counts=counts, cells_per_step=float(np.mean(cells)))
+        regrids = (it1["iter"] - it0["iter"]) // ww["p_refine"] if ww.get("amr") else 0
+        return dict(value=mlups, ms_per_step=t_ms / steps, flush=flush, tune=tune, clocks=clocks,
+                    launches=launches, counts=counts, cells_per_step=float(np.mean(cells)), regrids=regrids,
+                    ms_per_coarse_step=t_ms / steps / coarse_per_step(ww))
 
-    def learned_timed(wl: str, wl_src: str):
+    def learned_timed(wl: str, wl_src: str, steps: int):
         """The workload with the learned predictor driving its refinement: the
         network is trained on the GPU on snapshots of the plain FP32 run's
         spin-up (labelled by the percentile rule), then predicts the marks of
         every regrid of a fresh run, the rule judging every 4th regrid."""
         ww, ws_ = WORKLOADS[wl], WORKLOADS[wl_src]
-        dim = DIM_OF[ww["velocity_set"]]
         t0 = time.perf_counter()
         src = ag.Case(make_params(ws_, device=local))
-        m = ag.Learner(dim, seed=7)
+        m = ag.Learner(DIM_OF[ww["velocity_set"]], seed=7)
         m.attach(src, 1)
         develop(src, ws_)
         src.sync()
@@ -609,7 +714,7 @@ def main(argv=None) -> int:
         c0 = m.counts()
         barrier()
         torch.cuda.synchronize()
-        per_step, cells, launches = time_steps(case, torch, ww, a.steps, flush)
+        per_step, cells, launches = time_steps(case, torch, ww, steps, flush)
         c1 = m.counts()
         counts = case.counts()
         barrier()
@@ -618,68 +723,110 @@ def main(argv=None) -> int:
         m.attach(case, 0)
         case.close()
         m.close()
-        return dict(workload=wl, value=mlups, ms_per_step=t_ms / a.steps, snapshots=nl, class_weights=weights,
+        return dict(workload=wl, value=mlups, ms_per_step=t_ms / steps, snapshots=nl, class_weights=weights,
                     train_loss=loss, thresholds=thr, collect_and_train_s=train_s,
                     regrids=c1["regrids"] - c0["regrids"], judged=c1["judged"] - c0["judged"],
                     plain_refine_marks=c1["plain_refine"] - c0["plain_refine"],
                     missed=c1["missed"] - c0["missed"], blocks_per_level=counts["n_ids"][:-1],
                     cell_updates_per_step=float(np.mean(cells)), tune=tune)
 
-    # --- device-timed steps: headline workload, then the plain FP32 form -------
-    head = device_timed(a.workload, with_clocks=True)
-    learned = learned_timed(a.workload, a.plain_workload) if WORKLOADS[a.workload].get("amr") else None
-    plain = device_timed(a.plain_workload, with_clocks=False) if a.plain_workload != a.workload else None
+    def e2e_timed(wl: str, variant: int, steps: int) -> dict:
+        """The same steps through the public C ABI with host buffers."""
+        ww = WORKLOADS[wl]
+        case = ag.Case(make_params(ww, device=local))
+        develop(case, ww)
+        case.set_tuning(variant)
+        f0 = case.dump(_lib.ARR_F)
+        host_in = torch.from_numpy(f0).pin_memory().numpy()
+        host_out = torch.empty(f0.shape, dtype=torch.float64).pin_memory().numpy()
+        mm = torch.zeros((steps, 4), dtype=torch.float64).pin_memory().numpy()
+        lib = _lib.lib()
+        dim = DIM_OF[ww["velocity_set"]]
+        k = coarse_per_step(ww)
+        amr = bool(ww.get("amr"))
+        cells = 0
+        barrier()
+        t0 = time.perf_counter()
+        rc = lib.agal_load(case._h, _lib.ARR_F, host_in.ctypes.data_as(C.c_void_p), host_in.nbytes)
+        for i in range(steps):
+            cells += k * leaf_cells(case.counts(), dim)
+            rc |= lib.agal_advance_n(case._h, k, 1) if amr else lib.agal_advance(case._h, 0)
+            rc |= lib.agal_mass_momentum_async(case._h, mm[i].ctypes.data_as(C.c_void_p))
+        rc |= lib.agal_dump(case._h, _lib.ARR_F, host_out.ctypes.data_as(C.c_void_p), host_out.nbytes)
+        rc |= lib.agal_sync(case._h)
+        dt = time.perf_counter() - t0
+        if rc:
+            raise RuntimeError("e2e run failed: " + case._lib.agal_last_error(case._h).decode())
+        dt = allmax(dt)
+        case.close()
+        drift = float(np.abs(mm[:, 0] - mm[0, 0]).max() / mm[0, 0])
+        return {"value": allsum(float(cells)) / dt / 1e6, "unit": "MLUPS",
+                "h2d_bytes_per_step": int(host_in.nbytes / steps),
+                "d2h_bytes_per_step": int(host_out.nbytes / steps) + 8 * 4,
+                "wall_ms_per_step": dt * 1e3 / steps, "mass_rel_drift": drift}
 
-    # --- end to end through the C ABI with host buffers ----------------------
-    case = ag.Case(make_params(w, device=local))
-    develop(case, w)
-    case.set_tuning(head["tune"]["variant"])
-    f0 = case.dump(_lib.ARR_F)
-    pinned = torch.from_numpy(f0).pin_memory()
-    host_in = pinned.numpy()
-    host_out = torch.empty_like(pinned).pin_memory().numpy()
-    mm = (C.c_double * 4)()
-    lib = _lib.lib()
-    dim = DIM_OF[w["velocity_set"]]
-    amr = bool(w.get("amr"))
-    e2e_cells = 0
-    barrier()
-    t0 = time.perf_counter()
-    rc = lib.agal_load(case._h, _lib.ARR_F, host_in.ctypes.data_as(C.c_void_p), host_in.nbytes)
-    for _ in range(a.steps):
-        e2e_cells += leaf_cells(case.counts(), dim)
-        rc |= lib.agal_advance_n(case._h, 1, 1) if amr else lib.agal_advance(case._h, 0)
-        rc |= lib.agal_mass_momentum(case._h, mm)   # D2H of the step's FP64 mass/momentum
-    rc |= lib.agal_dump(case._h, _lib.ARR_F, host_out.ctypes.data_as(C.c_void_p), host_out.nbytes)
-    e2e_s = time.perf_counter() - t0
-    if rc:
-        raise RuntimeError("e2e run failed")
-    e2e_s = allmax(e2e_s)
-    case.close()
-    e2e = {"value": allsum(float(e2e_cells)) / e2e_s / 1e6, "unit": "MLUPS",
-           "h2d_bytes_per_step": int(host_in.nbytes / a.steps),
-           "d2h_bytes_per_step": int(host_out.nbytes / a.steps) + 8 * (dim + 1)}
-
-    # --- roofline of the fused step kernel on a large case -------------------
-    rwl = a.roofline_workload or ROOFLINE_FOR.get(w["storage"], "ldc2d_8192")
-    rw = WORKLOADS[rwl]
-    rcase = ag.Case(make_params(rw, device=local))
-    rcase.set_ic(0)
-    rtune = rcase.autotune(0, reps=5)
-    for _ in range(3):
-        rcase.advance()
-    rcase.sync()
-    rt, rcells, _ = time_steps(rcase, torch, rw, 20, flush=False)
-    rcase.close()
-    avg_ms = sum(rt) / len(rt)
-    alg_bytes = 2 * Q_OF[rw["velocity_set"]] * ESIZE[rw["storage"]] * rcells[0]
-    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
-    peak, peak_kind = measured_peak_hbm()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+    def roofline_of(rwl: str) -> dict:
+        rw = WORKLOADS[rwl]
+        rcase = ag.Case(make_params(rw, device=local))
+        rcase.set_ic(0)
+        rtune = rcase.autotune(0, reps=5)
+        for _ in range(3):
+            rcase.advance()
+        rcase.sync()
+        rt, rcells, _ = time_steps(rcase, torch, rw, 20, flush=False)
+        rcase.close()
+        avg_ms = sum(rt) / len(rt)
+        alg_bytes = 2 * Q_OF[rw["velocity_set"]] * ESIZE[rw["storage"]] * rcells[0]
+        achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+        peak, peak_kind = measured_peak_hbm()
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": dram_traffic_per_launch(rwl), "peak_source": peak_kind,
-                "kernel": "k_step (fused collide+BC+stream) + its stream-guard fix-up",
+                "kernel": "fused collide+BC+stream step (autotuned variant) + its stream-guard fix-up",
                 "workload": rwl, "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "autotune": rtune}
+
+    # --- device-timed steps: headline workload, learned, plain FP32 --------
+    head = device_timed(a.workload, with_clocks=True, steps=a.steps)
+    learned = learned_timed(a.workload, a.plain_workload, a.steps) if w.get("amr") else None
+    plain = device_timed(a.plain_workload, with_clocks=False, steps=a.steps) \
+        if a.plain_workload != a.workload else None
+    # the reference's own criterion, timed like the reference harness times
+    # it (coarse steps after the spin-up, no regrid in the window)
+    ref_rule = None
+    if w.get("amr"):
+        wr = WORKLOADS["amr_ldc2d_128_log2"]
+        c = ag.Case(make_params(wr, device=local))
+        develop(c, wr)
+        c.autotune(0, reps=5)
+        c.sync()
+        st = torch.cuda.ExternalStream(c.stream_ptr())
+        cells, ms_tot, n_t = 0, 0.0, 0
+        for _ in range(20):
+            # the first 63 coarse steps of a period (no refinement turn) timed,
+            # then the 64th with its regrid untimed
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            cells += (wr["p_refine"] - 1) * leaf_cells(c.counts(), 2)
+            e0.record(st)
+            c.advance_n(wr["p_refine"] - 1, use_graph=True)
+            e1.record(st)
+            c.advance_n(1, use_graph=True)
+            c.sync()
+            ms_tot += e0.elapsed_time(e1)
+            n_t += wr["p_refine"] - 1
+        ref_rule = {"workload": "amr_ldc2d_128_log2", "coarse_steps": n_t, "ms": ms_tot,
+                    "value": cells / (ms_tot * 1e-3) / 1e6, "blocks_per_level": c.counts()["n_ids"][:-1],
+                    "timed_like": "the reference harness: coarse steps after the spin-up, no refinement turn"}
+        c.close()
+
+    # --- end to end through the C ABI with host buffers ----------------------
+    e2e = e2e_timed(a.workload, head["tune"]["variant"], a.steps)
+
+    # --- roofline of the fused step kernel on large cases --------------------
+    roofline = roofline_of(a.roofline_workload or ROOFLINE_FOR.get(w["storage"], "ldc2d_8192"))
+    roofline_fp32 = roofline_of(ROOFLINE_FOR[_lib.STORE_FP32]) if w["storage"] != _lib.STORE_FP32 else None
+
+    # --- precision: FP32 / FP16 against FP64 on the headline case ----------
+    errors = error_vs_fp64(a.workload, a.error_steps, local) if (a.error_steps > 0 and w.get("amr")) else None
 
     # --- batched independent cases vs the same cases one at a time -----------
     batched = None
@@ -695,15 +842,18 @@ def main(argv=None) -> int:
         dist.destroy_process_group()
     if rank == 0:
         extra = {"parallelism": f"replicas x{ws}",
-                 "l2": "flushed between timed steps" if head["flush"] else "inputs larger than L2",
+                 "l2": "flushed before every timed step" if head["flush"] else "inputs larger than L2",
                  "autotune": head["tune"], "blocks_per_level": head["counts"]["n_ids"][:-1],
-                 "cell_updates_per_step": head["cells_per_step"]}
+                 "cell_updates_per_step": head["cells_per_step"], "regrids_timed": head["regrids"],
+                 "ms_per_coarse_step": head["ms_per_coarse_step"]}
         line = dict(base, value=head["value"], ms_per_step=head["ms_per_step"],
                     config=config_of(a.workload, extra), e2e=e2e, roofline=roofline, cpu_baseline=cpu,
                     clocks=head["clocks"], gpu_launches=head["launches"])
+        if roofline_fp32 is not None:
+            line["roofline_fp32"] = roofline_fp32
         if plain is not None:
             line["plain_fp32"] = {"workload": a.plain_workload, "value": plain["value"],
-                                  "ms_per_step": plain["ms_per_step"],
+                                  "ms_per_step": plain["ms_per_step"], "regrids_timed": plain["regrids"],
                                   "blocks_per_level": plain["counts"]["n_ids"][:-1],
                                   "ratio": head["value"] / plain["value"]}
         if learned is not None:
@@ -712,6 +862,10 @@ def main(argv=None) -> int:
             if plain is not None:
                 learned["ratio_vs_plain_fp32"] = learned["value"] / plain["value"]
             line["learned"] = learned
+        if ref_rule is not None:
+            line["reference_rule_fp32"] = ref_rule
+        if errors is not None:
+            line["error_vs_fp64"] = errors
         if batched is not None:
             line["batched"] = batched
         print(json.dumps(line), flush=True)

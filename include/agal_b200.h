@@ -380,8 +380,18 @@ int agal_dump(agal_ctx *ctx, int which, void *host_buf, size_t bytes);
 int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
 
 /* FP64 sums over every fluid leaf cell: out[0] = mass, out[1..dim] = momentum.
-   Reads the macros of agal_refresh-free state (computes them itself). */
+   Reads the macros of agal_refresh-free state (computes them itself).  The
+   partial sums are reduced on the device in a fixed order (deterministic).
+   No reference counterpart (the reference has no global conservation check;
+   its per-cell macros are S_ComputeProperties, solver_lbm_compute.cu:5). */
 int agal_mass_momentum(agal_ctx *ctx, double *out);
+/* The same sums enqueued on the context's stream without waiting: out[0..3]
+   (four doubles; out[3] = 0 in 2D) is written when the stream reaches the
+   copy, so it is valid after agal_sync.  Pass pinned host memory
+   (cudaHostAlloc / cudaHostRegister) for an asynchronous copy; with pageable
+   memory the copy waits.  Successive calls may share one buffer only if the
+   caller reads it in between. */
+int agal_mass_momentum_async(agal_ctx *ctx, double *out);
 
 /* Same sums as agal_mass_momentum, for callers that must not allocate device
    memory (a memory-capped serving process, a pool that is fully reserved, a

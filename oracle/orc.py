@@ -80,6 +80,52 @@ def lib() -> C.CDLL:
     return _lib
 
 
+# input.txt defaults of the reference's Parser (inc/parser.h:62-144),
+# restated so that the oracle can be configured without the CUDA library
+# (bench.py's reference arm loads nothing of agal_b200's native code).
+_PARSER_INT_DEFAULTS = dict(
+    MAX_LEVELS_WALL=5, MAX_LEVELS_INTERIOR=4, N_ITER_TOTAL=10 * 64, N_LEVEL_START=0, Nx=64, N_RESTART=1,
+    G_LOADTYPE=0, G_PRINT=1, G_VIS_TREE=0, G_BIN_DENSITY=1, G_BIN_APPROACH=0, G_BIN_LEVELS=1, G_BIN_SPEC=1,
+    G_BIN_MAKE_LINKS=0, PERIODIC_X=0, PERIODIC_Y=0, PERIODIC_Z=0, S_COLLISION=0, S_INTERP=1,
+    S_INTERP_HYBRID=0, S_AVERAGE=0, S_CRITERION=0, S_LES=0, S_FORCE_ORDER=0, S_FORCE_TYPE=0, S_BC_TYPE=0,
+    P_REFINE=32, N_PROBE=0, N_PROBE_DENSITY=4, N_PROBE_FREQUENCY=32, N_PROBE_FORCE=0, N_PROBE_F_START=0,
+    N_PROBE_F_FREQUENCY=16, N_PROBE_AVE=0, N_PROBE_AVE_FREQUENCY=1, N_PROBE_AVE_START=100 * 64,
+    N_PRINT_LEVELS=2, N_PRINT_LEVELS_VTHB=0, N_PRINT_LEVELS_PATCH=2, N_PRINT_LEVELS_IMAGE=2, P_OUTPUT=1 * 64,
+    N_OUTPUT=10, N_OUTPUT_START=0, VOL_I_MIN=0, VOL_I_MAX=64, VOL_J_MIN=0, VOL_J_MAX=64, VOL_K_MIN=0,
+    VOL_K_MAX=64, USE_CPU=1)
+_PARSER_DBL_DEFAULTS = dict(
+    L_c=1.0, L_fy=1.0, L_fz=1.0, v0=1.5625e-5, G_NEAR_WALL_DISTANCE=0.05, s1=1.19, s2=1.40, s3=1.20, s4=1.20,
+    s5=1.20, s6=1.98, V_PROBE_TOL=1e-4, N_REFINE_START=-3.0, N_REFINE_INC=1.0, N_REFINE_MAX=1.0,
+    S_FORCEVOLUME_Xm=0.0, S_FORCEVOLUME_XM=0.0, S_FORCEVOLUME_Ym=0.0, S_FORCEVOLUME_YM=0.0,
+    S_FORCEVOLUME_Zm=0.0, S_FORCEVOLUME_ZM=0.0)
+_PARSER_STR_DEFAULTS = dict(I_DIR_NAME="../input/", P_DIR_NAME="../out/TEST_UPLOAD/",
+                            G_FILENAME="bunny_ascii.stl")
+
+
+def default_params(**kw):
+    """agal_params with the reference's input.txt defaults and the solver
+    selections of its shipped build (D2Q9 BGK, cubic interpolation, main.cu:55;
+    FP32; no hook preset; u_ref = the custom.h literal 0.05), then ``kw``.
+    Field for field what agal_params_default gives (tests/test_abi.py)."""
+    from agal_b200._lib import AgalParams   # the Python structure only
+    p = AgalParams()
+    for k, v in _PARSER_INT_DEFAULTS.items():
+        setattr(p, k, v)
+    for k, v in _PARSER_DBL_DEFAULTS.items():
+        setattr(p, k, v)
+    for k, v in _PARSER_STR_DEFAULTS.items():
+        setattr(p, k, v.encode())
+    p.velocity_set, p.collision, p.interp_order, p.storage = 0, 0, 2, 0
+    p.bc_preset = p.ic_preset = p.region_preset = 0
+    p.ref_pct_hi, p.ref_pct_lo, p.u_ref, p.ic_noise, p.seed = 0.9, 0.5, 0.05, 0.0, 0
+    p.n_maxcblocks, p.mem_frac, p.device = 0, 0.975, -1
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v.encode() if isinstance(v, str) else v)
+    return p
+
+
 class OracleCase:
     """CPU oracle case with the same array selectors as agal_b200.Case."""
 

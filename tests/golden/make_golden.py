@@ -2,7 +2,7 @@
 """Generate the golden fixtures that pin the oracle and the CUDA library to
 the reference (KhodrJ/AGAL).
 
-    python tests/golden/make_golden.py tables [--ref /root/reference]
+    python tests/golden/make_golden.py tables [--ref DIR]   (default: $AGAL_REFERENCE_DIR)
         Extract the lattice tables (direction vectors, opposites, neighbour
         slot map, weights, block-neighbour directions) from the reference
         sources (inc/util.h:94-101, src/solver_lbm/solver_lbm_init.cu:79-91,
@@ -35,7 +35,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF_BIN = ROOT / "oracle" / "_ref"
+sys.path.insert(0, str(ROOT))
+from oracle.ref_run import BASE_KEYS, REF_BIN, run_ref, write_input  # noqa: E402,F401
 
 # Golden cases: (binary, input.txt keys, steps, keep_mb).  keep_mb is the free
 # device memory the reference sizes its block pool from; it must leave room
@@ -126,10 +127,6 @@ TIMING = {
     "ldc3d19_384": ("ref_d3q19_ldc", dict(Nx=384, v0=1.25e-4), 10, 24576),
 }
 
-BASE_KEYS = dict(MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, N_LEVEL_START=0, L_c=1.0, L_fy=1.0, L_fz=1.0,
-                 N_RESTART=0, PERIODIC_X=0, PERIODIC_Y=0, PERIODIC_Z=0, N_ITER_TOTAL=1000,
-                 S_FORCE_TYPE=2, S_BC_TYPE=0, S_CRITERION=0, N_PROBE=0, N_PROBE_FORCE=0, N_PRINT_LEVELS=0,
-                 N_PRINT_LEVELS_IMAGE=0, P_OUTPUT=100000)
 
 
 # ---------------------------------------------------------------------------
@@ -170,15 +167,6 @@ def cmd_tables(ref: Path) -> None:
 
 
 # ---------------------------------------------------------------------------
-def write_input(d: Path, keys: dict, out_dir: Path) -> None:
-    kv = dict(BASE_KEYS)
-    kv.update(keys)
-    kv["P_DIR_NAME"] = str(out_dir) + "/"
-    kv["I_DIR_NAME"] = str(d) + "/"
-    lines = [f"{k} {v}" for k, v in kv.items()]
-    (d / "input.txt").write_text("\n".join(lines) + "\n")
-
-
 LES_BINARIES = ("ref_d3q19_ldc_smag", "ref_d3q19_ldc_wale", "ref_d3q19_ldc_vreman")
 
 
@@ -254,45 +242,6 @@ def read_dump(path: Path, les: bool = False) -> dict:
             res["cells_f_X_b"] = take(np.float32, nxb).reshape(int(Qmax), mcb)
         res["Ff"] = take(np.float32, 6 * int(n_act)).reshape(int(n_act), 6)
     return res
-
-
-def run_ref(binary: str, keys: dict, steps: int, keep_mb: int, dump: Path | None, n_timed: int = 0,
-            region: int = 0, skip_last_regrid: bool = False, sphere: tuple | None = None,
-            restart: Path | None = None, uniform: Path | None = None, geometry_txt: str | None = None) -> str:
-    exe = REF_BIN / binary
-    if not exe.exists():
-        raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref` first")
-    with tempfile.TemporaryDirectory() as td:
-        td = Path(td)
-        (td / "out").mkdir()
-        write_input(td, keys, td / "out")
-        if sphere is not None:
-            sys.path.insert(0, str(ROOT))
-            from agal_b200.geometry import icosphere, write_stl_ascii
-            (td / "geometry").mkdir()
-            write_stl_ascii(td / "geometry" / keys["G_FILENAME"], icosphere(*sphere))
-        if geometry_txt is not None:
-            (td / "geometry.txt").write_text(geometry_txt)
-        cmd = [str(exe), str(td) + "/", str(dump) if dump else "-", str(steps), str(keep_mb), str(n_timed)]
-
-        def big_stack():
-            # M_Init builds the padded root grid as a stack VLA
-            # (mesh_init.cu:332): ~50 MB at 8192^2.
-            import resource
-            resource.setrlimit(resource.RLIMIT_STACK, (1 << 30, resource.RLIM_INFINITY))
-
-        env = dict(os.environ, REF_REGION=str(region), REF_SKIP_LAST_REGRID="1" if skip_last_regrid else "0",
-                   REF_GEOM="1" if (sphere is not None or geometry_txt is not None) else "0", REF_RESTART="1" if restart is not None else "0",
-                   REF_UNIFORM="1" if uniform is not None else "0")
-        r = subprocess.run(cmd, cwd=td, capture_output=True, text=True, timeout=900, preexec_fn=big_stack,
-                           env=env)
-        if r.returncode != 0:
-            raise RuntimeError(f"{binary} failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
-        if restart is not None:
-            restart.write_bytes((td / "out" / "restart.bin").read_bytes())
-        if uniform is not None:
-            uniform.write_bytes((td / "out" / "out_direct.dat").read_bytes())
-        return r.stdout
 
 
 def cmd_ref(out: Path, only: list[str] | None) -> None:
@@ -416,7 +365,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("tables")
-    t.add_argument("--ref", default="/root/reference")
+    t.add_argument("--ref", default=os.environ.get("AGAL_REFERENCE_DIR", "/root/reference"))
     r = sub.add_parser("ref")
     r.add_argument("--out", default=str(HERE))
     r.add_argument("--only", nargs="*")

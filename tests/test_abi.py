@@ -55,6 +55,17 @@ def test_defaults_match_parser():
     assert p.I_DIR_NAME == b"../input/" and p.G_FILENAME == b"bunny_ascii.stl"
 
 
+def test_oracle_defaults_equal_library_defaults():
+    """The oracle's restated defaults (used where the CUDA library must not be
+    loaded) equal agal_params_default field for field."""
+    import agal_b200 as ag
+    from agal_b200 import _lib
+    from oracle.orc import default_params as orc_default
+    a, b = ag.default_params(), orc_default()
+    for name, _ in _lib.AgalParams._fields_:
+        assert getattr(a, name) == getattr(b, name), name
+
+
 def test_params_read_nx_factors(tmp_path, capfd):
     import agal_b200 as ag
     (tmp_path / "input.txt").write_text(

@@ -330,3 +330,35 @@ def test_tile_step_refused_swaps_bit_identical():
             out.append(F)
     assert neg > 0, "the case did not produce a non-positive population"
     assert np.array_equal(out[0], out[1])
+
+
+def test_mass_momentum_async_equals_sync():
+    """The enqueued FP64 sums land in host memory after sync and equal the
+    blocking call's (same kernels, fixed reduction order)."""
+    p = ldc_params(19, 16, storage=_lib.STORE_FP16)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        c.advance_n(12, use_graph=True)
+        out = np.full(4, np.nan)
+        c.mass_momentum_async(out)
+        c.sync()
+        ref = c.mass_momentum()
+        assert np.array_equal(out[:4], ref)
+        assert abs(out[0] - 16 ** 3) < 1e-6 * 16 ** 3
+
+
+@pytest.mark.parametrize("storage", [_lib.STORE_FP16, _lib.STORE_FP32])
+def test_dump_load_round_trip_many_chunks(storage):
+    """Device-side layout conversion through the staging buffer over several
+    chunks (65,536 blocks): dump -> load into a fresh case -> dump is the
+    identity, and both cases then step bit for bit alike."""
+    p = ldc_params(9, 1024, storage=storage)
+    with ag.Case(p) as a, ag.Case(p) as b:
+        a.set_ic(0)
+        a.advance_n(5, use_graph=True)
+        Fa = a.dump(_lib.ARR_F)
+        b.load(_lib.ARR_F, Fa)
+        assert np.array_equal(b.dump(_lib.ARR_F), Fa)
+        a.advance_n(3, use_graph=True)
+        b.advance_n(3, use_graph=True)
+        assert np.array_equal(a.dump(_lib.ARR_F), b.dump(_lib.ARR_F))

@@ -22,6 +22,7 @@ D2Q9, D3Q19, D3Q27 = 0, 1, 2
 BGK, MRT = 0, 2
 INTERP_LINEAR, INTERP_CUBIC = 0, 2
 STORE_FP32, STORE_FP64, STORE_FP16, STORE_BF16 = 0, 1, 2, 3
+ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
 BC_NONE, BC_LDC2D, BC_LDC3D, BC_FPSC2D, BC_FPSC3D = 0, 1, 2, 3, 4
 IC_REST, IC_UNIFORM = 0, 1
 REGION_NONE, REGION_BOUNDARY, REGION_BOX = 0, 1, 2
@@ -61,7 +62,8 @@ class AgalParams(C.Structure):
                  ("storage", C.c_int), ("bc_preset", C.c_int), ("ic_preset", C.c_int),
                  ("region_preset", C.c_int), ("ref_pct_hi", C.c_double), ("ref_pct_lo", C.c_double),
                  ("u_ref", C.c_double), ("ic_noise", C.c_double), ("seed", C.c_uint64),
-                 ("n_maxcblocks", C.c_int64), ("mem_frac", C.c_double), ("device", C.c_int)])
+                 ("n_maxcblocks", C.c_int64), ("mem_frac", C.c_double), ("device", C.c_int),
+                 ("half_rounding", C.c_int)])
 
 
 # (name, restype, argtypes) of every exported entry point.

@@ -118,6 +118,7 @@ extern "C" int agal_params_default(agal_params *p)
     p->n_maxcblocks = 0;
     p->mem_frac = 0.975;                   // mesh.h:481 M_FRAC
     p->device = -1;
+    p->half_rounding = AGAL_ROUND_STOCHASTIC;
     return AGAL_OK;
 }
 

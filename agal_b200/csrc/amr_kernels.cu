@@ -81,6 +81,12 @@ __host__ __device__ constexpr double lag_w(int a, int m)
     return r;
 }
 
+// Seed of a transfer launch: the coarse-step counter and the launch's salt.
+__device__ __forceinline__ unsigned transfer_seed(int sr, const unsigned *ctr, unsigned salt)
+{
+    return sr ? (*ctr) * 0x9E3779B9u + salt * 0x85EBCA77u + 0x27D4EB2Fu : 0u;
+}
+
 struct InterpArgs {
     const int *ids;
     int n;
@@ -90,6 +96,10 @@ struct InterpArgs {
     const int *bmask, *ref, *cmask;
     double ratio;          // tau_{L+1} / tau_L in the compute type
     int var;               // AGAL_INTERP_INTERFACE / AGAL_INTERP_ADDED
+    // stochastic rounding of half-precision offsets (step_common.cuh)
+    int sr;
+    const unsigned *sr_ctr;
+    unsigned sr_salt;
 };
 
 template <int DIM, int Q, typename T, bool CUBIC>
@@ -147,6 +157,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     const int ci = ch & 1, cj = (ch >> 1) & 1, ck = (ch >> 2) & 1;
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     const long long cell = (long long)(bc + ch) * BLK + t;
+    const unsigned rnd = a.sr ? sr_cell((long long)(bc + ch) * MC + t, transfer_seed(a.sr, a.sr_ctr, a.sr_salt)) : 0u;
 #pragma unroll 1
     for (int p = 0; p < Q; p++) {
         const C *F = sF[p];
@@ -190,7 +201,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
                 }
             }
         }
-        fc[cell + lat_pb(DIM, p) * MC] = ST<T>::enc(val);
+        fc[cell + lat_pb(DIM, p) * MC] = enc_r<T>(val, rnd * sr_dir(p), a.sr);
     }
 }
 
@@ -202,7 +213,11 @@ struct AverageArgs {
     const int *nbr_child, *bmask, *cmask;
     double ratio;          // tau_L / tau_{L+1} in the compute type
     int var;               // AGAL_AVERAGE_INTERFACE / _BLOCK / _GRID
+    int sr;
+    const unsigned *sr_ctr;
+    unsigned sr_salt;
 };
+
 
 template <int DIM, int Q, typename T>
 __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const AverageArgs a)
@@ -234,6 +249,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     const int qd = (I >= 2 ? 1 : 0) + (J >= 2 ? 2 : 0) + ((DIM == 3 && K >= 2) ? 4 : 0);
     const int c0 = 2 * (I & 1) + 8 * (J & 1) + (DIM == 3 ? 32 * (K & 1) : 0);
     T *fp = static_cast<T *>(a.fpar) + (long long)b * BLK + tid;
+    const unsigned rnd = (a.sr && tid < MC) ? sr_cell((long long)b * MC + tid, transfer_seed(a.sr, a.sr_ctr, a.sr_salt)) : 0u;
     for (int p = 0; p < Q; p++) {
         const int slot = lat_pb(DIM, p);
         C *buf = sg[p & 1];
@@ -250,7 +266,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
             C val;
             if (DIM == 2) val = C(0.25) * (s[0] + s[1] + s[4] + s[5]);
             else val = C(0.125) * (s[0] + s[1] + s[4] + s[5] + s[16] + s[17] + s[20] + s[21]);
-            fp[slot * MC] = ST<T>::enc(val);
+            fp[slot * MC] = enc_r<T>(val, rnd * sr_dir(p), a.sr);
         }
     }
 }
@@ -577,6 +593,10 @@ template <int DIM, int Q, typename T> struct RunInterp {
         InterpArgs a;
         a.ids = c->id_set + (long long)L * c->nmb;
         a.n = n;
+        a.sr = (c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
+               c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
+        a.sr_ctr = c->d_sr;
+        a.sr_salt = (unsigned)c->sr_salt | 0x40000000u;
         // Interface interpolation touches the interface parents only.
         if (var == AGAL_INTERP_INTERFACE && (int)c->iface_n.size() > L) {
             a.ids = c->iface_ids + c->iface_off[L];
@@ -610,6 +630,10 @@ template <int DIM, int Q, typename T> struct RunAverage {
         AverageArgs a;
         a.ids = c->id_set + (long long)L * c->nmb;
         a.n = n;
+        a.sr = (c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
+               c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
+        a.sr_ctr = c->d_sr;
+        a.sr_salt = (unsigned)c->sr_salt | 0x80000000u;
         // Interface and block averaging touch the interface parents only.
         if (var != AGAL_AVERAGE_GRID && (int)c->iface_n.size() > L) {
             a.ids = c->iface_ids + c->iface_off[L];

@@ -126,6 +126,10 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "collision operator: BGK, or MRT with D3Q19");
     }
     if (p->S_LES < 0 || p->S_LES > 3) { delete c; return agal_set_err(nullptr, AGAL_ERR_PARAM, "S_LES: 0..3"); }
+    if (p->half_rounding != AGAL_ROUND_STOCHASTIC && p->half_rounding != AGAL_ROUND_NEAREST) {
+        delete c;
+        return agal_set_err(nullptr, AGAL_ERR_PARAM, "half_rounding");
+    }
     if (p->S_LES > 0 && (p->collision != AGAL_BGK || std::max(p->MAX_LEVELS_WALL, p->MAX_LEVELS_INTERIOR) != 1 ||
                          p->S_BC_TYPE != 0)) {
         delete c;
@@ -259,6 +263,7 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
     }
 #undef ALLOC
     cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);
+    c->d_sr = reinterpret_cast<unsigned *>(c->d_status + 2);
     cudaMemsetAsync(c->fix_count, 0, sizeof(int) * 4, c->stream);
 
     // Reset values, mesh_init.cu:285-304.
@@ -645,22 +650,44 @@ static int advance_rec(agal_ctx *c, int L)
     return AGAL_OK;
 }
 
+namespace {
+__global__ void k_sr_tick(unsigned *ctr) { *ctr += 1u; }
+__global__ void k_sr_set(unsigned *ctr, unsigned v) { *ctr = v; }
+}  // namespace
+
+int agal_sr_tick(agal_ctx *c)
+{
+    k_sr_tick<<<1, 1, 0, c->stream>>>(c->d_sr);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
+int agal_sr_set(agal_ctx *c, unsigned value)
+{
+    k_sr_set<<<1, 1, 0, c->stream>>>(c->d_sr, value);
+    AGAL_CUDA(c, cudaGetLastError());
+    return AGAL_OK;
+}
+
 extern "C" int agal_advance(agal_ctx *c, int L)
 {
     if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;
-    return advance_rec(c, L);
+    c->sr_salt = 0;
+    int rc = advance_rec(c, L);
+    return rc ? rc : agal_sr_tick(c);
 }
 
 // One coarse step of M_Advance_Step (mesh_advance.cu:156-182): 2^N_LEVEL_START
-// sub-steps from the starting level.
+// sub-steps from the starting level, then the tick of the rounding counter.
 int agal_record_coarse_step(agal_ctx *c)
 {
     const int mult = 1 << c->L0;
+    c->sr_salt = 0;
     for (int j = 0; j < mult; j++) {
         int rc = advance_rec(c, c->L0);
         if (rc) return rc;
     }
-    return AGAL_OK;
+    return agal_sr_tick(c);
 }
 
 static int capture(agal_ctx *c, int steps, cudaGraphExec_t *out)

@@ -78,6 +78,12 @@ struct agal_ctx {
     int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
+    // Stochastic rounding of half-precision offsets: the coarse-step counter
+    // in device memory (d_status[2]; one tick per coarse step, equal to iter
+    // under agal_advance_n and restored by restart loads) and the ordinal of
+    // the next step launch within the coarse step being recorded.
+    unsigned *d_sr = nullptr;
+    int sr_salt = 0;
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
     int *blk_solid = nullptr;          // [nmb] 1 = the block holds a solid cell (geometry cases)
     int *tiles = nullptr;              // root-level tile table of the 2D tile step (step_tile.cu)
@@ -178,6 +184,10 @@ void agal_drop_graphs(agal_ctx *c);         // after any change of the mesh or l
 // One coarse step's launches on the context's stream (flips cur[] as it
 // records), and the buffer-parity bookkeeping of replaying `steps` of them.
 int agal_record_coarse_step(agal_ctx *c);
+// Advance the device coarse-step counter of the stochastic rounding by one
+// (stream-ordered), or set it.
+int agal_sr_tick(agal_ctx *c);
+int agal_sr_set(agal_ctx *c, unsigned value);
 void agal_advance_parity(agal_ctx *c, int steps);
 // Populations of the first nb blocks in the reference's slot-major layout
 // (restart I/O without copying the whole pool).

@@ -266,7 +266,9 @@ int load_as(agal_ctx *c, FILE *f, int *iter)
     // at the next one (M_Advance_LoadRestartFile, mesh_advance.cu:124-134).
     c->iter = (long long)it + 1;
     if (iter) *iter = it;
-    return AGAL_OK;
+    // The stochastic-rounding counter of a run advanced by agal_advance_n is
+    // its coarse-step count: the loaded state continues as the saved run.
+    return agal_sr_set(c, (unsigned)c->iter);
 }
 
 }  // namespace

@@ -86,7 +86,30 @@ struct StepArgs {
     // (Cu_CollideLES, solver_lbm_kernels.cu:352-355).  Null otherwise.
     const void *nu_sgs;
     double nu, dxL;
+    // Stochastic rounding of half-precision offsets (agal_params
+    // half_rounding): on when sr is set.  The launch seed mixes the coarse-step
+    // counter in device memory (advanced once per coarse step, so replayed
+    // graphs see a new value) with this launch's ordinal in the coarse step.
+    int sr;
+    const unsigned *sr_ctr;
+    unsigned sr_salt;
 };
+
+// Seed of a step launch (read after the wait on the predecessor).
+__device__ __forceinline__ unsigned step_seed(const StepArgs &a)
+{
+    return a.sr ? (*a.sr_ctr) * 0x9E3779B9u + a.sr_salt * 0x85EBCA77u + 0x165667B1u : 0u;
+}
+
+// Random bits of the stochastic rounding of the values of cell t of block b:
+// one hash per cell (its index in the pool), sr_dir(p) per direction.  Keyed
+// by the cell and direction a value was collided for, so every variant
+// rounds it alike wherever it is stored.
+template <int DIM>
+__device__ __forceinline__ unsigned sr_cell_of(long long b, int t, unsigned seed)
+{
+    return sr_cell(b * Geo<DIM>::MC + t, seed);
+}
 
 // The stream-guard fix-ups applied by the last CTA of the step kernel: every
 // thread fences its stores, the CTA takes a ticket, and the CTA holding the
@@ -376,7 +399,8 @@ __device__ __forceinline__ void collide_cell(typename ST<T>::C (&g)[Q], const St
 template <int DIM, int Q, typename T, bool SOLID>
 __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typename ST<T>::C ux,
                                           typename ST<T>::C uy, typename ST<T>::C uz, int b, int t,
-                                          const int *nrow, bool hook, T *__restrict__ fo, const StepArgs &a)
+                                          const int *nrow, bool hook, T *__restrict__ fo, const StepArgs &a,
+                                          unsigned seed)
 {
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
@@ -390,6 +414,7 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
     const int sz[3] = {DIM == 3 ? (K > 0 ? 9 : 0) : 0, DIM == 3 ? 9 : 0, DIM == 3 ? (K < 3 ? 9 : 18) : 0};
     const int nz[3] = {16 * ((K + 3) & 3), 16 * K, 16 * ((K + 1) & 3)};
     T *__restrict__ own = fo + (long long)b * BLK + t;
+    const unsigned rc = a.sr ? sr_cell_of<DIM>(b, t, seed) : 0u;
     // The reference streams in place: the owner x of a pair (p in the half
     // set) swaps its f*_p with the neighbour y's f*_pb only if that value is
     // positive (kernels.cu:620-628, the solid-cell guard f_pb > 0).  Here each
@@ -419,7 +444,7 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
             if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
             const long long to = (long long)nb * BLK + lat_pb(DIM, p) * MC + nc;
             T *dst = open ? fo + to : own + p * MC;
-            *dst = ST<T>::enc(g[p]);
+            *dst = enc_r<T>(g[p], rc * sr_dir(p), a.sr);
             guard(p, open, to);
         }
     } else {
@@ -432,7 +457,7 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
             if (SOLID && open) open = __ldg(&a.cmask[(long long)nb * MC + nc]) != CELL_SOLID;
             if (open) {
                 const long long to = (long long)nb * BLK + lat_pb(DIM, p) * MC + nc;
-                fo[to] = ST<T>::enc(g[p]);
+                fo[to] = enc_r<T>(g[p], rc * sr_dir(p), a.sr);
                 guard(p, true, to);
             } else {
                 C v = g[p];
@@ -442,7 +467,7 @@ __device__ __forceinline__ void push_cell(const typename ST<T>::C (&g)[Q], typen
                     v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx - 1, cy - 1, cz - 1, C(a.u_ref)) -
                         off;
                 }
-                own[p * MC] = ST<T>::enc(v);
+                own[p * MC] = enc_r<T>(v, rc * sr_dir(p), a.sr);
             }
         }
     }

@@ -64,6 +64,7 @@ k_step(const StepArgs a)
     }
     const T *__restrict__ f0 = static_cast<const T *>(a.fin) + t;
     pdl_wait();
+    const unsigned seed = step_seed(a);
 
     // Load: slot pb(p) holds f_p (offset form g_p for half storage).
     C g[CPT][Q];
@@ -106,7 +107,7 @@ k_step(const StepArgs a)
         } else {
             collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
         }
-        push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b[h], t, nrow, hook, fo, a);
+        push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b[h], t, nrow, hook, fo, a, seed);
     }
     if (a.fix_ticket) fused_fixup<T>(a);
 }
@@ -570,6 +571,10 @@ template <int DIM, int Q, typename T> struct RunStep {
         const bool fused = cpt != 3 && !tile && !wall && n <= AGAL_FUSED_FIXUP_BLOCKS;
         a.fix_ticket = fused ? c->fix_count + 1 : nullptr;
         a.nu_sgs = c->nu_sgs;
+        a.sr = (c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
+               c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
+        a.sr_ctr = c->d_sr;
+        a.sr_salt = (unsigned)c->sr_salt;
         a.nu = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->P.v0 : c->P.v0;
         a.dxL = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->dxf[L] : c->dxf[L];
         if (c->nu_sgs) {
@@ -587,6 +592,7 @@ template <int DIM, int Q, typename T> struct RunStep {
             if (rc == AGAL_ERR_UNSUPPORTED) return agal_set_err(c, rc, "tile step not available");
             if (rc) return rc;
             if (flip) c->cur[L] = 1 - c->cur[L];
+            c->sr_salt++;
             return AGAL_OK;
         }
         rc = (cpt == 4)   ? launch_row_or_cell<DIM, Q, T>(c, a, n)
@@ -600,6 +606,7 @@ template <int DIM, int Q, typename T> struct RunStep {
                                     c->fix_count, c->fix_list, c->fix_cap, c->d_status));
         AGAL_CUDA(c, cudaGetLastError());
         if (flip) c->cur[L] = 1 - c->cur[L];
+        c->sr_salt++;
         return AGAL_OK;
     }
 };

@@ -73,14 +73,14 @@ template <typename T> struct Row4Half {
     __device__ static float get(const V &v, int k)
     {
         if constexpr (std::is_same<T, __half>::value)
-            return __half2float(__ushort_as_half(bits(v, k)));
+            return ST<T>::dec(__ushort_as_half(bits(v, k)));
         else
             return __bfloat162float(__ushort_as_bfloat16(bits(v, k)));
     }
     __device__ static unsigned pack(float a, float b)
     {
         if constexpr (std::is_same<T, __half>::value) {
-            const __half2 h = __floats2half2_rn(a, b);
+            const __half2 h = __floats2half2_rn(a * kHalfScale, b * kHalfScale);
             return *reinterpret_cast<const unsigned *>(&h);
         } else {
             const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -91,6 +91,14 @@ template <typename T> struct Row4Half {
     {
         if (k == 0) v.x = pack(a, b);
         else v.y = pack(a, b);
+    }
+    // cells k, k + 1 from already encoded values
+    __device__ static void set2_bits(V &v, int k, T a, T b)
+    {
+        const unsigned w = (unsigned)*reinterpret_cast<const unsigned short *>(&a) |
+                           ((unsigned)*reinterpret_cast<const unsigned short *>(&b) << 16);
+        if (k == 0) v.x = w;
+        else v.y = w;
     }
     using P = unsigned;
     __device__ static P pair(const V &v, int k)
@@ -177,6 +185,7 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
     for (int i = r; i < W; i += R) s_meta[lb][i] = (b >= 0) ? __ldg(&a.meta[(long long)b * W + i]) : 0;
     pdl_wait();
 
+    const unsigned seed = step_seed(a);
     const T *__restrict__ fin = static_cast<const T *>(a.fin);
     T *__restrict__ fo = static_cast<T *>(a.fout);
     const long long own = (long long)b * BLK + r * 4;   // element offset of slot 0 of this row
@@ -212,7 +221,7 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
             for (int p = 0; p < Q; p++) g[p] = RW::get(v[lat_pb(DIM, p)], k);
             C ux, uy, uz;
             collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
-            push_cell<DIM, Q, T, true>(g, ux, uy, uz, b, t, nrow, hook, fo, a);
+            push_cell<DIM, Q, T, true>(g, ux, uy, uz, b, t, nrow, hook, fo, a, seed);
         }
     } else if (run) {
         const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
@@ -241,8 +250,22 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
                 hook_closed<DIM, Q, C, ST<T>::OFF>(g0, k, J, K, nrow, a.bc_preset, ux0, uy0, uz0, C(a.u_ref));
                 hook_closed<DIM, Q, C, ST<T>::OFF>(g1, k + 1, J, K, nrow, a.bc_preset, ux1, uy1, uz1, C(a.u_ref));
             }
+            if constexpr (sizeof(T) == 2) {
+                if (a.sr) {
+                    const unsigned r0 = sr_cell_of<DIM>(b, r * 4 + k, seed);
+                    const unsigned r1 = sr_cell_of<DIM>(b, r * 4 + k + 1, seed);
 #pragma unroll
-            for (int p = 0; p < Q; p++) RW::set2(v[p], k, g0[p], g1[p]);
+                    for (int p = 0; p < Q; p++)
+                        RW::set2_bits(v[p], k, enc_r<T>(g0[p], r0 * sr_dir(p), true),
+                                      enc_r<T>(g1[p], r1 * sr_dir(p), true));
+                } else {
+#pragma unroll
+                    for (int p = 0; p < Q; p++) RW::set2(v[p], k, g0[p], g1[p]);
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < Q; p++) RW::set2(v[p], k, g0[p], g1[p]);
+            }
         }
         // Stream: direction p goes to row (J + c_y, K + c_z) of the block in
         // that y/z neighbour slot, shifted by c_x; closed links bounce back

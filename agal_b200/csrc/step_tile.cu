@@ -84,7 +84,7 @@ template <> __device__ __forceinline__ void load_row4<__half>(const __half *p, f
     const uint2 v = *reinterpret_cast<const uint2 *>(p);
     const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&v.x));
     const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&v.y));
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    o[0] = a.x * kHalfUnscale; o[1] = a.y * kHalfUnscale; o[2] = b.x * kHalfUnscale; o[3] = b.y * kHalfUnscale;
 }
 template <> __device__ __forceinline__ void load_row4<__nv_bfloat16>(const __nv_bfloat16 *p, float (&o)[4])
 {
@@ -108,8 +108,10 @@ __device__ __forceinline__ void store_rows2_half(T *dst, const float (&v)[8])
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         H2 h;
-        if constexpr (std::is_same<T, __half>::value) h = __floats2half2_rn(v[2 * k], v[2 * k + 1]);
-        else h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+        if constexpr (std::is_same<T, __half>::value)
+            h = __floats2half2_rn(v[2 * k] * kHalfScale, v[2 * k + 1] * kHalfScale);
+        else
+            h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
         w[k] = *reinterpret_cast<const unsigned *>(&h);
     }
     *reinterpret_cast<uint4 *>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -121,6 +123,17 @@ template <> __device__ __forceinline__ void store_rows2<__half>(__half *dst, con
 template <> __device__ __forceinline__ void store_rows2<__nv_bfloat16>(__nv_bfloat16 *dst, const float (&v)[8])
 {
     store_rows2_half<__nv_bfloat162>(dst, v);
+}
+
+// Eight already encoded half values as one 16-byte store.
+template <typename T> __device__ __forceinline__ void store_encoded8(T *dst, const T (&h)[8])
+{
+    unsigned w[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        w[k] = (unsigned)*reinterpret_cast<const unsigned short *>(&h[2 * k]) |
+               ((unsigned)*reinterpret_cast<const unsigned short *>(&h[2 * k + 1]) << 16);
+    *reinterpret_cast<uint4 *>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 struct TileArgs {
@@ -188,6 +201,7 @@ __global__ void __maxnreg__(96) k_step_tile2d(const TileArgs ta)
     }
     __syncthreads();
     pdl_wait();
+    const unsigned seed = step_seed(a);
     // The blocks of a tile and its ring: one bulk copy each (a contiguous
     // Q x 16 run); warp 0 counts them for the expected bytes.
     auto issue = [&](const int *ids) {
@@ -347,6 +361,10 @@ __global__ void __maxnreg__(96) k_step_tile2d(const TileArgs ta)
                 v[0] = r0.x; v[1] = r0.y; v[2] = r0.z; v[3] = r0.w;
                 v[4] = r1.x; v[5] = r1.y; v[6] = r1.z; v[7] = r1.w;
             }
+            // a value keeps the rounding key of the cell and direction it was
+            // collided for: (z + c_q, pb(q)) when gathered, (z, q) when it
+            // bounces back or its swap is refused
+            bool mine[8] = {false, false, false, false, false, false, false, false};
             if (slow && q != 0) {
                 const bool hook = (e & ONB_BIT) && a.bc_preset != AGAL_BC_NONE;
 #pragma unroll
@@ -365,13 +383,38 @@ __global__ void __maxnreg__(96) k_step_tile2d(const TileArgs ta)
                                  wq;
                         }
                         v[k] = vv;
+                        mine[k] = true;
                     } else {
                         const bool refused = halfq ? !(v[k] + wq > 0.f) : !(own + wq > 0.f);
-                        if (refused) v[k] = own;
+                        if (refused) {
+                            v[k] = own;
+                            mine[k] = true;
+                        }
                     }
                 }
             }
-            store_rows2<T>(fo + (long long)(e & ~ONB_BIT) * BLK + q * MC + hh * 8, v);
+            T *dst = fo + (long long)(e & ~ONB_BIT) * BLK + q * MC + hh * 8;
+            if constexpr (sizeof(T) == 2) {
+                if (a.sr) {
+                    T h[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int x = zx + (k & 3), y = zy + (k >> 2);
+                        unsigned rnd;
+                        if (mine[k]) {
+                            rnd = sr_cell_of<2>(e & ~ONB_BIT, (x & 3) + 4 * (y & 3), seed) * sr_dir(q);
+                        } else {
+                            const int sx = x + cxq, sy = y + cyq;
+                            rnd = sr_cell_of<2>(ids[ring_block(sx, sy)] & ~ONB_BIT, (sx & 3) + 4 * (sy & 3), seed) *
+                                  sr_dir(qb);
+                        }
+                        h[k] = enc_r<T>(v[k], rnd, true);
+                    }
+                    store_encoded8<T>(dst, h);
+                    continue;
+                }
+            }
+            store_rows2<T>(dst, v);
         }
         // Tile i + 2's IDs go where tile i - 1's were; the planes, the
         // velocities and this tile's IDs stay untouched until every thread is

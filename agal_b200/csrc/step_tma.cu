@@ -63,6 +63,7 @@ k_step_tma(const StepArgs a, int *status)
     unsigned char *stages = smem + Cfg::BARS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nchunks = (a.n + BPS - 1) / BPS;
+    const unsigned seed = step_seed(a);   // plain launch: the predecessor has completed
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < NS; s++) {
@@ -157,7 +158,7 @@ k_step_tma(const StepArgs a, int *status)
                 C ux, uy, uz;
                 collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
                 const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
-                push_cell<DIM, Q, T, SOLID>(g, ux, uy, uz, b, t, row, hook, fo, a);
+                push_cell<DIM, Q, T, SOLID>(g, ux, uy, uz, b, t, row, hook, fo, a, seed);
             }
             mbar_arrive(&empty[s]);
         }

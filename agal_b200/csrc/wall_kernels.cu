@@ -80,6 +80,7 @@ template <int DIM, int Q, typename T>
 __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
 {
     pdl_wait();
+    const unsigned seed = step_seed(w.s);
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, W = Meta<DIM>::W;
     const StepArgs &a = w.s;
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
         g[q] = fq - offq;
     }
     T *__restrict__ fo = static_cast<T *>(a.fout);
-    push_cell<DIM, Q, T, true>(g, ux, uy, uz, b, t, nrow, false, fo, a);
+    push_cell<DIM, Q, T, true>(g, ux, uy, uz, b, t, nrow, false, fo, a, seed);
 }
 
 struct ForceArgs {
@@ -310,6 +311,11 @@ StepArgs base_args(agal_ctx *c, int L, const void *fin, void *fout)
     a.fix_count = c->fix_count;
     a.fix_list = c->fix_list;
     a.fix_cap = c->fix_cap;
+    // the wall step rounds with the seed of its level step's main launch
+    a.sr = (c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
+           c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
+    a.sr_ctr = c->d_sr;
+    a.sr_salt = (unsigned)c->sr_salt;
     return a;
 }
 

@@ -119,6 +119,7 @@ def default_params(**kw):
     p.bc_preset = p.ic_preset = p.region_preset = 0
     p.ref_pct_hi, p.ref_pct_lo, p.u_ref, p.ic_noise, p.seed = 0.9, 0.5, 0.05, 0.0, 0
     p.n_maxcblocks, p.mem_frac, p.device = 0, 0.975, -1
+    p.half_rounding = 0   # stochastic
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

@@ -147,7 +147,9 @@ def test_library_reads_and_writes_the_reference_file(tmp_path):
 def test_save_load_continues_bit_for_bit(tmp_path, storage):
     """40 steps, save, a fresh case loads and runs 24 more: every mesh array
     and the populations equal those of 64 uninterrupted steps (the regrids
-    every 8 steps included: the coarse-step counter is restored)."""
+    every 8 steps included: the coarse-step counter, which also seeds the
+    stochastic rounding of FP16, is restored).  FP16 populations agree to the
+    FP32 rounding of the file's f = w + g."""
     import agal_b200 as ag
     from agal_b200 import _lib
     from test_gpu_amr import amr_params
@@ -170,4 +172,10 @@ def test_save_load_continues_bit_for_bit(tmp_path, storage):
             assert c.counts()["n_ids"] == a.counts()["n_ids"] and c.counts()["n_gaps"] == a.counts()["n_gaps"]
             assert c.refine_stats()["iter"] == a.refine_stats()["iter"]
             for k in arrays:
-                assert np.array_equal(c.dump(k), a.dump(k)), k
+                if k == _lib.ARR_F and storage == "STORE_FP16":
+                    # the file holds f = w + g in FP32, which near the weights
+                    # keeps fewer bits than the scaled FP16 offset g
+                    d = np.abs(c.dump(k) - a.dump(k))
+                    assert d.max() < 1e-4 and np.sqrt((d ** 2).mean()) < 1e-6, (d.max(), np.sqrt((d ** 2).mean()))
+                else:
+                    assert np.array_equal(c.dump(k), a.dump(k)), k

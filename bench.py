@@ -514,16 +514,63 @@ def regrid_launches(counts: dict) -> int:
     return 4 * (ml - 1) + 10 + 40
 
 
+def _copy_state(src, dst):
+    """Every mesh array, the populations and the counts of src into dst."""
+    for arr in (_lib.ARR_CELLS_ID_MASK, _lib.ARR_CBLOCK_F_X, _lib.ARR_CBLOCK_ID_MASK, _lib.ARR_CBLOCK_ID_NBR,
+                _lib.ARR_CBLOCK_ID_NBR_CHILD, _lib.ARR_CBLOCK_ID_ONB, _lib.ARR_CBLOCK_ID_REF, _lib.ARR_CBLOCK_LEVEL,
+                _lib.ARR_ID_SET, _lib.ARR_GAP_SET, _lib.ARR_F):
+        dst.load(arr, src.dump(arr))
+    cnt = src.counts()
+    dst.set_counts(cnt["n_ids"], cnt["id_max"], cnt["n_gaps"])
+
+
+def _rel(a, b) -> float:
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 def error_vs_fp64(wl: str, steps: int, device: int) -> dict:
-    """rho and u of the workload in FP32 and in FP16 weight-offset storage
-    against the same case in FP64 after `steps` coarse steps (regrids
-    included), all runs of this library.  The meshes may differ (each run
-    refines on its own solution), so the fields are compared on the uniform
-    grid of the finest level over the whole domain, prepared as the
-    reference's M_Advance_PrintData prepares its output: relative L2 norms
-    over every cell."""
+    """Precision of FP32 and FP16 storage against FP64 runs of this library
+    on the headline case, after `steps` coarse steps:
+      same_mesh    every storage continues the FP64 run's state after its
+                   spin-up, without regrids (the storage error alone), rho and
+                   u of every active cell;
+      independent  each storage runs the whole case with its own regrids (the
+                   meshes may differ: fields compared on the uniform grid of
+                   the finest level, prepared as the reference's
+                   M_Advance_PrintData prepares its output);
+      drag, lift   momentum-exchange forces of a tilted ellipsoid (D3Q19 64^3,
+                   two near-wall levels, interpolated bounce-back, Re 100,
+                   3,000 steps)."""
     ww = dict(WORKLOADS[wl])
-    fields = {}
+    dim, Q = DIM_OF[ww["velocity_set"]], Q_OF[ww["velocity_set"]]
+    pb = {9: [0, 3, 4, 1, 2, 7, 8, 5, 6]}[Q]
+
+    def leaf(c, p):
+        nmb, MC = p.n_maxcblocks, 4 ** dim
+        cnt = c.counts()
+        ids = c.dump(_lib.ARR_ID_SET).reshape(-1, nmb)
+        blocks = np.sort(np.concatenate([ids[L, :cnt["n_ids"][L]] for L in range(cnt["max_levels"])]))
+        F = c.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks.astype(np.int64), :].reshape(Q, -1)
+        cx = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1])[pb]   # slot s holds f_{pb(s)}
+        cy = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1])[pb]
+        rho = F.sum(axis=0)
+        return rho, np.stack([(cx[:, None] * F).sum(axis=0) / rho, (cy[:, None] * F).sum(axis=0) / rho])
+
+    out = {"workload": wl, "coarse_steps": steps, "bar_u_rel_l2": 1e-3}
+    same, indep = {}, {}
+    p64 = make_params(dict(ww, storage=_lib.STORE_FP64), device=device)
+    with ag.Case(p64) as s:
+        s.set_ic(0)
+        s.refine_near_wall()
+        s.advance_n(ww["spinup"], use_graph=True)
+        s.sync()
+        for name, st in (("fp64", _lib.STORE_FP64), ("fp32", _lib.STORE_FP32), ("fp16", _lib.STORE_FP16)):
+            p = make_params(dict(ww, storage=st), device=device, P_REFINE=10 ** 8)
+            with ag.Case(p) as c:
+                _copy_state(s, c)
+                c.advance_n(steps - ww["spinup"], use_graph=True)
+                c.sync()
+                same[name] = leaf(c, p)
     for name, st in (("fp64", _lib.STORE_FP64), ("fp32", _lib.STORE_FP32), ("fp16", _lib.STORE_FP16)):
         w = dict(ww, storage=st)
         p = make_params(w, device=device, N_PRINT_LEVELS=w["levels"], VOL_I_MIN=0, VOL_I_MAX=w["Nx"],
@@ -533,20 +580,48 @@ def error_vs_fp64(wl: str, steps: int, device: int) -> dict:
             c.refine_near_wall()
             c.advance_n(steps, use_graph=True)
             c.sync()
-            fields[name] = (c.render_prepared(), c.counts()["n_ids"][: w["levels"]])
-    ref, ref_blocks = fields["fp64"]
-
-    def rel(a, b):
-        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-
-    out = {"workload": wl, "coarse_steps": steps, "grid": "uniform, finest level, whole domain",
-           "blocks_per_level_fp64": ref_blocks}
+            indep[name] = (c.render_prepared(), c.counts()["n_ids"][: w["levels"]])
+    forces = drag_lift(device)
     for name in ("fp32", "fp16"):
-        f, blocks = fields[name]
-        u = np.stack([f["u"], f["v"]])
-        uref = np.stack([ref["u"], ref["v"]])
-        out[name] = {"rho_rel_l2": rel(f["rho"], ref["rho"]), "u_rel_l2": rel(u, uref),
-                     "blocks_per_level": blocks}
+        f, blocks = indep[name]
+        r0 = indep["fp64"][0]
+        out[name] = {"same_mesh": {"rho_rel_l2": _rel(same[name][0], same["fp64"][0]),
+                                   "u_rel_l2": _rel(same[name][1], same["fp64"][1])},
+                     "independent": {"rho_rel_l2": _rel(f["rho"], r0["rho"]),
+                                     "u_rel_l2": _rel(np.stack([f["u"], f["v"]]), np.stack([r0["u"], r0["v"]])),
+                                     "blocks_per_level": blocks},
+                     "drag_rel": abs(forces[name][0] - forces["fp64"][0]) / abs(forces["fp64"][0]),
+                     "lift_rel": abs(forces[name][1] - forces["fp64"][1]) / abs(forces["fp64"][1])}
+    out["independent_blocks_per_level_fp64"] = indep["fp64"][1]
+    out["drag_lift_case"] = ("tilted ellipsoid (semi-axes 0.16, 0.07, 0.08 of the unit box, 20 degrees about z), "
+                             "D3Q19 64^3, two near-wall levels, interpolated bounce-back, second-order momentum "
+                             "exchange, inflow 0.05, Re 100, forces of step 3,000")
+    out["fp64_drag_lift"] = [float(forces["fp64"][0]), float(forces["fp64"][1])]
+    return out
+
+
+def drag_lift(device: int) -> dict:
+    from agal_b200.geometry import icosphere
+    f = icosphere(3, 1.0, (0, 0, 0), seed=9).astype(np.float64)
+    th = 0.35
+    R = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+    f = ((f * np.array([0.16, 0.07, 0.08])) @ R.T + np.array([0.42, 0.5, 0.5])).astype(np.float32)
+    out = {}
+    for name, st in (("fp64", _lib.STORE_FP64), ("fp32", _lib.STORE_FP32), ("fp16", _lib.STORE_FP16)):
+        p = ag.default_params(velocity_set=_lib.D3Q19, Nx=64, MAX_LEVELS_WALL=2, MAX_LEVELS_INTERIOR=1,
+                              v0=0.05 * 0.32 / 100, P_REFINE=10 ** 8, G_BIN_DENSITY=8, G_BIN_LEVELS=2, G_BIN_SPEC=2,
+                              G_BIN_MAKE_LINKS=1, G_NEAR_WALL_DISTANCE=0.05, S_BC_TYPE=1, S_FORCE_TYPE=0,
+                              S_FORCE_ORDER=2, bc_preset=_lib.BC_FPSC3D, ic_preset=_lib.IC_UNIFORM, u_ref=0.05,
+                              storage=st, n_maxcblocks=4096 * 4 + 64, device=device)
+        with ag.Case(p) as c:
+            c.set_geometry(f)
+            c.set_ic(0)
+            c.refine_near_wall()
+            c.advance_n(2999, use_graph=True)
+            c.forces()
+            c.advance_n(1, use_graph=True)
+            fr = c.forces()
+            out[name] = np.array([fr[0] - fr[1], fr[2] - fr[3], fr[4] - fr[5]])
     return out
 
 

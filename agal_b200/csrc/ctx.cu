@@ -657,6 +657,10 @@ __global__ void k_sr_set(unsigned *ctr, unsigned v) { *ctr = v; }
 
 int agal_sr_tick(agal_ctx *c)
 {
+    // only the stochastic rounding of half-precision offsets reads the counter
+    if (!((c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
+          c->P.half_rounding == AGAL_ROUND_STOCHASTIC))
+        return AGAL_OK;
     k_sr_tick<<<1, 1, 0, c->stream>>>(c->d_sr);
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;

@@ -649,9 +649,29 @@ def main(argv=None) -> int:
     ap.add_argument("--batched-seed", type=int, default=2024)
     ap.add_argument("--spinup", type=int, default=None,
                     help="with --profile: coarse steps of the untimed spin-up of a multi-level workload")
+    ap.add_argument("--profile-batched", action="store_true",
+                    help="only build the batched cases (FP16), advance 40 coarse steps, then 2 inside "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off); prints no JSON line")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     w = WORKLOADS[a.workload]
+    if a.profile_batched:
+        import torch
+        specs = batched_specs(a.batched_cases, a.batched_seed)
+        cases = [batched_case(sp, _lib.STORE_FP16, 0) for sp in specs]
+        for c in cases:
+            c.autotune(0, reps=3)
+        with ag.Batch(cases) as b:
+            b.advance_n(40)
+            b.sync()
+            torch.cuda.cudart().cudaProfilerStart()
+            b.advance_n(2)
+            b.sync()
+            torch.cuda.cudart().cudaProfilerStop()
+        for c in cases:
+            c.close()
+        print(f"batched profile run done: {len(cases)} cases, 40 + 2 coarse steps")
+        return 0
     if a.profile:
         pw = dict(WORKLOADS[a.profile])
         if a.spinup is not None and pw.get("amr"):

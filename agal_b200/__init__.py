@@ -159,6 +159,12 @@ class Case:
     def refine_near_wall(self) -> None:
         self._c(self._lib.agal_refine_near_wall(self._h))
 
+    def mesh_ref_criteria(self, L: int, var: int = _lib.MESH_REF_NW_CASES) -> None:
+        self._c(self._lib.agal_mesh_ref_criteria(self._h, int(L), int(var)))
+
+    def freeze_refined_cells(self, var: int = 0) -> None:
+        self._c(self._lib.agal_freeze_refined_cells(self._h, int(var)))
+
     def refine_stats(self) -> dict:
         it, nr, nc = C.c_longlong(), C.c_int(), C.c_int()
         self._c(self._lib.agal_refine_stats(self._h, C.byref(it), C.byref(nr), C.byref(nc)))
@@ -250,6 +256,9 @@ class Case:
 
     def uniform_frame(self, path: str, iter: int) -> None:
         self._c(self._lib.agal_uniform_frame(self._h, str(path).encode(), int(iter)))
+
+    def uniform_append(self, path: str, iter: int) -> None:
+        self._c(self._lib.agal_uniform_append(self._h, str(path).encode(), int(iter)))
 
     # -- geometry -------------------------------------------------------
     def set_geometry(self, faces) -> None:

@@ -29,6 +29,7 @@ REGION_NONE, REGION_BOUNDARY, REGION_BOX = 0, 1, 2
 CRITERION_VORTICITY, CRITERION_Q, CRITERION_PERCENTILE, CRITERION_LEARNED = 0, 1, 2, 3
 INTERP_INTERFACE, INTERP_ADDED = 0, 1
 AVERAGE_INTERFACE, AVERAGE_BLOCK, AVERAGE_GRID = 0, 1, 2
+MESH_REF_NW_CASES, MESH_REF_UNIFORM, MESH_REF_SOLUTION = 0, 2, 3
 
 ARR_F, ARR_MACROS, ARR_CELLS_ID_MASK, ARR_CBLOCK_F_X, ARR_CBLOCK_ID_MASK, ARR_CBLOCK_ID_NBR, \
     ARR_CBLOCK_ID_NBR_CHILD, ARR_CBLOCK_ID_ONB, ARR_CBLOCK_ID_REF, ARR_CBLOCK_LEVEL, ARR_ID_SET, \
@@ -91,6 +92,7 @@ PROTOS = [
     ("agal_uniform_render", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("agal_uniform_header", C.c_int, [C.c_void_p, C.c_char_p]),
     ("agal_uniform_frame", C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    ("agal_uniform_append", C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     ("agal_mass_momentum", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_mass_momentum_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("agal_mass_momentum_async", C.c_int, [C.c_void_p, C.c_void_p]),
@@ -104,6 +106,8 @@ PROTOS = [
     ("agal_refine_coarsen", C.c_int, [C.c_void_p]),
     ("agal_refine_with_solution", C.c_int, [C.c_void_p]),
     ("agal_refine_near_wall", C.c_int, [C.c_void_p]),
+    ("agal_mesh_ref_criteria", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("agal_freeze_refined_cells", C.c_int, [C.c_void_p, C.c_int]),
     ("agal_refine_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("agal_set_geometry", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("agal_geometry_read_stl", C.c_int, [C.c_char_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),

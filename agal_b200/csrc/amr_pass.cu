@@ -424,13 +424,20 @@ __global__ void k_mark_level(const int *ids, int n, long long nmb, int dim, int 
     if (mark) ref[b] = REF_MARK_REFINE;
 }
 
-// Cu_FreezeRefined (mesh_amr.cu:1888).
-__global__ void k_freeze(int *ref, int n)
+// Cu_FreezeRefined / Cu_UnfreezeRefined (mesh_amr.cu:1888-1923): refined
+// blocks become permanent (thaw = 0) or eligible for coarsening again (1).
+__global__ void k_freeze(int *ref, int n, int thaw)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n) return;
-    if (ref[b] == REF_REFINED) ref[b] = REF_REFINED_PERM;
-    if (ref[b] == REF_REFINED_WCHILD) ref[b] = REF_REFINED_WCHILD_PERM;
+    const int r = ref[b];
+    if (!thaw) {
+        if (r == REF_REFINED) ref[b] = REF_REFINED_PERM;
+        if (r == REF_REFINED_WCHILD) ref[b] = REF_REFINED_WCHILD_PERM;
+    } else {
+        if (r == REF_REFINED_PERM) ref[b] = REF_REFINED;
+        if (r == REF_REFINED_WCHILD_PERM) ref[b] = REF_REFINED_WCHILD;
+    }
 }
 
 int read_small(agal_ctx *c, int *h, int off, int n)
@@ -494,11 +501,11 @@ int agal_build_iface_lists(agal_ctx *c)
     return AGAL_OK;
 }
 
-int agal_freeze_refined(agal_ctx *c)
+int agal_freeze_refined(agal_ctx *c, int thaw)
 {
     const int n = c->id_max[c->max_levels];
     if (n <= 0) return AGAL_OK;
-    k_freeze<<<grid_for(n), NT, 0, c->stream>>>(c->cblock_ID_ref, n);
+    k_freeze<<<grid_for(n), NT, 0, c->stream>>>(c->cblock_ID_ref, n, thaw);
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;
 }

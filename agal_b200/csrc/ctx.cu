@@ -495,7 +495,9 @@ extern "C" int agal_refine_with_solution(agal_ctx *c)
     if (!c) return AGAL_ERR_PARAM;
     const int ML = c->max_levels;
     int rc;
-    if (!(c->P.MAX_LEVELS_INTERIOR > 1 && c->P.N_PROBE_AVE == 0)) return AGAL_OK;
+    // mesh_advance.cu:191: not once the time average has started
+    const bool averaging = c->P.N_PROBE_AVE != 0 && !(c->P.N_PROBE_AVE == 1 && c->iter + 1 <= c->P.N_PROBE_AVE_START);
+    if (!(c->P.MAX_LEVELS_INTERIOR > 1) || averaging) return AGAL_OK;
     for (int L = ML - 2; L >= c->L0; L--)
         if ((rc = agal_average(c, L, AGAL_AVERAGE_GRID))) return rc;
     for (int L = c->L0; L < ML - 1; L++)
@@ -541,6 +543,25 @@ extern "C" int agal_refine_near_wall(agal_ctx *c)
     }
     if (ML > 1 && (rc = agal_freeze_refined(c))) return rc;
     return AGAL_OK;
+}
+
+extern "C" int agal_mesh_ref_criteria(agal_ctx *c, int L, int var)
+{
+    // Mesh::M_ComputeRefCriteria (mesh_criterion.cu:90-119).
+    if (!c || L < 0 || L >= c->max_levels) return AGAL_ERR_PARAM;
+    switch (var) {
+    case AGAL_MESH_REF_NW_CASES: return agal_mark_level(c, L, 0);
+    case AGAL_MESH_REF_UNIFORM: return agal_mark_level(c, L, 1);
+    case AGAL_MESH_REF_SOLUTION: return c->n_ids[L] > 0 ? agal_ref_criteria(c) : AGAL_OK;
+    default: return agal_set_err(c, AGAL_ERR_PARAM, "mesh_ref_criteria: unknown var");
+    }
+}
+
+extern "C" int agal_freeze_refined_cells(agal_ctx *c, int var)
+{
+    // Mesh::M_FreezeRefinedCells (mesh_amr.cu:2050-2074).
+    if (!c || (var != 0 && var != 1)) return AGAL_ERR_PARAM;
+    return agal_freeze_refined(c, var);
 }
 
 extern "C" int agal_refine_stats(const agal_ctx *c, long long *iter, int *n_refined, int *n_coarsened)

@@ -176,7 +176,7 @@ int agal_launch_criterion(agal_ctx *c);
 int agal_percentile_decisions(agal_ctx *c, int select, const int *ids, const int *lvl0, int n, float *Y, float *Wt);
 int agal_refine_pass(agal_ctx *c);          // Mesh::M_RefineAndCoarsenBlocks
 int agal_mark_level(agal_ctx *c, int L, int uniform);
-int agal_freeze_refined(agal_ctx *c);
+int agal_freeze_refined(agal_ctx *c, int thaw = 0);
 int agal_build_iface_lists(agal_ctx *c);    // after any mesh change (multi-level cases)
 size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
 #define AGAL_AMR_SMALL 128

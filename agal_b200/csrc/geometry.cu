@@ -1042,7 +1042,8 @@ extern "C" int agal_link_lengths(agal_ctx *c, int L)
     k_links_validate<<<n, MC3, 0, c->stream>>>(ids, c->nmb, c->cblock_ID_nbr, c->cells_ID_mask, c->onb_solid,
                                                c->n_maxcells_b, c->X_b);
     AGAL_CUDA(c, cudaGetLastError());
-    return AGAL_OK;
+    // the step's wall flags depend on the link lengths
+    return agal_build_meta(c);
 }
 
 extern "C" int agal_geometry_counts(const agal_ctx *c, long long *out)

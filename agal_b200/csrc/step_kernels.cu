@@ -23,7 +23,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -293,6 +292,7 @@ __device__ __forceinline__ C les_model(int model, int dim, C dx, C ux, C uy, C u
 struct EddyArgs {
     const int *ids;
     int n;
+    const int *nbr_child, *bmask;
     const void *f;
     void *nu_sgs;
     double dx;
@@ -307,6 +307,9 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_eddy(const EddyArgs a)
     constexpr int H = 6, HV = (DIM == 3) ? H * H * H : H * H;   // block plus a one-cell halo
     __shared__ C s[3][HV];
     const int b = a.ids[blockIdx.x];
+    // Cu_ComputeEddyViscosity (solver_lbm_kernels_les.cu:313-323): listed
+    // blocks that are leaves or not inside a solid (uniform per CTA)
+    if (b < 0 || !(a.nbr_child[b] < 0 || a.bmask[b] != BLOCK_SOLID)) return;
     const int t = threadIdx.x;
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     auto at = [&](int i, int j, int k) { return (i + 1) + H * (j + 1) + (DIM == 3 ? H * H * (k + 1) : 0); };
@@ -582,7 +585,7 @@ template <int DIM, int Q, typename T> struct RunStep {
             // and row-mapped variants have no per-cell relaxation rate, so
             // LES steps one cell per thread.
             if (cpt >= 3) cpt = 1;
-            EddyArgs e{a.ids, n, a.fin, c->nu_sgs, a.dxL, c->P.S_LES};
+            EddyArgs e{a.ids, n, c->cblock_ID_nbr_child, c->cblock_ID_mask, a.fin, c->nu_sgs, a.dxL, c->P.S_LES};
             k_eddy<DIM, Q, T><<<n, Geo<DIM>::MC, 0, c->stream>>>(e);
             AGAL_CUDA(c, cudaGetLastError());
         }
@@ -742,28 +745,22 @@ template <int DIM, int Q, typename T> struct RunMass {
 // same device) race on it and must be serialised by the caller.
 __device__ __align__(256) static double g_mass_scratch[4 * AGAL_MASS_NOALLOC_MAX_PARTIALS + 4];
 
-static std::mutex g_mass_scratch_mu;
-static double *g_mass_scratch_ptr[128];   // per device ordinal, set on first use
-
-// Device address of g_mass_scratch on device dev, looked up once per device
-// with that device current (cudaGetSymbolAddress may initialise the module,
-// so the first call on a device belongs before any stream capture).
+// Device address of g_mass_scratch on the context's device, looked up on
+// every call with that device current, so that a device reset (a new primary
+// context) between calls is followed.  The lookup allocates nothing; the
+// first one on a device may load the module and belongs before any stream
+// capture.
 static int mass_scratch_on(agal_ctx *c, double **out)
 {
     const int dev = c->device;
-    if (dev < 0 || dev >= 128) return agal_set_err(c, AGAL_ERR_PARAM, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_mass_scratch_mu);
-    if (!g_mass_scratch_ptr[dev]) {
-        int prev = -1;
-        AGAL_CUDA(c, cudaGetDevice(&prev));
-        if (prev != dev) AGAL_CUDA(c, cudaSetDevice(dev));
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_scratch);
-        if (prev != dev) cudaSetDevice(prev);
-        if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGetSymbolAddress(g_mass_scratch)");
-        g_mass_scratch_ptr[dev] = static_cast<double *>(p);
-    }
-    *out = g_mass_scratch_ptr[dev];
+    int prev = -1;
+    AGAL_CUDA(c, cudaGetDevice(&prev));
+    if (prev != dev) AGAL_CUDA(c, cudaSetDevice(dev));
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_scratch);
+    if (prev != dev) cudaSetDevice(prev);
+    if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGetSymbolAddress(g_mass_scratch)");
+    *out = static_cast<double *>(p);
     return AGAL_OK;
 }
 

@@ -235,9 +235,29 @@ extern "C" int agal_uniform_header(agal_ctx *c, const char *path)
     return ok ? AGAL_OK : agal_set_err(c, AGAL_ERR_IO, "uniform output: write failed");
 }
 
-// One frame (M_Advance_PrintData + M_RenderAndPrint_Uniform): grid average
-// and interface interpolation on a multi-level mesh, macros refreshed on every
-// level, then t = iter / Nx and the six fields appended to `path`.
+// One frame of the current macros (M_RenderAndPrint_Uniform): t = iter / Nx
+// and the six fields appended to `path`.
+extern "C" int agal_uniform_append(agal_ctx *c, const char *path, int iter)
+{
+    if (!c || !path) return AGAL_ERR_PARAM;
+    int rc;
+    int d[3];
+    agal_uniform_dims(c, d);
+    const long long vol = (long long)d[0] * d[1] * d[2];
+    std::vector<double> buf((size_t)std::max<long long>(6 * vol, 1));
+    if ((rc = agal_uniform_render(c, buf.data(), 6 * vol))) return rc;
+    FILE *f = fopen(path, "ab");
+    if (!f) return agal_set_err(c, AGAL_ERR_IO, std::string("uniform output: cannot open ") + path);
+    const double t = (double)iter / (double)c->Nx;
+    const bool ok = fwrite(&t, sizeof(double), 1, f) == 1 &&
+                    (vol == 0 || fwrite(buf.data(), sizeof(double), (size_t)(6 * vol), f) == (size_t)(6 * vol));
+    fclose(f);
+    return ok ? AGAL_OK : agal_set_err(c, AGAL_ERR_IO, "uniform output: write failed");
+}
+
+// One frame as M_Advance_PrintData makes it: grid average and interface
+// interpolation on a multi-level mesh, macros refreshed on every level, then
+// the frame appended.
 extern "C" int agal_uniform_frame(agal_ctx *c, const char *path, int iter)
 {
     if (!c || !path) return AGAL_ERR_PARAM;
@@ -251,16 +271,5 @@ extern "C" int agal_uniform_frame(agal_ctx *c, const char *path, int iter)
     }
     for (int L = 0; L < ML; L++)
         if ((rc = agal_refresh(c, L))) return rc;
-    int d[3];
-    agal_uniform_dims(c, d);
-    const long long vol = (long long)d[0] * d[1] * d[2];
-    std::vector<double> buf((size_t)std::max<long long>(6 * vol, 1));
-    if ((rc = agal_uniform_render(c, buf.data(), 6 * vol))) return rc;
-    FILE *f = fopen(path, "ab");
-    if (!f) return agal_set_err(c, AGAL_ERR_IO, std::string("uniform output: cannot open ") + path);
-    const double t = (double)iter / (double)c->Nx;
-    const bool ok = fwrite(&t, sizeof(double), 1, f) == 1 &&
-                    (vol == 0 || fwrite(buf.data(), sizeof(double), (size_t)(6 * vol), f) == (size_t)(6 * vol));
-    fclose(f);
-    return ok ? AGAL_OK : agal_set_err(c, AGAL_ERR_IO, "uniform output: write failed");
+    return agal_uniform_append(c, path, iter);
 }

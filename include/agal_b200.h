@@ -228,6 +228,17 @@ int agal_refine_coarsen(agal_ctx *ctx);
 /* Mesh::M_Advance_RefineWithSolution (mesh_advance.cu:185-243): grid
    average, interface interpolation, criterion, refine/coarsen. */
 int agal_refine_with_solution(agal_ctx *ctx);
+/* Mesh::M_ComputeRefCriteria (mesh_criterion.cu:90-119) on level L:
+   AGAL_MESH_REF_NW_CASES marks the unrefined blocks of the Cu_RefineRegion
+   preset (region_preset), AGAL_MESH_REF_UNIFORM every unrefined block,
+   AGAL_MESH_REF_SOLUTION runs agal_ref_criteria when level L has blocks. */
+#define AGAL_MESH_REF_NW_CASES 0
+#define AGAL_MESH_REF_UNIFORM  2
+#define AGAL_MESH_REF_SOLUTION 3
+int agal_mesh_ref_criteria(agal_ctx *ctx, int L, int var);
+/* Mesh::M_FreezeRefinedCells (mesh_amr.cu:2050-2074): var 0 makes refined
+   blocks permanent (not coarsened), var 1 releases them. */
+int agal_freeze_refined_cells(agal_ctx *ctx, int var);
 /* Mesh::M_Advance_RefineNearWall (mesh_advance.cu:54-122) without geometry:
    uniform refinement to N_LEVEL_START, Cu_RefineRegion marks (region_preset)
    up to MAX_LEVELS_WALL with S_SetIC per level, refined blocks frozen. */
@@ -388,11 +399,14 @@ int agal_restart_load(agal_ctx *ctx, const char *path, int *iter);
    average, interface interpolation, refresh of every level) and appends
    t = iter / Nx and the fields rho, u, v, w, level, block ID (doubles, x
    fastest).  agal_uniform_render fills out[6][nz][ny][nx] from the current
-   macros without preparing; agal_uniform_dims gives {nx, ny, nz}. */
+   macros without preparing; agal_uniform_append appends a frame of the
+   current macros without preparing (M_RenderAndPrint_Uniform alone);
+   agal_uniform_dims gives {nx, ny, nz}. */
 int agal_uniform_dims(const agal_ctx *ctx, int *dims);
 int agal_uniform_render(agal_ctx *ctx, double *out, long long n);
 int agal_uniform_header(agal_ctx *ctx, const char *path);
 int agal_uniform_frame(agal_ctx *ctx, const char *path, int iter);
+int agal_uniform_append(agal_ctx *ctx, const char *path, int iter);
 int agal_dump(agal_ctx *ctx, int which, void *host_buf, size_t bytes);
 int agal_load(agal_ctx *ctx, int which, const void *host_buf, size_t bytes);
 
@@ -417,8 +431,10 @@ int agal_mass_momentum_async(agal_ctx *ctx, double *out);
    (8 MiB), and no call allocates or frees.  One partial covers 256 active
    cells of one level, so a mesh of more than 67,108,864 active cells (summed
    per level, each level rounded up to 256) is rejected with AGAL_ERR_PARAM.
-   The first call on a device looks the array up (cudaGetSymbolAddress) with
-   that device current; make it before any stream capture.  The array is
+   Every call looks the array up (cudaGetSymbolAddress, no allocation) with
+   the context's device current, so a device reset between calls is
+   followed; the first call on a device may load the module and belongs
+   before any stream capture.  The array is
    shared by every context of the device: calls that overlap in time race
    and must be serialised by the caller.  No reference counterpart. */
 #define AGAL_MASS_NOALLOC_MAX_PARTIALS 262144

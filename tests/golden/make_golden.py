@@ -52,6 +52,10 @@ CASES = {
     "les_d3q19_ldc16_smag": ("ref_d3q19_ldc_smag", dict(Nx=16, v0=1.25e-4), 200, 4096),
     "les_d3q19_ldc16_wale": ("ref_d3q19_ldc_wale", dict(Nx=16, v0=1.25e-4), 200, 4096),
     "les_d3q19_ldc16_vreman": ("ref_d3q19_ldc_vreman", dict(Nx=16, v0=1.25e-4), 200, 4096),
+    # 2D models (the N_DIM == 2 branches of solver_lbm_kernels_les.cu:35-213)
+    "les_d2q9_ldc64_smag": ("ref_d2q9_ldc_smag", dict(Nx=64, v0=2.5e-5), 400, 4096),
+    "les_d2q9_ldc64_wale": ("ref_d2q9_ldc_wale", dict(Nx=64, v0=2.5e-5), 400, 4096),
+    "les_d2q9_ldc64_vreman": ("ref_d2q9_ldc_vreman", dict(Nx=64, v0=2.5e-5), 400, 4096),
 }
 
 # Multi-level cases: (binary, keys, steps, keep_mb, region preset of the

@@ -15,13 +15,17 @@ from test_oracle import GOLDEN, params_for_golden
 import agal_b200 as ag
 from agal_b200 import _lib
 
-LES_CASES = {"les_d3q19_ldc16_smag": 1, "les_d3q19_ldc16_wale": 2, "les_d3q19_ldc16_vreman": 3}
-TOL_U = 1e-4          # relative L2 of the velocity after 200 steps
+LES_CASES = {"les_d3q19_ldc16_smag": 1, "les_d3q19_ldc16_wale": 2, "les_d3q19_ldc16_vreman": 3,
+             "les_d2q9_ldc64_smag": 1, "les_d2q9_ldc64_wale": 2, "les_d2q9_ldc64_vreman": 3}
+TOL_U = 1e-4          # relative L2 of the velocity after 200 (3D) / 400 (2D) steps
+TOL_U_HALF = 2e-3     # the same with FP16 weight offsets (stochastic rounding)
 
 
-def run(g, model):
+def run(g, model, storage=None):
     p, steps = params_for_golden(g)
     p.S_LES = model
+    if storage is not None:
+        p.storage = storage
     Q, MC = int(g["Q"]), int(g["MC"])
     with ag.Case(p) as c:
         c.set_ic(0)
@@ -40,10 +44,17 @@ def macros(g, F):
     return rho, np.stack(u)
 
 
+def fixture(name):
+    path = GOLDEN / f"{name}.npz"
+    if not path.exists():
+        pytest.skip(f"{name} fixture not generated")
+    return np.load(path)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,model", sorted(LES_CASES.items()))
 def test_les_matches_the_reference_build(name, model):
-    g = np.load(GOLDEN / f"{name}.npz")
+    g = fixture(name)
     Q = int(g["Q"])
     Fr = np.transpose(g["F"][:, :Q, :], (1, 0, 2)).reshape(Q, -1)
     rho_r, u_r = macros(g, Fr)
@@ -67,3 +78,25 @@ def test_les_outside_its_scope_is_refused():
     p.S_LES = 4
     with pytest.raises(ag.AgalError):
         ag.Case(p)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,model", [("les_d3q19_ldc16_smag", 1), ("les_d2q9_ldc64_wale", 2)])
+@pytest.mark.parametrize("storage", ["STORE_FP16", "STORE_BF16"])
+def test_les_half_storage_near_the_reference(name, model, storage):
+    """FP16 / BF16 weight offsets: the eddy viscosity reads the decoded
+    populations and the per-cell relaxation writes rounded offsets; the
+    velocity stays within the half-precision floor of the reference and far
+    closer to it than the run without the model."""
+    g = fixture(name)
+    Q = int(g["Q"])
+    Fr = np.transpose(g["F"][:, :Q, :], (1, 0, 2)).reshape(Q, -1)
+    rho_r, u_r = macros(g, Fr)
+    st = getattr(_lib, storage)
+    rho, u = macros(g, run(g, model, st))
+    _, u0 = macros(g, run(g, 0, st))
+    e, e0 = rel_l2(u, u_r), rel_l2(u0, u_r)
+    tol = TOL_U_HALF if storage == "STORE_FP16" else 8 * TOL_U_HALF
+    print(f"{name} {storage}: u rel L2 {e:.3e} (no model {e0:.3e}), rho {rel_l2(rho, rho_r):.3e}")
+    assert e < tol, (e, e0)
+    assert e0 > 3 * e, (e, e0)

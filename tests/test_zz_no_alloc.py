@@ -74,3 +74,29 @@ def test_noalloc_rejects_more_partials_than_the_scratch_holds():
         assert "static scratch" in str(e.value)
         m = c.mass_momentum()
         assert abs(m[0] - 8192.0 * 8196.0) < 1e-6 * 8192.0 * 8196.0
+
+
+def test_noalloc_allocates_no_device_memory():
+    """On a fresh context whose mesh needs the largest scratch the entry point
+    accepts (8192^2 cells: 262,144 partials of 4 doubles, 8 MiB), repeated
+    noalloc calls leave the device's free memory (cudaMemGetInfo) unchanged;
+    the allocating entry point on the same context grows its own scratch."""
+    import torch
+    p = _case(9, 8192, _lib.STORE_FP16, bc_preset=_lib.BC_NONE, ic_preset=_lib.IC_REST,
+              n_maxcblocks=2048 * 2048 + 5)
+    torch.cuda.mem_get_info(0)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        c.sync()
+        free0, _ = torch.cuda.mem_get_info(0)
+        for _ in range(3):
+            a = c.mass_momentum_noalloc()
+        c.sync()
+        free1, _ = torch.cuda.mem_get_info(0)
+        assert free1 == free0, (free0, free1)
+        assert abs(a[0] - 8192.0 * 8192.0) < 1e-6 * 8192.0 * 8192.0
+        m = c.mass_momentum()
+        c.sync()
+        free2, _ = torch.cuda.mem_get_info(0)
+        assert free2 < free1, (free1, free2)
+        assert abs(m[0] - a[0]) <= RTOL * abs(m[0])

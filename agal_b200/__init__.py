@@ -172,7 +172,8 @@ class Case:
 
     STEP_VARIANTS = {1: "1 cell/thread", 2: "2 cells/thread", 3: "TMA-staged persistent pipeline",
                      4: "1 row of 4 cells/thread, vector loads and stores",
-                     5: "root-level tile of 8x8 blocks per CTA, gathered whole-block stores (2D)"}
+                     5: "root-level tile of 8x8 blocks per CTA, gathered whole-block stores (2D)",
+                     6: "root-level push tile of 8x4 blocks per CTA, shared-memory pushes, 16-byte row stores (2D)"}
 
     def autotune(self, L: int = 0, reps: int = 5) -> dict:
         """Pick the step kernel variant by timing each one (state unchanged)."""

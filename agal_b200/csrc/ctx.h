@@ -88,6 +88,7 @@ struct agal_ctx {
     int *blk_solid = nullptr;          // [nmb] 1 = the block holds a solid cell (geometry cases)
     int *tiles = nullptr;              // root-level tile table of the 2D tile step (step_tile.cu)
     int n_tiles = 0;                   // 0 = the tile step is not available
+    int n_ptiles = 0;                  // push tiles of the root level (step_ptile.cu); 0 = not available
     void *xfer = nullptr;              // 64 MiB FP64 staging of the population dumps and loads (xfer.cu)
     int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
     long long *fix_list = nullptr;
@@ -143,7 +144,7 @@ struct agal_ctx {
 // TMA-staged persistent pipeline, 4 one x-row of four cells per thread with
 // vector loads and stores (step_row.cu), 5 the root-level tile step of 2D
 // cases (step_tile.cu; other levels and cases run variant 4 in its place).
-#define AGAL_STEP_VARIANTS 5
+#define AGAL_STEP_VARIANTS 6
 
 // Error helpers shared by the translation units.
 int agal_set_err(agal_ctx *c, int code, const std::string &msg);
@@ -161,6 +162,7 @@ int agal_launch_tune(agal_ctx *c, int L, int reps, float *ms);
 int agal_prepare_step(agal_ctx *c);
 int agal_build_meta(agal_ctx *c);   // after any change of the block arrays
 int agal_build_tiles(agal_ctx *c);  // root-level tile table (agal_build_meta calls it)
+int agal_count_ptiles(const agal_ctx *c);   // root-level push tiles, 0 if not available
 int agal_launch_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);
 // Enqueue the FP64 sums and their copy into host memory (pinned for a truly

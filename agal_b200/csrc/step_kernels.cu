@@ -506,6 +506,8 @@ int launch_row_or_cell(agal_ctx *c, const StepArgs &a, int n)
 // the case or level has no tile table.
 template <int DIM, int Q, typename T>
 int launch_step_tile(agal_ctx *c, const StepArgs &a, int L);
+template <int DIM, int Q, typename T>
+int launch_step_ptile(agal_ctx *c, const StepArgs &a, int L);
 
 // Swap back the pushed entries of every link whose swap the reference's
 // stream guard refuses (recorded by push_cell), then clear the list for the
@@ -566,6 +568,10 @@ template <int DIM, int Q, typename T> struct RunStep {
         // variant takes its place.
         const bool tile = cpt == 5 && !std::is_same<T, double>::value && L == c->L0 && c->n_tiles > 0 && !c->nu_sgs;
         if (cpt == 5 && !tile) cpt = 4;
+        // The push-tile step likewise; elsewhere one cell per thread.
+        const bool ptile =
+            cpt == 6 && !std::is_same<T, double>::value && L == c->L0 && c->n_ptiles > 0 && !c->nu_sgs;
+        if (cpt == 6 && !ptile) cpt = 1;
         // Small one-shot grids apply the fix-ups in their last CTA (saves a
         // launch of a few µs per sub-step); large grids, the persistent
         // variant and levels with a wall step use the separate kernel.  The
@@ -598,7 +604,8 @@ template <int DIM, int Q, typename T> struct RunStep {
             c->sr_salt++;
             return AGAL_OK;
         }
-        rc = (cpt == 4)   ? launch_row_or_cell<DIM, Q, T>(c, a, n)
+        rc = (cpt == 6)   ? launch_step_ptile<DIM, Q, T>(c, a, L)
+             : (cpt == 4) ? launch_row_or_cell<DIM, Q, T>(c, a, n)
              : (cpt == 3) ? launch_step_tma<DIM, Q, T>(c, a)
              : (cpt == 2) ? launch_step<DIM, Q, T, 2>(c, a, n)
                           : launch_step<DIM, Q, T, 1>(c, a, n);
@@ -616,8 +623,8 @@ template <int DIM, int Q, typename T> struct RunStep {
 
 // Autotuner of the step kernel: times every variant (1: one cell per thread,
 // 2: two cells per thread, 3: TMA-staged persistent pipeline, 4: one row of
-// four cells per thread, 5: root-level tile step) on level L's current
-// state, writing only the scratch buffer.
+// four cells per thread, 5: root-level tile step, 6: root-level push tiles)
+// on level L's current state, writing only the scratch buffer.
 template <int DIM, int Q, typename T> struct RunTune {
     static int run(agal_ctx *c, int L, int reps, float *ms_out)
     {

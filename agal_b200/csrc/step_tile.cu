@@ -517,6 +517,7 @@ int agal_build_tiles(agal_ctx *c)
 {
     using namespace agal;
     c->n_tiles = 0;
+    c->n_ptiles = agal_count_ptiles(c);
     if (c->dim != 2 || c->geometry_init) return AGAL_OK;
     const int nbx = c->Nx / 4, nby = c->Ny / 4;
     if (nbx % TB || nby % TB || c->n_ids[c->L0] != nbx * nby) return AGAL_OK;

@@ -641,7 +641,7 @@ def main(argv=None) -> int:
                     help="coarse steps of the FP32/FP16-vs-FP64 error runs (0 skips them)")
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
                     help="only run W+K steps of this workload (for ncu captures); prints no JSON line")
-    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3, 4, 5],
+    ap.add_argument("--cpt", type=int, default=1, choices=[1, 2, 3, 4, 5, 6],
                     help="with --profile: step kernel variant (1, 2 cells per thread; 3 TMA pipeline; "
                          "4 one row of four cells per thread; 5 root-level tiles, 2D)")
     ap.add_argument("--batched-cases", type=int, default=64,

@@ -447,14 +447,18 @@ int agal_mass_momentum_noalloc(agal_ctx *ctx, double *out);
    run variant 1 in its place), 5 = the root level of 2D cases as tiles of
    8 x 8 cell-blocks per CTA, each output block written whole (root blocks per
    side a multiple of 8, no geometry, no LES; elsewhere variant 4 runs in its
-   place).  Times each variant reps times on level L's current state without
+   place), 6 = the root level of 2D cases as tiles of 8 x 4 cell-blocks
+   whose in-tile pushes go through shared memory and whose output block rows
+   are written with 16-byte stores (root blocks per side a multiple of 8 in x
+   and 4 in y, no geometry, no LES; elsewhere variant 1 runs in its place).
+   Times each variant reps times on level L's current state without
    advancing it (the step writes only the scratch population buffer) and
-   keeps the fastest for the context.  ms[5] (may be NULL) receives the
+   keeps the fastest for the context.  ms[6] (may be NULL) receives the
    per-launch times, *variant (may be NULL) the choice.
    All variants give bit-identical populations.  No reference counterpart:
    the reference launches one fixed 16/64-thread shape (cppspec.h:96). */
 int agal_autotune(agal_ctx *ctx, int L, int reps, float *ms, int *variant);
-/* Set the step kernel variant explicitly (1..5, as for agal_autotune). */
+/* Set the step kernel variant explicitly (1..6, as for agal_autotune). */
 int agal_set_tuning(agal_ctx *ctx, int variant);
 
 /* Synchronise the context's stream; returns the first pending CUDA error, or

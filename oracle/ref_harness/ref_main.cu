@@ -175,9 +175,12 @@ int main(int argc, char **argv)
         geometry->G_Init_Arrays_CoordsList_CPU();
         geometry->G_InitBins(BinMake::GPU, 0);
     }
-    // With an LES model the field also holds the eddy viscosity in row
-    // N_Q + 4 (solver_lbm_kernels_les.cu:591; main.cu:109's commented size).
-    const int N_U = LPh.N_Q + APh.N_DIM + 1 + (LPh.LM != LESModel::None ? 1 : 0);
+    // With an LES model the field also holds the eddy viscosity, which the
+    // kernels write to row N_Q + 4 in 2D and 3D alike
+    // (solver_lbm_kernels_les.cu:450, 597).  main.cu:109's commented size,
+    // N_Q + N_DIM + 2, ends one row short of it in 2D, so the field is sized
+    // N_Q + 5 whenever a model is on.
+    const int N_U = (LPh.LM != LESModel::None) ? LPh.N_Q + 5 : LPh.N_Q + APh.N_DIM + 1;
     Mesh<REAL_h, REAL_h, &APh> mesh(&parser, N_U);
     if (geom) mesh.M_AddGeometry(geometry);
     Solver_LBM<REAL_h, REAL_h, &APh, &LPh> solver(&mesh);

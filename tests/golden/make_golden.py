@@ -171,7 +171,8 @@ def cmd_tables(ref: Path) -> None:
 
 
 # ---------------------------------------------------------------------------
-LES_BINARIES = ("ref_d3q19_ldc_smag", "ref_d3q19_ldc_wale", "ref_d3q19_ldc_vreman")
+LES_BINARIES = ("ref_d3q19_ldc_smag", "ref_d3q19_ldc_wale", "ref_d3q19_ldc_vreman",
+                "ref_d2q9_ldc_smag", "ref_d2q9_ldc_wale", "ref_d2q9_ldc_vreman")
 
 
 def read_dump(path: Path, les: bool = False) -> dict:
@@ -198,7 +199,7 @@ def read_dump(path: Path, les: bool = False) -> dict:
     gaps_tail = take(np.int32, int(n_gap_keep))
     n_act = take(np.int32, 1)[0]
     blocks = take(np.int32, int(n_act))
-    NU = Q + dim + 1 + (1 if les else 0)
+    NU = Q + 5 if les else Q + dim + 1   # the harness sizes LES fields N_Q + 5 (eddy viscosity in row N_Q + 4)
     rec = [("fX", np.float32, dim), ("bmask", np.int32, 1), ("nbr", np.int32, Qmax), ("nbr_child", np.int32, Qmax),
            ("onb", np.int32, 1), ("ref", np.int32, 1), ("level", np.int32, 1), ("cmask", np.int32, MC),
            ("F", np.float32, NU * MC)]

@@ -252,11 +252,11 @@ def test_percentile_refinement_fp64_matches_oracle(Q, N, steps):
 def test_row_variant_bit_identical_on_multilevel_runs(Q, N, storage, kw):
     """The row-mapped step (variant 4) through interface blocks with missing
     same-level neighbours, the boundary hook and regrids, and the root-level
-    tile step (variant 5, 2D): the same populations and mesh as one cell per
-    thread, bit for bit."""
+    tile steps (variants 5 and 6, 2D): the same populations and mesh as one
+    cell per thread, bit for bit."""
     p = amr_params(Q, N, storage=storage, **kw)
     out = []
-    for v in (1, 4, 5):
+    for v in (1, 4, 5, 6):
         with ag.Case(p) as c:
             c.set_ic(0)
             c.set_tuning(v)

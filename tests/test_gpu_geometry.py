@@ -195,7 +195,7 @@ def test_wall_step_variants_and_graph_bit_identical(name):
     solid cells (the row variant's per-cell path next to solid cells)."""
     g = load(name)
     runs = []
-    for variant, graph in [(1, True), (2, True), (3, True), (4, True), (5, True), (1, False)]:
+    for variant, graph in [(1, True), (2, True), (3, True), (4, True), (5, True), (6, True), (1, False)]:
         c, p = run_case(g, variant=variant, use_graph=graph, steps=8)
         runs.append((c.dump(_lib.ARR_F), c.dump(_lib.ARR_CBLOCK_F_FF)))
         c.close()

@@ -75,7 +75,7 @@ def test_mrt_half_storage_vs_fp64_oracle(storage, tol_u):
 def test_mrt_step_variants_bit_identical(storage):
     p = mrt_params(12, storage=storage)
     out = []
-    for v in (1, 2, 3, 4, 5):
+    for v in (1, 2, 3, 4, 5, 6):
         with ag.Case(p) as c:
             c.set_ic(0)
             c.set_tuning(v)

@@ -157,14 +157,15 @@ def test_graph_replay_bit_identical():
 @pytest.mark.parametrize("Q,storage", [(9, _lib.STORE_FP32), (19, _lib.STORE_FP16), (27, _lib.STORE_FP32),
                                        (9, _lib.STORE_FP64)])
 def test_step_variants_bit_identical_and_autotune_pure(Q, storage):
-    """The five step kernels (1 and 2 cells per thread, TMA-staged
-    pipeline, one row of four cells per thread, root-level tiles) do the same
+    """The six step kernels (1 and 2 cells per thread, TMA-staged
+    pipeline, one row of four cells per thread, root-level tiles, root-level
+    push tiles) do the same
     arithmetic per cell, so their results agree bit for bit; autotuning leaves
     the state untouched."""
     N = 32 if Q == 9 else 12
     p = ldc_params(Q, N, storage=storage)
     out = []
-    for v in (1, 2, 3, 4, 5):
+    for v in (1, 2, 3, 4, 5, 6):
         with ag.Case(p) as c:
             c.set_ic(0)
             c.set_tuning(v)
@@ -178,7 +179,7 @@ def test_step_variants_bit_identical_and_autotune_pure(Q, storage):
         c.advance_n(5, use_graph=False)
         before = c.dump(_lib.ARR_F)
         r = c.autotune(0, reps=3)
-        assert r["variant"] in (1, 2, 3, 4, 5) and min(r["ms"]) > 0
+        assert r["variant"] in (1, 2, 3, 4, 5, 6) and min(r["ms"]) > 0
         c.sync()
         assert np.array_equal(c.dump(_lib.ARR_F), before)   # tuning does not advance the state
 
@@ -291,10 +292,11 @@ def test_large_grid_properties():
     (_lib.STORE_FP32, dict(Ny_factor=2)),
 ])
 def test_tile_step_bit_identical(storage, extra):
-    """The root-level tile step (variant 5): fully periodic tiles (the
-    select-free gather), a periodic channel with closed y walls, and lid-driven
-    cavities (closed links, the lid hook) give the populations of one cell per
-    thread bit for bit, with graph replay."""
+    """The root-level tile steps (variant 5 and the push tiles of variant 6):
+    fully periodic tiles (the select-free gather; every tile edge pushes into
+    a neighbouring tile), a periodic channel with closed y walls, and
+    lid-driven cavities (closed links, the lid hook) give the populations of
+    one cell per thread bit for bit, with graph replay."""
     extra = dict(extra)
     ny = extra.pop("Ny_factor", 1)
     p = ldc_params(9, 64, storage=storage, extra=extra)
@@ -302,7 +304,7 @@ def test_tile_step_bit_identical(storage, extra):
         p.L_fy = float(ny)
         p.n_maxcblocks = 16 * 16 * ny
     out = []
-    for v in (1, 5):
+    for v in (1, 5, 6):
         with ag.Case(p) as c:
             c.set_ic(0)
             c.set_tuning(v)
@@ -310,16 +312,18 @@ def test_tile_step_bit_identical(storage, extra):
             c.sync()
             out.append(c.dump(_lib.ARR_F))
     assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[2])
 
 
 def test_tile_step_refused_swaps_bit_identical():
     """A lid-driven cavity driven hard enough (tau near 1/2, lid 0.3) that
     populations go non-positive at the lid corners: the reference's stream
-    guard refuses those swaps.  The tile step decides them locally and must
-    match the push variants' fix-up list bit for bit."""
+    guard refuses those swaps.  The tile step decides them locally, the push
+    tiles record them (in and across tiles) in the fix-up list, and both must
+    match the push variants bit for bit."""
     p = ldc_params(9, 64, extra=dict(v0=1e-7, u_ref=0.3))
     out, neg = [], 0
-    for v in (1, 5):
+    for v in (1, 5, 6):
         with ag.Case(p) as c:
             c.set_ic(0)
             c.set_tuning(v)
@@ -330,6 +334,7 @@ def test_tile_step_refused_swaps_bit_identical():
             out.append(F)
     assert neg > 0, "the case did not produce a non-positive population"
     assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[2])
 
 
 def test_mass_momentum_async_equals_sync():

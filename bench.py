@@ -40,7 +40,9 @@ step as solver_lbm_advance.cu:74-89 counts them.
 Multi-GPU: one process per GPU under torchrun; every rank runs an
 independent replica of the workload (a single case does not shard), so the
 scaling is weak and `value` is the sum over ranks divided by the slowest
-rank's time.
+rank's time.  The batched measurement instead splits its fixed case list
+across the ranks (LPT packing, agal_b200.shard): strong scaling, the sum of
+the ranks' cell updates over the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -365,12 +367,23 @@ def batched_case(s: dict, storage: int, device: int):
     return case
 
 
-def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device: int) -> dict:
+def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device: int,
+                rank: int = 0, ws: int = 1, allsum=None, allmax=None, barrier=None) -> dict:
     """Aggregate MLUPS of the batch (FP16 populations, batched graph) and of
     the same cases in FP32 advanced one at a time; both after the same
     spin-up, timed with CUDA events over `steps` coarse steps that hold no
-    regrid (P_REFINE = 32, spin-up past the first regrid)."""
-    specs = batched_specs(n_cases, seed)
+    regrid (P_REFINE = 32, spin-up past the first regrid).  Under torchrun the
+    case list is split across the ranks by LPT packing (agal_b200.shard): each
+    rank builds and times only its cases; the figures are the sum of the
+    ranks' cell updates over the slowest rank's time."""
+    from agal_b200.shard import aggregate, case_cost, lpt_shards, shard_loads
+    allsum = allsum or (lambda x: x)
+    allmax = allmax or (lambda x: x)
+    barrier = barrier or (lambda: None)
+    specs_all = batched_specs(n_cases, seed)
+    costs = [case_cost(s) for s in specs_all]
+    shards = lpt_shards(costs, ws)
+    specs = [specs_all[i] for i in shards[rank]]
 
     def build(storage):
         cases = [batched_case(s, storage, device) for s in specs]
@@ -389,6 +402,7 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     upd16 = cells(cases)
     torch.cuda.synchronize()
+    barrier()
     e0.record(stream)
     batch.advance_n(steps)
     e1.record(stream)
@@ -415,24 +429,31 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
         t32 += a.elapsed_time(b)
     for c in cases:
         c.close()
-    v16 = upd16 * steps / (t16 * 1e-3) / 1e6
-    v32 = upd32 * steps / (t32 * 1e-3) / 1e6
+    agg16 = aggregate(upd16 * steps, t16, allsum, allmax)
+    agg32 = aggregate(upd32 * steps, t32, allsum, allmax)
+    v16, v32 = agg16["mlups"], agg32["mlups"]
+    upd16, upd32 = agg16["cell_updates"] / steps, agg32["cell_updates"] / steps
+    t16, t32 = agg16["ms"], agg32["ms"]
     peak, kind = measured_peak_hbm()
-    gbs = upd16 * steps * 2 * 19 * 2 / (t16 * 1e-3) / 1e9
+    gbs = upd16 * steps * 2 * 19 * 2 / (t16 * 1e-3) / 1e9 / ws   # per GPU
     return {"workload": "batched_d3q19_64", "n_cases": n_cases, "seed": seed,
             "desc": "independent D3Q19 BGK cases, base N^3 with N in {32,48,64,96}, 1-3 levels, Re log-uniform "
                     "[100,1000], half lid-driven cavities with percentile solution refinement, half flow past "
                     "a seeded ellipsoid (axes 8-24 cells) with near-wall refinement, interpolated bounce-back "
                     "and MEA forces; refinement by the plain criterion (no learned predictor)",
             "spinup_steps": spinup, "timed_steps": steps,
+            "sharding": {"ranks": ws, "scaling": "strong" if ws > 1 else "n/a",
+                         "packing": "LPT on base cells x 2^(levels-1)",
+                         "cases_per_rank": [len(x) for x in shards],
+                         "load_per_rank": shard_loads(costs, shards)},
             "value": v16, "unit": "MLUPS", "storage": "f16-offset", "ms_per_step": t16 / steps,
             "cell_updates_per_step": upd16,
             "one_at_a_time_fp32": {"value": v32, "ms_per_step": t32 / steps, "cell_updates_per_step": upd32},
             "ratio_vs_one_at_a_time_fp32": v16 / v32,
-            "hbm": {"achieved_gbs": gbs, "peak": peak, "frac": gbs / peak, "peak_source": kind,
+            "hbm": {"achieved_gbs_per_gpu": gbs, "peak": peak, "frac": gbs / peak, "peak_source": kind,
                     "bytes_per_update": 2 * 19 * 2},
             "autotune_variants": {"fp16": tunes16, "fp32": tunes32},
-            "blocks_per_level_fp16": levels16}
+            "blocks_per_level_fp16": levels16, "blocks_per_level_of": "rank 0's cases"}
 
 
 def run_cpu_oracle(w: dict, seconds: float, threads: int, max_steps: int | None = None) -> dict:
@@ -926,7 +947,8 @@ def main(argv=None) -> int:
     # --- batched independent cases vs the same cases one at a time -----------
     batched = None
     if a.batched_cases > 0:
-        batched = run_batched(torch, a.batched_cases, a.batched_seed, spinup=40, steps=20, device=local)
+        batched = run_batched(torch, a.batched_cases, a.batched_seed, spinup=40, steps=20, device=local,
+                              rank=rank, ws=ws, allsum=allsum, allmax=allmax, barrier=barrier)
 
     # --- CPU baseline (rank 0 only) -------------------------------------------
     cpu = None

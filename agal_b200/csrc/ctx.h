@@ -25,6 +25,7 @@
 // geometry_bins.h:66-86): n = faces per bin, N = start, ids = face IDs.
 struct agal_bins_d {
     int density = 0, n_bins = 0;
+    float sx = 0.f, sy = 0.f, sz = 0.f;   // bins per unit length along x, y, z
     long long n_entries = 0;
     int *n = nullptr, *N = nullptr, *ids = nullptr;
 };

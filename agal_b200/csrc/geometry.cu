@@ -144,8 +144,16 @@ __device__ __forceinline__ float fminf3(float a, float b, float c) { return fmin
 __device__ __forceinline__ float fmaxf3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
 
 // ---- binning --------------------------------------------------------------
+// The reference indexes bins as coordinate x density and cells as
+// coordinate x N (geometry_bins_gpu.cu:174-560, mesh_voxelizer_voxelize.cu:
+// 253-258), which is right on the unit cube it is built for but disagrees
+// with its own bin sizes L / density on any other box.  Here bins are
+// indexed per axis with sx = density / Lx (sy, sz alike) and cells with
+// cpl = Nx / Lx (cells per unit length): the same floats on the unit cube,
+// consistent bins on a channel.
 struct BinGrid {
     float dxL, Lx, Ly, Lz, L0x, L0y, L0z;
+    float sx, sy, sz, cpl;
     int dens, Nx, Ny, Nz;
 };
 
@@ -159,8 +167,8 @@ __global__ void k_ray_filter(const float *X, int nf, BinGrid g, int md, int *fou
     const v3 n = face_normal_unit(a, b, c);
     const float dxL = g.dxL, dxo2 = fmul(0.5f, g.dxL);
     int hit = 0;
-    const int iymin = (int)fmul(fminf3(a.y, b.y, c.y), (float)g.Ny), iymax = (int)fmul(fmaxf3(a.y, b.y, c.y), (float)g.Ny);
-    const int izmin = (int)fmul(fminf3(a.z, b.z, c.z), (float)g.Nz), izmax = (int)fmul(fmaxf3(a.z, b.z, c.z), (float)g.Nz);
+    const int iymin = (int)fmul(fminf3(a.y, b.y, c.y), g.cpl), iymax = (int)fmul(fmaxf3(a.y, b.y, c.y), g.cpl);
+    const int izmin = (int)fmul(fminf3(a.z, b.z, c.z), g.cpl), izmax = (int)fmul(fmaxf3(a.z, b.z, c.z), g.cpl);
     if (!md) {
         for (int iz = izmin; iz <= izmax && !hit; iz++)
             for (int iy = iymin; iy <= iymax && !hit; iy++) {
@@ -170,7 +178,7 @@ __global__ void k_ray_filter(const float *X, int nf, BinGrid g, int md, int *fou
                 if (point_in_face_aabb(q, a, b, c)) hit = 1;
             }
     } else {
-        const int ixmin = (int)fmul(fminf3(a.x, b.x, c.x), (float)g.Nx), ixmax = (int)fmul(fmaxf3(a.x, b.x, c.x), (float)g.Nx);
+        const int ixmin = (int)fmul(fminf3(a.x, b.x, c.x), g.cpl), ixmax = (int)fmul(fmaxf3(a.x, b.x, c.x), g.cpl);
         for (int p = 1; p < 27 && !hit; p++) {
             if (!lat_half(3, p)) continue;
             const v3 ray = V((float)lat_c(3, 0, p), (float)lat_c(3, 1, p), (float)lat_c(3, 2, p));
@@ -213,9 +221,8 @@ __global__ void k_bin_limits(const float *X, int nf, BinGrid g, const int *rank,
     if ((bm.x < -dx && bM.x < -dx) || (bm.x > Lxd && bM.x > Lxd)) return;
     if ((bm.y < -dx && bM.y < -dx) || (bm.y > Lyd && bM.y > Lyd)) return;
     if ((bm.z < -dx && bM.z < -dx) || (bm.z > Lzd && bM.z > Lzd)) return;
-    const float D = (float)g.dens;
-    const int xl = (int)fmul(bm.x, D) - 1, yl = (int)fmul(bm.y, D) - 1, zl = (int)fmul(bm.z, D) - 1;
-    const int xL = (int)fmul(bM.x, D) + 1, yL = (int)fmul(bM.y, D) + 1, zL = (int)fmul(bM.z, D) + 1;
+    const int xl = (int)fmul(bm.x, g.sx) - 1, yl = (int)fmul(bm.y, g.sy) - 1, zl = (int)fmul(bm.z, g.sz) - 1;
+    const int xL = (int)fmul(bM.x, g.sx) + 1, yL = (int)fmul(bM.y, g.sy) + 1, zL = (int)fmul(bM.z, g.sz) + 1;
     int counter = 0;
     for (int K = zl; K < zL + 1; K++)
         for (int J = yl; J < yL + 1; J++)
@@ -305,7 +312,15 @@ constexpr int N_LEFT = 2, N_RIGHT = 1;   // neighbour rows of -x / +x in 3D
 struct BinsView {
     const int *n, *N, *ids;
     int density, n_bins;
+    float sx, sy, sz;
 };
+
+// Bin of a point (per-axis bins per unit length, see BinGrid).
+__device__ __forceinline__ int bin_of(const BinsView &b, v3 p)
+{
+    const int D = b.density;
+    return (int)fmul(p.x, b.sx) + D * (int)fmul(p.y, b.sy) + D * D * (int)fmul(p.z, b.sz);
+}
 
 // Cu_Voxelize_V1 (mesh_voxelizer_voxelize.cu:203-351), one CTA of 64 threads
 // per block: each cell takes the closest face of its bin crossed by its +x
@@ -320,8 +335,7 @@ __global__ void __launch_bounds__(MC3) k_voxelize(const int *ids, long long nmb,
     const int t = threadIdx.x, I = t & 3, J = (t >> 2) & 3, K = t >> 4;
     if (t == 0) s_any = 0;
     const v3 p = V(cell_centre(fX[b], I, dxL), cell_centre(fX[b + nmb], J, dxL), cell_centre(fX[b + 2 * nmb], K, dxL));
-    const int D = bins.density;
-    const int gb = (int)fmul(p.x, (float)D) + D * (int)fmul(p.y, (float)D) + D * D * (int)fmul(p.z, (float)D);
+    const int gb = bin_of(bins, p);
     const int n_f = (gb >= 0 && gb < bins.n_bins) ? bins.n[gb] : 0;
     int pmin = -1, mask = CELL_INTERIOR;
     float dmin = 1.0f;
@@ -607,8 +621,7 @@ __global__ void __launch_bounds__(MC3) k_links(const int *ids, long long nmb, fl
     if (slot < 0) return;
     const int t = threadIdx.x, I = t & 3, J = (t >> 2) & 3, K = t >> 4;
     const v3 p = V(cell_centre(fX[b], I, dxL), cell_centre(fX[b + nmb], J, dxL), cell_centre(fX[b + 2 * nmb], K, dxL));
-    const int D = bins.density;
-    const int gb = (int)fmul(p.x, (float)D) + D * (int)fmul(p.y, (float)D) + D * D * (int)fmul(p.z, (float)D);
+    const int gb = bin_of(bins, p);
     const int n_f = (gb >= 0 && gb < bins.n_bins) ? bins.n[gb] : 0;
     if (n_f <= 0) return;
     float dQ[27];
@@ -711,6 +724,8 @@ BinGrid bin_grid(const agal_ctx *c, int L, int *nbl_out)
     }
     g.dxL = dxf; g.L0x = L0x; g.L0y = L0y; g.L0z = L0z;
     g.dens = dens; g.Nx = nx; g.Ny = ny; g.Nz = nz;
+    g.sx = (float)dens / Lx; g.sy = (float)dens / Ly; g.sz = (float)dens / Lz;
+    g.cpl = (float)nx / Lx;
     return g;
 }
 
@@ -775,6 +790,7 @@ int make_bins(agal_ctx *c, int L, int md, agal_bins_d &out)
         out.N = start;
         cnt = start = nullptr;
         out.density = g.dens;
+        out.sx = g.sx; out.sy = g.sy; out.sz = g.sz;
         out.n_bins = (int)n_bins;
         out.n_entries = ne;
         AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -810,7 +826,7 @@ int ensure_geometry_state(agal_ctx *c)
     return AGAL_OK;
 }
 
-BinsView view(const agal_bins_d &b) { return BinsView{b.n, b.N, b.ids, b.density, b.n_bins}; }
+BinsView view(const agal_bins_d &b) { return BinsView{b.n, b.N, b.ids, b.density, b.n_bins, b.sx, b.sy, b.sz}; }
 
 }  // namespace
 

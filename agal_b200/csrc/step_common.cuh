@@ -59,6 +59,7 @@ constexpr int META_ACTIVE = 1;   // collide/stream this block (kernels.cu:236)
 constexpr int META_ONB = 2;      // block touches a domain boundary (kernels.cu:736)
 constexpr int META_WALL = 4;     // wall block stepped by k_step_wall (interpolated bounce-back)
 constexpr int META_NEARSOLID = 8;   // a solid cell in this block or a neighbour (geometry cases)
+constexpr int META_CLOSED = 16;     // some neighbour slot holds no block (closed links possible)
 
 struct StepArgs {
     const int *ids;

@@ -441,6 +441,8 @@ __global__ void k_build_meta(long long nmb, const int *nbr, const int *nbr_child
     } else if (i == Meta<DIM>::FLAGS) {
         if (nbr_child[b] < 0 || bmask[b] != BLOCK_SOLID) v |= META_ACTIVE;
         if (onb[b] == 1) v |= META_ONB;
+        for (int k = 0; k < QMAX; k++)
+            if (nbr[b + (long long)k * nmb] < 0) v |= META_CLOSED;
         if (onb_solid && onb[b] == 1 && onb_solid[b] >= 0) v |= META_WALL;
         if (blk_solid) {
             // A solid cell in the block or in a block of its neighbourhood:

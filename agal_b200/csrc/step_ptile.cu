@@ -10,15 +10,17 @@
 // cell per thread):
 //  1. each thread loads its cell's Q populations (as variant 1) and collides
 //     them (collide_cell, the same arithmetic as every variant);
-//  2. a value whose destination lies in the tile goes to shared memory at a
-//     compile-time offset from the thread's own cell (slot planes of the
-//     tile, row-major); a value that leaves the tile, or a bounce-back at a
-//     closed link, takes variant 1's path (neighbour from the block's
-//     metadata row, boundary hook, direct store);
+//  2. every post-collision value goes to shared memory at a compile-time
+//     offset from the thread's own cell (slot planes of the tile and a
+//     one-cell halo ring, row-major), so the pushes are uniform across the
+//     warp; only blocks with a missing neighbour (the domain boundary) add
+//     the bounce-back of their closed links (boundary hook included) into
+//     their own cells;
 //  3. after one barrier the tile's output is written block by block: every
 //     16-byte chunk of a block's slot rows whose values all came from inside
 //     the tile (or from bounce-back) is one vector store; a chunk with
-//     values pushed in from a neighbouring tile writes only its own cells.
+//     values pushed in from a neighbouring tile writes only its own cells;
+//     the halo ring's values go to the neighbouring tiles' blocks.
 // Stochastic rounding is keyed by the source cell and direction, and the
 // reference's stream guard is recorded in the fix-up list as in variant 1,
 // so the output is bit-identical to every other variant.  DRAM traffic stays
@@ -46,15 +48,19 @@ constexpr int PNB = PBX * PBY;                // 32 blocks
 constexpr int PNT = PCX * PCY;                // 512 threads, one cell each
 
 template <typename T> struct PTile {
-    // Row stride of a slot plane (elements): a warp's two 4 x 4-cell blocks
-    // push to distinct banks, and each chunk's rows start 8-byte (half) or
-    // 16-byte (float) aligned.
-    static constexpr int RS = sizeof(T) == 2 ? 36 : 40;
-    static constexpr int PS = RS * PCY;                 // plane stride (elements)
+    // Slot planes hold the tile and a one-cell halo ring: cell (x, y) of the
+    // tile, x in -1..32, y in -1..16, sits at row y + 1, column x + 4, so
+    // that the tile's rows start 8-byte (half) or 16-byte (float) aligned.
+    // With 40 elements per row a warp's two 4 x 4-cell blocks push to
+    // (nearly) distinct banks.
+    static constexpr int RS = 40;
+    static constexpr int X0 = 4, Y0 = 1;               // column / row of tile cell (0, 0)
+    static constexpr int PS = RS * (PCY + 2);           // plane stride (elements)
     static constexpr int CH = 16 / (int)sizeof(T);      // cells per 16-byte chunk (8 or 4)
     static constexpr int CPB = 9 * 16 / CH;             // chunks per block
     static constexpr int NCH = PNB * CPB;               // chunks per tile
-    static_assert((PS * (int)sizeof(T)) % 16 == 0, "plane alignment");
+    static constexpr int NHALO = 2 * (PCX + 2) + 2 * PCY;   // halo cells (100)
+    static_assert((PS * (int)sizeof(T)) % 16 == 0 && (RS * (int)sizeof(T)) % 16 == 0, "plane alignment");
 };
 
 template <typename T>
@@ -76,6 +82,7 @@ __global__ void __launch_bounds__(PNT, 3) k_step_ptile(const StepArgs a, int nbx
     using C = typename ST<T>::C;
     constexpr int MC = 16, BLK = 9 * MC, W = Meta<2>::W;
     constexpr int RS = PTile<T>::RS, PS = PTile<T>::PS, CH = PTile<T>::CH, CPB = PTile<T>::CPB;
+    constexpr int X0 = PTile<T>::X0, Y0 = PTile<T>::Y0;
     __shared__ __align__(16) T s_out[9 * PS];
     __shared__ int s_meta[PNB][W];
     const int tid = threadIdx.x, lb = tid >> 4, t = tid & 15;
@@ -101,66 +108,68 @@ __global__ void __launch_bounds__(PNT, 3) k_step_ptile(const StepArgs a, int nbx
     __syncthreads();
 
     const int *nrow = s_meta[lb];
-    const bool hook = (nrow[Meta<2>::FLAGS] & META_ONB) && a.bc_preset != AGAL_BC_NONE;
+    const int flags = nrow[Meta<2>::FLAGS];
     C ux, uy, uz;
     collide_cell<2, 9, T>(g, a, ux, uy, uz);
     const int x = 4 * lbx + I, y = 4 * lby + J;
-    T *own_s = s_out + y * RS + x;
+    T *own_s = s_out + (y + Y0) * RS + (x + X0);
     T *__restrict__ fo = static_cast<T *>(a.fout);
     const unsigned rc = a.sr ? sr_cell_of<2>(b, t, seed) : 0u;
-    // The stream guard of push_cell: the non-owning side of an open link
-    // records it when its value is not positive.
-    auto guard = [&](int p, long long dst) {
-        if (p == 0 || lat_half(2, p)) return;
-        if (g[p] + (ST<T>::OFF ? C(lat_w(9, p)) : C(0)) > C(0)) return;
-        const int k = atomicAdd(a.fix_count, 1);
-        if (k < a.fix_cap) {
-            a.fix_list[2 * k] = dst;
-            a.fix_list[2 * k + 1] = (long long)b * BLK + p * MC + t;
-        }
-    };
+    // Every value goes to the tile's planes (the halo ring for destinations
+    // outside the tile): slot pb(p) of the cell x + c_p.
 #pragma unroll
     for (int p = 0; p < 9; p++) {
         const int cx = lat_c(2, 0, p), cy = lat_c(2, 1, p);
-        const bool in = (unsigned)(x + cx) < (unsigned)PCX && (unsigned)(y + cy) < (unsigned)PCY;
-        if (in) {
-            // every root block of the tile exists: an open link
-            own_s[lat_pb(2, p) * PS + cy * RS + cx] = enc_r<T>(g[p], rc * sr_dir(p), a.sr);
-            if (p != 0 && !lat_half(2, p) &&
-                !(g[p] + (ST<T>::OFF ? C(lat_w(9, p)) : C(0)) > C(0))) {
-                const int X = x + cx, Y = y + cy;
-                const long long bd = (bx0 + (X >> 2)) + (long long)nbx * (by0 + (Y >> 2));
-                guard(p, bd * BLK + lat_pb(2, p) * MC + (X & 3) + 4 * (Y & 3));
-            }
-        } else {
+        own_s[lat_pb(2, p) * PS + cy * RS + cx] = enc_r<T>(g[p], rc * sr_dir(p), a.sr);
+    }
+    // Blocks with a missing neighbour (the domain boundary): closed links
+    // bounce back into slot p of the cell itself, through the boundary hook
+    // on boundary blocks (push_cell's closed links).
+    if (flags & META_CLOSED) {
+        const bool hook = (flags & META_ONB) && a.bc_preset != AGAL_BC_NONE;
+#pragma unroll
+        for (int p = 1; p < 9; p++) {
+            const int cx = lat_c(2, 0, p), cy = lat_c(2, 1, p);
             const int nb = nrow[nbr_slot(2, I + cx, J + cy, 0)];
-            if (nb >= 0) {
-                const long long to = (long long)nb * BLK + lat_pb(2, p) * MC + nbr_cell(2, I + cx, J + cy, 0);
-                fo[to] = enc_r<T>(g[p], rc * sr_dir(p), a.sr);
-                guard(p, to);
-            } else {
-                C v = g[p];
-                if (hook && nb != N_SKIPID) {   // domain boundary: Cu_ImposeBC hook (kernels.cu:791-792)
-                    const C wp = C(lat_w(9, p));
-                    const C off = ST<T>::OFF ? wp : C(0);
-                    v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx, cy, 0, C(a.u_ref)) - off;
-                }
-                own_s[p * PS] = enc_r<T>(v, rc * sr_dir(p), a.sr);
+            if (nb >= 0) continue;
+            C v = g[p];
+            if (hook && nb != N_SKIPID) {   // domain boundary: Cu_ImposeBC hook (kernels.cu:791-792)
+                const C wp = C(lat_w(9, p));
+                const C off = ST<T>::OFF ? wp : C(0);
+                v = bc_hook<C>(a.bc_preset, nb, v + off, ux, uy, uz, wp, cx, cy, 0, C(a.u_ref)) - off;
             }
+            own_s[p * PS] = enc_r<T>(v, rc * sr_dir(p), a.sr);
+        }
+    }
+    // The stream guard of push_cell: the non-owning side of an open link
+    // records it when its value is not positive (rare; the destination's
+    // global index is worked out only then).
+#pragma unroll
+    for (int p = 1; p < 9; p++) {
+        if (lat_half(2, p)) continue;
+        if (g[p] + (ST<T>::OFF ? C(lat_w(9, p)) : C(0)) > C(0)) continue;
+        const int cx = lat_c(2, 0, p), cy = lat_c(2, 1, p);
+        const int nb = nrow[nbr_slot(2, I + cx, J + cy, 0)];
+        if (nb < 0) continue;   // closed link: bounce-back, nothing to refuse
+        const long long to = (long long)nb * BLK + lat_pb(2, p) * MC + nbr_cell(2, I + cx, J + cy, 0);
+        const int k = atomicAdd(a.fix_count, 1);
+        if (k < a.fix_cap) {
+            a.fix_list[2 * k] = to;
+            a.fix_list[2 * k + 1] = (long long)b * BLK + p * MC + t;
         }
     }
     __syncthreads();
 
-    // Output: chunk k = 16 bytes of slot s of tile block kb.  Slot s of cell
-    // X holds the value pushed from X + c_s; it is this tile's unless X + c_s
-    // lies outside the tile in an existing block.
+    // Output 1: chunk k = 16 bytes of slot s of tile block kb.  Slot s of
+    // cell X holds the value pushed from X + c_s; it is this tile's unless
+    // X + c_s lies outside the tile in an existing block (that tile stores it).
     for (int k = tid; k < PTile<T>::NCH; k += PNT) {
         const int kb = k / CPB, r = k - kb * CPB;
         const int s = r / (16 / CH), c0 = (r - s * (16 / CH)) * CH;
         const int kbx = kb % PBX, kby = kb / PBX;
         const int cxs = lat_c(2, 0, s), cys = lat_c(2, 1, s);
         const int x0 = 4 * kbx, y0 = 4 * kby + (c0 >> 2);
-        const T *src = s_out + s * PS + y0 * RS + x0;
+        const T *src = s_out + s * PS + (y0 + Y0) * RS + (x0 + X0);
         T *dst = fo + ((long long)(bx0 + kbx) + (long long)nbx * (by0 + kby)) * BLK + s * MC + c0;
         const bool inside = x0 + cxs >= 0 && x0 + 3 + cxs < PCX && y0 + cys >= 0 && y0 + CH / 4 - 1 + cys < PCY;
         if (inside) {
@@ -174,6 +183,33 @@ __global__ void __launch_bounds__(PNT, 3) k_step_ptile(const StepArgs a, int nbx
                                  s_meta[kb][nbr_slot(2, Ic + cxs, Jc + cys, 0)] >= 0;
                 if (!ext) dst[c] = src[(c >> 2) * RS + (c & 3)];
             }
+        }
+    }
+    // Output 2: the halo ring, pushed into the neighbouring tiles' blocks.
+    // Halo cell h (x in -1..32, y in -1..16 on the ring) receives, in slot
+    // pb(p), the value of the tile cell h - c_p for each direction p whose
+    // source lies in the tile.
+    for (int k = tid; k < PTile<T>::NHALO; k += PNT) {
+        int hx, hy;
+        if (k < PCX + 2) {
+            hx = k - 1, hy = -1;
+        } else if (k < 2 * (PCX + 2)) {
+            hx = k - (PCX + 2) - 1, hy = PCY;
+        } else if (k < 2 * (PCX + 2) + PCY) {
+            hx = -1, hy = k - 2 * (PCX + 2);
+        } else {
+            hx = PCX, hy = k - 2 * (PCX + 2) - PCY;
+        }
+#pragma unroll
+        for (int p = 1; p < 9; p++) {
+            const int cx = lat_c(2, 0, p), cy = lat_c(2, 1, p);
+            const int sx = hx - cx, sy = hy - cy;   // source cell in the tile
+            if (!((unsigned)sx < (unsigned)PCX && (unsigned)sy < (unsigned)PCY)) continue;
+            const int sb = (sx >> 2) + PBX * (sy >> 2), Is = sx & 3, Js = sy & 3;
+            const int nb = s_meta[sb][nbr_slot(2, Is + cx, Js + cy, 0)];
+            if (nb < 0) continue;                     // closed link: bounced back in the tile
+            fo[(long long)nb * BLK + lat_pb(2, p) * MC + nbr_cell(2, Is + cx, Js + cy, 0)] =
+                s_out[lat_pb(2, p) * PS + (hy + Y0) * RS + (hx + X0)];
         }
     }
     if (a.fix_ticket) fused_fixup<T>(a);

@@ -646,6 +646,63 @@ def drag_lift(device: int) -> dict:
     return out
 
 
+def config4(torch, device: int, steps: int) -> dict:
+    """The D3Q27 icosphere channel: external flow over a seeded icosphere
+    (20,480 faces, diameter 32 root cells) in a 256 x 128 x 128 channel, 4
+    levels with the finest band around the body (near-wall refinement),
+    uniform inflow u = 0.05 with seeded 1% noise, Re = 200 on the diameter,
+    interpolated bounce-back and momentum-exchange forces.  FP64, FP32 and
+    FP16 storage run the same `steps` coarse steps; drag and lift are the MEA
+    forces of the last one; MLUPS over 20 coarse steps (CUDA events).  The
+    reference's own build cannot run this box like for like (its bins assume
+    the unit cube), so FP64 of this library is the judge."""
+    from agal_b200.geometry import icosphere
+    N, R = 256, 16.0 / 256
+    faces = icosphere(5, R, (0.25, 0.25, 0.25), seed=2024)
+    out = {"workload": "channel3d27_256x128x128_icosphere", "n_faces": int(len(faces)), "coarse_steps": steps,
+           "desc": "D3Q27 BGK channel 256x128x128 (1 x 0.5 x 0.5), seeded icosphere of 20,480 faces, diameter 32 "
+                   "root cells, 4 levels near the wall, inflow 0.05 with 1% seeded noise, Re 200, Bouzidi walls, "
+                   "MEA drag/lift; plain criterion only"}
+    forces = {}
+    for name, st in (("fp64", _lib.STORE_FP64), ("fp32", _lib.STORE_FP32), ("fp16", _lib.STORE_FP16)):
+        p = ag.default_params(velocity_set=_lib.D3Q27, Nx=N, L_fy=0.5, L_fz=0.5, MAX_LEVELS_WALL=4,
+                              MAX_LEVELS_INTERIOR=1, v0=0.05 * 2 * R / 200.0, P_REFINE=10 ** 8, G_BIN_DENSITY=8,
+                              G_BIN_LEVELS=4, G_BIN_SPEC=2, G_BIN_MAKE_LINKS=1, G_NEAR_WALL_DISTANCE=0.02,
+                              S_BC_TYPE=1, S_FORCE_TYPE=0, S_FORCE_ORDER=2, bc_preset=_lib.BC_FPSC3D,
+                              ic_preset=_lib.IC_UNIFORM, u_ref=0.05, ic_noise=0.01, seed=2024,
+                              interp_order=_lib.INTERP_LINEAR, storage=st, n_maxcblocks=500000, device=device)
+        with ag.Case(p) as c:
+            c.set_geometry(faces)
+            c.set_ic(0)
+            c.refine_near_wall()
+            c.autotune(0, reps=3)
+            n_pre = max(steps - 21, 0)
+            c.advance_n(n_pre, use_graph=True)
+            cnt = c.counts()
+            upd = leaf_cells(cnt, 3)
+            c.sync()
+            stream = torch.cuda.ExternalStream(c.stream_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            c.advance_n(20, use_graph=True)
+            e1.record(stream)
+            c.sync()
+            ms = e0.elapsed_time(e1) / 20
+            c.forces()                       # partials reset: the last step's forces follow
+            c.advance_n(steps - n_pre - 20, use_graph=True)
+            fr = c.forces()
+            forces[name] = np.array([fr[0] - fr[1], fr[2] - fr[3], fr[4] - fr[5]])
+            out[name] = {"mlups": upd / (ms * 1e-3) / 1e6, "ms_per_coarse_step": ms, "cell_updates_per_step": upd,
+                         "blocks_per_level": cnt["n_ids"][:-1], "drag": float(forces[name][0]),
+                         "lift": [float(forces[name][1]), float(forces[name][2])]}
+    ref = forces["fp64"]
+    for name in ("fp32", "fp16"):
+        out[name]["drag_rel_vs_fp64"] = float(abs(forces[name][0] - ref[0]) / abs(ref[0]))
+        out[name]["lift_rel_vs_fp64_drag"] = float(np.abs(forces[name][1:] - ref[1:]).max() / abs(ref[0]))
+    out["fp16_over_fp32_mlups"] = out["fp16"]["mlups"] / out["fp32"]["mlups"]
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -658,6 +715,8 @@ def main(argv=None) -> int:
     ap.add_argument("--roofline-workload", default=None, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--config4-steps", type=int, default=600,
+                    help="coarse steps of the D3Q27 icosphere channel leg (0 skips it)")
     ap.add_argument("--error-steps", type=int, default=20000,
                     help="coarse steps of the FP32/FP16-vs-FP64 error runs (0 skips them)")
     ap.add_argument("--profile", choices=sorted(WORKLOADS), default=None,
@@ -943,6 +1002,7 @@ def main(argv=None) -> int:
 
     # --- precision: FP32 / FP16 against FP64 on the headline case ----------
     errors = error_vs_fp64(a.workload, a.error_steps, local) if (a.error_steps > 0 and w.get("amr")) else None
+    channel = config4(torch, local, a.config4_steps) if a.config4_steps > 0 else None
 
     # --- batched independent cases vs the same cases one at a time -----------
     batched = None
@@ -983,6 +1043,8 @@ def main(argv=None) -> int:
             line["reference_rule_fp32"] = ref_rule
         if errors is not None:
             line["error_vs_fp64"] = errors
+        if channel is not None:
+            line["channel_d3q27"] = channel
         if batched is not None:
             line["batched"] = batched
         print(json.dumps(line), flush=True)

@@ -308,8 +308,11 @@ static int make_bins(orc_case *c, const bin_grid *g, int L, int md, orc_bins *ou
     if (use_ray) {
 #pragma omp parallel for schedule(dynamic, 64)
         for (int f = 0; f < nf; f++) {
-            const int hit = md ? ray_filter_md(c, f, dxL, dxLo2, (float)g->Nxi[0][L], (float)g->Nxi[1][L], (float)g->Nxi[2][L])
-                               : ray_filter_1d(c, f, dxL, dxLo2, (float)g->Nxi[1][L], (float)g->Nxi[2][L]);
+            /* cells per unit length on every axis: the reference's
+               coordinate x N per axis, which agrees with it on the unit
+               cube and stays consistent on a channel */
+            const float cpl = (float)g->Nxi[0][L] / g->Lx;
+            const int hit = md ? ray_filter_md(c, f, dxL, dxLo2, cpl, cpl, cpl) : ray_filter_1d(c, f, dxL, dxLo2, cpl, cpl);
             ray[f] = hit ? f : -1;
         }
         /* copy_if + scatter: ray[f] becomes the rank of f among the kept faces. */
@@ -326,6 +329,9 @@ static int make_bins(orc_case *c, const bin_grid *g, int L, int md, orc_bins *ou
     const float dx = g->dxf[0][L] + FLT_EPSILON;
     const float Lx = g->Lx, Ly = g->Ly, Lz = g->Lz;
     const float L0x = g->Lx0g[0][L], L0y = g->Lx0g[1][L], L0z = g->Lx0g[2][L];
+    /* bins per unit length per axis (the reference's coordinate x density on
+       the unit cube) */
+    const float sx = (float)dens / Lx, sy = (float)dens / Ly, sz = (float)dens / Lz;
     int bad = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
     for (int f = 0; f < nf; f++) {
@@ -338,8 +344,8 @@ static int make_bins(orc_case *c, const bin_grid *g, int L, int md, orc_bins *ou
         if ((bm.x < -dx && bM.x < -dx) || (bm.x > Lx + dx && bM.x > Lx + dx)) continue;
         if ((bm.y < -dx && bM.y < -dx) || (bm.y > Ly + dx && bM.y > Ly + dx)) continue;
         if ((bm.z < -dx && bM.z < -dx) || (bm.z > Lz + dx && bM.z > Lz + dx)) continue;
-        const int xl = (int)(bm.x * (float)dens) - 1, yl = (int)(bm.y * (float)dens) - 1, zl = (int)(bm.z * (float)dens) - 1;
-        const int xL = (int)(bM.x * (float)dens) + 1, yL = (int)(bM.y * (float)dens) + 1, zL = (int)(bM.z * (float)dens) + 1;
+        const int xl = (int)(bm.x * sx) - 1, yl = (int)(bm.y * sy) - 1, zl = (int)(bm.z * sz) - 1;
+        const int xL = (int)(bM.x * sx) + 1, yL = (int)(bM.y * sy) + 1, zL = (int)(bM.z * sz) + 1;
         int counter = 0;
         for (int K = zl; K < zL + 1; K++)
             for (int J = yl; J < yL + 1; J++)
@@ -375,6 +381,7 @@ static int make_bins(orc_case *c, const bin_grid *g, int L, int md, orc_bins *ou
     free(pos); free(key); free(val);
     free_bins(out);
     out->density = dens;
+    out->sx = sx; out->sy = sy; out->sz = sz;
     out->n_bins = n_bins;
     out->n_entries = ne;
     out->n = cnt;
@@ -460,8 +467,8 @@ static void voxelize_block(orc_case *c, int b, float dxL, const orc_bins *bins)
         const int I = t % 4, J = (t / 4) % 4, K = t / 16;
         const v3 vp = V(cell_centre(c->cblock_f_X[b + 0 * nmb], I, dxL), cell_centre(c->cblock_f_X[b + 1 * nmb], J, dxL),
                         cell_centre(c->cblock_f_X[b + 2 * nmb], K, dxL));
-        const int gb = (int)(vp.x * (float)dens) + dens * (int)(vp.y * (float)dens) +
-                       dens * dens * (int)(vp.z * (float)dens);
+        const int gb = (int)(vp.x * bins->sx) + dens * (int)(vp.y * bins->sy) +
+                       dens * dens * (int)(vp.z * bins->sz);
         int pmin = -1, mask = ORC_CELL_INTERIOR;
         float dmin = 1.0f;
         const int n_f = (gb >= 0 && gb < bins->n_bins) ? bins->n[gb] : 0;
@@ -803,8 +810,8 @@ int orc_link_lengths(orc_case *c, int L)
             const int I = t % 4, J = (t / 4) % 4, K = t / 16;
             const v3 vp = V(cell_centre(c->cblock_f_X[b + 0 * nmb], I, dxL), cell_centre(c->cblock_f_X[b + 1 * nmb], J, dxL),
                             cell_centre(c->cblock_f_X[b + 2 * nmb], K, dxL));
-            const int gb = (int)(vp.x * (float)dens) + dens * (int)(vp.y * (float)dens) +
-                           dens * dens * (int)(vp.z * (float)dens);
+            const int gb = (int)(vp.x * bins->sx) + dens * (int)(vp.y * bins->sy) +
+                           dens * dens * (int)(vp.z * bins->sz);
             const int n_f = (gb >= 0 && gb < bins->n_bins) ? bins->n[gb] : 0;
             if (n_f <= 0) continue;
             float dQ[27];

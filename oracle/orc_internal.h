@@ -45,6 +45,7 @@
 /* One CSR set of face bins (Bins::binned_face_ids_{n,N,}, geometry_bins.h:66-86). */
 typedef struct orc_bins {
     int density, n_bins;
+    float sx, sy, sz;   /* bins per unit length along x, y, z (density / L) */
     int64_t n_entries;
     int *n, *N, *ids;
 } orc_bins;

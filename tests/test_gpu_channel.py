@@ -37,11 +37,12 @@ def sphere_faces(subdiv=4):
     return icosphere(subdiv, RADIUS, CENTRE, seed=3)
 
 
-def solid_centres(c, p):
-    """Centres of the solid cells of the finest level, in domain units."""
+def solid_centres(c, p, L=None):
+    """Centres of the solid cells of level L (default: the finest), in
+    domain units, and the level's cell size."""
     nmb = p.n_maxcblocks
     cnt = c.counts()
-    L = cnt["max_levels"] - 1
+    L = cnt["max_levels"] - 1 if L is None else L
     ids = c.dump(_lib.ARR_ID_SET).reshape(-1, nmb)[L, : cnt["n_ids"][L]].astype(np.int64)
     cm = c.dump(_lib.ARR_CELLS_ID_MASK).reshape(nmb, 64)[ids]
     fX = c.dump(_lib.ARR_CBLOCK_F_X).reshape(3, nmb)[:, ids].T
@@ -50,6 +51,22 @@ def solid_centres(c, p):
     off = np.stack([t % 4, (t // 4) % 4, t // 16], axis=1) * dx + 0.5 * dx
     pts = fX[:, None, :] + off[None, :, :]
     return pts[cm == -1], dx
+
+
+def solid_volume(c, p):
+    """Volume of the solid cells of the leaf blocks (blocks without children)
+    over all levels."""
+    nmb = p.n_maxcblocks
+    cnt = c.counts()
+    child = c.dump(_lib.ARR_CBLOCK_ID_NBR_CHILD).reshape(-1, nmb)[0]
+    ids_all = c.dump(_lib.ARR_ID_SET).reshape(-1, nmb)
+    cm = c.dump(_lib.ARR_CELLS_ID_MASK).reshape(nmb, 64)
+    vol = 0.0
+    for L in range(cnt["max_levels"]):
+        ids = ids_all[L, : cnt["n_ids"][L]].astype(np.int64)
+        leaf = ids[child[ids] < 0]
+        vol += float((cm[leaf] == -1).sum()) * ((1.0 / NX) / 2 ** L) ** 3
+    return vol
 
 
 def test_channel_voxelizes_like_the_cube():
@@ -62,13 +79,16 @@ def test_channel_voxelizes_like_the_cube():
             c.refine_near_wall()
             pts, dx = solid_centres(c, p)
             out[cube] = np.round(pts / dx).astype(np.int64)
+            if not cube:
+                vol = solid_volume(c, p)
+                coarse, dx0 = solid_centres(c, p, 0)
     a = {tuple(r) for r in out[True]}
     b = {tuple(r) for r in out[False]}
     assert a == b and len(a) > 0
-    vol = 4.0 / 3.0 * np.pi * (RADIUS / dx) ** 3
-    assert abs(len(a) - vol) < 0.06 * vol, (len(a), vol)
-    centre = np.asarray(list(a)).mean(axis=0) * dx
-    assert np.abs(centre - np.asarray(CENTRE)).max() < dx
+    # the solid leaf cells fill the sphere, centred on it
+    sphere = 4.0 / 3.0 * np.pi * RADIUS ** 3
+    assert abs(vol - sphere) < 0.06 * sphere, (vol, sphere)
+    assert np.abs(coarse.mean(axis=0) - np.asarray(CENTRE)).max() < dx0
 
 
 def test_channel_fp64_matches_oracle():

@@ -490,6 +490,11 @@ class Learner:
         case._learner = self if mode else None
         self._attached = [c for c in getattr(self, "_attached", []) if c is not case] + ([case] if mode else [])
 
+    def set_horizon(self, horizon: int) -> None:
+        """Label snapshots with the rule's decisions over the next `horizon`
+        regrids (set before collecting)."""
+        self._c(self._lib.agal_learn_set_horizon(self._h, int(horizon)))
+
     def set_thresholds(self, refine: float, coarsen: float) -> None:
         """Probability thresholds of the two outputs in predict mode."""
         self._c(self._lib.agal_learn_set_thresholds(self._h, refine, coarsen))

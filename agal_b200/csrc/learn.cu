@@ -335,6 +335,24 @@ __global__ void k_judge(const int *ids, int n, const int *pred_flag, const int *
     }
 }
 
+// Labels over a horizon of H regrids: refine if the rule decides to refine
+// at any of them, coarsen only if it decides to coarsen at all of them, and
+// weight 1 only for a block that keeps its level through all of them.
+__global__ void k_label_acc(float *Y, float *Wt, const float *Yn, const float *Wn, int n, int first)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    if (first) {
+        Y[2 * j] = Yn[2 * j];
+        Y[2 * j + 1] = Yn[2 * j + 1];
+        Wt[j] = Wn[j];
+    } else {
+        Y[2 * j] = fmaxf(Y[2 * j], Yn[2 * j]);
+        Y[2 * j + 1] = fminf(Y[2 * j + 1], Yn[2 * j + 1]);
+        Wt[j] = Wt[j] * Wn[j];
+    }
+}
+
 unsigned gridn(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace learn
@@ -357,6 +375,7 @@ struct agal_learn {
         int *ids = nullptr, *lvl = nullptr;  // block IDs and their levels at the snapshot
         float *Y = nullptr, *Wt = nullptr;   // labels [n][2], weights [n]
         float *D = nullptr;                  // the rule's decisions on the snapshot's own state [n][2]
+        int got = 0;                         // regrids of the horizon folded into Y so far
         bool labelled = false;
     };
     std::vector<Snap> snaps;
@@ -369,6 +388,9 @@ struct agal_learn {
     cudaStream_t s = nullptr;
     // solver coupling
     int judge_every = 4;
+    int horizon = 1;                         // regrids ahead that a snapshot's labels cover
+    float *lab_Y = nullptr, *lab_W = nullptr;   // one regrid's decisions, folded into the labels
+    long long lab_cap = 0;
     long long regrids = 0, judged = 0, plain_refine = 0, missed = 0;
     float thr[NO] = {0.f, 0.f};              // logit thresholds of the two outputs (0 = probability 1/2)
     int pred_n = 0;                          // prediction made at the last regrid
@@ -656,7 +678,8 @@ extern "C" int agal_learn_destroy(agal_learn *m)
     }
     void *ps[] = {m->w, m->g, m->m, m->v, m->W1b, m->W2b, m->W3b, m->W2t, m->W3t, m->X1b, m->X2b, m->X3b, m->Xt,
                   m->dYt, m->dYb, m->dZb, m->Y, m->H1, m->H2, m->Z, m->dZ, m->dX, m->dH, m->dY, m->gT, m->logits,
-                  m->scal, m->flags, m->status, m->counts, m->pred_ids, m->pred_lvl, m->pred_X, m->pred_logits};
+                  m->scal, m->flags, m->status, m->counts, m->pred_ids, m->pred_lvl, m->pred_X, m->pred_logits,
+                  m->lab_Y, m->lab_W};
     for (void *p : ps)
         if (p) cudaFree(p);
     if (m->s) cudaStreamDestroy(m->s);
@@ -736,22 +759,39 @@ extern "C" int agal_learn_record(agal_learn *m, agal_ctx *c)
     return AGAL_OK;
 }
 
-// Labels of the most recent unlabelled snapshot: the decisions of the
-// percentile rule's last run on the case (a block above the upper quantile,
-// below the lower one), for the snapshot's blocks that still exist on the
-// same level.
+// Labels of the unlabelled snapshots: the decisions of the percentile
+// rule's last run on the case (a block above the upper quantile, below the
+// lower one), for each snapshot's blocks that still exist on the same level,
+// folded over the next `horizon` regrids after the snapshot (k_label_acc).
 extern "C" int agal_learn_label(agal_learn *m, agal_ctx *c)
 {
     if (!m || !c) return AGAL_ERR_PARAM;
     if (!c->crit) return lerr(m, AGAL_ERR_STATE, "labels need the percentile rule of a multi-level case");
     for (auto it = m->snaps.rbegin(); it != m->snaps.rend(); ++it) {
-        if (it->labelled) continue;
-        const int rc = agal_percentile_decisions(c, 0, it->ids, it->lvl, it->n, it->Y, it->Wt);
+        if (it->labelled) break;   // older snapshots are complete
+        if (it->n > m->lab_cap) {
+            LCUDA(m, cudaStreamSynchronize(c->stream));
+            LCUDA(m, grow(&m->lab_Y, 2LL * it->n));
+            LCUDA(m, grow(&m->lab_W, (long long)it->n));
+            m->lab_cap = it->n;
+        }
+        const int rc = agal_percentile_decisions(c, 0, it->ids, it->lvl, it->n, m->lab_Y, m->lab_W);
         if (rc) return lerr(m, rc, c->err);
-        LCUDA(m, cudaStreamSynchronize(c->stream));
-        it->labelled = true;
-        return AGAL_OK;
+        if (it->n > 0)
+            k_label_acc<<<gridn(it->n), 256, 0, c->stream>>>(it->Y, it->Wt, m->lab_Y, m->lab_W, it->n, it->got == 0);
+        LCUDA(m, cudaGetLastError());
+        if (++it->got >= m->horizon) it->labelled = true;
     }
+    LCUDA(m, cudaStreamSynchronize(c->stream));
+    return AGAL_OK;
+}
+
+extern "C" int agal_learn_set_horizon(agal_learn *m, int horizon)
+{
+    if (!m || horizon < 1 || horizon > 64) return AGAL_ERR_PARAM;
+    for (const auto &sn : m->snaps)
+        if (!sn.labelled && sn.got > 0) return lerr(m, AGAL_ERR_STATE, "horizon changed while snapshots are being labelled");
+    m->horizon = horizon;
     return AGAL_OK;
 }
 

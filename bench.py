@@ -24,8 +24,14 @@ step as solver_lbm_advance.cu:74-89 counts them.
                the populations loaded from pinned host memory, K x (period +
                an asynchronous FP64 mass/momentum read back into pinned
                memory), the populations dumped; timed by wall clock
-  plain_fp32   the same case in FP32 populations; learned: the FP16 case with
-               the learned refinement predictor driving the regrids
+  plain_fp32   the same case in FP32 populations
+  learned      the learned predictor on a 2D periodic vortex flow: trained on
+               2000 snapshots labelled 4 regrids ahead, an FP16 run regridding
+               4x less often (the rule judging every regrid) against plain
+               FP16 / FP32 runs: MLUPS, regrid time per 1000 steps, missed
+               refinements
+  channel_d3q27  the D3Q27 icosphere channel (FP64 / FP32 / FP16 MLUPS and
+               drag/lift against FP64)
   roofline     the fused step kernel on a large single-level case of the same
                physics (FP16 and FP32), algorithmic bytes 2*Q*s per update
   error_vs_fp64  rho and u of FP32 and FP16 runs of the headline case against
@@ -646,6 +652,105 @@ def drag_lift(device: int) -> dict:
     return out
 
 
+def _vortex_params(storage: int, p_refine: int, device: int):
+    """2D periodic flow carrying vortices across the domain: D2Q9 128^2,
+    periodic in x and y, uniform u = 0.05 with 30% seeded velocity noise,
+    Re 500, up to 3 levels by the percentile rule (refine > p90, coarsen <
+    p50) every `p_refine` coarse steps, cubic interpolation."""
+    nb = 32 * 32
+    return ag.default_params(velocity_set=_lib.D2Q9, Nx=128, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=3,
+                             P_REFINE=p_refine, S_CRITERION=_lib.CRITERION_PERCENTILE, ref_pct_hi=0.9,
+                             ref_pct_lo=0.5, interp_order=_lib.INTERP_CUBIC, PERIODIC_X=1, PERIODIC_Y=1,
+                             bc_preset=_lib.BC_NONE, ic_preset=_lib.IC_UNIFORM, u_ref=0.05, ic_noise=0.3,
+                             seed=2024, v0=0.05 / 500.0, storage=storage, n_maxcblocks=nb * 21 + 64,
+                             device=device)
+
+
+def _time_periods(torch, case, period: int, n_periods: int) -> dict:
+    """Device time of n_periods regrid periods, split into the coarse steps
+    and the regrid (the last coarse step's time beyond a plain step's)."""
+    stream = torch.cuda.ExternalStream(case.stream_ptr())
+    total = regrid = 0.0
+    cells = 0
+    for _ in range(n_periods):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        cells += period * leaf_cells(case.counts(), 2)
+        e0.record(stream)
+        case.advance_n(period - 1, use_graph=True)
+        e1.record(stream)
+        case.advance_n(1, use_graph=True)   # the last step and its regrid
+        e2.record(stream)
+        case.sync()
+        t_steps, t_last = e0.elapsed_time(e1), e1.elapsed_time(e2)
+        total += t_steps + t_last
+        regrid += max(t_last - t_steps / (period - 1), 0.0)
+    steps = period * n_periods
+    return {"mlups": cells / (total * 1e-3) / 1e6, "ms": total, "coarse_steps": steps,
+            "regrids": n_periods, "regrids_per_1000_steps": 1000.0 * n_periods / steps,
+            "regrid_ms_per_1000_steps": 1000.0 * regrid / steps, "blocks_per_level": case.counts()["n_ids"][:-1]}
+
+
+def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epochs: int = 2,
+                  window: int = 1024, spinup: int = 1024) -> dict:
+    """The learned predictor adapting the grid less often, on the periodic
+    vortex flow (_vortex_params).  The network is trained on n_snap snapshots
+    of the plain FP32 run (a regrid every 16 coarse steps), each labelled with
+    the percentile rule's decisions over the next `horizon` regrids; a fresh
+    FP16 run driven by the network regrids every horizon x 16 steps, the rule
+    judging every regrid (its refinements the network missed are counted and
+    applied).  Against the plain FP16 and FP32 runs regridding every 16 steps,
+    after the same spin-up: MLUPS, regrids and regrid time per 1000 coarse
+    steps, and the missed-refinement fraction."""
+    base = 16
+    t0 = time.perf_counter()
+    src = ag.Case(_vortex_params(_lib.STORE_FP32, base, device))
+    m = ag.Learner(2, seed=7)
+    m.set_horizon(horizon)
+    m.attach(src, 1)
+    src.set_ic(0)
+    src.refine_near_wall()
+    src.advance_n(base * (n_snap + horizon), use_graph=True)
+    src.sync()
+    collect_s = time.perf_counter() - t0
+    nl = m.counts()["labelled"]
+    weights = m.balance_classes(0, nl)
+    loss = m.train(0, nl, epochs, lr=2e-3, seed=7)
+    thr = m.calibrate_thresholds(0, nl)
+    m.attach(src, 0)
+    src.close()
+    train_s = time.perf_counter() - t0 - collect_s
+    out = {"workload": "vortices2d_128_periodic", "desc": _vortex_params.__doc__.split("\n\n")[0].strip(),
+           "horizon": horizon, "snapshots": nl, "epochs": epochs, "class_weights": weights, "train_loss": loss,
+           "thresholds": thr, "collect_s": collect_s, "train_s": train_s, "spinup_steps": spinup}
+    runs = (("plain_fp32", _lib.STORE_FP32, base, False), ("plain_fp16", _lib.STORE_FP16, base, False),
+            ("learned_fp16", _lib.STORE_FP16, base * horizon, True))
+    for name, st, period, learned in runs:
+        c = ag.Case(_vortex_params(st, period, device))
+        if learned:
+            m.attach(c, 2, judge_every=1)
+            m.set_thresholds(*thr)
+        c.set_ic(0)
+        c.refine_near_wall()
+        c.advance_n(spinup, use_graph=True)
+        c.autotune(0, reps=5)
+        c0 = m.counts()
+        r = _time_periods(torch, c, period, window // period)
+        if learned:
+            c1 = m.counts()
+            r.update(judged=c1["judged"] - c0["judged"], plain_refine_marks=c1["plain_refine"] - c0["plain_refine"],
+                     missed=c1["missed"] - c0["missed"])
+            r["missed_fraction"] = r["missed"] / r["plain_refine_marks"] if r["plain_refine_marks"] else 0.0
+            m.attach(c, 0)
+        c.close()
+        out[name] = r
+    m.close()
+    out["regrid_ms_saved_per_1000_steps"] = (out["plain_fp16"]["regrid_ms_per_1000_steps"] -
+                                             out["learned_fp16"]["regrid_ms_per_1000_steps"])
+    out["ratio_learned_fp16_vs_plain_fp32"] = out["learned_fp16"]["mlups"] / out["plain_fp32"]["mlups"]
+    out["ratio_learned_fp16_vs_plain_fp16"] = out["learned_fp16"]["mlups"] / out["plain_fp16"]["mlups"]
+    return out
+
+
 def config4(torch, device: int, steps: int) -> dict:
     """The D3Q27 icosphere channel: external flow over a seeded icosphere
     (20,480 faces, diameter 32 root cells) in a 256 x 128 x 128 channel, 4
@@ -715,6 +820,10 @@ def main(argv=None) -> int:
     ap.add_argument("--roofline-workload", default=None, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--learn-snapshots", type=int, default=2000,
+                    help="snapshots the learned predictor is trained on (0 skips the learned leg)")
+    ap.add_argument("--learn-horizon", type=int, default=4, help="regrid periods the predictor looks ahead")
+    ap.add_argument("--learn-epochs", type=int, default=2)
     ap.add_argument("--config4-steps", type=int, default=600,
                     help="coarse steps of the D3Q27 icosphere channel leg (0 skips it)")
     ap.add_argument("--error-steps", type=int, default=20000,
@@ -857,54 +966,6 @@ def main(argv=None) -> int:
                     launches=launches, counts=counts, cells_per_step=float(np.mean(cells)), regrids=regrids,
                     ms_per_coarse_step=t_ms / steps / coarse_per_step(ww))
 
-    def learned_timed(wl: str, wl_src: str, steps: int):
-        """The workload with the learned predictor driving its refinement: the
-        network is trained on the GPU on snapshots of the plain FP32 run's
-        spin-up (labelled by the percentile rule), then predicts the marks of
-        every regrid of a fresh run, the rule judging every 4th regrid."""
-        ww, ws_ = WORKLOADS[wl], WORKLOADS[wl_src]
-        t0 = time.perf_counter()
-        src = ag.Case(make_params(ws_, device=local))
-        m = ag.Learner(DIM_OF[ww["velocity_set"]], seed=7)
-        m.attach(src, 1)
-        develop(src, ws_)
-        src.sync()
-        nl = m.counts()["labelled"]
-        weights = m.balance_classes(0, nl)
-        loss = m.train(0, nl, 40, lr=2e-3, seed=7)
-        thr = m.calibrate_thresholds(0, nl)
-        m.attach(src, 0)
-        src.close()
-        train_s = time.perf_counter() - t0
-        case = ag.Case(make_params(ww, device=local))
-        m.attach(case, 2, judge_every=4)
-        m.set_thresholds(*thr)
-        develop(case, ww)
-        tune = case.autotune(0, reps=10)
-        step = step_fn(case, ww)
-        for _ in range(a.warmup):
-            step()
-        case.sync()
-        flush = state_bytes(case, ww) * 2 < L2_BYTES
-        c0 = m.counts()
-        barrier()
-        torch.cuda.synchronize()
-        per_step, cells, launches = time_steps(case, torch, ww, steps, flush)
-        c1 = m.counts()
-        counts = case.counts()
-        barrier()
-        t_ms = allmax(sum(per_step))
-        mlups = allsum(float(sum(cells))) / (t_ms * 1e-3) / 1e6
-        m.attach(case, 0)
-        case.close()
-        m.close()
-        return dict(workload=wl, value=mlups, ms_per_step=t_ms / steps, snapshots=nl, class_weights=weights,
-                    train_loss=loss, thresholds=thr, collect_and_train_s=train_s,
-                    regrids=c1["regrids"] - c0["regrids"], judged=c1["judged"] - c0["judged"],
-                    plain_refine_marks=c1["plain_refine"] - c0["plain_refine"],
-                    missed=c1["missed"] - c0["missed"], blocks_per_level=counts["n_ids"][:-1],
-                    cell_updates_per_step=float(np.mean(cells)), tune=tune)
-
     def e2e_timed(wl: str, variant: int, steps: int) -> dict:
         """The same steps through the public C ABI with host buffers."""
         ww = WORKLOADS[wl]
@@ -962,7 +1023,8 @@ def main(argv=None) -> int:
 
     # --- device-timed steps: headline workload, learned, plain FP32 --------
     head = device_timed(a.workload, with_clocks=True, steps=a.steps)
-    learned = learned_timed(a.workload, a.plain_workload, a.steps) if w.get("amr") else None
+    learned = learned_ahead(torch, local, horizon=a.learn_horizon, n_snap=a.learn_snapshots,
+                            epochs=a.learn_epochs) if a.learn_snapshots > 0 else None
     plain = device_timed(a.plain_workload, with_clocks=False, steps=a.steps) \
         if a.plain_workload != a.workload else None
     # the reference's own criterion, timed like the reference harness times
@@ -1034,10 +1096,6 @@ def main(argv=None) -> int:
                                   "blocks_per_level": plain["counts"]["n_ids"][:-1],
                                   "ratio": head["value"] / plain["value"]}
         if learned is not None:
-            mk = learned["plain_refine_marks"]
-            learned["missed_fraction"] = learned["missed"] / mk if mk > 0 else 0.0
-            if plain is not None:
-                learned["ratio_vs_plain_fp32"] = learned["value"] / plain["value"]
             line["learned"] = learned
         if ref_rule is not None:
             line["reference_rule_fp32"] = ref_rule

@@ -358,6 +358,15 @@ int agal_learn_predict_snapshot(agal_learn *m, int k, float *out);
    the refinements the network missed are counted and applied); mode 0
    detaches.  The predictor must outlive the coupling. */
 int agal_learn_attach(agal_ctx *ctx, agal_learn *m, int mode, int judge_every, double threshold);
+/* Look-ahead of the labels collected in mode 1: a snapshot taken after a
+   regrid is labelled with the rule's decisions at the next `horizon` regrids
+   (1..64; default 1): refine if any of them refines a block, coarsen only if
+   all of them coarsen it, weight 0 for a block that changes level in between.
+   A network trained on such labels marks, at one regrid, what the rule would
+   want over the next `horizon` periods, so a predicting case can regrid
+   `horizon` times less often (its P_REFINE times `horizon`).  Set it before
+   collecting. */
+int agal_learn_set_horizon(agal_learn *m, int horizon);
 /* Separate probability thresholds of the refinement and coarsening outputs in
    predict mode (after agal_learn_attach, which sets both to `threshold`). */
 int agal_learn_set_thresholds(agal_learn *m, double refine, double coarsen);

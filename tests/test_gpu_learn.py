@@ -49,11 +49,13 @@ def learn_params(Q, N, **kw):
     return amr_params(Q, N, **base)
 
 
-def collect(Q, N, steps, seed=1, **kw):
+def collect(Q, N, steps, seed=1, horizon=1, **kw):
     """A learner in collect mode over a plain percentile-criterion run."""
     p = learn_params(Q, N, **kw)
     c = ag.Case(p)
     m = ag.Learner(2 if Q == 9 else 3, seed=seed)
+    if horizon != 1:
+        m.set_horizon(horizon)
     m.attach(c, 1)
     run_like_reference(c, p, steps)
     c.sync()
@@ -246,6 +248,71 @@ def test_predict_mode_judged_refinement():
             assert 0.5 * sum(plain_ids[1:]) <= sum(ids[1:]) <= 2.0 * sum(plain_ids[1:])
             mm = c2.mass_momentum()
             assert np.isfinite(mm).all()
+            m.attach(c2, 0)
+    finally:
+        m.close()
+
+
+def test_horizon_labels_cover_later_regrids():
+    """Labels over a horizon of 3 regrids, against the same (deterministic)
+    run labelled one regrid ahead: a block the rule refines at the next regrid
+    is labelled for refinement, one it does not coarsen at the next regrid is
+    not labelled for coarsening, and a block that changes level within the
+    horizon carries no weight; the last 3 snapshots stay unlabelled."""
+    out = {}
+    for h in (1, 3):
+        p, c, m = collect(9, 64, 160, horizon=h, **CHANNEL)
+        try:
+            cnt = m.counts()
+            out[h] = (cnt, [m.snapshot(k) for k in range(cnt["labelled"])])
+        finally:
+            m.attach(c, 0)
+            m.close()
+            c.close()
+    (c1, s1), (c3, s3) = out[1], out[3]
+    assert c1["snapshots"] == c3["snapshots"] == 160 // 8
+    assert c1["labelled"] == c1["snapshots"] - 1 and c3["labelled"] == c3["snapshots"] - 3
+    wider = 0
+    for (X1, Y1, W1), (X3, Y3, W3) in zip(s1, s3):
+        assert np.array_equal(X1, X3)                      # the same states
+        assert np.all(W3 <= W1)
+        v = W3 > 0
+        assert np.all(Y3[v, 0] >= Y1[v, 0])               # refine: any of the regrids
+        assert np.all(Y3[v, 1] <= Y1[v, 1])               # coarsen: all of them
+        wider += int((Y3[v, 0] > Y1[v, 0]).sum())
+    assert wider > 0                                       # the horizon adds refinement labels
+
+
+def test_predict_ahead_regrids_less_often():
+    """A network trained on labels 4 regrids ahead drives a run that regrids
+    4 times less often (P_REFINE x 4), the rule judging every regrid: the
+    regrid count drops 4x, the missed fraction is reported, the mesh stays
+    within a factor 2 of the plain run's and the flow stays bounded."""
+    p, c, m = collect(9, 64, 320, horizon=4, **CHANNEL)
+    try:
+        nl = m.counts()["labelled"]
+        plain_ids = c.counts()["n_ids"]
+        m.balance_classes(0, nl)
+        m.train(0, nl, 30, lr=2e-3, seed=5)
+        thr = m.calibrate_thresholds(0, nl)
+        m.attach(c, 0)
+        c.close()
+        p.P_REFINE *= 4
+        with ag.Case(p) as c2:
+            m.attach(c2, 2, judge_every=1)
+            m.set_thresholds(*thr)
+            run_like_reference(c2, p, 320)
+            c2.sync()
+            cnt = m.counts()
+            ids = c2.counts()["n_ids"]
+            frac = cnt["missed"] / max(cnt["plain_refine"], 1)
+            print(f"horizon 4: {cnt['regrids']} regrids (plain run 40), missed {cnt['missed']} of "
+                  f"{cnt['plain_refine']} plain refinement marks ({frac:.2f}); blocks {ids} (plain {plain_ids})")
+            assert cnt["regrids"] == 320 // p.P_REFINE == 10
+            assert cnt["judged"] == cnt["regrids"]
+            assert 0 <= cnt["missed"] <= cnt["plain_refine"]
+            assert 0.5 * sum(plain_ids[1:]) <= sum(ids[1:]) <= 2.0 * sum(plain_ids[1:])
+            assert np.isfinite(c2.mass_momentum()).all()
             m.attach(c2, 0)
     finally:
         m.close()

@@ -327,9 +327,11 @@ class Case:
 
 
 class Batch:
-    """Independent cases advanced together: one CUDA graph per coarse step with
-    one branch per case (agal_batch_*).  Each case ends where advancing it
-    alone would have left it."""
+    """Independent cases advanced together (agal_batch_*): one CUDA graph per
+    coarse step; in work-list mode (the default where every case allows it)
+    the fused steps of all cases run as one persistent kernel per phase over
+    a global (case, chunk) list, otherwise each case is one graph branch.
+    Each case ends where advancing it alone would have left it."""
 
     def __init__(self, cases):
         self._lib = _lib.lib()
@@ -350,6 +352,9 @@ class Batch:
 
     def sync(self) -> None:
         self._c(self._lib.agal_batch_sync(self._h))
+
+    def set_worklist(self, on: bool) -> None:
+        self._c(self._lib.agal_batch_set_worklist(self._h, 1 if on else 0))
 
     def stream(self) -> int:
         s = C.c_void_p()
@@ -491,8 +496,10 @@ class Learner:
         self._attached = [c for c in getattr(self, "_attached", []) if c is not case] + ([case] if mode else [])
 
     def set_horizon(self, horizon: int) -> None:
-        """Label snapshots with the rule's decisions over the next `horizon`
-        regrids (set before collecting)."""
+        """Look-ahead: snapshots taken at a regrid are labelled with the rule's
+        decisions at that regrid and the next horizon - 1, and predictions
+        apply at the regrid they are made (0: the one-regrid-delayed mode).
+        Set before collecting."""
         self._c(self._lib.agal_learn_set_horizon(self._h, int(horizon)))
 
     def set_thresholds(self, refine: float, coarsen: float) -> None:

@@ -60,14 +60,23 @@ def up_to_date() -> bool:
     return all(p.stat().st_mtime <= t for p in sources() + headers() + [Path(__file__)])
 
 
+def _stale(src: Path, newest_header: float) -> bool:
+    obj = OBJ / (src.name + ".o")
+    return not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
+
+
 def build(force: bool = False, jobs: int | None = None, verbose_ptxas: bool = False) -> Path:
     if not force and up_to_date():
         return OUT
     OBJ.mkdir(exist_ok=True)
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
     srcs = sources()
+    # Objects newer than their source and every header are reused.
+    newest_header = max([p.stat().st_mtime for p in headers()] + [Path(__file__).stat().st_mtime])
+    todo = [s for s in srcs if force or _stale(s, newest_header)]
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, extra), srcs))
+        list(ex.map(lambda s: _compile(s, extra), todo))
+    objs = [OBJ / (s.name + ".o") for s in srcs]
     cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(OUT), *map(str, objs)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

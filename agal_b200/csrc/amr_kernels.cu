@@ -657,8 +657,16 @@ template <int DIM, int Q, typename T> struct RunAverage {
 
 }  // namespace agal
 
-int agal_launch_interp(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunInterp>(c, L, var); }
-int agal_launch_average(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunAverage>(c, L, var); }
+int agal_launch_interp(agal_ctx *c, int L, int var)
+{
+    if (c->rec) return agal_record_other(c, AGAL_OP_INTERP, L, [L, var](agal_ctx *x) { return agal_launch_interp(x, L, var); });
+    return agal::dispatch<agal::RunInterp>(c, L, var);
+}
+int agal_launch_average(agal_ctx *c, int L, int var)
+{
+    if (c->rec) return agal_record_other(c, AGAL_OP_AVERAGE, L, [L, var](agal_ctx *x) { return agal_launch_average(x, L, var); });
+    return agal::dispatch<agal::RunAverage>(c, L, var);
+}
 
 // Block values and the two quantiles of the percentile rule (no marks).
 static int percentile_select(agal_ctx *c, int idm)

@@ -11,12 +11,96 @@
 // case runs between graph replays on its own stream, every P_REFINE coarse
 // steps as in M_AdvanceLoop (mesh_advance.cu:421-463); a regrid invalidates
 // the batch graphs.
+//
+// Work-list mode (the default when every case allows it): the fused steps of
+// all cases are one launch per phase.  A coarse step of every case is first
+// recorded, not launched (agal_ctx::rec): each launcher appends its launch to
+// the case's list.  The lists are merged into one sequence of phases that
+// keeps every case's own order (a phase is one launch kind at one level, e.g.
+// the second sub-step of level 1); a step phase is one persistent kernel over
+// the chunks of every case stepping in it (k_step_batch, a global work list
+// of (case, chunk) with each case's arguments in a device table), then the
+// wall steps of the cases that have walls, then one batched fix-up launch;
+// any other phase (interpolation, averaging, forces, the rounding counter)
+// runs each case's launch on its own stream.  Every case's kernels and their
+// order are those of advancing it alone, so the results are identical.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "ctx.h"
+#include "step_common.cuh"
+
+// A launch recorded for the batch: a fused step (kind 0) or a closure.
+struct agal_op {
+    int kind = 0;              // 0: fused step; else AGAL_OP_*
+    int L = 0;
+    int key = 0;               // fused step: batched-kernel key
+    int n_blocks = 0;          // fused step: blocks of the level
+    agal::StepArgs step{};
+    const void *fin = nullptr;
+    void *fout = nullptr;
+    std::function<int(agal_ctx *)> fn;
+    // the case's launch state when the launch was recorded (launchers read
+    // the buffer parities and the rounding salt when they launch)
+    std::vector<int> cur;
+    int sr_salt = 0, liter = 0;
+};
+
+// Issue a recorded closure (or a step's wall step) in the launch state it was
+// recorded in.
+static int run_in_state(agal_ctx *c, const agal_op &op, const std::function<int(agal_ctx *)> &fn)
+{
+    const std::vector<int> cur = c->cur;
+    const int salt = c->sr_salt, liter = c->liter;
+    c->cur = op.cur;
+    c->sr_salt = op.sr_salt;
+    c->liter = op.liter;
+    const int rc = fn(c);
+    c->cur = cur;
+    c->sr_salt = salt;
+    c->liter = liter;
+    return rc;
+}
+struct agal_oplist {
+    std::vector<agal_op> ops;
+};
+
+int agal_record_step(agal_ctx *c, int L, const void *args, size_t bytes, int key, int n_blocks, const void *fin,
+                     void *fout)
+{
+    if (bytes != sizeof(agal::StepArgs)) return agal_set_err(c, AGAL_ERR_PARAM, "batch: step arguments size");
+    agal_op op;
+    op.L = L;
+    op.key = key;
+    op.n_blocks = n_blocks;
+    std::memcpy(&op.step, args, bytes);
+    op.fin = fin;
+    op.fout = fout;
+    op.cur = c->cur;
+    op.sr_salt = c->sr_salt;
+    op.liter = c->liter;
+    c->rec->ops.push_back(std::move(op));
+    return AGAL_OK;
+}
+
+int agal_record_other(agal_ctx *c, int tag, int L, std::function<int(agal_ctx *)> fn)
+{
+    agal_op op;
+    op.kind = tag;
+    op.L = L;
+    op.fn = std::move(fn);
+    op.cur = c->cur;
+    op.sr_salt = c->sr_salt;
+    op.liter = c->liter;
+    c->rec->ops.push_back(std::move(op));
+    return AGAL_OK;
+}
 
 struct agal_batch {
     std::vector<agal_ctx *> cases;
@@ -25,6 +109,9 @@ struct agal_batch {
     std::vector<cudaEvent_t> join;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     std::vector<std::vector<int>> graph_cur[2];   // every case's cur[] at capture
+    bool worklist = false;                        // work-list mode in force
+    char *tables[3] = {nullptr, nullptr, nullptr};   // step tables of graph 0, 1 and of direct launches
+    size_t tables_cap[3] = {0, 0, 0};
     std::string err;
 };
 
@@ -47,6 +134,188 @@ int bcuda(agal_batch *b, cudaError_t e, const char *what)
         cudaError_t e_ = (call);                         \
         if (e_ != cudaSuccess) return bcuda((b), e_, #call); \
     } while (0)
+
+// One phase of a merged coarse step: launch kind, level, occurrence, and the
+// (case, op) pairs in it.
+struct Phase {
+    int kind, L, occ;
+    std::vector<std::pair<int, int>> items;
+};
+
+// Record one coarse step of every case (nothing launched; the cases' buffer
+// parities advance as if it ran) and merge the lists into phases.
+int plan_step(agal_batch *b, std::vector<agal_oplist> &lists, std::vector<Phase> &phases)
+{
+    const int n = (int)b->cases.size();
+    lists.assign(n, agal_oplist{});
+    for (int i = 0; i < n; i++) {
+        agal_ctx *c = b->cases[i];
+        c->rec = &lists[i];
+        const int rc = agal_record_coarse_step(c);
+        c->rec = nullptr;
+        if (rc) return berr(b, rc, "case " + std::to_string(i) + ": " + c->err);
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return lists[x].ops.size() > lists[y].ops.size(); });
+    phases.clear();
+    for (int i : order) {
+        std::map<std::pair<int, int>, int> occ;
+        int pos = -1;
+        for (int j = 0; j < (int)lists[i].ops.size(); j++) {
+            const agal_op &op = lists[i].ops[j];
+            const int k = occ[{op.kind, op.L}]++;
+            int at = -1;
+            for (int p = pos + 1; p < (int)phases.size(); p++)
+                if (phases[p].kind == op.kind && phases[p].L == op.L && phases[p].occ == k) {
+                    at = p;
+                    break;
+                }
+            if (at < 0) {
+                at = pos + 1;
+                phases.insert(phases.begin() + at, Phase{op.kind, op.L, k, {}});
+            }
+            phases[at].items.push_back({i, j});
+            pos = at;
+        }
+    }
+    return AGAL_OK;
+}
+
+// Device tables of the step phases: per phase and kernel key, the cases'
+// StepArgs then the chunk prefix (n + 1 ints).  Written to tables[slot]
+// before the launches that read them are issued.
+struct StepGroup {
+    int phase, key, n, total;
+    size_t off_args, off_start;
+    std::vector<int> items;   // indices into the phase's items
+};
+
+int build_tables(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, const std::vector<Phase> &phases,
+                 std::vector<StepGroup> &groups)
+{
+    groups.clear();
+    std::vector<char> host;
+    auto align = [&](size_t a) { host.resize((host.size() + a - 1) / a * a); };
+    for (int p = 0; p < (int)phases.size(); p++) {
+        if (phases[p].kind != 0) continue;
+        std::map<int, std::vector<int>> by_key;
+        for (int t = 0; t < (int)phases[p].items.size(); t++) {
+            const auto &it = phases[p].items[t];
+            by_key[lists[it.first].ops[it.second].key].push_back(t);
+        }
+        for (auto &kv : by_key) {
+            StepGroup g{p, kv.first, (int)kv.second.size(), 0, 0, 0, kv.second};
+            align(alignof(agal::StepArgs) > 16 ? alignof(agal::StepArgs) : 16);
+            g.off_args = host.size();
+            host.resize(host.size() + sizeof(agal::StepArgs) * g.n);
+            align(16);
+            g.off_start = host.size();
+            host.resize(host.size() + sizeof(int) * (g.n + 1));
+            int acc = 0;
+            for (int q = 0; q < g.n; q++) {
+                const auto &it = phases[p].items[g.items[q]];
+                const agal_op &op = lists[it.first].ops[it.second];
+                const int mc = b->cases[it.first]->MC;
+                std::memcpy(host.data() + g.off_args + sizeof(agal::StepArgs) * q, &op.step, sizeof(agal::StepArgs));
+                reinterpret_cast<int *>(host.data() + g.off_start)[q] = acc;
+                acc += (op.n_blocks + 256 / mc - 1) / (256 / mc);
+            }
+            reinterpret_cast<int *>(host.data() + g.off_start)[g.n] = acc;
+            g.total = acc;
+            groups.push_back(std::move(g));
+        }
+    }
+    if (host.empty()) return AGAL_OK;
+    if (host.size() > b->tables_cap[slot]) {
+        if (b->tables[slot]) cudaFree(b->tables[slot]);
+        b->tables[slot] = nullptr;
+        b->tables_cap[slot] = 0;
+        BCUDA(b, cudaMalloc(&b->tables[slot], host.size()));
+        b->tables_cap[slot] = host.size();
+    }
+    BCUDA(b, cudaStreamSynchronize(b->master));   // earlier launches may still read the slot
+    BCUDA(b, cudaMemcpy(b->tables[slot], host.data(), host.size(), cudaMemcpyHostToDevice));
+    return AGAL_OK;
+}
+
+// Run fn(case) for the listed cases, each on its own stream, between a fork
+// from and a join back to the master stream.
+template <class F>
+int fan_out(agal_batch *b, const std::vector<int> &cases, F fn)
+{
+    if (cases.empty()) return AGAL_OK;
+    BCUDA(b, cudaEventRecord(b->fork, b->master));
+    for (int i : cases) {
+        agal_ctx *c = b->cases[i];
+        BCUDA(b, cudaStreamWaitEvent(c->stream, b->fork, 0));
+        const int rc = fn(c);
+        if (rc) return berr(b, rc, "case " + std::to_string(i) + ": " + c->err);
+        BCUDA(b, cudaEventRecord(b->join[i], c->stream));
+        BCUDA(b, cudaStreamWaitEvent(b->master, b->join[i], 0));
+    }
+    return AGAL_OK;
+}
+
+// Issue the planned phases on the master stream (under capture or not).
+int issue_step(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, const std::vector<Phase> &phases,
+               const std::vector<StepGroup> &groups)
+{
+    size_t g = 0;
+    for (int p = 0; p < (int)phases.size(); p++) {
+        const Phase &ph = phases[p];
+        if (ph.kind != 0) {
+            std::vector<int> cs;
+            for (const auto &it : ph.items) cs.push_back(it.first);
+            size_t q = 0;
+            const int rc = fan_out(b, cs, [&](agal_ctx *c) {
+                const auto &it = ph.items[q++];
+                const agal_op &op = lists[it.first].ops[it.second];
+                return run_in_state(c, op, op.fn);
+            });
+            if (rc) return rc;
+            continue;
+        }
+        for (; g < groups.size() && groups[g].phase == p; g++) {
+            const StepGroup &sg = groups[g];
+            const char *base = b->tables[slot];
+            int rc = agal_launch_step_batch(sg.key, b->master, base + sg.off_args,
+                                            reinterpret_cast<const int *>(base + sg.off_start), sg.n, sg.total, 0);
+            if (rc) return berr(b, rc, "batched step launch failed");
+            // the wall steps of cases with walls, then the fix-ups of all
+            std::vector<int> cs;
+            std::vector<const agal_op *> ops;
+            for (int t : sg.items) {
+                const auto &it = ph.items[t];
+                const agal_op &op = lists[it.first].ops[it.second];
+                if (agal_wall_active(b->cases[it.first])) {
+                    cs.push_back(it.first);
+                    ops.push_back(&op);
+                }
+            }
+            size_t q = 0;
+            rc = fan_out(b, cs, [&](agal_ctx *c) {
+                const agal_op *op = ops[q++];
+                return run_in_state(c, *op, [op](agal_ctx *x) { return agal_launch_wall_step(x, op->L, op->fin, op->fout); });
+            });
+            if (rc) return rc;
+            rc = agal_launch_step_batch(sg.key, b->master, base + sg.off_args,
+                                        reinterpret_cast<const int *>(base + sg.off_start), sg.n, 0, 1);
+            if (rc) return berr(b, rc, "batched fix-up launch failed");
+        }
+    }
+    return AGAL_OK;
+}
+
+// Work-list mode needs every case on one launch path: no LES, no control-volume
+// forces (their launch sequence interleaves levels differently).
+bool worklist_ok(const agal_batch *b)
+{
+    for (const agal_ctx *c : b->cases)
+        if (c->nu_sgs || c->P.S_FORCE_TYPE == 1) return false;
+    return true;
+}
 
 void drop(agal_batch *b)
 {
@@ -82,12 +351,24 @@ int record_step(agal_batch *b)
     return AGAL_OK;
 }
 
-int capture(agal_batch *b, cudaGraphExec_t *out)
+int capture(agal_batch *b, int slot, cudaGraphExec_t *out)
 {
     std::vector<std::vector<int>> cur0 = curs(b);
+    std::vector<agal_oplist> lists;
+    std::vector<Phase> phases;
+    std::vector<StepGroup> groups;
+    if (b->worklist) {
+        // plan and upload the step tables before the capture begins
+        int rc = plan_step(b, lists, phases);
+        if (!rc) rc = build_tables(b, slot, lists, phases, groups);
+        if (rc) {
+            for (size_t i = 0; i < b->cases.size(); i++) b->cases[i]->cur = cur0[i];
+            return rc;
+        }
+    }
     cudaGraph_t g = nullptr;
     BCUDA(b, cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
-    int rc = record_step(b);
+    int rc = b->worklist ? issue_step(b, slot, lists, phases, groups) : record_step(b);
     cudaError_t e = cudaStreamEndCapture(b->master, &g);
     for (size_t i = 0; i < b->cases.size(); i++) b->cases[i]->cur = cur0[i];   // only recorded
     if (rc) {
@@ -122,6 +403,7 @@ extern "C" int agal_batch_create(agal_ctx *const *cases, int n_cases, agal_batch
               cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
     b->join.assign(n_cases, nullptr);
+    b->worklist = worklist_ok(b);
     for (int i = 0; ok && i < n_cases; i++) ok = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -142,11 +424,25 @@ extern "C" int agal_batch_destroy(agal_batch *b)
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->done) cudaEventDestroy(b->done);
     if (b->master) cudaStreamDestroy(b->master);
+    for (char *t : b->tables)
+        if (t) cudaFree(t);
     delete b;
     return AGAL_OK;
 }
 
 extern "C" const char *agal_batch_last_error(const agal_batch *b) { return b ? b->err.c_str() : ""; }
+
+// Work-list mode on (1, where every case allows it) or off (0: one graph
+// branch per case); returns AGAL_ERR_UNSUPPORTED for 1 when a case does not
+// allow it (LES, control-volume forces).
+extern "C" int agal_batch_set_worklist(agal_batch *b, int on)
+{
+    if (!b) return AGAL_ERR_PARAM;
+    if (on && !worklist_ok(b)) return berr(b, AGAL_ERR_UNSUPPORTED, "work-list mode: a case has LES or CV forces");
+    if ((on != 0) != b->worklist) drop(b);
+    b->worklist = on != 0;
+    return AGAL_OK;
+}
 
 // n coarse steps of every case.  use_graph replays one captured step of the
 // whole batch (two cached, for the alternating buffer parities).
@@ -166,11 +462,18 @@ extern "C" int agal_batch_advance_n(agal_batch *b, int n, int use_graph)
             if (k < 0) {
                 k = b->graph[0] ? 1 : 0;
                 if (b->graph[k]) { cudaGraphExecDestroy(b->graph[k]); b->graph[k] = nullptr; }
-                if ((rc = capture(b, &b->graph[k]))) return rc;
+                if ((rc = capture(b, k, &b->graph[k]))) return rc;
                 b->graph_cur[k] = now;
             }
             BCUDA(b, cudaGraphLaunch(b->graph[k], b->master));
             for (agal_ctx *c : b->cases) agal_advance_parity(c, 1);
+        } else if (b->worklist) {
+            std::vector<agal_oplist> lists;
+            std::vector<Phase> phases;
+            std::vector<StepGroup> groups;
+            if ((rc = plan_step(b, lists, phases))) return rc;
+            if ((rc = build_tables(b, 2, lists, phases, groups))) return rc;
+            if ((rc = issue_step(b, 2, lists, phases, groups))) return rc;
         } else {
             if ((rc = record_step(b))) return rc;
         }

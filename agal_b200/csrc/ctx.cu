@@ -604,6 +604,10 @@ static int step_f(agal_ctx *c, int L, bool forces)
 static int interp_beside_step(agal_ctx *c, int L, bool forces)
 {
     int rc;
+    if (c->rec) {   // batch recording: the batch orders the launches itself
+        if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
+        return step_f(c, L, forces);
+    }
     AGAL_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
     AGAL_CUDA(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
     cudaStream_t main = c->stream;
@@ -682,6 +686,7 @@ int agal_sr_tick(agal_ctx *c)
     if (!((c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
           c->P.half_rounding == AGAL_ROUND_STOCHASTIC))
         return AGAL_OK;
+    if (c->rec) return agal_record_other(c, AGAL_OP_SR_TICK, 0, [](agal_ctx *x) { return agal_sr_tick(x); });
     k_sr_tick<<<1, 1, 0, c->stream>>>(c->d_sr);
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;

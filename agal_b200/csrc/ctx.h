@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -90,6 +91,9 @@ struct agal_ctx {
     int *tiles = nullptr;              // root-level tile table of the 2D tile step (step_tile.cu)
     int n_tiles = 0;                   // 0 = the tile step is not available
     int n_ptiles = 0;                  // push tiles of the root level (step_ptile.cu); 0 = not available
+    // Batch recording (batch.cu): while set, the launchers of a coarse step
+    // append what they would launch to this list instead of launching.
+    struct agal_oplist *rec = nullptr;
     void *xfer = nullptr;              // 64 MiB FP64 staging of the population dumps and loads (xfer.cu)
     int *fix_count = nullptr;          // stream-guard fix-ups of the running step (k_stream_fixup)
     long long *fix_list = nullptr;
@@ -207,6 +211,17 @@ int agal_wall_active(const agal_ctx *c);    // interpolated bounce-back in force
 int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout);
 int agal_launch_forces(agal_ctx *c, int L, int post);
 int agal_launch_forces_cv(agal_ctx *c, int L, int post);   // S_FORCE_TYPE 1
+// Batch recording (batch.cu): a fused step (its StepArgs as bytes, the
+// batched-kernel key of agal_step_batch_key, the level's block count and the
+// buffers of the wall step that follows it), or any other launch as a
+// closure that issues it on the context's stream.
+int agal_record_step(agal_ctx *c, int L, const void *args, size_t bytes, int key, int n_blocks, const void *fin,
+                     void *fout);
+int agal_record_other(agal_ctx *c, int tag, int L, std::function<int(agal_ctx *)> fn);
+enum { AGAL_OP_INTERP = 1, AGAL_OP_AVERAGE, AGAL_OP_FORCES, AGAL_OP_FORCES_CV, AGAL_OP_SR_TICK };
+int agal_step_batch_key(const agal_ctx *c);
+int agal_launch_step_batch(int key, cudaStream_t s, const void *dev_args, const int *dev_start, int n, int total,
+                           int fixup_only);
 // Learned predictor hooks of the solution-based refinement (learn.cu).
 int agal_learn_marks(agal_ctx *c);          // instead of the criterion when a learner is attached
 int agal_learn_after_regrid(agal_ctx *c);   // after the refine/coarsen pass

@@ -388,7 +388,12 @@ struct agal_learn {
     cudaStream_t s = nullptr;
     // solver coupling
     int judge_every = 4;
-    int horizon = 1;                         // regrids ahead that a snapshot's labels cover
+    // 0: a snapshot is taken after a regrid and labelled by the next one, and
+    // the prediction made after a regrid is applied at the next.  h >= 1
+    // (look-ahead): a snapshot is taken at a regrid before its refinement
+    // pass and labelled by that regrid and the next h - 1, and the
+    // prediction is made and applied at the same regrid.
+    int horizon = 0;
     float *lab_Y = nullptr, *lab_W = nullptr;   // one regrid's decisions, folded into the labels
     long long lab_cap = 0;
     long long regrids = 0, judged = 0, plain_refine = 0, missed = 0;
@@ -780,7 +785,7 @@ extern "C" int agal_learn_label(agal_learn *m, agal_ctx *c)
         if (it->n > 0)
             k_label_acc<<<gridn(it->n), 256, 0, c->stream>>>(it->Y, it->Wt, m->lab_Y, m->lab_W, it->n, it->got == 0);
         LCUDA(m, cudaGetLastError());
-        if (++it->got >= m->horizon) it->labelled = true;
+        if (++it->got >= std::max(m->horizon, 1)) it->labelled = true;
     }
     LCUDA(m, cudaStreamSynchronize(c->stream));
     return AGAL_OK;
@@ -788,7 +793,7 @@ extern "C" int agal_learn_label(agal_learn *m, agal_ctx *c)
 
 extern "C" int agal_learn_set_horizon(agal_learn *m, int horizon)
 {
-    if (!m || horizon < 1 || horizon > 64) return AGAL_ERR_PARAM;
+    if (!m || horizon < 0 || horizon > 64) return AGAL_ERR_PARAM;
     for (const auto &sn : m->snaps)
         if (!sn.labelled && sn.got > 0) return lerr(m, AGAL_ERR_STATE, "horizon changed while snapshots are being labelled");
     m->horizon = horizon;
@@ -944,6 +949,8 @@ extern "C" int agal_learn_set_thresholds(agal_learn *m, double refine, double co
     return AGAL_OK;
 }
 
+static int predict_now(agal_learn *m, agal_ctx *c);
+
 // Marks of a regrid (called by agal_refine_with_solution instead of the
 // criterion while a learner is attached).
 int agal_learn_marks(agal_ctx *c)
@@ -952,6 +959,9 @@ int agal_learn_marks(agal_ctx *c)
     int rc;
     if (c->learn_mode == 1) {
         if ((rc = agal_launch_criterion(c))) return rc;
+        // look-ahead: this regrid's state is a snapshot, its first label the
+        // rule's decisions now
+        if (m->horizon > 0 && (rc = agal_learn_record(m, c))) return agal_set_err(c, rc, "learned predictor: " + m->err);
         if ((rc = agal_learn_label(m, c))) return agal_set_err(c, rc, "learned predictor: " + m->err);
         return AGAL_OK;
     }
@@ -961,6 +971,8 @@ int agal_learn_marks(agal_ctx *c)
         if ((rc = agal_launch_criterion(c))) return rc;
         m->judged++;
     }
+    // look-ahead: predict from this regrid's state and apply it now
+    if (m->horizon > 0 && (rc = predict_now(m, c))) return rc;
     if (m->pred_n > 0) {
         // flags of the predicted refinements, on a judged regrid the count of
         // the plain refinement marks the network missed, then the predicted
@@ -998,11 +1010,20 @@ int agal_learn_marks(agal_ctx *c)
 int agal_learn_after_regrid(agal_ctx *c)
 {
     agal_learn *m = c->learner;
-    int rc;
+    if (m->horizon > 0) return AGAL_OK;   // look-ahead: snapshots and predictions happen at the regrid
     if (c->learn_mode == 1) {
-        if ((rc = agal_learn_record(m, c))) return agal_set_err(c, rc, "learned predictor: " + m->err);
-        return AGAL_OK;
+        const int rc = agal_learn_record(m, c);
+        return rc ? agal_set_err(c, rc, "learned predictor: " + m->err) : AGAL_OK;
     }
+    return predict_now(m, c);
+}
+
+// Features and forward pass of every active block of the case's current
+// state, asynchronous on its stream; the logits become the prediction that
+// the next call of k_apply_marks applies.
+static int predict_now(agal_learn *m, agal_ctx *c)
+{
+    int rc;
     const int n = total_blocks(c);
     if (n > m->pred_cap) {
         const long long cap = std::max<long long>(n, m->pred_cap * 3 / 2);

@@ -21,6 +21,7 @@
 // Algorithmic traffic: 2 * Q * sizeof(storage) bytes per cell update.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <type_traits>
@@ -34,15 +35,15 @@
 
 namespace agal {
 
+// The step of chunk `cta` of the level's block list (CPT x 256 / M_CBLOCK
+// blocks), given the CTA's shared metadata rows.
 template <int DIM, int Q, typename T, int CPT, bool SOLID>
-__global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
-k_step(const StepArgs a)
+__device__ __forceinline__ void step_body(const StepArgs &a, int cta, int (*s_meta)[Meta<DIM>::W])
 {
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, BLK = Q * MC;
     constexpr int NB = 256 / MC;           // cell-blocks per CTA and round
     constexpr int W = Meta<DIM>::W;
-    __shared__ int s_meta[CPT * NB][W];
     const int tid = threadIdx.x;
     const int lb = tid / MC, t = tid % MC;
 
@@ -56,7 +57,7 @@ k_step(const StepArgs a)
     int b[CPT];
 #pragma unroll
     for (int h = 0; h < CPT; h++) {
-        const int kap = (blockIdx.x * CPT + h) * NB + lb;
+        const int kap = (cta * CPT + h) * NB + lb;
         b[h] = (kap < a.n) ? __ldg(&a.ids[kap]) : -1;
         for (int i = t; i < W; i += MC)
             s_meta[h * NB + lb][i] = (b[h] >= 0) ? __ldg(&a.meta[(long long)b[h] * W + i]) : 0;
@@ -108,7 +109,35 @@ k_step(const StepArgs a)
         }
         push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b[h], t, nrow, hook, fo, a, seed);
     }
+}
+
+template <int DIM, int Q, typename T, int CPT, bool SOLID>
+__global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, CPT>::value))
+k_step(const StepArgs a)
+{
+    __shared__ int s_meta[CPT * (256 / Geo<DIM>::MC)][Meta<DIM>::W];
+    step_body<DIM, Q, T, CPT, SOLID>(a, blockIdx.x, s_meta);
     if (a.fix_ticket) fused_fixup<T>(a);
+}
+
+// Batched form: one persistent kernel over the chunks of many cases' block
+// lists (a global work list).  Chunk w belongs to case i with
+// start[i] <= w < start[i + 1] and is stepped with that case's arguments A[i];
+// each case's chunks are the chunks k_step would give it alone, so every
+// case's populations are those of advancing it alone.
+template <int DIM, int Q, typename T, bool SOLID>
+__global__ void __launch_bounds__(256, (StepOcc<DIM, Q, T, 1>::value))
+k_step_batch(const StepArgs *__restrict__ A, const int *__restrict__ start, int n_cases)
+{
+    __shared__ int s_meta[256 / Geo<DIM>::MC][Meta<DIM>::W];
+    const int total = start[n_cases];
+    int i = 0;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        while (start[i + 1] <= w) i++;   // w only grows: the case index only moves forward
+        const StepArgs a = A[i];
+        step_body<DIM, Q, T, 1, SOLID>(a, w - start[i], s_meta);
+        __syncthreads();                 // the metadata rows are refilled for the next chunk
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -534,6 +563,48 @@ __global__ void __launch_bounds__(1024) k_stream_fixup(T *fo, int *count, const 
     }
 }
 
+// Batched fix-up: CTA i applies case i's list (A[i]); k_stream_fixup per case.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_stream_fixup_batch(const StepArgs *__restrict__ A)
+{
+    const StepArgs &a = A[blockIdx.x];
+    T *fo = static_cast<T *>(a.fout);
+    const int n = *a.fix_count;
+    const int m = n < a.fix_cap ? n : a.fix_cap;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const long long x = a.fix_list[2 * i], y = a.fix_list[2 * i + 1];
+        const T vx = fo[x];
+        fo[x] = fo[y];
+        fo[y] = vx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n > a.fix_cap) atomicCAS(a.status, 0, AGAL_ERR_STATE);
+        *a.fix_count = 0;
+    }
+}
+
+template <int DIM, int Q, typename T> struct StepBatch {
+    // One persistent launch over the chunks of n cases (dev_start[n] of them),
+    // then the fix-ups of every case.  Grid: resident CTAs per SM x SMs.
+    static int run(cudaStream_t s, const StepArgs *dev_args, const int *dev_start, int n, int total, bool solid,
+                   bool fixup)
+    {
+        if (total > 0) {
+            auto kern = solid ? k_step_batch<DIM, Q, T, true> : k_step_batch<DIM, Q, T, false>;
+            int dev = 0, sms = 0, per_sm = 0;
+            if (cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess)
+                return AGAL_ERR_CUDA;
+            const int grid = std::min(total, std::max(per_sm, 1) * sms);
+            kern<<<grid, 256, 0, s>>>(dev_args, dev_start, n);
+        }
+        if (fixup && n > 0) k_stream_fixup_batch<T><<<n, 1024, 0, s>>>(dev_args);
+        return cudaGetLastError() == cudaSuccess ? AGAL_OK : AGAL_ERR_CUDA;
+    }
+};
+
 template <int DIM, int Q, typename T> struct RunStep {
     // flip = false launches the kernel from the current buffer into the
     // other one without making it current (used by the autotuner: the step is
@@ -588,6 +659,16 @@ template <int DIM, int Q, typename T> struct RunStep {
         a.sr_salt = (unsigned)c->sr_salt;
         a.nu = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->P.v0 : c->P.v0;
         a.dxL = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->dxf[L] : c->dxf[L];
+        if (c->rec) {
+            // Batch recording: the batched kernel steps this case with the
+            // one-cell-per-thread body; its fix-ups follow in one batched launch.
+            a.fix_ticket = nullptr;
+            const int rc = agal_record_step(c, L, &a, sizeof(a), agal_step_batch_key(c), n, a.fin, a.fout);
+            if (rc) return rc;
+            if (flip) c->cur[L] = 1 - c->cur[L];
+            c->sr_salt++;
+            return AGAL_OK;
+        }
         if (c->nu_sgs) {
             // The eddy viscosity of the current populations; the persistent
             // and row-mapped variants have no per-cell relaxation rate, so
@@ -880,4 +961,33 @@ int agal_launch_mass(agal_ctx *c, double *out)
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
     for (int k = 0; k < c->dim + 1; k++) out[k] = h[k];
     return AGAL_OK;
+}
+
+// Batched step of many cases (batch.cu): `key` is agal_step_batch_key of the
+// cases, all of one velocity set and storage; fixup_only launches the
+// batched fix-ups instead of the step.
+int agal_step_batch_key(const agal_ctx *c) { return (c->Q * 8 + c->storage) * 2 + (c->geometry_init ? 1 : 0); }
+
+int agal_launch_step_batch(int key, cudaStream_t s, const void *dev_args, const int *dev_start, int n, int total,
+                           int fixup_only)
+{
+    const bool solid = key & 1;
+    const int storage = (key >> 1) % 8, Q = (key >> 1) / 8;
+    const auto *A = static_cast<const agal::StepArgs *>(dev_args);
+    auto go = [&](auto tag) -> int {
+        using T = decltype(tag);
+        switch (Q) {
+        case 9: return agal::StepBatch<2, 9, T>::run(s, A, dev_start, n, fixup_only ? 0 : total, solid, fixup_only);
+        case 19: return agal::StepBatch<3, 19, T>::run(s, A, dev_start, n, fixup_only ? 0 : total, solid, fixup_only);
+        case 27: return agal::StepBatch<3, 27, T>::run(s, A, dev_start, n, fixup_only ? 0 : total, solid, fixup_only);
+        default: return AGAL_ERR_PARAM;
+        }
+    };
+    switch (storage) {
+    case AGAL_STORE_FP32: return go(float{});
+    case AGAL_STORE_FP64: return go(double{});
+    case AGAL_STORE_FP16: return go(__half{});
+    case AGAL_STORE_BF16: return go(__nv_bfloat16{});
+    default: return AGAL_ERR_PARAM;
+    }
 }

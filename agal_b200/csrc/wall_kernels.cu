@@ -558,12 +558,16 @@ int agal_launch_wall_step(agal_ctx *c, int L, const void *fin, void *fout)
 
 int agal_launch_forces_cv(agal_ctx *c, int L, int post)
 {
+    if (c->rec)
+        return agal_record_other(c, AGAL_OP_FORCES_CV, L, [L, post](agal_ctx *x) { return agal_launch_forces_cv(x, L, post); });
     if (c->P.S_FORCE_TYPE != 1) return AGAL_OK;
     return agal::dispatch<agal::RunForcesCv>(c, L, post);
 }
 
 int agal_launch_forces(agal_ctx *c, int L, int post)
 {
+    if (c->rec)
+        return agal_record_other(c, AGAL_OP_FORCES, L, [L, post](agal_ctx *x) { return agal_launch_forces(x, L, post); });
     if (!c->onb_solid || !c->X_b || c->P.S_FORCE_TYPE != 0) return AGAL_OK;
     return agal::dispatch<agal::RunForces>(c, L, post);
 }

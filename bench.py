@@ -415,6 +415,17 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
     batch.sync()
     t16 = e0.elapsed_time(e1)
     levels16 = [c.counts()["n_ids"][:-1] for c in cases]
+    # the same batch with one graph branch per case instead of the work list
+    batch.set_worklist(False)
+    batch.advance_n(2)
+    batch.sync()
+    upd16b = cells(cases)
+    barrier()
+    e0.record(stream)
+    batch.advance_n(steps)
+    e1.record(stream)
+    batch.sync()
+    t16b = e0.elapsed_time(e1)
     batch.close()
     for c in cases:
         c.close()
@@ -435,6 +446,7 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
         t32 += a.elapsed_time(b)
     for c in cases:
         c.close()
+    agg16b = aggregate(upd16b * steps, t16b, allsum, allmax)
     agg16 = aggregate(upd16 * steps, t16, allsum, allmax)
     agg32 = aggregate(upd32 * steps, t32, allsum, allmax)
     v16, v32 = agg16["mlups"], agg32["mlups"]
@@ -455,6 +467,10 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
             "value": v16, "unit": "MLUPS", "storage": "f16-offset", "ms_per_step": t16 / steps,
             "cell_updates_per_step": upd16,
             "one_at_a_time_fp32": {"value": v32, "ms_per_step": t32 / steps, "cell_updates_per_step": upd32},
+            "graph_branches_fp16": {"value": agg16b["mlups"], "ms_per_step": agg16b["ms"] / steps,
+                                    "what": "the same batch, one graph branch per case (no work list)"},
+            "mode": "work list: one persistent step kernel per phase over all cases' (case, chunk) items, "
+                    "batched fix-ups; transfers, walls and forces per case",
             "ratio_vs_one_at_a_time_fp32": v16 / v32,
             "hbm": {"achieved_gbs_per_gpu": gbs, "peak": peak, "frac": gbs / peak, "peak_source": kind,
                     "bytes_per_update": 2 * 19 * 2},

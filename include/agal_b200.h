@@ -358,14 +358,15 @@ int agal_learn_predict_snapshot(agal_learn *m, int k, float *out);
    the refinements the network missed are counted and applied); mode 0
    detaches.  The predictor must outlive the coupling. */
 int agal_learn_attach(agal_ctx *ctx, agal_learn *m, int mode, int judge_every, double threshold);
-/* Look-ahead of the labels collected in mode 1: a snapshot taken after a
-   regrid is labelled with the rule's decisions at the next `horizon` regrids
-   (1..64; default 1): refine if any of them refines a block, coarsen only if
-   all of them coarsen it, weight 0 for a block that changes level in between.
-   A network trained on such labels marks, at one regrid, what the rule would
-   want over the next `horizon` periods, so a predicting case can regrid
-   `horizon` times less often (its P_REFINE times `horizon`).  Set it before
-   collecting. */
+/* Look-ahead (horizon 1..64; 0, the default, is the one-regrid-delayed
+   mode above).  In mode 1 a snapshot is taken at each regrid before its
+   refinement pass and labelled with the rule's decisions at that regrid and
+   the next horizon - 1: refine if any of them refines a block, coarsen only
+   if all of them coarsen it, weight 0 for a block that changes level in
+   between.  In mode 2 the network predicts from the state at a regrid and its
+   marks apply at that same regrid, so they cover the next `horizon` periods
+   and a predicting case can regrid `horizon` times less often (its P_REFINE
+   times `horizon`).  Set it before collecting. */
 int agal_learn_set_horizon(agal_learn *m, int horizon);
 /* Separate probability thresholds of the refinement and coarsening outputs in
    predict mode (after agal_learn_attach, which sets both to `threshold`). */
@@ -378,6 +379,14 @@ int agal_batch_advance_n(agal_batch *batch, int n, int use_graph);
 int agal_batch_sync(agal_batch *batch);
 int agal_batch_get_stream(const agal_batch *batch, void **stream);
 const char *agal_batch_last_error(const agal_batch *batch);
+/* Work-list mode (on by default where every case allows it: no LES, no
+   control-volume forces): each coarse step of the batch runs the fused steps
+   of all cases as one persistent kernel per phase over a global list of
+   (case, chunk of blocks), each case's arguments read from a device table,
+   followed by one batched fix-up launch; the other launches of a phase run
+   per case.  0 returns to one graph branch per case.  Results are identical
+   either way.  AGAL_ERR_UNSUPPORTED when a case does not allow it. */
+int agal_batch_set_worklist(agal_batch *batch, int on);
 
 /* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
    bytes must equal the size reported by agal_array_bytes. */

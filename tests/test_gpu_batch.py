@@ -45,8 +45,9 @@ def state(c):
     return out
 
 
+@pytest.mark.parametrize("worklist", [True, False])
 @pytest.mark.parametrize("use_graph", [True, False])
-def test_batch_equals_cases_alone(use_graph):
+def test_batch_equals_cases_alone(use_graph, worklist):
     steps = 20
     alone = []
     for spec in case_specs():
@@ -57,6 +58,7 @@ def test_batch_equals_cases_alone(use_graph):
         c.close()
     cases = [make(spec) for spec in case_specs()]
     with ag.Batch(cases) as b:
+        b.set_worklist(worklist)
         b.advance_n(7, use_graph=use_graph)
         b.advance_n(steps - 7, use_graph=use_graph)
         b.sync()
@@ -76,3 +78,35 @@ def test_batch_rejects_duplicates():
     with pytest.raises(RuntimeError):
         ag.Batch([c, c])
     c.close()
+
+
+def test_worklist_many_cases_of_one_kernel():
+    """Work-list mode with several cases on one batched kernel: D2Q9 FP16
+    cavities of different sizes and level counts (regrids every 8 steps), so
+    each step phase holds cases with different chunk counts and some phases
+    only part of the cases; every case ends bit for bit where it ends alone."""
+    specs = []
+    for k, (N, ml) in enumerate([(32, 3), (64, 1), (48, 2), (32, 2), (64, 3), (16, 1)]):
+        specs.append(dict(velocity_set=_lib.D2Q9, Nx=N, MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=ml, v0=5e-4 * (k + 1),
+                          P_REFINE=8, S_CRITERION=_lib.CRITERION_PERCENTILE, bc_preset=_lib.BC_LDC2D,
+                          storage=_lib.STORE_FP16, n_maxcblocks=(N // 4) ** 2 * 21 + 64))
+    steps = 24
+    alone = []
+    for spec in specs:
+        c = make(spec)
+        c.advance_n(steps)
+        c.sync()
+        alone.append(state(c))
+        c.close()
+    cases = [make(spec) for spec in specs]
+    with ag.Batch(cases) as b:
+        b.set_worklist(True)
+        b.advance_n(steps)
+        b.sync()
+    for i, c in enumerate(cases):
+        s = state(c)
+        assert s["counts"] == alone[i]["counts"], i
+        for k in s:
+            if k != "counts":
+                assert np.array_equal(s[k], alone[i][k]), (i, k)
+        c.close()

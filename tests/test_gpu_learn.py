@@ -254,11 +254,11 @@ def test_predict_mode_judged_refinement():
 
 
 def test_horizon_labels_cover_later_regrids():
-    """Labels over a horizon of 3 regrids, against the same (deterministic)
-    run labelled one regrid ahead: a block the rule refines at the next regrid
-    is labelled for refinement, one it does not coarsen at the next regrid is
-    not labelled for coarsening, and a block that changes level within the
-    horizon carries no weight; the last 3 snapshots stay unlabelled."""
+    """Look-ahead labels over 3 regrids against the same (deterministic) run
+    labelled over 1: a block the rule refines at the snapshot's regrid is
+    labelled for refinement, one it does not coarsen there is not labelled
+    for coarsening, and a block that changes level within the horizon carries
+    no weight; the last 2 snapshots stay unlabelled."""
     out = {}
     for h in (1, 3):
         p, c, m = collect(9, 64, 160, horizon=h, **CHANNEL)
@@ -271,7 +271,7 @@ def test_horizon_labels_cover_later_regrids():
             c.close()
     (c1, s1), (c3, s3) = out[1], out[3]
     assert c1["snapshots"] == c3["snapshots"] == 160 // 8
-    assert c1["labelled"] == c1["snapshots"] - 1 and c3["labelled"] == c3["snapshots"] - 3
+    assert c1["labelled"] == c1["snapshots"] and c3["labelled"] == c3["snapshots"] - 2
     wider = 0
     for (X1, Y1, W1), (X3, Y3, W3) in zip(s1, s3):
         assert np.array_equal(X1, X3)                      # the same states
@@ -284,10 +284,11 @@ def test_horizon_labels_cover_later_regrids():
 
 
 def test_predict_ahead_regrids_less_often():
-    """A network trained on labels 4 regrids ahead drives a run that regrids
-    4 times less often (P_REFINE x 4), the rule judging every regrid: the
-    regrid count drops 4x, the missed fraction is reported, the mesh stays
-    within a factor 2 of the plain run's and the flow stays bounded."""
+    """A network trained on labels covering 4 regrids drives a run that
+    regrids 4 times less often (P_REFINE x 4), predicting at each regrid for
+    that regrid, the rule judging every regrid: the regrid count drops 4x, the
+    missed fraction is reported, the mesh stays within a factor 2 of the plain
+    run's and the flow stays bounded."""
     p, c, m = collect(9, 64, 320, horizon=4, **CHANNEL)
     try:
         nl = m.counts()["labelled"]

@@ -23,6 +23,7 @@
 // equilibrium difference formed as a small quantity.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "ctx.h"
@@ -102,8 +103,9 @@ struct InterpArgs {
     unsigned sr_salt;
 };
 
+// Interpolation into the children of block a.ids[blk].
 template <int DIM, int Q, typename T, bool CUBIC>
-__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const InterpArgs a)
+__device__ __forceinline__ void interp_body(const InterpArgs &a, int blk)
 {
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, BLK = Q * MC, NT = Geo<DIM>::NCH * Geo<DIM>::MC;
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     // Uniform per CTA: every early return below depends on blockIdx only.
     // The mesh arrays are read before the wait for the predecessor (no kernel
     // that launches this one early writes them), the populations after it.
-    const int b = a.ids[blockIdx.x];
+    const int b = a.ids[blk];
     if (b < 0) return;
     const bool b1 = a.var == AGAL_INTERP_INTERFACE && a.bmask[b] == BLOCK_INTERFACE;
     const bool b2 = a.var == AGAL_INTERP_ADDED && a.ref[b] == REF_MARK_REFINE;
@@ -205,6 +207,28 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const I
     }
 }
 
+template <int DIM, int Q, typename T, bool CUBIC>
+__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_interp(const InterpArgs a)
+{
+    interp_body<DIM, Q, T, CUBIC>(a, blockIdx.x);
+}
+
+// Batched forms (the batch's work list): item w is block w - start[i] of case
+// i's list, transferred with that case's arguments A[i].
+template <int DIM, int Q, typename T, bool CUBIC>
+__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC)
+k_interp_batch(const InterpArgs *__restrict__ A, const int *__restrict__ start, int n_cases)
+{
+    const int total = start[n_cases];
+    int i = 0;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        while (start[i + 1] <= w) i++;
+        const InterpArgs a = A[i];
+        interp_body<DIM, Q, T, CUBIC>(a, w - start[i]);
+        __syncthreads();   // the shared staging is refilled for the next item
+    }
+}
+
 struct AverageArgs {
     const int *ids;
     int n;
@@ -219,8 +243,9 @@ struct AverageArgs {
 };
 
 
+// Averaging of the children of block a.ids[blk] into it.
 template <int DIM, int Q, typename T>
-__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const AverageArgs a)
+__device__ __forceinline__ void average_body(const AverageArgs &a, int blk)
 {
     using C = typename ST<T>::C;
     constexpr int MC = Geo<DIM>::MC, NCH = Geo<DIM>::NCH, BLK = Q * MC;
@@ -228,7 +253,7 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
     __shared__ C sg[2][NCH * MC];   // double-buffered: one barrier per direction
     __shared__ int smask[NCH * MC];
     // Mesh arrays before the wait for the predecessor, populations after it.
-    const int b = a.ids[blockIdx.x];
+    const int b = a.ids[blk];
     if (b < 0) return;
     const int bc = a.nbr_child[b];
     if (!(bc > -1 && (a.var == AGAL_AVERAGE_GRID || a.bmask[b] == BLOCK_INTERFACE))) return;
@@ -268,6 +293,26 @@ __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const 
             else val = C(0.125) * (s[0] + s[1] + s[4] + s[5] + s[16] + s[17] + s[20] + s[21]);
             fp[slot * MC] = enc_r<T>(val, rnd * sr_dir(p), a.sr);
         }
+    }
+}
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const AverageArgs a)
+{
+    average_body<DIM, Q, T>(a, blockIdx.x);
+}
+
+template <int DIM, int Q, typename T>
+__global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC)
+k_average_batch(const AverageArgs *__restrict__ A, const int *__restrict__ start, int n_cases)
+{
+    const int total = start[n_cases];
+    int i = 0;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        while (start[i + 1] <= w) i++;
+        const AverageArgs a = A[i];
+        average_body<DIM, Q, T>(a, w - start[i]);
+        __syncthreads();   // the shared buffers are refilled for the next item
     }
 }
 
@@ -612,6 +657,9 @@ template <int DIM, int Q, typename T> struct RunInterp {
         a.ratio = c->tau[L + 1] / c->tau[L];
         if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L + 1] / (float)c->tau[L]);
         a.var = var;
+        if (c->rec)   // batch recording: one batched launch per phase (batch.cu)
+            return agal_record_args(c, AGAL_OP_INTERP, L, &a, sizeof(a),
+                                    agal_transfer_batch_key(c, c->P.interp_order == AGAL_INTERP_CUBIC), a.n);
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
         if (c->P.interp_order == AGAL_INTERP_CUBIC)
             AGAL_CUDA(c, launch_pdl(k_interp<DIM, Q, T, true>, dim3((unsigned)a.n), dim3(NT), 0, c->stream, a));
@@ -648,6 +696,8 @@ template <int DIM, int Q, typename T> struct RunAverage {
         a.ratio = c->tau[L] / c->tau[L + 1];
         if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L] / (float)c->tau[L + 1]);
         a.var = var;
+        if (c->rec)   // batch recording: one batched launch per phase (batch.cu)
+            return agal_record_args(c, AGAL_OP_AVERAGE, L, &a, sizeof(a), agal_transfer_batch_key(c, false), a.n);
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
         AGAL_CUDA(c, launch_pdl(k_average<DIM, Q, T>, dim3((unsigned)a.n), dim3(NT), 0, c->stream, a));
         AGAL_CUDA(c, cudaGetLastError());
@@ -657,15 +707,65 @@ template <int DIM, int Q, typename T> struct RunAverage {
 
 }  // namespace agal
 
-int agal_launch_interp(agal_ctx *c, int L, int var)
+int agal_launch_interp(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunInterp>(c, L, var); }
+int agal_launch_average(agal_ctx *c, int L, int var) { return agal::dispatch<agal::RunAverage>(c, L, var); }
+
+// Batched transfers of many cases (batch.cu).  key: velocity set, storage and
+// (interpolation) the cubic flag.
+int agal_transfer_batch_key(const agal_ctx *c, bool cubic) { return (c->Q * 8 + c->storage) * 2 + (cubic ? 1 : 0); }
+
+namespace {
+template <int DIM, int Q, typename T>
+int transfer_batch(int kind, bool cubic, cudaStream_t s, const void *args, const int *start, int n, int total)
 {
-    if (c->rec) return agal_record_other(c, AGAL_OP_INTERP, L, [L, var](agal_ctx *x) { return agal_launch_interp(x, L, var); });
-    return agal::dispatch<agal::RunInterp>(c, L, var);
+    constexpr int NT = agal::Geo<DIM>::NCH * agal::Geo<DIM>::MC;
+    if (total <= 0) return AGAL_OK;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (kind == AGAL_OP_INTERP) {
+        const auto *A = static_cast<const agal::InterpArgs *>(args);
+        auto k = cubic ? agal::k_interp_batch<DIM, Q, T, true> : agal::k_interp_batch<DIM, Q, T, false>;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, 0);
+        if (e != cudaSuccess) return AGAL_ERR_CUDA;
+        k<<<std::min(total, std::max(per_sm, 1) * sms), NT, 0, s>>>(A, start, n);
+    } else {
+        const auto *A = static_cast<const agal::AverageArgs *>(args);
+        auto k = agal::k_average_batch<DIM, Q, T>;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, 0);
+        if (e != cudaSuccess) return AGAL_ERR_CUDA;
+        k<<<std::min(total, std::max(per_sm, 1) * sms), NT, 0, s>>>(A, start, n);
+    }
+    return cudaGetLastError() == cudaSuccess ? AGAL_OK : AGAL_ERR_CUDA;
 }
-int agal_launch_average(agal_ctx *c, int L, int var)
+}  // namespace
+
+int agal_launch_transfer_batch(int kind, int key, cudaStream_t s, const void *args, const int *start, int n, int total)
 {
-    if (c->rec) return agal_record_other(c, AGAL_OP_AVERAGE, L, [L, var](agal_ctx *x) { return agal_launch_average(x, L, var); });
-    return agal::dispatch<agal::RunAverage>(c, L, var);
+    const bool cubic = key & 1;
+    const int storage = (key >> 1) % 8, Q = (key >> 1) / 8;
+    auto go = [&](auto tag) -> int {
+        using T = decltype(tag);
+        switch (Q) {
+        case 9: return transfer_batch<2, 9, T>(kind, cubic, s, args, start, n, total);
+        case 19: return transfer_batch<3, 19, T>(kind, cubic, s, args, start, n, total);
+        case 27: return transfer_batch<3, 27, T>(kind, cubic, s, args, start, n, total);
+        default: return AGAL_ERR_PARAM;
+        }
+    };
+    switch (storage) {
+    case AGAL_STORE_FP32: return go(float{});
+    case AGAL_STORE_FP64: return go(double{});
+    case AGAL_STORE_FP16: return go(__half{});
+    case AGAL_STORE_BF16: return go(__nv_bfloat16{});
+    default: return AGAL_ERR_PARAM;
+    }
+}
+
+// Argument-structure sizes the batch checks recorded launches against.
+size_t agal_transfer_args_size(int kind)
+{
+    return kind == AGAL_OP_INTERP ? sizeof(agal::InterpArgs) : sizeof(agal::AverageArgs);
 }
 
 // Block values and the two quantiles of the percentile rule (no marks).

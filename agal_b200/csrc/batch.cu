@@ -21,8 +21,9 @@
 // the chunks of every case stepping in it (k_step_batch, a global work list
 // of (case, chunk) with each case's arguments in a device table), then the
 // wall steps of the cases that have walls, then one batched fix-up launch;
-// any other phase (interpolation, averaging, forces, the rounding counter)
-// runs each case's launch on its own stream.  Every case's kernels and their
+// an interpolation or averaging phase is one launch over (case, parent block)
+// items; the other phases (forces, the rounding counter) run each case's
+// launch on its own stream.  Every case's kernels and their
 // order are those of advancing it alone, so the results are identical.
 #include <cuda_runtime.h>
 
@@ -43,6 +44,8 @@ struct agal_op {
     int key = 0;               // fused step: batched-kernel key
     int n_blocks = 0;          // fused step: blocks of the level
     agal::StepArgs step{};
+    std::vector<unsigned char> args;   // transfers: the argument structure
+    int n_items = 0;                   // transfers: blocks of the launch
     const void *fin = nullptr;
     void *fout = nullptr;
     std::function<int(agal_ctx *)> fn;
@@ -82,6 +85,22 @@ int agal_record_step(agal_ctx *c, int L, const void *args, size_t bytes, int key
     std::memcpy(&op.step, args, bytes);
     op.fin = fin;
     op.fout = fout;
+    op.cur = c->cur;
+    op.sr_salt = c->sr_salt;
+    op.liter = c->liter;
+    c->rec->ops.push_back(std::move(op));
+    return AGAL_OK;
+}
+
+int agal_record_args(agal_ctx *c, int kind, int L, const void *args, size_t bytes, int key, int n_items)
+{
+    if (bytes != agal_transfer_args_size(kind)) return agal_set_err(c, AGAL_ERR_PARAM, "batch: transfer arguments size");
+    agal_op op;
+    op.kind = kind;
+    op.L = L;
+    op.key = key;
+    op.n_items = n_items;
+    op.args.assign(static_cast<const unsigned char *>(args), static_cast<const unsigned char *>(args) + bytes);
     op.cur = c->cur;
     op.sr_salt = c->sr_salt;
     op.liter = c->liter;
@@ -183,9 +202,13 @@ int plan_step(agal_batch *b, std::vector<agal_oplist> &lists, std::vector<Phase>
     return AGAL_OK;
 }
 
-// Device tables of the step phases: per phase and kernel key, the cases'
-// StepArgs then the chunk prefix (n + 1 ints).  Written to tables[slot]
-// before the launches that read them are issued.
+// Launch kinds run as one batched kernel per phase: fused steps and transfers.
+static bool batched_kind(int kind) { return kind == 0 || kind == AGAL_OP_INTERP || kind == AGAL_OP_AVERAGE; }
+
+// Device tables of the batched phases: per phase and kernel key, the cases'
+// argument structures then the work prefix (n + 1 ints: chunks of a step,
+// blocks of a transfer).  Written to tables[slot] before the launches that
+// read them are issued.
 struct StepGroup {
     int phase, key, n, total;
     size_t off_args, off_start;
@@ -199,7 +222,8 @@ int build_tables(agal_batch *b, int slot, const std::vector<agal_oplist> &lists,
     std::vector<char> host;
     auto align = [&](size_t a) { host.resize((host.size() + a - 1) / a * a); };
     for (int p = 0; p < (int)phases.size(); p++) {
-        if (phases[p].kind != 0) continue;
+        const int kind = phases[p].kind;
+        if (!batched_kind(kind)) continue;
         std::map<int, std::vector<int>> by_key;
         for (int t = 0; t < (int)phases[p].items.size(); t++) {
             const auto &it = phases[p].items[t];
@@ -207,9 +231,10 @@ int build_tables(agal_batch *b, int slot, const std::vector<agal_oplist> &lists,
         }
         for (auto &kv : by_key) {
             StepGroup g{p, kv.first, (int)kv.second.size(), 0, 0, 0, kv.second};
-            align(alignof(agal::StepArgs) > 16 ? alignof(agal::StepArgs) : 16);
+            const size_t asz = kind == 0 ? sizeof(agal::StepArgs) : agal_transfer_args_size(kind);
+            align(16);
             g.off_args = host.size();
-            host.resize(host.size() + sizeof(agal::StepArgs) * g.n);
+            host.resize(host.size() + asz * g.n);
             align(16);
             g.off_start = host.size();
             host.resize(host.size() + sizeof(int) * (g.n + 1));
@@ -218,9 +243,9 @@ int build_tables(agal_batch *b, int slot, const std::vector<agal_oplist> &lists,
                 const auto &it = phases[p].items[g.items[q]];
                 const agal_op &op = lists[it.first].ops[it.second];
                 const int mc = b->cases[it.first]->MC;
-                std::memcpy(host.data() + g.off_args + sizeof(agal::StepArgs) * q, &op.step, sizeof(agal::StepArgs));
+                std::memcpy(host.data() + g.off_args + asz * q, kind == 0 ? (const void *)&op.step : op.args.data(), asz);
                 reinterpret_cast<int *>(host.data() + g.off_start)[q] = acc;
-                acc += (op.n_blocks + 256 / mc - 1) / (256 / mc);
+                acc += kind == 0 ? (op.n_blocks + 256 / mc - 1) / (256 / mc) : op.n_items;
             }
             reinterpret_cast<int *>(host.data() + g.off_start)[g.n] = acc;
             g.total = acc;
@@ -265,6 +290,17 @@ int issue_step(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, c
     size_t g = 0;
     for (int p = 0; p < (int)phases.size(); p++) {
         const Phase &ph = phases[p];
+        if (ph.kind == AGAL_OP_INTERP || ph.kind == AGAL_OP_AVERAGE) {
+            for (; g < groups.size() && groups[g].phase == p; g++) {
+                const StepGroup &sg = groups[g];
+                const char *base = b->tables[slot];
+                const int rc = agal_launch_transfer_batch(ph.kind, sg.key, b->master, base + sg.off_args,
+                                                          reinterpret_cast<const int *>(base + sg.off_start), sg.n,
+                                                          sg.total);
+                if (rc) return berr(b, rc, "batched transfer launch failed");
+            }
+            continue;
+        }
         if (ph.kind != 0) {
             std::vector<int> cs;
             for (const auto &it : ph.items) cs.push_back(it.first);

@@ -218,6 +218,12 @@ int agal_launch_forces_cv(agal_ctx *c, int L, int post);   // S_FORCE_TYPE 1
 int agal_record_step(agal_ctx *c, int L, const void *args, size_t bytes, int key, int n_blocks, const void *fin,
                      void *fout);
 int agal_record_other(agal_ctx *c, int tag, int L, std::function<int(agal_ctx *)> fn);
+// A transfer (interpolation or averaging): its argument structure, the key of
+// its batched kernel and its block count.
+int agal_record_args(agal_ctx *c, int kind, int L, const void *args, size_t bytes, int key, int n_items);
+int agal_transfer_batch_key(const agal_ctx *c, bool cubic);
+int agal_launch_transfer_batch(int kind, int key, cudaStream_t s, const void *args, const int *start, int n, int total);
+size_t agal_transfer_args_size(int kind);
 enum { AGAL_OP_INTERP = 1, AGAL_OP_AVERAGE, AGAL_OP_FORCES, AGAL_OP_FORCES_CV, AGAL_OP_SR_TICK };
 int agal_step_batch_key(const agal_ctx *c);
 int agal_launch_step_batch(int key, cudaStream_t s, const void *dev_args, const int *dev_start, int n, int total,

@@ -415,9 +415,10 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
     batch.sync()
     t16 = e0.elapsed_time(e1)
     levels16 = [c.counts()["n_ids"][:-1] for c in cases]
-    # the same batch with one graph branch per case instead of the work list
+    # the same batch with one graph branch per case instead of the work list,
+    # timed past the next regrid (P_REFINE = 32) so neither window holds one
     batch.set_worklist(False)
-    batch.advance_n(2)
+    batch.advance_n(64 - (spinup + steps) + 1)
     batch.sync()
     upd16b = cells(cases)
     barrier()
@@ -470,7 +471,8 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
             "graph_branches_fp16": {"value": agg16b["mlups"], "ms_per_step": agg16b["ms"] / steps,
                                     "what": "the same batch, one graph branch per case (no work list)"},
             "mode": "work list: one persistent step kernel per phase over all cases' (case, chunk) items, "
-                    "batched fix-ups; transfers, walls and forces per case",
+                    "batched fix-ups, one launch per interpolation / averaging phase over (case, parent block) "
+                    "items; walls and forces per case",
             "ratio_vs_one_at_a_time_fp32": v16 / v32,
             "hbm": {"achieved_gbs_per_gpu": gbs, "peak": peak, "frac": gbs / peak, "peak_source": kind,
                     "bytes_per_update": 2 * 19 * 2},
@@ -740,6 +742,20 @@ def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epoc
            "thresholds": thr, "collect_s": collect_s, "train_s": train_s, "spinup_steps": spinup}
     runs = (("plain_fp32", _lib.STORE_FP32, base, False), ("plain_fp16", _lib.STORE_FP16, base, False),
             ("learned_fp16", _lib.STORE_FP16, base * horizon, True))
+    meshes = {}
+
+    def refined_cells(c):
+        """Root-grid positions covered by each finer level (2D), as sets."""
+        cnt = c.counts()
+        nmb = c.params.n_maxcblocks
+        ids = c.dump(_lib.ARR_ID_SET).reshape(-1, nmb)
+        fx = c.dump(_lib.ARR_CBLOCK_F_X).reshape(2, nmb)
+        out = {}
+        for L in range(1, cnt["max_levels"]):
+            b = ids[L, : cnt["n_ids"][L]].astype(np.int64)
+            out[L] = {(int(round(x * 128 * 2 ** L)), int(round(y * 128 * 2 ** L))) for x, y in zip(fx[0, b], fx[1, b])}
+        return out
+
     for name, st, period, learned in runs:
         c = ag.Case(_vortex_params(st, period, device))
         if learned:
@@ -757,9 +773,17 @@ def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epoc
                      missed=c1["missed"] - c0["missed"])
             r["missed_fraction"] = r["missed"] / r["plain_refine_marks"] if r["plain_refine_marks"] else 0.0
             m.attach(c, 0)
+        meshes[name] = refined_cells(c)
         c.close()
         out[name] = r
     m.close()
+    # both runs end on a regrid of theirs at the same coarse step: the share of
+    # the plain FP16 run's refined blocks (per level) the learned run also has
+    cov = {}
+    for L, pl in meshes["plain_fp16"].items():
+        le = meshes["learned_fp16"].get(L, set())
+        cov[f"L{L}"] = len(pl & le) / len(pl) if pl else 1.0
+    out["learned_fp16"]["coverage_of_plain_mesh"] = cov
     out["regrid_ms_saved_per_1000_steps"] = (out["plain_fp16"]["regrid_ms_per_1000_steps"] -
                                              out["learned_fp16"]["regrid_ms_per_1000_steps"])
     out["ratio_learned_fp16_vs_plain_fp32"] = out["learned_fp16"]["mlups"] / out["plain_fp32"]["mlups"]

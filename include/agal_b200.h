@@ -383,8 +383,9 @@ const char *agal_batch_last_error(const agal_batch *batch);
    control-volume forces): each coarse step of the batch runs the fused steps
    of all cases as one persistent kernel per phase over a global list of
    (case, chunk of blocks), each case's arguments read from a device table,
-   followed by one batched fix-up launch; the other launches of a phase run
-   per case.  0 returns to one graph branch per case.  Results are identical
+   followed by one batched fix-up launch; interpolation and averaging phases
+   are one launch each over (case, parent block) items; forces and the
+   rounding counter run per case.  0 returns to one graph branch per case.  Results are identical
    either way.  AGAL_ERR_UNSUPPORTED when a case does not allow it. */
 int agal_batch_set_worklist(agal_batch *batch, int on);
 

@@ -49,12 +49,13 @@ def learn_params(Q, N, **kw):
     return amr_params(Q, N, **base)
 
 
-def collect(Q, N, steps, seed=1, horizon=1, **kw):
-    """A learner in collect mode over a plain percentile-criterion run."""
+def collect(Q, N, steps, seed=1, horizon=None, **kw):
+    """A learner in collect mode over a plain percentile-criterion run
+    (horizon None: the one-regrid-delayed mode)."""
     p = learn_params(Q, N, **kw)
     c = ag.Case(p)
     m = ag.Learner(2 if Q == 9 else 3, seed=seed)
-    if horizon != 1:
+    if horizon is not None:
         m.set_horizon(horizon)
     m.attach(c, 1)
     run_like_reference(c, p, steps)

@@ -356,6 +356,13 @@ class Batch:
     def set_worklist(self, on: bool) -> None:
         self._c(self._lib.agal_batch_set_worklist(self._h, 1 if on else 0))
 
+    def autotune(self, steps: int = 4) -> dict:
+        """Time both launch modes (the cases advance) and keep the faster."""
+        ms = (C.c_float * 2)()
+        mode = C.c_int()
+        self._c(self._lib.agal_batch_autotune(self._h, int(steps), ms, C.byref(mode)))
+        return {"worklist": bool(mode.value), "ms_branches": ms[0], "ms_worklist": ms[1]}
+
     def stream(self) -> int:
         s = C.c_void_p()
         self._c(self._lib.agal_batch_get_stream(self._h, C.byref(s)))

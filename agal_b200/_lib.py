@@ -133,6 +133,7 @@ PROTOS = [
     ("agal_batch_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("agal_batch_last_error", C.c_char_p, [C.c_void_p]),
     ("agal_batch_set_worklist", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_batch_autotune", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("agal_learn_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     ("agal_learn_destroy", C.c_int, [C.c_void_p]),
     ("agal_learn_last_error", C.c_char_p, [C.c_void_p]),

@@ -537,6 +537,39 @@ extern "C" int agal_batch_advance_n(agal_batch *b, int n, int use_graph)
     return AGAL_OK;
 }
 
+// Time `steps` graph-replayed coarse steps in each launch mode (work list,
+// where allowed, and one branch per case) after a warm-up of two steps each,
+// and keep the faster.  The cases advance by 2 x (steps + 2) coarse steps,
+// with their regrids as usual; both modes give identical results.
+extern "C" int agal_batch_autotune(agal_batch *b, int steps, float *ms, int *mode)
+{
+    if (!b || steps < 1) return AGAL_ERR_PARAM;
+    float t[2] = {-1.f, -1.f};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BCUDA(b, cudaEventCreate(&e0));
+    BCUDA(b, cudaEventCreate(&e1));
+    int rc = AGAL_OK;
+    for (int on = 1; on >= 0 && rc == AGAL_OK; on--) {
+        if (on && !worklist_ok(b)) continue;
+        if ((rc = agal_batch_set_worklist(b, on))) break;
+        if ((rc = agal_batch_advance_n(b, 2, 1))) break;
+        if ((rc = agal_batch_sync(b))) break;
+        if (cudaEventRecord(e0, b->master) != cudaSuccess) { rc = AGAL_ERR_CUDA; break; }
+        if ((rc = agal_batch_advance_n(b, steps, 1))) break;
+        if (cudaEventRecord(e1, b->master) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&t[on], e0, e1) != cudaSuccess)
+            rc = AGAL_ERR_CUDA;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc == AGAL_ERR_CUDA ? berr(b, rc, "batch autotune timing failed") : rc;
+    const int best = (t[1] >= 0.f && t[1] <= t[0]) ? 1 : 0;
+    if ((rc = agal_batch_set_worklist(b, best))) return rc;
+    if (ms) { ms[0] = t[0] / steps; ms[1] = t[1] >= 0.f ? t[1] / steps : -1.f; }
+    if (mode) *mode = best;
+    return AGAL_OK;
+}
+
 extern "C" int agal_batch_sync(agal_batch *b)
 {
     if (!b) return AGAL_ERR_PARAM;

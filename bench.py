@@ -399,34 +399,37 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
     def cells(cases):
         return sum(leaf_cells(c.counts(), 3) for c in cases)
 
-    # batched, FP16
+    # batched, FP16: the autotuner picks the launch mode (work list or one
+    # graph branch per case); both modes are then timed over 20 coarse steps
+    # that hold no regrid (P_REFINE = 32)
     cases, tunes16 = build(_lib.STORE_FP16)
     batch = ag.Batch(cases)
     batch.advance_n(spinup)
-    batch.sync()
+    tuned = batch.autotune(4)
+    at = spinup + 2 * (4 + 2)
     stream = torch.cuda.ExternalStream(batch.stream())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    upd16 = cells(cases)
-    torch.cuda.synchronize()
-    barrier()
-    e0.record(stream)
-    batch.advance_n(steps)
-    e1.record(stream)
-    batch.sync()
-    t16 = e0.elapsed_time(e1)
+
+    def timed_window(start_at):
+        """Advance to step `start_at`, then time `steps` coarse steps."""
+        batch.advance_n(start_at - timed_window.at)
+        batch.sync()
+        upd = cells(cases)
+        barrier()
+        a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a_.record(stream)
+        batch.advance_n(steps)
+        b_.record(stream)
+        batch.sync()
+        timed_window.at = start_at + steps
+        return upd, a_.elapsed_time(b_)
+    timed_window.at = at
+    period = 32
+    first = (at + period - 1) // period * period          # the step after a regrid
+    upd16, t16 = timed_window(first)
     levels16 = [c.counts()["n_ids"][:-1] for c in cases]
-    # the same batch with one graph branch per case instead of the work list,
-    # timed past the next regrid (P_REFINE = 32) so neither window holds one
-    batch.set_worklist(False)
-    batch.advance_n(64 - (spinup + steps) + 1)
-    batch.sync()
-    upd16b = cells(cases)
-    barrier()
-    e0.record(stream)
-    batch.advance_n(steps)
-    e1.record(stream)
-    batch.sync()
-    t16b = e0.elapsed_time(e1)
+    # the other mode, in the next regrid-free window
+    batch.set_worklist(not tuned["worklist"])
+    upd16b, t16b = timed_window((timed_window.at + period - 1) // period * period)
     batch.close()
     for c in cases:
         c.close()
@@ -468,11 +471,13 @@ def run_batched(torch, n_cases: int, seed: int, spinup: int, steps: int, device:
             "value": v16, "unit": "MLUPS", "storage": "f16-offset", "ms_per_step": t16 / steps,
             "cell_updates_per_step": upd16,
             "one_at_a_time_fp32": {"value": v32, "ms_per_step": t32 / steps, "cell_updates_per_step": upd32},
-            "graph_branches_fp16": {"value": agg16b["mlups"], "ms_per_step": agg16b["ms"] / steps,
-                                    "what": "the same batch, one graph branch per case (no work list)"},
-            "mode": "work list: one persistent step kernel per phase over all cases' (case, chunk) items, "
-                    "batched fix-ups, one launch per interpolation / averaging phase over (case, parent block) "
-                    "items; walls and forces per case",
+            "other_mode_fp16": {"value": agg16b["mlups"], "ms_per_step": agg16b["ms"] / steps,
+                                "mode": "graph branches" if tuned["worklist"] else "work list"},
+            "mode": "work list" if tuned["worklist"] else "graph branches",
+            "autotune": tuned,
+            "modes": "work list: one persistent step kernel per phase over all cases' (case, chunk) items, batched "
+                     "fix-ups, one launch per interpolation / averaging phase over (case, parent block) items, walls "
+                     "and forces per case; graph branches: each case's launches as its own branch of the graph",
             "ratio_vs_one_at_a_time_fp32": v16 / v32,
             "hbm": {"achieved_gbs_per_gpu": gbs, "peak": peak, "frac": gbs / peak, "peak_source": kind,
                     "bytes_per_update": 2 * 19 * 2},
@@ -779,11 +784,13 @@ def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epoc
     m.close()
     # both runs end on a regrid of theirs at the same coarse step: the share of
     # the plain FP16 run's refined blocks (per level) the learned run also has
-    cov = {}
-    for L, pl in meshes["plain_fp16"].items():
-        le = meshes["learned_fp16"].get(L, set())
-        cov[f"L{L}"] = len(pl & le) / len(pl) if pl else 1.0
-    out["learned_fp16"]["coverage_of_plain_mesh"] = cov
+    def coverage(ref, other):
+        return {f"L{L}": (len(pl & meshes[other].get(L, set())) / len(pl) if pl else 1.0)
+                for L, pl in meshes[ref].items()}
+    out["learned_fp16"]["coverage_of_plain_mesh"] = coverage("plain_fp16", "learned_fp16")
+    # the same measure between the two plain runs (FP32 against FP16): how far
+    # two runs of this flow drift apart in where they refine
+    out["plain_fp32"]["coverage_of_plain_fp16_mesh"] = coverage("plain_fp16", "plain_fp32")
     out["regrid_ms_saved_per_1000_steps"] = (out["plain_fp16"]["regrid_ms_per_1000_steps"] -
                                              out["learned_fp16"]["regrid_ms_per_1000_steps"])
     out["ratio_learned_fp16_vs_plain_fp32"] = out["learned_fp16"]["mlups"] / out["plain_fp32"]["mlups"]

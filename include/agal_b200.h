@@ -388,6 +388,13 @@ const char *agal_batch_last_error(const agal_batch *batch);
    rounding counter run per case.  0 returns to one graph branch per case.  Results are identical
    either way.  AGAL_ERR_UNSUPPORTED when a case does not allow it. */
 int agal_batch_set_worklist(agal_batch *batch, int on);
+/* Autotuner of the batch's launch mode: times `steps` graph-replayed coarse
+   steps in work-list mode (where allowed) and with one branch per case, each
+   after two warm-up steps, and keeps the faster.  The cases really advance
+   (2 x (steps + 2) coarse steps, regrids included).  ms[2] (may be NULL)
+   receives the per-step times {branches, work list (-1 if not allowed)},
+   *mode (may be NULL) 1 for the work list, 0 for branches. */
+int agal_batch_autotune(agal_batch *batch, int steps, float *ms, int *mode);
 
 /* Device <-> host transfers of one mesh/solver array (AGAL_ARR_*).
    bytes must equal the size reported by agal_array_bytes. */

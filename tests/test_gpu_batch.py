@@ -110,3 +110,31 @@ def test_worklist_many_cases_of_one_kernel():
             if k != "counts":
                 assert np.array_equal(s[k], alone[i][k]), (i, k)
         c.close()
+
+
+def test_batch_autotune_picks_a_mode_and_keeps_results():
+    """The launch-mode autotuner times both modes on real steps: the cases
+    advance 2 x (steps + 2) coarse steps and end where advancing them alone
+    leaves them."""
+    steps = 3
+    total = 2 * (steps + 2) + 5
+    alone = []
+    for spec in case_specs():
+        c = make(spec)
+        c.advance_n(total)
+        c.sync()
+        alone.append(state(c))
+        c.close()
+    cases = [make(spec) for spec in case_specs()]
+    with ag.Batch(cases) as b:
+        r = b.autotune(steps)
+        assert r["ms_branches"] > 0 and r["ms_worklist"] > 0
+        b.advance_n(5)
+        b.sync()
+    for i, c in enumerate(cases):
+        s = state(c)
+        assert s["counts"] == alone[i]["counts"], i
+        for k in s:
+            if k != "counts":
+                assert np.array_equal(s[k], alone[i][k]), (i, k)
+        c.close()

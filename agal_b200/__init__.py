@@ -170,6 +170,11 @@ class Case:
         self._c(self._lib.agal_refine_stats(self._h, C.byref(it), C.byref(nr), C.byref(nc)))
         return {"iter": it.value, "n_refined": nr.value, "n_coarsened": nc.value}
 
+    def graph_stats(self) -> dict:
+        b, u = C.c_longlong(), C.c_longlong()
+        self._c(self._lib.agal_graph_stats(self._h, C.byref(b), C.byref(u)))
+        return {"builds": b.value, "updates": u.value}
+
     STEP_VARIANTS = {1: "1 cell/thread", 2: "2 cells/thread", 3: "TMA-staged persistent pipeline",
                      4: "1 row of 4 cells/thread, vector loads and stores",
                      5: "root-level tile of 8x8 blocks per CTA, gathered whole-block stores (2D)",
@@ -307,7 +312,7 @@ class Case:
 
     # -- arrays ---------------------------------------------------------
     _DTYPES = {_lib.ARR_F: np.float64, _lib.ARR_MACROS: np.float64, _lib.ARR_CBLOCK_F_X: np.float32,
-               _lib.ARR_CELLS_F_X_B: np.float32, _lib.ARR_CBLOCK_F_FF: np.float64}
+               _lib.ARR_CELLS_F_X_B: np.float32, _lib.ARR_CBLOCK_F_FF: np.float64, _lib.ARR_NU_SGS: np.float64}
 
     def array_bytes(self, which: int) -> int:
         n = C.c_size_t()

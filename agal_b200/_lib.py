@@ -34,7 +34,7 @@ MESH_REF_NW_CASES, MESH_REF_UNIFORM, MESH_REF_SOLUTION = 0, 2, 3
 ARR_F, ARR_MACROS, ARR_CELLS_ID_MASK, ARR_CBLOCK_F_X, ARR_CBLOCK_ID_MASK, ARR_CBLOCK_ID_NBR, \
     ARR_CBLOCK_ID_NBR_CHILD, ARR_CBLOCK_ID_ONB, ARR_CBLOCK_ID_REF, ARR_CBLOCK_LEVEL, ARR_ID_SET, \
     ARR_GAP_SET = range(12)
-ARR_CBLOCK_ID_ONB_SOLID, ARR_CELLS_F_X_B, ARR_CBLOCK_F_FF = 12, 13, 14
+ARR_CBLOCK_ID_ONB_SOLID, ARR_CELLS_F_X_B, ARR_CBLOCK_F_FF, ARR_NU_SGS = 12, 13, 14, 15
 
 INT_KEYS = ["MAX_LEVELS_WALL", "MAX_LEVELS_INTERIOR", "N_ITER_TOTAL", "N_LEVEL_START", "Nx", "N_RESTART",
             "PERIODIC_X", "PERIODIC_Y", "PERIODIC_Z",
@@ -109,6 +109,7 @@ PROTOS = [
     ("agal_mesh_ref_criteria", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("agal_freeze_refined_cells", C.c_int, [C.c_void_p, C.c_int]),
     ("agal_refine_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("agal_graph_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     ("agal_set_geometry", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("agal_geometry_read_stl", C.c_int, [C.c_char_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),
     ("agal_geometry_read_text", C.c_int, [C.POINTER(AgalParams), C.c_char_p, C.c_void_p, C.c_longlong,

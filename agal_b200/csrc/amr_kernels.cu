@@ -432,7 +432,9 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_criterion(const CriterionArgs 
 // rounded in the order the oracle writes it.  The ref_pct_hi / ref_pct_lo
 // quantiles of the leaf blocks' values are then selected exactly on the
 // device by a radix select over the bits of the (non-negative, so
-// order-preserving) FP64 keys, 16 bits per pass, and k_pct_mark marks.
+// order-preserving) FP64 keys (one CTA, 8 bits per pass, on pools of up to
+// 65,536 blocks; 16 bits per pass over the whole grid beyond), and
+// k_pct_mark marks.
 __device__ __forceinline__ float r_sqrt(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ double r_sqrt(double a) { return __dsqrt_rn(a); }
 
@@ -592,6 +594,72 @@ __global__ void __launch_bounds__(1024) k_pct_pick(int *hist, PctState *st, int 
     }
     __syncthreads();
     for (int i = 0; i < 64; i++) h[t * 64 + i] = 0;
+}
+
+// The whole selection in one CTA, for pools of up to kPctOneCta blocks: eight
+// passes of 8 key bits, histograms in shared memory, warp r picking the bin
+// of quantile r.  Selects the same keys as the 16-bit passes above.
+constexpr int kPctOneCta = 1 << 16;
+
+__global__ void __launch_bounds__(1024) k_pct_select(const double *wval, const int *pop, int idm, PctState *st,
+                                                     double pct_hi, double pct_lo)
+{
+    __shared__ int s_hist[2][256];
+    __shared__ unsigned long long s_prefix[2];
+    __shared__ int s_k[2];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int n = st->n;
+    if (n <= 0) return;   // uniform
+    if (t < 2) {
+        s_prefix[t] = 0ull;
+        s_k[t] = (int)floor((t == 0 ? pct_hi : pct_lo) * (double)(n - 1));
+    }
+    for (int pass = 0; pass < 8; pass++) {
+        const int sh = 56 - 8 * pass;
+        for (int i = t; i < 512; i += blockDim.x) s_hist[i >> 8][i & 255] = 0;
+        __syncthreads();
+        const unsigned long long p0 = s_prefix[0], p1 = s_prefix[1];
+        for (int b = t; b < idm; b += blockDim.x) {
+            if (!pop[b]) continue;
+            const unsigned long long key = (unsigned long long)__double_as_longlong(wval[b]);
+            const int bin = (int)((key >> sh) & 0xFFull);
+            const unsigned long long hi = pass ? (key >> (sh + 8)) : 0ull;
+            if (hi == p0) atomicAdd(&s_hist[0][bin], 1);
+            if (hi == p1) atomicAdd(&s_hist[1][bin], 1);
+        }
+        __syncthreads();
+        if (wid < 2) {
+            const int r = wid, k = s_k[r];
+            int c[8], sum = 0;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                c[i] = s_hist[r][lane * 8 + i];
+                sum += c[i];
+            }
+            int x = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            int start = x - sum;
+            if (start <= k && k < start + sum) {
+                for (int i = 0; i < 8; i++) {
+                    if (k < start + c[i]) {
+                        s_prefix[r] = (s_prefix[r] << 8) | (unsigned long long)(lane * 8 + i);
+                        s_k[r] = k - start;
+                        break;
+                    }
+                    start += c[i];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (t < 2) {
+        st->prefix[t] = s_prefix[t];
+        st->k[t] = s_k[t];
+    }
 }
 
 __global__ void k_pct_mark(const double *wval, const PctState *st, const int *nbr, long long nmb, int qmax,
@@ -775,8 +843,9 @@ static int percentile_select(agal_ctx *c, int idm)
     double *wval = static_cast<double *>(c->crit);
     int *hist = reinterpret_cast<int *>(wval + c->nmb);
     agal::PctState *st = reinterpret_cast<agal::PctState *>(hist + 2 * 65536);
+    const bool one_cta = idm <= agal::kPctOneCta;
     AGAL_CUDA(c, cudaMemsetAsync(st, 0, sizeof(agal::PctState), c->stream));
-    AGAL_CUDA(c, cudaMemsetAsync(hist, 0, sizeof(int) * 2 * 65536, c->stream));
+    if (!one_cta) AGAL_CUDA(c, cudaMemsetAsync(hist, 0, sizeof(int) * 2 * 65536, c->stream));
     agal::WmaxArgs a;
     a.idm = idm;
     a.nmc = c->nmc;
@@ -798,9 +867,13 @@ static int percentile_select(agal_ctx *c, int idm)
         else agal::k_wmax<3, float><<<(unsigned)idm, 64, 0, c->stream>>>(a);
     }
     const unsigned g = (unsigned)((idm + 255) / 256);
-    for (int pass = 0; pass < 4; pass++) {
-        agal::k_pct_hist<<<g, 256, 0, c->stream>>>(wval, c->amr_a, idm, st, pass, hist);
-        agal::k_pct_pick<<<2, 1024, 0, c->stream>>>(hist, st, pass, c->P.ref_pct_hi, c->P.ref_pct_lo);
+    if (one_cta) {
+        agal::k_pct_select<<<1, 1024, 0, c->stream>>>(wval, c->amr_a, idm, st, c->P.ref_pct_hi, c->P.ref_pct_lo);
+    } else {
+        for (int pass = 0; pass < 4; pass++) {
+            agal::k_pct_hist<<<g, 256, 0, c->stream>>>(wval, c->amr_a, idm, st, pass, hist);
+            agal::k_pct_pick<<<2, 1024, 0, c->stream>>>(hist, st, pass, c->P.ref_pct_hi, c->P.ref_pct_lo);
+        }
     }
     AGAL_CUDA(c, cudaGetLastError());
     return AGAL_OK;

@@ -524,7 +524,10 @@ int agal_refine_pass(agal_ctx *c)
     AGAL_CUDA(c, cudaGetLastError());
     if ((rc = read_small(c, h, 0, 2))) return rc;
     int nR = h[S_NR], nC = h[S_NC];
-    int idm_wnew = idm + NCH * nR;
+    // Bound of the IDs a pass can touch (mesh_amr.cu:2186 and :2341).  The
+    // reference's sum can pass n_maxcblocks when the pool is nearly full,
+    // although every ID lies below it; the passes stop at n_maxcblocks.
+    int idm_wnew = (int)std::min<long long>((long long)idm + (long long)NCH * nR, nmb);
     const bool proceed_ref = nR > 0 && (long long)NCH * nR <= c->n_gaps;
     bool proceed_coarse = nC > 0;
     if (!proceed_ref && nR > 0) {   // mesh_amr.cu:2197-2205
@@ -545,7 +548,7 @@ int agal_refine_pass(agal_ctx *c)
         AGAL_CUDA(c, cudaMemcpyAsync(c->amr_small + S_GMAX, &mn, sizeof(int), cudaMemcpyHostToDevice, c->stream));
         k_max_range<<<grid_for(hi - lo), NT, 0, c->stream>>>(c->gap_set, lo, hi, c->amr_small + S_GMAX);
         if ((rc = read_small(c, h, S_GMAX, 1))) return rc;
-        if (h[0] + 1 > idm_wnew) idm_wnew = h[0] + 1;
+        if (h[0] + 1 > idm_wnew) idm_wnew = (int)std::min<long long>(h[0] + 1, nmb);
         k_s2_1<<<grid_for(idm), NT, 0, c->stream>>>(c->amr_emap, nbr, ref, c->amr_first, nmb, Qmax, idm, nch);
     }
     // S3: 2:1 quality control of coarsening.
@@ -637,7 +640,7 @@ int agal_refine_pass(agal_ctx *c)
     k_masks_1<<<grid_for(idmN), NT, 0, c->stream>>>(ref, nch, nmb, Qmax, idmN, c->cblock_ID_mask);
     AGAL_CUDA(c, cudaGetLastError());
     for (int L = 0; L < ML - 1; L++)
-        if ((rc = agal_launch_interp(c, L, AGAL_INTERP_ADDED))) return rc;
+        if ((rc = agal_les_refresh(c, L)) || (rc = agal_launch_interp(c, L, AGAL_INTERP_ADDED))) return rc;
     k_s3<<<grid_for(idm_wnew), NT, 0, c->stream>>>(ref, idm_wnew);
     AGAL_CUDA(c, cudaMemcpyAsync(c->amr_snap, ref, sizeof(int) * (size_t)idm_wnew, cudaMemcpyDeviceToDevice,
                                  c->stream));

@@ -126,6 +126,8 @@ struct agal_batch {
     cudaStream_t master = nullptr;
     cudaEvent_t fork = nullptr, done = nullptr;
     std::vector<cudaEvent_t> join;
+    std::vector<cudaStream_t> gstream;            // one stream per phase group (work-list mode)
+    std::vector<cudaEvent_t> gjoin;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     std::vector<std::vector<int>> graph_cur[2];   // every case's cur[] at capture
     bool worklist = false;                        // work-list mode in force
@@ -159,6 +161,7 @@ int bcuda(agal_batch *b, cudaError_t e, const char *what)
 struct Phase {
     int kind, L, occ;
     std::vector<std::pair<int, int>> items;
+    int group = 0;   // cases of one level count share a phase sequence
 };
 
 // Record one coarse step of every case (nothing launched; the cases' buffer
@@ -174,30 +177,40 @@ int plan_step(agal_batch *b, std::vector<agal_oplist> &lists, std::vector<Phase>
         c->rec = nullptr;
         if (rc) return berr(b, rc, "case " + std::to_string(i) + ": " + c->err);
     }
-    std::vector<int> order(n);
-    for (int i = 0; i < n; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int x, int y) { return lists[x].ops.size() > lists[y].ops.size(); });
+    // Cases with the same number of levels run the same sequence: each such
+    // group gets its own merged phases (issued on its own stream, so light
+    // phases of one group overlap the others).
+    std::map<int, std::vector<int>> groups;
+    for (int i = 0; i < n; i++) groups[b->cases[i]->max_levels].push_back(i);
     phases.clear();
-    for (int i : order) {
-        std::map<std::pair<int, int>, int> occ;
-        int pos = -1;
-        for (int j = 0; j < (int)lists[i].ops.size(); j++) {
-            const agal_op &op = lists[i].ops[j];
-            const int k = occ[{op.kind, op.L}]++;
-            int at = -1;
-            for (int p = pos + 1; p < (int)phases.size(); p++)
-                if (phases[p].kind == op.kind && phases[p].L == op.L && phases[p].occ == k) {
-                    at = p;
-                    break;
+    int gi = 0;
+    for (auto &gv : groups) {
+        std::vector<int> order = gv.second;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return lists[x].ops.size() > lists[y].ops.size(); });
+        std::vector<Phase> ph;
+        for (int i : order) {
+            std::map<std::pair<int, int>, int> occ;
+            int pos = -1;
+            for (int j = 0; j < (int)lists[i].ops.size(); j++) {
+                const agal_op &op = lists[i].ops[j];
+                const int k = occ[{op.kind, op.L}]++;
+                int at = -1;
+                for (int p = pos + 1; p < (int)ph.size(); p++)
+                    if (ph[p].kind == op.kind && ph[p].L == op.L && ph[p].occ == k) {
+                        at = p;
+                        break;
+                    }
+                if (at < 0) {
+                    at = pos + 1;
+                    ph.insert(ph.begin() + at, Phase{op.kind, op.L, k, {}, gi});
                 }
-            if (at < 0) {
-                at = pos + 1;
-                phases.insert(phases.begin() + at, Phase{op.kind, op.L, k, {}});
+                ph[at].items.push_back({i, j});
+                pos = at;
             }
-            phases[at].items.push_back({i, j});
-            pos = at;
         }
+        phases.insert(phases.end(), ph.begin(), ph.end());
+        gi++;
     }
     return AGAL_OK;
 }
@@ -268,33 +281,65 @@ int build_tables(agal_batch *b, int slot, const std::vector<agal_oplist> &lists,
 // Run fn(case) for the listed cases, each on its own stream, between a fork
 // from and a join back to the master stream.
 template <class F>
-int fan_out(agal_batch *b, const std::vector<int> &cases, F fn)
+int fan_out(agal_batch *b, cudaStream_t s, const std::vector<int> &cases, F fn)
 {
     if (cases.empty()) return AGAL_OK;
-    BCUDA(b, cudaEventRecord(b->fork, b->master));
+    BCUDA(b, cudaEventRecord(b->fork, s));
     for (int i : cases) {
         agal_ctx *c = b->cases[i];
         BCUDA(b, cudaStreamWaitEvent(c->stream, b->fork, 0));
         const int rc = fn(c);
         if (rc) return berr(b, rc, "case " + std::to_string(i) + ": " + c->err);
         BCUDA(b, cudaEventRecord(b->join[i], c->stream));
-        BCUDA(b, cudaStreamWaitEvent(b->master, b->join[i], 0));
+        BCUDA(b, cudaStreamWaitEvent(s, b->join[i], 0));
     }
     return AGAL_OK;
 }
 
-// Issue the planned phases on the master stream (under capture or not).
+// Stream of phase group g (created on first use), forked from the master.
+int group_stream(agal_batch *b, int g, cudaStream_t *out)
+{
+    while ((int)b->gstream.size() <= g) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        BCUDA(b, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        BCUDA(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->gstream.push_back(st);
+        b->gjoin.push_back(ev);
+    }
+    *out = b->gstream[g];
+    return AGAL_OK;
+}
+
+// Issue the planned phases (under capture or not): each phase group on its
+// own stream, forked from the master and joined back into it.
 int issue_step(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, const std::vector<Phase> &phases,
                const std::vector<StepGroup> &groups)
 {
     size_t g = 0;
+    int cur_group = -1;
+    cudaStream_t s = b->master;
+    BCUDA(b, cudaEventRecord(b->done, b->master));   // every group starts after the master's work
+    auto end_group = [&]() -> int {
+        if (cur_group < 0) return AGAL_OK;
+        BCUDA(b, cudaEventRecord(b->gjoin[cur_group], s));
+        BCUDA(b, cudaStreamWaitEvent(b->master, b->gjoin[cur_group], 0));
+        return AGAL_OK;
+    };
     for (int p = 0; p < (int)phases.size(); p++) {
         const Phase &ph = phases[p];
+        if (ph.group != cur_group) {
+            int rc = end_group();
+            if (!rc) rc = group_stream(b, ph.group, &s);
+            if (rc) return rc;
+            cur_group = ph.group;
+            BCUDA(b, cudaStreamWaitEvent(s, b->done, 0));
+        }
         if (ph.kind == AGAL_OP_INTERP || ph.kind == AGAL_OP_AVERAGE) {
             for (; g < groups.size() && groups[g].phase == p; g++) {
                 const StepGroup &sg = groups[g];
                 const char *base = b->tables[slot];
-                const int rc = agal_launch_transfer_batch(ph.kind, sg.key, b->master, base + sg.off_args,
+                const int rc = agal_launch_transfer_batch(ph.kind, sg.key, s, base + sg.off_args,
                                                           reinterpret_cast<const int *>(base + sg.off_start), sg.n,
                                                           sg.total);
                 if (rc) return berr(b, rc, "batched transfer launch failed");
@@ -305,7 +350,7 @@ int issue_step(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, c
             std::vector<int> cs;
             for (const auto &it : ph.items) cs.push_back(it.first);
             size_t q = 0;
-            const int rc = fan_out(b, cs, [&](agal_ctx *c) {
+            const int rc = fan_out(b, s, cs, [&](agal_ctx *c) {
                 const auto &it = ph.items[q++];
                 const agal_op &op = lists[it.first].ops[it.second];
                 return run_in_state(c, op, op.fn);
@@ -316,7 +361,7 @@ int issue_step(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, c
         for (; g < groups.size() && groups[g].phase == p; g++) {
             const StepGroup &sg = groups[g];
             const char *base = b->tables[slot];
-            int rc = agal_launch_step_batch(sg.key, b->master, base + sg.off_args,
+            int rc = agal_launch_step_batch(sg.key, s, base + sg.off_args,
                                             reinterpret_cast<const int *>(base + sg.off_start), sg.n, sg.total, 0);
             if (rc) return berr(b, rc, "batched step launch failed");
             // the wall steps of cases with walls, then the fix-ups of all
@@ -331,17 +376,17 @@ int issue_step(agal_batch *b, int slot, const std::vector<agal_oplist> &lists, c
                 }
             }
             size_t q = 0;
-            rc = fan_out(b, cs, [&](agal_ctx *c) {
+            rc = fan_out(b, s, cs, [&](agal_ctx *c) {
                 const agal_op *op = ops[q++];
                 return run_in_state(c, *op, [op](agal_ctx *x) { return agal_launch_wall_step(x, op->L, op->fin, op->fout); });
             });
             if (rc) return rc;
-            rc = agal_launch_step_batch(sg.key, b->master, base + sg.off_args,
+            rc = agal_launch_step_batch(sg.key, s, base + sg.off_args,
                                         reinterpret_cast<const int *>(base + sg.off_start), sg.n, 0, 1);
             if (rc) return berr(b, rc, "batched fix-up launch failed");
         }
     }
-    return AGAL_OK;
+    return end_group();
 }
 
 // Work-list mode needs every case on one launch path: no LES, no control-volume
@@ -459,6 +504,10 @@ extern "C" int agal_batch_destroy(agal_batch *b)
         if (e) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->done) cudaEventDestroy(b->done);
+    for (cudaEvent_t e : b->gjoin)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t st : b->gstream)
+        if (st) cudaStreamDestroy(st);
     if (b->master) cudaStreamDestroy(b->master);
     for (char *t : b->tables)
         if (t) cudaFree(t);

@@ -73,12 +73,19 @@ size_t compute_size(const agal_ctx *c) { return c->storage == AGAL_STORE_FP64 ? 
 
 void agal_drop_graphs(agal_ctx *c)
 {
+    c->graph_steps = 0;
+    c->graph_cur_in.clear();
+    for (int k = 0; k < 2; k++) c->ml_graph_cur[k].clear();
+}
+
+void agal_free_graphs(agal_ctx *c)
+{
+    agal_drop_graphs(c);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     c->graph_exec = nullptr;
     for (int k = 0; k < 2; k++) {
         if (c->ml_graph[k]) cudaGraphExecDestroy(c->ml_graph[k]);
         c->ml_graph[k] = nullptr;
-        c->ml_graph_cur[k].clear();
     }
 }
 
@@ -86,7 +93,7 @@ namespace {
 
 void release(agal_ctx *c)
 {
-    agal_drop_graphs(c);
+    agal_free_graphs(c);
     agal_geometry_release(c);
     void *ptrs[] = {c->F[0], c->F[1], c->macro, c->cells_ID_mask, c->cblock_f_X, c->cblock_ID_mask,
                     c->cblock_ID_nbr, c->cblock_ID_nbr_child, c->cblock_ID_onb, c->cblock_ID_ref,
@@ -130,11 +137,9 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         delete c;
         return agal_set_err(nullptr, AGAL_ERR_PARAM, "half_rounding");
     }
-    if (p->S_LES > 0 && (p->collision != AGAL_BGK || std::max(p->MAX_LEVELS_WALL, p->MAX_LEVELS_INTERIOR) != 1 ||
-                         p->S_BC_TYPE != 0)) {
+    if (p->S_LES > 0 && (p->collision != AGAL_BGK || p->S_BC_TYPE != 0)) {
         delete c;
-        return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED,
-                            "S_LES: built for BGK on one-level meshes without interpolated bounce-back");
+        return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "S_LES: built for BGK without interpolated bounce-back");
     }
     c->Qmax = (c->dim == 2) ? 9 : 27;
     c->MC = (c->dim == 2) ? 16 : 64;
@@ -596,6 +601,14 @@ static int step_f(agal_ctx *c, int L, bool forces)
     return AGAL_OK;
 }
 
+// S_Average inside the recursion: the refresh of level L+1 (LES macro mode),
+// then the averaging.
+static int average_rec(agal_ctx *c, int L, int var)
+{
+    const int rc = agal_les_refresh(c, L + 1);
+    return rc ? rc : agal_launch_average(c, L, var);
+}
+
 // The interface interpolation of level L beside the step of level L: the
 // interpolation reads F[cur[L]] and writes ghost cells of F[cur[L+1]], the
 // step reads F[cur[L]] and writes level L's other buffer, so they are
@@ -604,6 +617,9 @@ static int step_f(agal_ctx *c, int L, bool forces)
 static int interp_beside_step(agal_ctx *c, int L, bool forces)
 {
     int rc;
+    // The refresh of S_Interpolate (LES macro mode) precedes both branches:
+    // the step's eddy viscosity reads the rows it writes.
+    if ((rc = agal_les_refresh(c, L))) return rc;
     if (c->rec) {   // batch recording: the batch orders the launches itself
         if ((rc = agal_launch_interp(c, L, AGAL_INTERP_INTERFACE))) return rc;
         return step_f(c, L, forces);
@@ -639,14 +655,15 @@ static int advance_rec(agal_ctx *c, int L)
                 if ((rc = agal_launch_forces_cv(c, K, 0))) return rc;
         if ((rc = interp_beside_step(c, L, false))) return rc;
         if ((rc = advance_rec(c, L + 1))) return rc;
-        if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
+        if ((rc = average_rec(c, L, avg_mode(c)))) return rc;
         if (cv) {
             // the control volume sees every level consistent: grid average,
             // interface interpolation, then the post-step pass
             for (int K = ML - 2; K >= c->L0; K--)
-                if ((rc = agal_launch_average(c, K, AGAL_AVERAGE_GRID))) return rc;
+                if ((rc = average_rec(c, K, AGAL_AVERAGE_GRID))) return rc;
             for (int K = c->L0; K < ML - 1; K++)
-                if ((rc = agal_launch_interp(c, K, AGAL_INTERP_INTERFACE))) return rc;
+                if ((rc = agal_les_refresh(c, K)) || (rc = agal_launch_interp(c, K, AGAL_INTERP_INTERFACE)))
+                    return rc;
             for (int K = c->L0; K < ML; K++)
                 if ((rc = agal_launch_forces_cv(c, K, 1))) return rc;
         }
@@ -662,7 +679,7 @@ static int advance_rec(agal_ctx *c, int L)
     const bool f2 = mea && L == ML - 1 && c->liter == (1 << (ML - 1)) - 1;
     if (L < ML - 1) {                                                                       // :106-111
         if ((rc = advance_rec(c, L + 1))) return rc;
-        if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
+        if ((rc = average_rec(c, L, avg_mode(c)))) return rc;
         if ((rc = interp_beside_step(c, L, f2))) return rc;
     } else if ((rc = step_f(c, L, f2))) {
         return rc;
@@ -670,7 +687,7 @@ static int advance_rec(agal_ctx *c, int L)
     if (L == ML - 1) c->liter++;
     if (L < ML - 1) {                                                                       // :130-134
         if ((rc = advance_rec(c, L + 1))) return rc;
-        if ((rc = agal_launch_average(c, L, avg_mode(c)))) return rc;
+        if ((rc = average_rec(c, L, avg_mode(c)))) return rc;
     }
     return AGAL_OK;
 }
@@ -720,6 +737,9 @@ int agal_record_coarse_step(agal_ctx *c)
     return agal_sr_tick(c);
 }
 
+// Capture `steps` coarse steps into *out: an existing executable is updated
+// in place when the new graph has its topology (the usual case after a regrid:
+// the same launches with new sizes and arguments), else replaced.
 static int capture(agal_ctx *c, int steps, cudaGraphExec_t *out)
 {
     std::vector<int> cur0 = c->cur;
@@ -731,9 +751,29 @@ static int capture(agal_ctx *c, int steps, cudaGraphExec_t *out)
     c->cur = cur0;   // the capture only recorded the launches
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaStreamEndCapture");
+    if (*out) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(*out, g, &info) == cudaSuccess) {
+            cudaGraphDestroy(g);
+            c->graph_updates++;
+            return AGAL_OK;
+        }
+        cudaGetLastError();   // topology changed: rebuild
+        cudaGraphExecDestroy(*out);
+        *out = nullptr;
+    }
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return agal_cuda_check(c, e, "cudaGraphInstantiate");
+    c->graph_builds++;
+    return AGAL_OK;
+}
+
+extern "C" int agal_graph_stats(const agal_ctx *c, long long *builds, long long *updates)
+{
+    if (!c || !builds || !updates) return AGAL_ERR_PARAM;
+    *builds = c->graph_builds;
+    *updates = c->graph_updates;
     return AGAL_OK;
 }
 
@@ -767,7 +807,6 @@ extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
                 if ((rc = agal_record_coarse_step(c))) return rc;
         } else if (n > 0) {
             if (!c->graph_exec || c->graph_steps != n || c->graph_cur_in != c->cur) {
-                if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
                 if ((rc = capture(c, n, &c->graph_exec))) return rc;
                 c->graph_steps = n;
                 c->graph_cur_in = c->cur;
@@ -786,8 +825,8 @@ extern "C" int agal_advance_n(agal_ctx *c, int n, int use_graph)
                     : (c->ml_graph[1] && c->ml_graph_cur[1] == c->cur) ? 1
                                                                        : -1;
             if (k < 0) {
-                k = c->ml_graph[0] ? 1 : 0;
-                if (c->ml_graph[k]) { cudaGraphExecDestroy(c->ml_graph[k]); c->ml_graph[k] = nullptr; }
+                // a slot whose mesh changed (its executable is updated), else slot 1
+                k = c->ml_graph_cur[0].empty() ? 0 : 1;
                 if ((rc = capture(c, 1, &c->ml_graph[k]))) return rc;
                 c->ml_graph_cur[k] = c->cur;
             }
@@ -824,6 +863,10 @@ extern "C" int agal_array_bytes(const agal_ctx *c, int which, size_t *bytes)
     case AGAL_ARR_CBLOCK_ID_ONB_SOLID:
         if (!c->onb_solid) return AGAL_ERR_PARAM;
         *bytes = sizeof(int) * nmb;
+        break;
+    case AGAL_ARR_NU_SGS:
+        if (!c->nu_sgs) return AGAL_ERR_PARAM;
+        *bytes = sizeof(double) * nmc;
         break;
     case AGAL_ARR_CELLS_F_X_B:
         if (!c->X_b) return AGAL_ERR_PARAM;
@@ -884,14 +927,16 @@ extern "C" int agal_dump(agal_ctx *c, int which, void *host_buf, size_t bytes)
     if (rc) return rc;
     if (!host_buf || bytes != need) return agal_set_err(c, AGAL_ERR_PARAM, "dump size mismatch");
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (which == AGAL_ARR_CBLOCK_F_FF) {
+    if (which == AGAL_ARR_CBLOCK_F_FF || which == AGAL_ARR_NU_SGS) {
+        // compute-type arrays, widened to FP64
         double *o = static_cast<double *>(host_buf);
-        const size_t n = 6 * (size_t)c->nmb;
+        const void *src = which == AGAL_ARR_NU_SGS ? c->nu_sgs : c->Ff;
+        const size_t n = need / sizeof(double);
         if (c->storage == AGAL_STORE_FP64) {
-            AGAL_CUDA(c, cudaMemcpy(o, c->Ff, n * 8, cudaMemcpyDeviceToHost));
+            AGAL_CUDA(c, cudaMemcpy(o, src, n * 8, cudaMemcpyDeviceToHost));
         } else {
             std::vector<float> t(n);
-            AGAL_CUDA(c, cudaMemcpy(t.data(), c->Ff, n * 4, cudaMemcpyDeviceToHost));
+            AGAL_CUDA(c, cudaMemcpy(t.data(), src, n * 4, cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < n; i++) o[i] = t[i];
         }
         return AGAL_OK;
@@ -930,6 +975,7 @@ extern "C" int agal_load(agal_ctx *c, int which, const void *host_buf, size_t by
     }
     if (which == AGAL_ARR_MACROS) return agal_set_err(c, AGAL_ERR_PARAM, "macros are derived, not loaded");
     if (which == AGAL_ARR_CBLOCK_F_FF) return agal_set_err(c, AGAL_ERR_PARAM, "force partials are derived, not loaded");
+    if (which == AGAL_ARR_NU_SGS) return agal_set_err(c, AGAL_ERR_PARAM, "eddy viscosity is derived, not loaded");
     AGAL_CUDA(c, cudaMemcpy(int_array(c, which), host_buf, need, cudaMemcpyHostToDevice));
     if (which == AGAL_ARR_CELLS_ID_MASK) {
         // Geometry present when any cell is solid.

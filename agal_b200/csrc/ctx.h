@@ -77,6 +77,7 @@ struct agal_ctx {
     std::vector<int> ml_graph_cur[2];
     int graph_steps = 0;
     std::vector<int> graph_cur_in;     // cur[] the graph was captured with
+    long long graph_builds = 0, graph_updates = 0;   // instantiations / in-place updates
     int liter = 0;                     // global_Liter (solver_lbm_advance.cu:6)
     int step_cpt = 1;                  // step kernel variant, 1..AGAL_STEP_VARIANTS (autotuned)
     int *d_status = nullptr;           // device status word: AGAL_ERR_TIMEOUT from bounded waits
@@ -169,6 +170,16 @@ int agal_build_meta(agal_ctx *c);   // after any change of the block arrays
 int agal_build_tiles(agal_ctx *c);  // root-level tile table (agal_build_meta calls it)
 int agal_count_ptiles(const agal_ctx *c);   // root-level push tiles, 0 if not available
 int agal_launch_refresh(agal_ctx *c, int L);
+
+// Multi-level LES: the eddy viscosity reads the macro rows as the reference
+// leaves them -- refreshed by every interpolation (level L) and averaging
+// (level L+1) and by the initial condition, rewritten by every collide from
+// its pre-collision populations -- instead of the current populations
+// (S_Collide refreshes first only when MAX_LEVELS is 1,
+// solver_lbm_kernels.cu:467-471).
+inline bool agal_les_macros(const agal_ctx *c) { return c->nu_sgs && c->max_levels > 1; }
+// The refresh a transfer performs first (level L), in that mode only.
+int agal_les_refresh(agal_ctx *c, int L);
 int agal_launch_mass(agal_ctx *c, double *out);
 // Enqueue the FP64 sums and their copy into host memory (pinned for a truly
 // asynchronous copy); the values are valid once the stream has reached it.
@@ -187,7 +198,11 @@ int agal_freeze_refined(agal_ctx *c, int thaw = 0);
 int agal_build_iface_lists(agal_ctx *c);    // after any mesh change (multi-level cases)
 size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
 #define AGAL_AMR_SMALL 128
-void agal_drop_graphs(agal_ctx *c);         // after any change of the mesh or launch shapes
+// After any change of the mesh or launch shapes: the captured graphs no
+// longer match; their executables are kept and updated in place from the next
+// capture (cudaGraphExecUpdate, same topology), else rebuilt.
+void agal_drop_graphs(agal_ctx *c);
+void agal_free_graphs(agal_ctx *c);          // destroys them (context release)
 // One coarse step's launches on the context's stream (flips cur[] as it
 // records), and the buffer-parity bookkeeping of replaying `steps` of them.
 int agal_record_coarse_step(agal_ctx *c);

@@ -87,6 +87,13 @@ struct StepArgs {
     // (Cu_CollideLES, solver_lbm_kernels.cu:352-355).  Null otherwise.
     const void *nu_sgs;
     double nu, dxL;
+    // Multi-level LES: the macro rows rho, u, v(, w) [dim+1][nmc] that the
+    // collide rewrites from the pre-collision populations of every cell of
+    // the blocks it steps, solid cells included (Cu_CollideLES,
+    // solver_lbm_kernels.cu:337-350); the level's next eddy viscosity reads
+    // them.  Null otherwise.
+    void *macro;
+    long long nmc;
     // Stochastic rounding of half-precision offsets (agal_params
     // half_rounding): on when sr is set.  The launch seed mixes the coarse-step
     // counter in device memory (advanced once per coarse step, so replayed
@@ -222,6 +229,22 @@ __device__ __forceinline__ C cdot(int p, C ux, C uy, C uz)
 // the even part of the equilibrium, feq_{p,pb} = w rho (1 + 4.5 cu^2 -
 // 1.5 u^2) +- 3 w rho cu, so each pair is evaluated once
 // (Cu_Collide, kernels.cu:249-286).  Returns the macros for the boundary hook.
+// Macro rows of one cell from its populations (offset form when OFF), as
+// Cu_CollideLES stores them before relaxing: rho, then u = j / rho.
+template <int DIM, int Q, typename C, bool OFF>
+__device__ __forceinline__ void store_macros(const C (&g)[Q], void *macro, long long nmc, long long cell)
+{
+    C drho = C(0);
+#pragma unroll
+    for (int p = 0; p < Q; p++) drho = r_add(drho, g[p]);
+    const C rho = OFF ? r_add(C(1), drho) : drho;
+    C *m = static_cast<C *>(macro);
+    m[cell] = rho;
+    m[nmc + cell] = r_div(moment1<DIM, Q, 0>(g), rho);
+    m[2 * nmc + cell] = r_div(moment1<DIM, Q, 1>(g), rho);
+    if (DIM == 3) m[3 * nmc + cell] = r_div(moment1<DIM, Q, 2>(g), rho);
+}
+
 template <int DIM, int Q, typename C, bool OFF>
 __device__ __forceinline__ void bgk_collide(C (&g)[Q], C omeg, C &ux, C &uy, C &uz)
 {

@@ -94,12 +94,14 @@ __device__ __forceinline__ void step_body(const StepArgs &a, int cta, int (*s_me
             continue;
         }
         if (SOLID && __ldg(&a.cmask[(long long)b[h] * MC + t]) == CELL_SOLID) {
+            if (a.macro) store_macros<DIM, Q, C, ST<T>::OFF>(g[h], a.macro, a.nmc, (long long)b[h] * MC + t);
             carry();
             continue;
         }
         const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
         C ux, uy, uz;
         if (a.nu_sgs) {
+            if (a.macro) store_macros<DIM, Q, C, ST<T>::OFF>(g[h], a.macro, a.nmc, (long long)b[h] * MC + t);
             const C nus = static_cast<const C *>(a.nu_sgs)[(long long)b[h] * MC + t];
             const C dx = C(a.dxL);
             const C tau = r_fma(C(3), r_add(C(a.nu), nus), r_mul(C(0.5), dx));
@@ -326,6 +328,8 @@ struct EddyArgs {
     void *nu_sgs;
     double dx;
     int model;
+    const void *macro;   // multi-level: velocity from the macro rows [dim+1][nmc] instead of f
+    long long nmc;
 };
 
 template <int DIM, int Q, typename T>
@@ -342,16 +346,22 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_eddy(const EddyArgs a)
     const int t = threadIdx.x;
     const int I = t & 3, J = (t >> 2) & 3, K = (DIM == 3) ? (t >> 4) : 0;
     auto at = [&](int i, int j, int k) { return (i + 1) + H * (j + 1) + (DIM == 3 ? H * H * (k + 1) : 0); };
-    const T *f = static_cast<const T *>(a.f) + (long long)b * BLK + t;
-    C rho = 0, m[3] = {0, 0, 0};
+    if (a.macro) {
+        // solver_lbm_kernels_les.cu:502-507: the macro rows as they stand
+        const C *mr = static_cast<const C *>(a.macro) + (long long)b * MC + t;
+        for (int d = 0; d < 3; d++) s[d][at(I, J, K)] = d < DIM ? mr[(d + 1) * a.nmc] : C(0);
+    } else {
+        const T *f = static_cast<const T *>(a.f) + (long long)b * BLK + t;
+        C rho = 0, m[3] = {0, 0, 0};
 #pragma unroll
-    for (int p = 0; p < Q; p++) {
-        const C fp = ST<T>::dec(f[lat_pb(DIM, p) * MC]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
-        rho += fp;
+        for (int p = 0; p < Q; p++) {
+            const C fp = ST<T>::dec(f[lat_pb(DIM, p) * MC]) + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
+            rho += fp;
 #pragma unroll
-        for (int d = 0; d < DIM; d++) m[d] += C(lat_c(DIM, d, p)) * fp;
+            for (int d = 0; d < DIM; d++) m[d] += C(lat_c(DIM, d, p)) * fp;
+        }
+        for (int d = 0; d < 3; d++) s[d][at(I, J, K)] = d < DIM ? m[d] / rho : C(0);
     }
-    for (int d = 0; d < 3; d++) s[d][at(I, J, K)] = d < DIM ? m[d] / rho : C(0);
     __syncthreads();
     auto ext = [](C d1, C d2, C d3, C d4) {
         return r_add(r_add(r_add(r_mul(C(4), d1), r_mul(C(-6), d2)), r_mul(C(4), d3)), -d4);
@@ -653,6 +663,8 @@ template <int DIM, int Q, typename T> struct RunStep {
         const bool fused = cpt != 3 && !tile && !wall && n <= AGAL_FUSED_FIXUP_BLOCKS;
         a.fix_ticket = fused ? c->fix_count + 1 : nullptr;
         a.nu_sgs = c->nu_sgs;
+        a.macro = agal_les_macros(c) ? c->macro : nullptr;
+        a.nmc = c->nmc;
         a.sr = (c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
                c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
         a.sr_ctr = c->d_sr;
@@ -674,7 +686,8 @@ template <int DIM, int Q, typename T> struct RunStep {
             // and row-mapped variants have no per-cell relaxation rate, so
             // LES steps one cell per thread.
             if (cpt >= 3) cpt = 1;
-            EddyArgs e{a.ids, n, c->cblock_ID_nbr_child, c->cblock_ID_mask, a.fin, c->nu_sgs, a.dxL, c->P.S_LES};
+            EddyArgs e{a.ids, n, c->cblock_ID_nbr_child, c->cblock_ID_mask, a.fin, c->nu_sgs, a.dxL, c->P.S_LES,
+                       a.macro, c->nmc};
             k_eddy<DIM, Q, T><<<n, Geo<DIM>::MC, 0, c->stream>>>(e);
             AGAL_CUDA(c, cudaGetLastError());
         }
@@ -950,7 +963,16 @@ int agal_build_meta(agal_ctx *c)
     if (c->onb_solid) return agal_build_wall_lists(c);
     return AGAL_OK;
 }
-int agal_launch_set_ic(agal_ctx *c, int L) { return agal::dispatch<agal::RunIc>(c, L); }
+int agal_launch_set_ic(agal_ctx *c, int L)
+{
+    // Cu_SetInitialConditions also writes the level's macro rows
+    // (solver_lbm_kernels.cu:70-74); in LES macro mode they are refreshed from
+    // the new populations.
+    const int rc = agal::dispatch<agal::RunIc>(c, L);
+    return rc ? rc : agal_les_refresh(c, L);
+}
+
+int agal_les_refresh(agal_ctx *c, int L) { return agal_les_macros(c) ? agal_launch_refresh(c, L) : AGAL_OK; }
 int agal_launch_refresh(agal_ctx *c, int L) { return agal::dispatch<agal::RunRefresh>(c, L); }
 int agal_launch_mass_async(agal_ctx *c, double *host_out) { return agal::dispatch<agal::RunMass>(c, host_out); }
 int agal_launch_mass(agal_ctx *c, double *out)

@@ -104,6 +104,7 @@ extern "C" {
 #define AGAL_ARR_CBLOCK_ID_ONB_SOLID 12 /* int32 [n_maxcblocks] wall-block slot, -1 = none  mesh.h:515      */
 #define AGAL_ARR_CELLS_F_X_B   13  /* float32 [N_Q_max][n_maxcells_b] link lengths, -1 = none   mesh.h:491   */
 #define AGAL_ARR_CBLOCK_F_FF   14  /* float64 [6][n_maxcblocks] MEA force partials per block   mesh.h:518    */
+#define AGAL_ARR_NU_SGS        15  /* float64 [n_maxcells] LES eddy viscosity (S_LES > 0), field row N_Q+4 */
 
 /* ---- parameters: every input.txt key of inc/parser.h:62-144 ------------- */
 typedef struct agal_params {
@@ -247,6 +248,10 @@ int agal_refine_near_wall(agal_ctx *ctx);
    coarsened by the last refine/coarsen pass (mesh_amr.cu:2714-2744 prints
    them).  Pointers may be NULL. */
 int agal_refine_stats(const agal_ctx *ctx, long long *iter, int *n_refined, int *n_coarsened);
+/* CUDA graphs of agal_advance_n built (instantiated) and updated in place
+   (after a regrid the captured step usually keeps its topology and only its
+   launch sizes and arguments change).  No reference counterpart. */
+int agal_graph_stats(const agal_ctx *ctx, long long *builds, long long *updates);
 
 /* ---- Geometry (3D velocity sets) -------------------------------------------
    agal_set_geometry: faces = n_faces x 9 floats (v1x v1y v1z v2x v2y v2z v3x

@@ -379,7 +379,9 @@ int orc_refine_coarsen(orc_case *c)
         nR += (ref[b] == ORC_REF_MARK_REFINE);
         nC += (ref[b] == ORC_REF_MARK_COARSEN);
     }
-    int idm_wnew = idm + NCH * nR;
+    /* :2186, :2341; the sum can pass n_maxcblocks on a nearly full pool
+       although every ID lies below it: the passes stop at n_maxcblocks. */
+    int idm_wnew = (int)(((int64_t)idm + (int64_t)NCH * nR) < nmb ? idm + NCH * nR : nmb);
     int proceed_ref = nR > 0 && NCH * nR <= c->n_gaps;
     int proceed_coarse = nC > 0;
     if (!proceed_ref && nR > 0) {                                   /* :2197-2205 */
@@ -406,7 +408,7 @@ int orc_refine_coarsen(orc_case *c)
         for (int k = 0; k < NCH * nR; k++) rev[k] = c->gap_set[c->n_gaps - 1 - k];
         int mx = rev[0];
         for (int k = 1; k < NCH * nR; k++) mx = rev[k] > mx ? rev[k] : mx;
-        if (mx + 1 > idm_wnew) idm_wnew = mx + 1;
+        if (mx + 1 > idm_wnew) idm_wnew = (mx + 1 < nmb) ? mx + 1 : (int)nmb;
         int i = 0;
         for (int b = 0; b < idm; b++)
             if (ref[b] == ORC_REF_MARK_REFINE) c->first_child[b] = rev[NCH * (i++)];

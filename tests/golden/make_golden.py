@@ -78,6 +78,14 @@ AMR_CASES = {
                             200, 4096, 1),
     "amr_d3q19_box2": ("ref_d3q19_ldc", dict(AMR, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2), 60, 4096, 2),
     "amr_d3q27_sol2": ("ref_d3q27_ldc", dict(AMR, Nx=16, v0=2.5e-5, MAX_LEVELS_INTERIOR=2, P_REFINE=8), 48, 4096, 0),
+    # Multi-level LES: the eddy viscosity reads the macro rows as the
+    # transfers and collides leave them; the field's rows Q..Q+dim hold the
+    # last macros, row Q+4 the last eddy viscosity.
+    "les_d2q9_wall2_smag_lin": ("ref_d2q9_ldc_smag_lin", dict(AMR, Nx=64, v0=2.5e-5, MAX_LEVELS_WALL=2), 400, 4096,
+                                1),
+    "les_d3q19_box2_wale": ("ref_d3q19_ldc_wale", dict(AMR, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2), 100, 4096, 2),
+    "les_d2q9_sol2_vreman_lin": ("ref_d2q9_ldc_vreman_lin", dict(AMR, Nx=64, v0=5e-5, MAX_LEVELS_INTERIOR=2),
+                                 160, 4096, 0),
 }
 
 # Regrid pairs: the reference state just before the refinement of the last
@@ -172,7 +180,8 @@ def cmd_tables(ref: Path) -> None:
 
 # ---------------------------------------------------------------------------
 LES_BINARIES = ("ref_d3q19_ldc_smag", "ref_d3q19_ldc_wale", "ref_d3q19_ldc_vreman",
-                "ref_d2q9_ldc_smag", "ref_d2q9_ldc_wale", "ref_d2q9_ldc_vreman")
+                "ref_d2q9_ldc_smag", "ref_d2q9_ldc_wale", "ref_d2q9_ldc_vreman", "ref_d2q9_ldc_smag_lin",
+                "ref_d2q9_ldc_vreman_lin")
 
 
 def read_dump(path: Path, les: bool = False) -> dict:

@@ -137,7 +137,8 @@ def test_transfers_fp64_match_oracle():
 @pytest.mark.parametrize("storage", [_lib.STORE_FP32, _lib.STORE_FP16])
 def test_graph_replay_matches_eager(storage):
     """Captured coarse steps (two parities cached) give the same bits as eager
-    launches, across refinement passes."""
+    launches, across refinement passes; after a regrid the captured step is
+    updated in place rather than instantiated again."""
     p = amr_params(9, 32, storage=storage)
     res = []
     for graph in (False, True):
@@ -147,6 +148,10 @@ def test_graph_replay_matches_eager(storage):
             c.advance_n(40, use_graph=graph)
             c.sync()
             res.append((c.dump(_lib.ARR_F), c.dump(_lib.ARR_ID_SET), c.counts()))
+            if graph:
+                gs = c.graph_stats()
+                print(gs)
+                assert gs["updates"] >= 1 and gs["builds"] >= 1, gs
     assert res[0][2] == res[1][2]
     assert (res[0][1] == res[1][1]).all()
     assert (res[0][0] == res[1][0]).all()
@@ -199,15 +204,18 @@ def test_cuda_regrid_vs_reference_build(name):
 ALL_ARRAYS = INT_ARRAYS + (_lib.ARR_ID_SET, _lib.ARR_GAP_SET, _lib.ARR_F)
 
 
-@pytest.mark.parametrize("Q,N,storage", [(9, 32, _lib.STORE_FP32), (9, 32, _lib.STORE_FP64),
-                                         (19, 16, _lib.STORE_FP32), (27, 16, _lib.STORE_FP64)])
-def test_percentile_marks_bit_exact_on_identical_inputs(Q, N, storage):
+@pytest.mark.parametrize("Q,N,storage,ml", [(9, 32, _lib.STORE_FP32, 3), (9, 32, _lib.STORE_FP64, 3),
+                                            (19, 16, _lib.STORE_FP32, 3), (27, 16, _lib.STORE_FP64, 3),
+                                            (9, 1032, _lib.STORE_FP32, 2)])
+def test_percentile_marks_bit_exact_on_identical_inputs(Q, N, storage, ml):
     """The percentile criterion (block vorticity maxima, exact device
     quantile selection, marks) on the CUDA library and on the oracle, given
-    the same populations and mesh: identical marks."""
+    the same populations and mesh: identical marks.  The 1032^2 case holds
+    more than 65,536 blocks, so its quantiles come from the multi-CTA passes
+    instead of the one-CTA selection."""
     from oracle.orc import OracleCase
     p = amr_params(Q, N, storage=storage, S_CRITERION=_lib.CRITERION_PERCENTILE, P_REFINE=8,
-                   MAX_LEVELS_INTERIOR=3, v0=5e-4)
+                   MAX_LEVELS_INTERIOR=ml, v0=5e-4)
     with ag.Case(p) as c:
         run_like_reference(c, p, 12)   # one regrid done, the hierarchy still growing
         c.sync()
@@ -240,6 +248,39 @@ def test_percentile_refinement_fp64_matches_oracle(Q, N, steps):
     with ag.Case(p) as c:
         run_like_reference(c, p, steps)
         c.sync()
+        compare_states(c, o, p, 1e-11)
+
+
+def test_nearly_full_pool_matches_oracle():
+    """A block pool of 175 on a 64-block root grid with three levels: at some
+    regrid the blocks marked for refinement fit the gap stack although
+    id_max + 4 x marks passes the pool size (mesh_amr.cu:2186).  Every pass
+    stops at the pool size; mesh bit-exact, populations within 1e-11 of the
+    FP64 oracle through the regrids that follow."""
+    from oracle.orc import OracleCase
+    nmb, P = 175, 8
+    p = amr_params(9, 32, n_maxcblocks=nmb, P_REFINE=10 ** 8, S_CRITERION=_lib.CRITERION_PERCENTILE,
+                   ref_pct_hi=0.8, ref_pct_lo=0.5, v0=5e-4)
+    o = OracleCase(p, nmb, fp64=True)
+    hit = False
+    with ag.Case(p) as c:
+        for case in (c, o):
+            case.set_ic(0)
+        for _ in range(16):
+            for case in (c, o):
+                case.advance_n(P)
+                for L in (1, 0):
+                    case.average(L, _lib.AVERAGE_GRID)
+                for L in (0, 1):
+                    case.interpolate(L, _lib.INTERP_INTERFACE)
+                case.ref_criteria()
+            cnt = o.counts()
+            n_r = int((o.dump(_lib.ARR_CBLOCK_ID_REF) == 4).sum())
+            hit |= 0 < 4 * n_r <= cnt["n_gaps"] and cnt["id_max"][3] + 4 * n_r > nmb
+            for case in (c, o):
+                case.refine_coarsen()
+        c.sync()
+        assert hit
         compare_states(c, o, p, 1e-11)
 
 

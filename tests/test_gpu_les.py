@@ -5,7 +5,9 @@ solver_lbm_kernels_les.cu:460-600, solver_lbm_kernels.cu:293-380).
 
 The velocity field after 200 steps must agree with the reference's within
 the FP32 floor of two implementations that round differently, and lie far
-closer to it than the same run without the model does."""
+closer to it than the same run without the model does.  Multi-level meshes
+(static near-wall and box hierarchies, solution refinement) are held to the
+same bar, and their macro rows and eddy viscosity to the reference's."""
 import numpy as np
 import pytest
 
@@ -78,13 +80,95 @@ def test_les_outside_its_scope_is_refused():
     g = np.load(GOLDEN / "les_d3q19_ldc16_smag.npz")
     p, _ = params_for_golden(g)
     p.S_LES = 1
-    p.MAX_LEVELS_INTERIOR = 2
+    p.S_BC_TYPE = 1          # interpolated bounce-back
     with pytest.raises(ag.AgalError):
         ag.Case(p)
-    p.MAX_LEVELS_INTERIOR = 1
+    p.S_BC_TYPE = 0
     p.S_LES = 4
     with pytest.raises(ag.AgalError):
         ag.Case(p)
+
+
+# Multi-level LES against the reference's multi-level LES builds: a static
+# two-level hierarchy near the walls (2D, Smagorinsky), a two-level box (3D,
+# WALE) and solution refinement every 16 steps (2D, Vreman); linear
+# interpolation throughout.
+ML_LES_CASES = {"les_d2q9_wall2_smag_lin": 1, "les_d3q19_box2_wale": 2, "les_d2q9_sol2_vreman_lin": 3}
+
+
+def run_ml(g, model, storage=None, use_graph=True):
+    """The reference driver's sequence (IC, near-wall refinement, the loop)
+    with the LES model; populations, macro rows and eddy viscosity of the
+    fixture's blocks, and the mesh counts."""
+    p, steps = params_for_golden(g)
+    p.S_LES = model
+    if storage is not None:
+        p.storage = storage
+    Q, MC, dim = int(g["Q"]), int(g["MC"]), int(g["dim"])
+    blocks = g["blocks"].astype(np.int64)
+    with ag.Case(p) as c:
+        c.set_ic(0)
+        c.refine_near_wall()
+        c.advance_n(steps, use_graph=use_graph)
+        c.sync()
+        nmb = p.n_maxcblocks
+        cnt = c.counts()
+        ids = c.dump(_lib.ARR_ID_SET).reshape(-1, nmb)
+        active = np.sort(np.concatenate([ids[L, : cnt["n_ids"][L]] for L in range(cnt["max_levels"])]))
+        out = dict(counts=cnt, active=active,
+                   F=c.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks, :].reshape(Q, -1),
+                   M=c.dump(_lib.ARR_MACROS).reshape(dim + 1, nmb, MC)[:, blocks, :].reshape(dim + 1, -1))
+        if model:
+            out["nu"] = c.dump(_lib.ARR_NU_SGS).reshape(nmb, MC)[blocks].reshape(-1)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,model", sorted(ML_LES_CASES.items()))
+def test_multilevel_les_matches_the_reference_build(name, model):
+    """Same mesh as the reference build; FP32 velocity within max(TOL_U, 3 x
+    this library's FP32-vs-FP64 distance) of the reference's; the macro rows
+    the next eddy viscosity would read (stale by the sub-steps since their
+    last refresh or collide) match the reference's rows better than the
+    current velocity does; the eddy viscosity row within max(1e-3, 10 x its
+    own FP32-vs-FP64 distance)."""
+    g = fixture(name)
+    Q, dim = int(g["Q"]), int(g["dim"])
+    ref = run_ml(g, model)
+    assert list(ref["counts"]["n_ids"][: int(g["max_levels"])]) == [int(x) for x in g["n_ids"]][: int(g["max_levels"])]
+    assert np.array_equal(ref["active"], np.sort(g["blocks"].astype(np.int64)))
+    Fr = np.transpose(g["F"][:, :Q, :], (1, 0, 2)).reshape(Q, -1)
+    Mr = np.transpose(g["F"][:, Q + 1:Q + 1 + dim, :], (1, 0, 2)).reshape(dim, -1).astype(np.float64)
+    nur = g["F"][:, Q + 4, :].reshape(-1).astype(np.float64)
+    _, u_r = macros(g, Fr)
+    _, u = macros(g, ref["F"])
+    r64 = run_ml(g, model, _lib.STORE_FP64)
+    _, u64 = macros(g, r64["F"])
+    _, u0 = macros(g, run_ml(g, 0)["F"])
+    e, e0, floor = rel_l2(u, u_r), rel_l2(u0, u_r), rel_l2(u, u64)
+    tol = max(TOL_U, 3 * floor)
+    e_m = rel_l2(ref["M"][1:], Mr)
+    e_fresh = rel_l2(u_r, Mr)           # the reference's current velocity against its own rows
+    e_nu, nu_floor = rel_l2(ref["nu"], nur), rel_l2(ref["nu"], r64["nu"])
+    print(f"{name}: u vs reference {e:.3e} (floor {floor:.3e}, no model {e0:.3e}); macro rows {e_m:.3e} "
+          f"(current velocity {e_fresh:.3e}); nu_SGS {e_nu:.3e} (floor {nu_floor:.3e})")
+    assert e < tol, (e, floor)
+    assert e_m < tol, (e_m, floor)
+    if e_fresh > 3 * tol:
+        assert e_m < e_fresh / 3, (e_m, e_fresh)
+    assert e_nu < max(1e-3, 10 * nu_floor), (e_nu, nu_floor)
+    assert e0 > 5 * e, (e, e0)
+
+
+@pytest.mark.gpu
+def test_multilevel_les_graph_replay_matches_eager():
+    """The refreshes precede the side-stream interpolation and the eddy
+    viscosity in the captured graph exactly as in eager launches."""
+    g = fixture("les_d2q9_sol2_vreman_lin")
+    a = run_ml(g, 3, use_graph=True)
+    b = run_ml(g, 3, use_graph=False)
+    for k in ("F", "M", "nu"):
+        assert np.array_equal(a[k], b[k]), k
 
 
 @pytest.mark.gpu

@@ -58,6 +58,13 @@ template <> struct Row4<float> {
     }
     __device__ static void store_pair(float *p, const P &x) { *reinterpret_cast<float2 *>(p) = x; }
     __device__ static void store_one(float *p, const V &v, int k) { *p = get(v, k); }
+    // Warp exchange of a row's edge cell: cell 3 (for the right neighbour's
+    // x-shift by +1) and cell 0 (for the left neighbour's shift by -1).
+    using E = float;
+    __device__ static E last(const V &v) { return v.w; }
+    __device__ static E first(const V &v) { return v.x; }
+    __device__ static V shift_in_left(const V &v, E l) { return make_float4(l, v.x, v.y, v.z); }
+    __device__ static V shift_in_right(const V &v, E r) { return make_float4(v.y, v.z, v.w, r); }
 };
 
 // Half-precision rows (weight offsets): four 16-bit values in a uint2.
@@ -107,6 +114,18 @@ template <typename T> struct Row4Half {
     }
     __device__ static void store_pair(T *p, const P &x) { *reinterpret_cast<unsigned *>(p) = x; }
     __device__ static void store_one(T *p, const V &v, int k) { *reinterpret_cast<unsigned short *>(p) = bits(v, k); }
+    // Exchanged words: the one holding cell 3 (high half) / cell 0 (low half).
+    using E = unsigned;
+    __device__ static E last(const V &v) { return v.y; }
+    __device__ static E first(const V &v) { return v.x; }
+    __device__ static V shift_in_left(const V &v, E l)
+    {
+        return make_uint2(__byte_perm(l, v.x, 0x5432), __byte_perm(v.x, v.y, 0x5432));
+    }
+    __device__ static V shift_in_right(const V &v, E r)
+    {
+        return make_uint2(__byte_perm(v.x, v.y, 0x5432), __byte_perm(v.y, r, 0x5432));
+    }
 };
 template <> struct Row4<__half> : Row4Half<__half> {};
 template <> struct Row4<__nv_bfloat16> : Row4Half<__nv_bfloat16> {};
@@ -198,6 +217,7 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
     const int *nrow = s_meta[lb];
     const int fl = nrow[Meta<DIM>::FLAGS];
     const bool run = b >= 0 && !(fl & META_WALL);
+    bool main = false;   // the row-wise path: collided here, streamed below
     if (run && !(fl & META_ACTIVE)) {
         // Inactive (refined solid) block: carried unchanged, as k_step does.
         if (SOLID) {
@@ -224,6 +244,7 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
             push_cell<DIM, Q, T, true>(g, ux, uy, uz, b, t, nrow, hook, fo, a, seed);
         }
     } else if (run) {
+        main = true;
         const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
         bool bad = false;
         // Collide the row two cells at a time; v[p] then holds the
@@ -267,43 +288,6 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
                 for (int p = 0; p < Q; p++) RW::set2(v[p], k, g0[p], g1[p]);
             }
         }
-        // Stream: direction p goes to row (J + c_y, K + c_z) of the block in
-        // that y/z neighbour slot, shifted by c_x; closed links bounce back
-        // into the cell's own slot p.
-#pragma unroll
-        for (int p = 0; p < Q; p++) {
-            const int cx = lat_c(DIM, 0, p), cy = lat_c(DIM, 1, p), cz = lat_c(DIM, 2, p);
-            const int q = lat_pb(DIM, p);
-            const int Jn = J + cy, Kn = K + cz;
-            const int syz = (Jn < 0 ? 0 : Jn > 3 ? 6 : 3) + (DIM == 3 ? (Kn < 0 ? 0 : Kn > 3 ? 18 : 9) : 0);
-            const int rn = (Jn & 3) + (DIM == 3 ? 4 * (Kn & 3) : 0);
-            const int Byz = nrow[syz + 1];
-            T *back = fo + own + p * MC;
-            T *dst = fo + (long long)Byz * BLK + q * MC + rn * 4;
-            if (cx == 0) {
-                RW::store(Byz >= 0 ? dst : back, v[p]);
-            } else if (cx > 0) {
-                const int Bx = nrow[syz + 2];
-                if (Byz >= 0) {
-                    RW::store_one(dst + 1, v[p], 0);
-                    RW::store_pair(dst + 2, RW::pair(v[p], 1));
-                } else {
-                    RW::store_pair(back, RW::pair(v[p], 0));
-                    RW::store_one(back + 2, v[p], 2);
-                }
-                RW::store_one(Bx >= 0 ? fo + (long long)Bx * BLK + q * MC + rn * 4 : back + 3, v[p], 3);
-            } else {
-                const int Bx = nrow[syz + 0];
-                if (Byz >= 0) {
-                    RW::store_pair(dst, RW::pair(v[p], 1));
-                    RW::store_one(dst + 2, v[p], 3);
-                } else {
-                    RW::store_one(back + 1, v[p], 1);
-                    RW::store_pair(back + 2, RW::pair(v[p], 2));
-                }
-                RW::store_one(Bx >= 0 ? fo + (long long)Bx * BLK + q * MC + rn * 4 + 3 : back, v[p], 0);
-            }
-        }
         if (bad) {
             // Rare: recompute the row's collisions from the input and record
             // the links the reference's guard refuses.
@@ -315,6 +299,85 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
                 C ux, uy, uz;
                 collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
                 guard_cell<DIM, Q, T>(g, b, r * 4 + k, nrow, a);
+            }
+        }
+    }
+
+    // Stream of the row-wise path (all lanes take part in the exchanges).
+    // Direction p goes to row (J + c_y, K + c_z) of the block in that y/z
+    // neighbour slot, shifted by c_x; closed links bounce back into the
+    // cell's own slot p.  For c_x = +1 the destination row's cell 0 comes
+    // from cell 3 of the left neighbour's row: when that row belongs to lane
+    // - R of this warp and lands in the same destination block, it is
+    // exchanged and the destination row is written whole (one aligned vector
+    // store, full sectors), and the neighbour leaves its cell 3 out; likewise
+    // for c_x = -1 with the right neighbour (lane + R).  Rows at the warp's
+    // edges, or next to a block on another path, keep the element-wise
+    // stores.  Every element is written once either way.
+    constexpr unsigned ALL = 0xffffffffu;
+    const int lane = tid & 31;
+    const bool has_l = lane >= R, has_r = lane + R < 32;
+    const int s0 = (DIM == 3) ? 12 : 3;   // slot of the (0, 0, 0) offset minus one: x - 1
+    const int left_b = __shfl_up_sync(ALL, b, R);
+    const bool left_main = __shfl_up_sync(ALL, main, R);
+    const bool left_ok = main && has_l && left_main && nrow[s0] == left_b && left_b >= 0;
+    // Every lane executes every exchange (never inside a short-circuit): a
+    // lane that skipped one would leave the rest of the warp waiting.
+    const bool right_left_ok = __shfl_down_sync(ALL, left_ok, R);
+    const bool right_ok = has_r && right_left_ok;
+#pragma unroll
+    for (int p = 0; p < Q; p++) {
+        const int cx = lat_c(DIM, 0, p), cy = lat_c(DIM, 1, p), cz = lat_c(DIM, 2, p);
+        const int q = lat_pb(DIM, p);
+        const int Jn = J + cy, Kn = K + cz;
+        const int syz = (Jn < 0 ? 0 : Jn > 3 ? 6 : 3) + (DIM == 3 ? (Kn < 0 ? 0 : Kn > 3 ? 18 : 9) : 0);
+        const int rn = (Jn & 3) + (DIM == 3 ? 4 * (Kn & 3) : 0);
+        const int Byz = nrow[syz + 1];
+        T *back = fo + own + p * MC;
+        T *dst = fo + (long long)Byz * BLK + q * MC + rn * 4;
+        if (cx == 0) {
+            if (main) RW::store(Byz >= 0 ? dst : back, v[p]);
+        } else if (cx > 0) {
+            const int Bx = nrow[syz + 2];
+            const typename RW::E lv = __shfl_up_sync(ALL, RW::last(v[p]), R);
+            const int lBx = __shfl_up_sync(ALL, Bx, R);
+            const bool full = left_ok && Byz >= 0 && lBx == Byz;
+            const bool r_full = __shfl_down_sync(ALL, full, R);
+            const bool given = has_r && r_full;   // cell 3 written by lane + R
+            if (main) {
+                if (Byz >= 0) {
+                    if (full) {
+                        RW::store(dst, RW::shift_in_left(v[p], lv));
+                    } else {
+                        RW::store_one(dst + 1, v[p], 0);
+                        RW::store_pair(dst + 2, RW::pair(v[p], 1));
+                    }
+                } else {
+                    RW::store_pair(back, RW::pair(v[p], 0));
+                    RW::store_one(back + 2, v[p], 2);
+                }
+                if (!given) RW::store_one(Bx >= 0 ? fo + (long long)Bx * BLK + q * MC + rn * 4 : back + 3, v[p], 3);
+            }
+        } else {
+            const int Bx = nrow[syz + 0];
+            const typename RW::E rv = __shfl_down_sync(ALL, RW::first(v[p]), R);
+            const int rBx = __shfl_down_sync(ALL, Bx, R);
+            const bool full = right_ok && Byz >= 0 && rBx == Byz;
+            const bool l_full = __shfl_up_sync(ALL, full, R);
+            const bool given = has_l && l_full;   // cell 0 written by lane - R
+            if (main) {
+                if (Byz >= 0) {
+                    if (full) {
+                        RW::store(dst, RW::shift_in_right(v[p], rv));
+                    } else {
+                        RW::store_pair(dst, RW::pair(v[p], 1));
+                        RW::store_one(dst + 2, v[p], 3);
+                    }
+                } else {
+                    RW::store_one(back + 1, v[p], 1);
+                    RW::store_pair(back + 2, RW::pair(v[p], 2));
+                }
+                if (!given) RW::store_one(Bx >= 0 ? fo + (long long)Bx * BLK + q * MC + rn * 4 + 3 : back, v[p], 0);
             }
         }
     }

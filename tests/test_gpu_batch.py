@@ -73,6 +73,46 @@ def test_batch_equals_cases_alone(use_graph, worklist):
     assert alone[0]["counts"]["n_ids"][1] > 0
 
 
+@pytest.mark.parametrize("worklist", [True, False])
+def test_learned_cases_in_a_batch_equal_alone(worklist):
+    """Cases driven by the learned predictor (look-ahead over 2 regrids, the
+    rule judging every other regrid), each with its own network of the same
+    weights, regrid inside a batch exactly as alone."""
+    spec = dict(case_specs()[0], P_REFINE=4)
+    specs = [dict(spec, v0=5e-4), dict(spec, v0=2.5e-4, Nx=48, n_maxcblocks=144 * 21 + 64)]
+    steps = 24
+
+    def learned(sp):
+        c = make(sp)
+        m = ag.Learner(2, seed=11)
+        m.set_horizon(2)
+        m.attach(c, 2, judge_every=2)
+        m.set_thresholds(0.5, 0.5)
+        return c, m
+
+    alone = []
+    for sp in specs:
+        c, m = learned(sp)
+        c.advance_n(steps)
+        c.sync()
+        alone.append(state(c))
+        c.close()
+        m.close()
+    pairs = [learned(sp) for sp in specs]
+    with ag.Batch([c for c, _ in pairs]) as b:
+        b.set_worklist(worklist)
+        b.advance_n(steps)
+        b.sync()
+    for i, (c, m) in enumerate(pairs):
+        s = state(c)
+        assert s["counts"] == alone[i]["counts"], i
+        for k in s:
+            if k != "counts":
+                assert np.array_equal(s[k], alone[i][k]), (i, k)
+        c.close()
+        m.close()
+
+
 def test_batch_rejects_duplicates():
     c = make(case_specs()[1])
     with pytest.raises(RuntimeError):

@@ -135,6 +135,10 @@ template <int DIM, int Q, typename T> struct RowCfg {
     static constexpr int NT = (DIM == 2) ? 256 : 128;
     static constexpr int R = (DIM == 2) ? 4 : 16;              // rows per cell-block
     static constexpr int NB = NT / R;                           // cell-blocks per CTA
+    // A warp holds the same XR rows of 32 / XR consecutive blocks (2D: all 4
+    // rows of 8 blocks; 3D: half of the 16 rows of 4 blocks), so that most
+    // x neighbours of a block sit in the same warp, XR lanes away.
+    static constexpr int XR = (DIM == 2) ? 4 : 8;
     static constexpr int words = Q * (sizeof(T) == 4 ? 4 : 2);  // registers of the row's populations
     static constexpr int MINB = (DIM == 2) ? (sizeof(T) == 4 ? 3 : 4) : (words <= 40 ? 4 : words <= 80 ? 2 : 1);
 };
@@ -194,7 +198,9 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
     constexpr int W = Meta<DIM>::W;
     __shared__ int s_meta[NB][W];
     const int tid = threadIdx.x;
-    const int lb = tid / R, r = tid % R;
+    constexpr int XR = RowCfg<DIM, Q, T>::XR, BPW = 32 / XR, SL = R / XR;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int lb = (warp / SL) * BPW + lane / XR, r = (warp % SL) * XR + lane % XR;
     const int J = r & 3, K = (DIM == 3) ? (r >> 2) : 0;
 
     // Block IDs and metadata rows are written only by mesh passes, so they are
@@ -308,22 +314,21 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
     // neighbour slot, shifted by c_x; closed links bounce back into the
     // cell's own slot p.  For c_x = +1 the destination row's cell 0 comes
     // from cell 3 of the left neighbour's row: when that row belongs to lane
-    // - R of this warp and lands in the same destination block, it is
+    // - XR of this warp and lands in the same destination block, it is
     // exchanged and the destination row is written whole (one aligned vector
     // store, full sectors), and the neighbour leaves its cell 3 out; likewise
-    // for c_x = -1 with the right neighbour (lane + R).  Rows at the warp's
+    // for c_x = -1 with the right neighbour (lane + XR).  Rows at the warp's
     // edges, or next to a block on another path, keep the element-wise
     // stores.  Every element is written once either way.
     constexpr unsigned ALL = 0xffffffffu;
-    const int lane = tid & 31;
-    const bool has_l = lane >= R, has_r = lane + R < 32;
+    const bool has_l = lane >= XR, has_r = lane + XR < 32;
     const int s0 = (DIM == 3) ? 12 : 3;   // slot of the (0, 0, 0) offset minus one: x - 1
-    const int left_b = __shfl_up_sync(ALL, b, R);
-    const bool left_main = __shfl_up_sync(ALL, main, R);
+    const int left_b = __shfl_up_sync(ALL, b, XR);
+    const bool left_main = __shfl_up_sync(ALL, main, XR);
     const bool left_ok = main && has_l && left_main && nrow[s0] == left_b && left_b >= 0;
     // Every lane executes every exchange (never inside a short-circuit): a
     // lane that skipped one would leave the rest of the warp waiting.
-    const bool right_left_ok = __shfl_down_sync(ALL, left_ok, R);
+    const bool right_left_ok = __shfl_down_sync(ALL, left_ok, XR);
     const bool right_ok = has_r && right_left_ok;
 #pragma unroll
     for (int p = 0; p < Q; p++) {
@@ -339,11 +344,11 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
             if (main) RW::store(Byz >= 0 ? dst : back, v[p]);
         } else if (cx > 0) {
             const int Bx = nrow[syz + 2];
-            const typename RW::E lv = __shfl_up_sync(ALL, RW::last(v[p]), R);
-            const int lBx = __shfl_up_sync(ALL, Bx, R);
+            const typename RW::E lv = __shfl_up_sync(ALL, RW::last(v[p]), XR);
+            const int lBx = __shfl_up_sync(ALL, Bx, XR);
             const bool full = left_ok && Byz >= 0 && lBx == Byz;
-            const bool r_full = __shfl_down_sync(ALL, full, R);
-            const bool given = has_r && r_full;   // cell 3 written by lane + R
+            const bool r_full = __shfl_down_sync(ALL, full, XR);
+            const bool given = has_r && r_full;   // cell 3 written by lane + XR
             if (main) {
                 if (Byz >= 0) {
                     if (full) {
@@ -360,11 +365,11 @@ __global__ void __launch_bounds__(RowCfg<DIM, Q, T>::NT, RowCfg<DIM, Q, T>::MINB
             }
         } else {
             const int Bx = nrow[syz + 0];
-            const typename RW::E rv = __shfl_down_sync(ALL, RW::first(v[p]), R);
-            const int rBx = __shfl_down_sync(ALL, Bx, R);
+            const typename RW::E rv = __shfl_down_sync(ALL, RW::first(v[p]), XR);
+            const int rBx = __shfl_down_sync(ALL, Bx, XR);
             const bool full = right_ok && Byz >= 0 && rBx == Byz;
-            const bool l_full = __shfl_up_sync(ALL, full, R);
-            const bool given = has_l && l_full;   // cell 0 written by lane - R
+            const bool l_full = __shfl_up_sync(ALL, full, XR);
+            const bool given = has_l && l_full;   // cell 0 written by lane - XR
             if (main) {
                 if (Byz >= 0) {
                     if (full) {

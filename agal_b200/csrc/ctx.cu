@@ -137,9 +137,9 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         delete c;
         return agal_set_err(nullptr, AGAL_ERR_PARAM, "half_rounding");
     }
-    if (p->S_LES > 0 && (p->collision != AGAL_BGK || p->S_BC_TYPE != 0)) {
+    if (p->S_LES > 0 && p->collision != AGAL_BGK) {
         delete c;
-        return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "S_LES: built for BGK without interpolated bounce-back");
+        return agal_set_err(nullptr, AGAL_ERR_UNSUPPORTED, "S_LES: built for BGK (Cu_CollideLES)");
     }
     c->Qmax = (c->dim == 2) ? 9 : 27;
     c->MC = (c->dim == 2) ? 16 : 64;

@@ -416,6 +416,24 @@ __device__ __forceinline__ void collide_cell(typename ST<T>::C (&g)[Q], const St
     bgk_collide<DIM, Q, C, ST<T>::OFF>(g, C(a.omega), ux, uy, uz);
 }
 
+// The collision of one cell of the pool (index cell = b * MC + t): with LES,
+// BGK at omega = dx / (3 (nu + nu_SGS) + dx / 2) from the cell's eddy
+// viscosity (Cu_CollideLES, solver_lbm_kernels.cu:352-355); else collide_cell.
+template <int DIM, int Q, typename T>
+__device__ __forceinline__ void collide_at(typename ST<T>::C (&g)[Q], const StepArgs &a, long long cell,
+                                           typename ST<T>::C &ux, typename ST<T>::C &uy, typename ST<T>::C &uz)
+{
+    using C = typename ST<T>::C;
+    if (a.nu_sgs) {
+        const C nus = static_cast<const C *>(a.nu_sgs)[cell];
+        const C dx = C(a.dxL);
+        const C tau = r_fma(C(3), r_add(C(a.nu), nus), r_mul(C(0.5), dx));
+        bgk_collide<DIM, Q, C, ST<T>::OFF>(g, r_div(dx, tau), ux, uy, uz);
+    } else {
+        collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+    }
+}
+
 // Stream one collided cell (cell t of block b, populations g) into the
 // output buffer: push along open links, bounce back along closed ones with
 // the boundary hook on domain boundaries (kernels.cu:534-633, 693-887).

@@ -100,15 +100,8 @@ __device__ __forceinline__ void step_body(const StepArgs &a, int cta, int (*s_me
         }
         const bool hook = (fl & META_ONB) && a.bc_preset != AGAL_BC_NONE;
         C ux, uy, uz;
-        if (a.nu_sgs) {
-            if (a.macro) store_macros<DIM, Q, C, ST<T>::OFF>(g[h], a.macro, a.nmc, (long long)b[h] * MC + t);
-            const C nus = static_cast<const C *>(a.nu_sgs)[(long long)b[h] * MC + t];
-            const C dx = C(a.dxL);
-            const C tau = r_fma(C(3), r_add(C(a.nu), nus), r_mul(C(0.5), dx));
-            bgk_collide<DIM, Q, C, ST<T>::OFF>(g[h], r_div(dx, tau), ux, uy, uz);
-        } else {
-            collide_cell<DIM, Q, T>(g[h], a, ux, uy, uz);
-        }
+        if (a.macro) store_macros<DIM, Q, C, ST<T>::OFF>(g[h], a.macro, a.nmc, (long long)b[h] * MC + t);
+        collide_at<DIM, Q, T>(g[h], a, (long long)b[h] * MC + t, ux, uy, uz);
         push_cell<DIM, Q, T, SOLID>(g[h], ux, uy, uz, b[h], t, nrow, hook, fo, a, seed);
     }
 }

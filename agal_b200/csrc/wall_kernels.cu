@@ -62,7 +62,7 @@ __device__ typename ST<T>::C post_collision(const StepArgs &a, int nb, int nc, i
 #pragma unroll
     for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[lat_pb(DIM, p) * MC]);
     C ux, uy, uz;
-    collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+    collide_at<DIM, Q, T>(g, a, (long long)nb * MC + nc, ux, uy, uz);
     return g[k] + (ST<T>::OFF ? C(lat_w(Q, k)) : C(0));
 }
 
@@ -107,7 +107,10 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_step_wall(const WallArgs w)
 #pragma unroll
     for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[lat_pb(DIM, p) * MC]);
     C ux = C(0), uy = C(0), uz = C(0);
-    if (!solid) collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+    // multi-level LES: the macro rows of every cell of the block, before the
+    // collision (Cu_CollideLES, solver_lbm_kernels.cu:337-350)
+    if (a.macro) store_macros<DIM, Q, C, ST<T>::OFF>(g, a.macro, a.nmc, (long long)b * MC + t);
+    if (!solid) collide_at<DIM, Q, T>(g, a, (long long)b * MC + t, ux, uy, uz);
 #pragma unroll
     for (int p = 0; p < Q; p++) sPost[p][t] = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
     __syncthreads();
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(Geo<DIM>::MC) k_forces(const ForceArgs fa)
 #pragma unroll
         for (int p = 0; p < Q; p++) g[p] = ST<T>::dec(fin[(long long)b * BLK + lat_pb(DIM, p) * MC + t]);
         C ux, uy, uz;
-        if (collide) collide_cell<DIM, Q, T>(g, a, ux, uy, uz);
+        if (collide) collide_at<DIM, Q, T>(g, a, (long long)b * MC + t, ux, uy, uz);
 #pragma unroll
         for (int p = 0; p < Q; p++) sPost[p][t] = g[p] + (ST<T>::OFF ? C(lat_w(Q, p)) : C(0));
         __syncthreads();
@@ -316,6 +319,14 @@ StepArgs base_args(agal_ctx *c, int L, const void *fin, void *fout)
            c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
     a.sr_ctr = c->d_sr;
     a.sr_salt = (unsigned)c->sr_salt;
+    // LES: the eddy viscosity of the level's step (the wall step and the
+    // force passes recompute the same collisions); the macro rows are written
+    // by the wall step only (set by its launcher)
+    a.nu_sgs = c->nu_sgs;
+    a.nu = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->P.v0 : c->P.v0;
+    a.dxL = (sizeof(typename ST<T>::C) == 4) ? (double)(float)c->dxf[L] : c->dxf[L];
+    a.macro = nullptr;
+    a.nmc = c->nmc;
     return a;
 }
 
@@ -329,6 +340,7 @@ template <int DIM, int Q, typename T> struct RunWallStep {
             if (n <= 0) return AGAL_OK;
             WallArgs w;
             w.s = base_args<DIM, Q, T>(c, L, fin, fout);
+            w.s.macro = agal_les_macros(c) ? c->macro : nullptr;
             w.wall = c->wall_ids + c->wall_off[L];
             w.onb_solid = c->onb_solid;
             w.Xb = c->X_b;

@@ -115,8 +115,8 @@ typedef struct agal_params {
     int G_LOADTYPE, G_PRINT, G_VIS_TREE, G_BIN_DENSITY, G_BIN_APPROACH, G_BIN_LEVELS, G_BIN_SPEC, G_BIN_MAKE_LINKS;
     /* SOLVER (integer keys) */
     /* S_LES: 0 none, 1 Smagorinsky, 2 WALE, 3 Vreman (inc/solver_lbm.h:31-37,
-       solver_lbm_kernels_les.cu); with BGK on one-level meshes without
-       interpolated bounce-back, else agal_create returns AGAL_ERR_UNSUPPORTED */
+       solver_lbm_kernels_les.cu); with BGK (one or several levels, walls
+       included), else agal_create returns AGAL_ERR_UNSUPPORTED */
     int S_COLLISION, S_INTERP, S_INTERP_HYBRID, S_AVERAGE, S_CRITERION, S_LES, S_FORCE_ORDER, S_FORCE_TYPE, S_BC_TYPE;
     /* REFINEMENT / PROBING / OUTPUT (integer keys) */
     int P_REFINE, N_PROBE, N_PROBE_DENSITY, N_PROBE_FREQUENCY, N_PROBE_FORCE, N_PROBE_F_START, N_PROBE_F_FREQUENCY;

@@ -127,6 +127,12 @@ GEOM_CASES = {
                                             S_FORCEVOLUME_XM=0.66, S_FORCEVOLUME_Ym=0.31, S_FORCEVOLUME_YM=0.69,
                                             S_FORCEVOLUME_Zm=0.3, S_FORCEVOLUME_ZM=0.7), 16, 4096,
                       (3, 0.07, (0.45, 0.5, 0.5), 7)),
+    # LES (Smagorinsky) with the interpolated bounce-back on a two-level mesh:
+    # the field carries the macro rows and the eddy viscosity row.
+    "geom_les_d3q19_wall2_smag": ("ref_d3q19_fps_smag", dict(GEO, Nx=16, v0=1.25e-4, MAX_LEVELS_WALL=2,
+                                                             MAX_LEVELS_INTERIOR=2, G_BIN_LEVELS=2, S_BC_TYPE=1,
+                                                             S_FORCE_ORDER=2), 40, 4096,
+                                  (3, 0.1, (0.46, 0.49, 0.51), 11)),
     "geom_d3q19_uniform": ("ref_d3q19_fps", dict(GEO, Nx=32, v0=1.25e-4, G_BIN_DENSITY=16, G_BIN_LEVELS=1,
                                                  MAX_LEVELS_WALL=1, MAX_LEVELS_INTERIOR=1, S_BC_TYPE=1,
                                                  S_FORCE_ORDER=2), 20, 4096, (3, 0.15, (0.47, 0.52, 0.49), 3)),
@@ -181,7 +187,7 @@ def cmd_tables(ref: Path) -> None:
 # ---------------------------------------------------------------------------
 LES_BINARIES = ("ref_d3q19_ldc_smag", "ref_d3q19_ldc_wale", "ref_d3q19_ldc_vreman",
                 "ref_d2q9_ldc_smag", "ref_d2q9_ldc_wale", "ref_d2q9_ldc_vreman", "ref_d2q9_ldc_smag_lin",
-                "ref_d2q9_ldc_vreman_lin")
+                "ref_d2q9_ldc_vreman_lin", "ref_d3q19_fps_smag")
 
 
 def read_dump(path: Path, les: bool = False) -> dict:

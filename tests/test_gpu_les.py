@@ -80,10 +80,11 @@ def test_les_outside_its_scope_is_refused():
     g = np.load(GOLDEN / "les_d3q19_ldc16_smag.npz")
     p, _ = params_for_golden(g)
     p.S_LES = 1
-    p.S_BC_TYPE = 1          # interpolated bounce-back
+    p.collision = _lib.MRT   # LES relaxes with BGK only
+    p.velocity_set = _lib.D3Q19
     with pytest.raises(ag.AgalError):
         ag.Case(p)
-    p.S_BC_TYPE = 0
+    p.collision = _lib.BGK
     p.S_LES = 4
     with pytest.raises(ag.AgalError):
         ag.Case(p)
@@ -157,6 +158,72 @@ def test_multilevel_les_matches_the_reference_build(name, model):
     if e_fresh > 3 * tol:
         assert e_m < e_fresh / 3, (e_m, e_fresh)
     assert e_nu < max(1e-3, 10 * nu_floor), (e_nu, nu_floor)
+    assert e0 > 5 * e, (e, e0)
+
+
+def run_geom(g, model, storage=None):
+    """The LES flow past the fixture's sphere (interpolated bounce-back, two
+    levels near the wall): populations, macro rows, eddy viscosity and MEA
+    partials of the fixture's blocks."""
+    from test_oracle_geometry import faces_of, geom_params
+    p, steps = geom_params(g)
+    p.S_LES = model
+    if storage is not None:
+        p.storage = storage
+    Q, MC, dim = int(g["Q"]), int(g["MC"]), int(g["dim"])
+    blocks = g["blocks"].astype(np.int64)
+    nmb = p.n_maxcblocks
+    with ag.Case(p) as c:
+        c.set_geometry(faces_of(g))
+        c.set_ic(0)
+        c.refine_near_wall()
+        c.advance_n(steps)
+        c.sync()
+        cnt = c.counts()
+        out = dict(counts=cnt, F=c.dump(_lib.ARR_F).reshape(Q, nmb, MC)[:, blocks, :].reshape(Q, -1),
+                   M=c.dump(_lib.ARR_MACROS).reshape(dim + 1, nmb, MC)[:, blocks, :].reshape(dim + 1, -1),
+                   Ff=c.dump(_lib.ARR_CBLOCK_F_FF).reshape(6, nmb)[:, blocks].T,
+                   cmask=c.dump(_lib.ARR_CELLS_ID_MASK).reshape(nmb, MC)[blocks])
+        if model:
+            out["nu"] = c.dump(_lib.ARR_NU_SGS).reshape(nmb, MC)[blocks].reshape(-1)
+    return out
+
+
+@pytest.mark.gpu
+def test_les_with_interpolated_bounce_back_matches_the_reference_build():
+    """Smagorinsky LES past a sphere with the interpolated bounce-back
+    (S_BC_TYPE 1) on a two-level near-wall mesh: the wall step and the MEA
+    force passes collide with the cells' own eddy viscosity.  Same mesh and
+    solid cells as the reference build; fluid velocity, macro rows and eddy
+    viscosity within the bars of the cavity cases; the force partials within
+    5e-4 of their largest magnitude."""
+    g = fixture("geom_les_d3q19_wall2_smag")
+    Q, dim = int(g["Q"]), int(g["dim"])
+    ref = run_geom(g, 1)
+    ml = int(g["max_levels"])
+    assert ref["counts"]["n_ids"][:ml] == [int(v) for v in g["n_ids"][:ml]]
+    assert np.array_equal(ref["cmask"], g["cmask"])
+    fluid = (g["cmask"].reshape(-1) != -1)
+    Fr = np.transpose(g["F"][:, :Q, :], (1, 0, 2)).reshape(Q, -1)
+    Mr = np.transpose(g["F"][:, Q + 1:Q + 1 + dim, :], (1, 0, 2)).reshape(dim, -1).astype(np.float64)
+    nur = g["F"][:, Q + 4, :].reshape(-1).astype(np.float64)
+    _, u_r = macros(g, Fr[:, fluid])
+    _, u = macros(g, ref["F"][:, fluid])
+    r64 = run_geom(g, 1, _lib.STORE_FP64)
+    _, u64 = macros(g, r64["F"][:, fluid])
+    _, u0 = macros(g, run_geom(g, 0)["F"][:, fluid])
+    e, e0, floor = rel_l2(u, u_r), rel_l2(u0, u_r), rel_l2(u, u64)
+    tol = max(TOL_U, 3 * floor)
+    e_m = rel_l2(ref["M"][1:][:, fluid], Mr[:, fluid])
+    e_nu, nu_floor = rel_l2(ref["nu"][fluid], nur[fluid]), rel_l2(ref["nu"][fluid], r64["nu"][fluid])
+    ffr = g["Ff"].astype(np.float64)
+    e_f = np.abs(ref["Ff"] - ffr).max() / np.abs(ffr).max()
+    print(f"LES + Bouzidi: u vs reference {e:.3e} (floor {floor:.3e}, no model {e0:.3e}); macro rows {e_m:.3e}; "
+          f"nu_SGS {e_nu:.3e} (floor {nu_floor:.3e}); MEA partials {e_f:.3e}")
+    assert e < tol, (e, floor)
+    assert e_m < tol, (e_m, floor)
+    assert e_nu < max(1e-3, 10 * nu_floor), (e_nu, nu_floor)
+    assert e_f < 5e-4, e_f
     assert e0 > 5 * e, (e, e0)
 
 

@@ -514,6 +514,11 @@ class Learner:
         Set before collecting."""
         self._c(self._lib.agal_learn_set_horizon(self._h, int(horizon)))
 
+    def set_implicit(self, on: bool) -> None:
+        """Inference convolutions as implicit GEMMs (default) or through
+        materialised im2col columns; the logits are identical."""
+        self._c(self._lib.agal_learn_set_implicit(self._h, 1 if on else 0))
+
     def set_thresholds(self, refine: float, coarsen: float) -> None:
         """Probability thresholds of the two outputs in predict mode."""
         self._c(self._lib.agal_learn_set_thresholds(self._h, refine, coarsen))

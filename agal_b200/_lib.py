@@ -154,6 +154,7 @@ PROTOS = [
     ("agal_learn_set_thresholds", C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     ("agal_learn_attach", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double]),
     ("agal_learn_set_horizon", C.c_int, [C.c_void_p, C.c_int]),
+    ("agal_learn_set_implicit", C.c_int, [C.c_void_p, C.c_int]),
 ]
 
 _lib = None

@@ -64,6 +64,41 @@ __device__ __forceinline__ int tap_cell(int dim, int c, int t)
     return i + 4 * j + 16 * k;
 }
 
+// Implicit-GEMM A operand of a convolution: the im2col column block [kc, kc +
+// 8 g8) of rows m0.. built directly in the GEMM's shared-memory stage from
+// the layer input H [rows][cin] (FP32): each 16-byte core-matrix row is 8
+// channels of one tap of one cell, i.e. 32 contiguous bytes of H, converted
+// to BF16 as k_im2col converts them (zero outside the block and past the
+// taps), so the product is the same bit for bit without the columns ever
+// reaching global memory.
+struct GatherA {
+    const float *H;
+    int M, cin, dim, P, ntaps;
+    __device__ void operator()(unsigned char *sA, int m0, int kc, int g8, int tid) const
+    {
+        for (int i = tid; i < umma::TM * g8; i += umma::THREADS) {
+            const int r = i / g8, kg = i % g8;
+            const int row = m0 + r, k0 = kc + kg * 8;
+            const int t = k0 / cin, ch = k0 - t * cin;
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (row < M && t < ntaps) {
+                const int cell = row % P;
+                const int nc = tap_cell(dim, cell, t);
+                if (nc >= 0) {
+                    const float4 *src = reinterpret_cast<const float4 *>(H + ((size_t)(row - cell + nc) * cin + ch));
+                    const float4 a = __ldg(src), b = __ldg(src + 1);
+                    auto pk = [](float x, float y) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(x, y);
+                        return *reinterpret_cast<const unsigned *>(&h);
+                    };
+                    w = make_uint4(pk(a.x, a.y), pk(a.z, a.w), pk(b.x, b.y), pk(b.z, b.w));
+                }
+            }
+            *reinterpret_cast<uint4 *>(sA + umma::core_off(r, kg)) = w;
+        }
+    }
+};
+
 // ---- features --------------------------------------------------------------
 struct FeatArgs {
     const int *ids;
@@ -394,6 +429,7 @@ struct agal_learn {
     // pass and labelled by that regrid and the next h - 1, and the
     // prediction is made and applied at the same regrid.
     int horizon = 0;
+    int implicit = 1;                        // inference convolutions as implicit GEMMs
     float *lab_Y = nullptr, *lab_W = nullptr;   // one regrid's decisions, folded into the labels
     long long lab_cap = 0;
     long long regrids = 0, judged = 0, plain_refine = 0, missed = 0;
@@ -473,6 +509,16 @@ int gemm(agal_learn *m, const bf16 *A, const bf16 *B, float *D, int M, int N, in
     return AGAL_OK;
 }
 
+// Convolution of the layer input H [rows][cin] by the BF16 weights B [N][K]:
+// D = im2col(H) . B^T, the columns gathered inside the GEMM.
+int conv_gemm(agal_learn *m, const float *H, int cin, int rows, const bf16 *B, float *D, int N, int K, int ldd,
+              cudaStream_t s)
+{
+    const GatherA ga{H, rows, cin, m->dim, m->P, taps(m->dim)};
+    LCUDA(m, umma::gemm_bf16_with(ga, B, D, rows, N, K, ldd, m->status, s));
+    return AGAL_OK;
+}
+
 // Transposed BF16 copy of a rows x cols matrix into [cols][ld] (ld >= rows).
 template <typename S>
 void transpose(const S *in, int rows, int cols, int ld, bf16 *out, cudaStream_t s)
@@ -488,6 +534,19 @@ int forward(agal_learn *m, const float *X0, int n, const float *Ylab, const floa
     const int P = m->P, rows = n * P, rp = pad16(rows), K1p = m->K1p, K2 = m->K2;
     int rc = ensure(m, rows);
     if (rc) return rc;
+    if (!Ylab && m->implicit) {
+        // Inference: the three convolutions as implicit GEMMs (no columns in
+        // global memory); bit for bit the path below.
+        if ((rc = conv_gemm(m, X0, C0, rows, m->W1b, m->Y, CH, K1p, CH, s))) return rc;
+        k_bias_relu<<<gridn((long long)rows * CH), 256, 0, s>>>(m->Y, m->w + m->ob1, rows, CH, m->H1);
+        if ((rc = conv_gemm(m, m->H1, CH, rows, m->W2b, m->Y, CH, K2, CH, s))) return rc;
+        k_bias_relu<<<gridn((long long)rows * CH), 256, 0, s>>>(m->Y, m->w + m->ob2, rows, CH, m->H2);
+        if ((rc = conv_gemm(m, m->H2, CH, rows, m->W3b, m->Z, NO, K2, NO, s))) return rc;
+        k_pool_loss<<<gridn(n, 128), 128, 0, s>>>(m->Z, m->w + m->ob3, n, P, nullptr, nullptr, m->pw[0], m->pw[1],
+                                                  inv_count, m->logits, m->dZ, m->dZb, 16, m->scal, m->g + m->ob3);
+        LCUDA(m, cudaGetLastError());
+        return AGAL_OK;
+    }
     k_im2col<<<gridn((long long)rows * K1p), 256, 0, s>>>(X0, rows, m->dim, C0, K1p, m->X1b);
     if ((rc = gemm(m, m->X1b, m->W1b, m->Y, rows, CH, K1p, CH, s))) return rc;
     k_bias_relu<<<gridn((long long)rows * CH), 256, 0, s>>>(m->Y, m->w + m->ob1, rows, CH, m->H1);
@@ -797,6 +856,16 @@ extern "C" int agal_learn_set_horizon(agal_learn *m, int horizon)
     for (const auto &sn : m->snaps)
         if (!sn.labelled && sn.got > 0) return lerr(m, AGAL_ERR_STATE, "horizon changed while snapshots are being labelled");
     m->horizon = horizon;
+    return AGAL_OK;
+}
+
+// Inference convolutions as implicit GEMMs (1, the default: the columns are
+// gathered inside the GEMM) or through materialised im2col columns (0).
+// Both give the same logits bit for bit.
+extern "C" int agal_learn_set_implicit(agal_learn *m, int on)
+{
+    if (!m) return AGAL_ERR_PARAM;
+    m->implicit = on ? 1 : 0;
     return AGAL_OK;
 }
 

@@ -5,8 +5,10 @@
 // One CTA of 128 threads per 128-row tile of D and K slice, N <= 32 (one
 // 128 x 32 FP32 accumulator in tensor memory, 32 columns).  K is walked in
 // chunks of KC through two shared-memory stages: the four warps copy chunk
-// k+1 of A and B with cp.async (16 bytes per copy, all in flight at once,
-// rows past M or N zero-filled) into the tensor core's no-swizzle K-major
+// k+1 of B with cp.async, and stage chunk k+1 of A through a loader functor
+// (a row-major matrix with cp.async, or an implicit-GEMM gather that builds
+// the columns from another array) (16 bytes per copy, rows past M or N
+// zero-filled) into the tensor core's no-swizzle K-major
 // layout (8-row x 16-byte core matrices; K-adjacent core matrices 128 B
 // apart, 8-row groups KC x 2 B apart) while the tensor core multiplies chunk
 // k; one thread issues KC/16 tcgen05.mma (kind::f16, M = 128, N = 32, K = 16)
@@ -105,9 +107,25 @@ __device__ __forceinline__ void cp_async16(unsigned dst, const void *src, bool v
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A,
-                                                       const __nv_bfloat16 *__restrict__ B, float *__restrict__ D,
-                                                       int M, int N, int K, int ldd, int kslice, int *status)
+// A operand staged from a row-major BF16 matrix [M][K] with cp.async.
+struct DenseA {
+    const __nv_bfloat16 *A;
+    int M, K;
+    // Chunk of columns [kc, kc + 8 g8) of rows m0.. into the stage sA.
+    __device__ void operator()(unsigned char *sA, int m0, int kc, int g8, int tid) const
+    {
+        for (int i = tid; i < TM * g8; i += THREADS) {
+            const int r = i / g8, kg = i % g8;
+            const bool ok = m0 + r < M;
+            cp_async16(smem_u32(sA + core_off(r, kg)), A + (size_t)(ok ? m0 + r : 0) * K + kc + kg * 8, ok);
+        }
+    }
+};
+
+template <class ALoad>
+__global__ void __launch_bounds__(THREADS) k_gemm_bf16(const ALoad aload, const __nv_bfloat16 *__restrict__ B,
+                                                       float *__restrict__ D, int M, int N, int K, int ldd,
+                                                       int kslice, int *status)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar[2];
@@ -139,11 +157,7 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
         unsigned char *sB = sA + (size_t)TM * KC * 2;
         const int kc = k_begin + c * KC;
         const int g8 = min(KC, k_end - kc) / 8;
-        for (int i = tid; i < TM * g8; i += THREADS) {
-            const int r = i / g8, kg = i % g8;
-            const bool ok = m0 + r < M;
-            cp_async16(smem_u32(sA + core_off(r, kg)), A + (size_t)(ok ? m0 + r : 0) * K + kc + kg * 8, ok);
-        }
+        aload(sA, m0, kc, g8, tid);
         for (int i = tid; i < TN * g8; i += THREADS) {
             const int r = i / g8, kg = i % g8;
             const bool ok = r < N;
@@ -226,12 +240,14 @@ __global__ void __launch_bounds__(THREADS) k_gemm_bf16(const __nv_bfloat16 *__re
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(TN) : "memory");
 }
 
-// D = A . B^T for M rows (any), N <= 32, K a multiple of 16 (rows 16-byte
-// aligned).  A long K with few row tiles is split over CTAs (K slices of a
-// multiple of KC) whose partial tiles are added atomically into D, which is
-// zeroed first; that needs ldd == N (D contiguous).
-inline cudaError_t gemm_bf16(const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *D, int M, int N, int K, int ldd,
-                             int *status, cudaStream_t s)
+// D = A . B^T for M rows (any), N <= 32, K a multiple of 16, the A operand
+// staged by aload (DenseA: a row-major matrix; or an implicit-GEMM gather that
+// builds the columns in shared memory).  A long K with few row tiles is split
+// over CTAs (K slices of a multiple of KC) whose partial tiles are added
+// atomically into D, which is zeroed first; that needs ldd == N (D contiguous).
+template <class ALoad>
+inline cudaError_t gemm_bf16_with(const ALoad &aload, const __nv_bfloat16 *B, float *D, int M, int N, int K, int ldd,
+                                  int *status, cudaStream_t s)
 {
     if (M <= 0) return cudaSuccess;
     if (N < 1 || N > TN || K <= 0 || K % 16) return cudaErrorInvalidValue;
@@ -239,7 +255,8 @@ inline cudaError_t gemm_bf16(const __nv_bfloat16 *A, const __nv_bfloat16 *B, flo
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_gemm_bf16<ALoad>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attr[dev] = true;
     }
@@ -252,8 +269,15 @@ inline cudaError_t gemm_bf16(const __nv_bfloat16 *A, const __nv_bfloat16 *B, flo
         const cudaError_t e = cudaMemsetAsync(D, 0, sizeof(float) * (size_t)M * ldd, s);
         if (e != cudaSuccess) return e;
     }
-    k_gemm_bf16<<<dim3((unsigned)mt, (unsigned)splits), THREADS, SMEM, s>>>(A, B, D, M, N, K, ldd, kslice, status);
+    k_gemm_bf16<ALoad><<<dim3((unsigned)mt, (unsigned)splits), THREADS, SMEM, s>>>(aload, B, D, M, N, K, ldd, kslice,
+                                                                                   status);
     return cudaGetLastError();
+}
+
+inline cudaError_t gemm_bf16(const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *D, int M, int N, int K, int ldd,
+                             int *status, cudaStream_t s)
+{
+    return gemm_bf16_with(DenseA{A, M, K}, B, D, M, N, K, ldd, status, s);
 }
 
 }  // namespace umma

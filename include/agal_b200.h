@@ -373,6 +373,10 @@ int agal_learn_attach(agal_ctx *ctx, agal_learn *m, int mode, int judge_every, d
    and a predicting case can regrid `horizon` times less often (its P_REFINE
    times `horizon`).  Set it before collecting. */
 int agal_learn_set_horizon(agal_learn *m, int horizon);
+/* Inference convolutions as implicit GEMMs (on = 1, the default: the im2col
+   columns are gathered into the tcgen05 GEMM's shared-memory stages) or
+   through materialised columns (0).  The logits are the same bit for bit. */
+int agal_learn_set_implicit(agal_learn *m, int on);
 /* Separate probability thresholds of the refinement and coarsening outputs in
    predict mode (after agal_learn_attach, which sets both to `threshold`). */
 int agal_learn_set_thresholds(agal_learn *m, double refine, double coarsen);

@@ -164,6 +164,29 @@ def test_gradients_match_numpy(Q, N, steps, mli):
         c.close()
 
 
+@pytest.mark.parametrize("Q,N", [(9, 32), (19, 16)])
+def test_implicit_gemm_logits_equal_im2col(Q, N):
+    """Inference convolutions as implicit GEMMs (columns gathered into the
+    tensor-core GEMM's shared memory) give the logits of the im2col path bit
+    for bit, on every snapshot of a run, after some training."""
+    p, c, m = collect(Q, N, 48 if Q == 9 else 24, MAX_LEVELS_INTERIOR=3 if Q == 9 else 2)
+    try:
+        n, nl = m.counts()["snapshots"], m.counts()["labelled"]
+        assert n > 0 and nl > 0
+        m.train(0, nl, 1, lr=1e-3, seed=5)
+        for k in range(n):
+            m.set_implicit(True)
+            a = m.predict(k)
+            m.set_implicit(False)
+            b = m.predict(k)
+            assert a.shape == b.shape and len(a) > 0
+            assert np.array_equal(a, b), k
+    finally:
+        m.attach(c, 0)
+        m.close()
+        c.close()
+
+
 def f1(pred, true):
     tp = (pred & true).sum()
     return 2.0 * tp / max(pred.sum() + true.sum(), 1)

@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -49,8 +50,10 @@ using cmp::SCAN_CHUNK;
 constexpr int NT = 256;   // threads per CTA of the per-block kernels
 
 // Small device counters (amr_small, AGAL_AMR_SMALL ints).
-enum { S_NR = 0, S_NC = 1, S_GMAX = 2, S_TOTAL = 3, S_NEW = 8, S_IDMAX = 32, S_NIDS = 64 };
-static_assert(S_NIDS + 17 <= AGAL_AMR_SMALL, "small counter layout");
+// S_KEEP / S_MERGE: the sizes of the S5 / S6 compactions per level, checked
+// on the host with the S7 readback (one wait instead of one per level).
+enum { S_NR = 0, S_NC = 1, S_GMAX = 2, S_TOTAL = 3, S_NEW = 8, S_IDMAX = 32, S_NIDS = 64, S_KEEP = 96, S_MERGE = 128 };
+static_assert(S_MERGE + 17 <= AGAL_AMR_SMALL, "small counter layout");
 
 unsigned grid_for(long long n, int per = NT) { return (unsigned)((n + per - 1) / per); }
 
@@ -62,8 +65,20 @@ int compact(agal_ctx *c, const F &f, int n, int *count)
     *count = 0;
     if (n <= 0) return AGAL_OK;
     AGAL_CUDA(c, cmp::compact_async(c->stream, c->amr_parts, c->amr_small + S_TOTAL, f, n));
-    AGAL_CUDA(c, cudaMemcpyAsync(count, c->amr_small + S_TOTAL, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    int *h = c->h_small ? c->h_small : count;   // pinned: a direct copy
+    AGAL_CUDA(c, cudaMemcpyAsync(h, c->amr_small + S_TOTAL, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    *count = *h;
+    return AGAL_OK;
+}
+
+// The same without reading the count back (a compaction whose count the host
+// does not need).
+template <class F>
+int compact_nowait(agal_ctx *c, const F &f, int n)
+{
+    if (n <= 0) return AGAL_OK;
+    AGAL_CUDA(c, cmp::compact_async(c->stream, c->amr_parts, c->amr_small + S_TOTAL, f, n));
     return AGAL_OK;
 }
 
@@ -224,16 +239,29 @@ __global__ void k_mark_removed_ids(int *ids, int n, const int *ref)
     if (k < n && ref[ids[k]] == REF_REMOVE) ids[k] = N_SKIPID;
 }
 
-__global__ void k_copy(const int *src, int *dst, int n)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) dst[k] = src[k];
-}
 
 __global__ void k_fill_int(int *dst, int n, int v)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) dst[k] = v;
+}
+
+// small[slot] = small[S_TOTAL]: keeps a compaction's size past the next one.
+__global__ void k_keep_total(int *small, int slot) { small[slot] = small[S_TOTAL]; }
+
+// dst[k] = src[k] for k < *count (count on the device, n an upper bound).
+__global__ void k_copy_counted(const int *src, int *dst, const int *count, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n && k < *count) dst[k] = src[k];
+}
+
+struct Ints17 {
+    int v[17];
+};
+__global__ void k_set_ints(int *dst, Ints17 a)
+{
+    if (threadIdx.x < 17) dst[threadIdx.x] = a.v[threadIdx.x];
 }
 
 // Cu_ConcatReverse (mesh_amr.cu:40): removed IDs onto the gap stack, reversed.
@@ -442,8 +470,10 @@ __global__ void k_freeze(int *ref, int n, int thaw)
 
 int read_small(agal_ctx *c, int *h, int off, int n)
 {
-    AGAL_CUDA(c, cudaMemcpyAsync(h, c->amr_small + off, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+    int *dst = c->h_small ? c->h_small : h;   // pinned: a direct copy
+    AGAL_CUDA(c, cudaMemcpyAsync(dst, c->amr_small + off, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
     AGAL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (dst != h) std::memcpy(h, dst, sizeof(int) * n);
     return AGAL_OK;
 }
 
@@ -540,28 +570,29 @@ int agal_refine_pass(agal_ctx *c)
         k_emap<<<grid_for(idm), NT, 0, c->stream>>>(ref, nbr, nmb, Qmax, idm, c->amr_emap);
     // S2: first children from the top of the gap stack.
     if (proceed_ref) {
-        int cnt = 0;
         FirstChild fc{ref, c->gap_set, c->amr_first, c->n_gaps, NCH};
-        if ((rc = compact(c, fc, idm, &cnt))) return rc;
+        if ((rc = compact_nowait(c, fc, idm))) return rc;   // its count is nR
         const int lo = c->n_gaps - NCH * nR, hi = c->n_gaps;
-        const int mn = INT_MIN;
-        AGAL_CUDA(c, cudaMemcpyAsync(c->amr_small + S_GMAX, &mn, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        k_fill_int<<<1, 1, 0, c->stream>>>(c->amr_small + S_GMAX, 1, INT_MIN);
         k_max_range<<<grid_for(hi - lo), NT, 0, c->stream>>>(c->gap_set, lo, hi, c->amr_small + S_GMAX);
-        if ((rc = read_small(c, h, S_GMAX, 1))) return rc;
-        if (h[0] + 1 > idm_wnew) idm_wnew = (int)std::min<long long>(h[0] + 1, nmb);
         k_s2_1<<<grid_for(idm), NT, 0, c->stream>>>(c->amr_emap, nbr, ref, c->amr_first, nmb, Qmax, idm, nch);
     }
-    // S3: 2:1 quality control of coarsening.
+    // S3: 2:1 quality control of coarsening.  The largest new child ID (S2)
+    // is read back with the recount of the marks (one wait for both).
     if (proceed_coarse) {
         k_q1_1<<<grid_for(idm), NT, 0, c->stream>>>(nch, nmb, Qmax, idm, ref);
         k_q1_2<<<grid_for(idm), NT, 0, c->stream>>>(nch, NCH, idm, ref);
         AGAL_CUDA(c, cudaMemsetAsync(c->amr_small, 0, sizeof(int) * 2, c->stream));
         k_count_marks<<<grid_for(idm), NT, 0, c->stream>>>(ref, idm, c->amr_small);
-        if ((rc = read_small(c, h, 0, 2))) return rc;
+        if ((rc = read_small(c, h, 0, 3))) return rc;   // S_NR, S_NC, S_GMAX
         nC = h[S_NC];
         proceed_coarse = nC > 0;
         if (proceed_coarse) k_s2_2<<<grid_for(idm), NT, 0, c->stream>>>(c->amr_emap, nbr, ref, nmb, Qmax, idm, nch);
+    } else if (proceed_ref) {
+        if ((rc = read_small(c, h, S_GMAX, 1))) return rc;
+        h[S_GMAX] = h[0];
     }
+    if (proceed_ref && h[S_GMAX] + 1 > idm_wnew) idm_wnew = (int)std::min<long long>(h[S_GMAX] + 1, nmb);
     AGAL_CUDA(c, cudaGetLastError());
     if (!(proceed_ref || proceed_coarse)) {
         c->n_ref_last = 0;
@@ -573,6 +604,8 @@ int agal_refine_pass(agal_ctx *c)
                                                       c->cblock_level, c->cblock_f_X);
     AGAL_CUDA(c, cudaGetLastError());
     // S5: removed children leave the ID sets and return to the gap stack.
+    int expect_keep[17], expect_merge[17];
+    for (int L = 0; L < 17; L++) expect_keep[L] = expect_merge[L] = -1;
     if (proceed_coarse) {
         int prev = 0;
         for (int L = 1; L < ML; L++) {
@@ -583,10 +616,11 @@ int agal_refine_pass(agal_ctx *c)
             int *ids = c->id_set + (long long)L * nmb;
             const int n = c->n_ids[L];
             k_mark_removed_ids<<<grid_for(n), NT, 0, c->stream>>>(ids, n, ref);
-            int w = 0;
             KeepIds ki{ids, c->amr_a};
-            if ((rc = compact(c, ki, n, &w))) return rc;
-            if (w > 0) k_copy<<<grid_for(w), NT, 0, c->stream>>>(c->amr_a, ids, w);
+            if ((rc = compact_nowait(c, ki, n))) return rc;   // n - cnt kept, checked at S7
+            k_keep_total<<<1, 1, 0, c->stream>>>(c->amr_small, S_KEEP + L);
+            k_copy_counted<<<grid_for(n), NT, 0, c->stream>>>(c->amr_a, ids, c->amr_small + S_KEEP + L, n);
+            expect_keep[L] = n - cnt;
             c->n_ids[L] -= cnt;
             prev += cnt;
         }
@@ -609,28 +643,36 @@ int agal_refine_pass(agal_ctx *c)
             const int n = c->n_ids[L];
             k_fill_int<<<grid_for(idm_wnew), NT, 0, c->stream>>>(c->amr_a, idm_wnew, 0);
             if (n > 0) k_scatter_member<<<grid_for(n), NT, 0, c->stream>>>(ids, n, c->amr_a);
-            int tot = 0;
             MergeLevel ml{c->amr_a, ref, c->cblock_level, L, ids};
-            if ((rc = compact(c, ml, idm_wnew, &tot))) return rc;
+            if ((rc = compact_nowait(c, ml, idm_wnew))) return rc;   // checked at S7
+            k_keep_total<<<1, 1, 0, c->stream>>>(c->amr_small, S_MERGE + L);
             c->n_ids[L] += cnt;
-            if (tot != c->n_ids[L]) return agal_set_err(c, AGAL_ERR_STATE, "ID set merge size mismatch");
+            expect_merge[L] = c->n_ids[L];
         }
         c->n_gaps -= NCH * nR;
     }
     // S7: id_max per level.
     {
-        std::vector<int> init(17, INT_MIN), nn(17, 0);
-        for (int L = 0; L < ML; L++) nn[L] = c->n_ids[L];
-        AGAL_CUDA(c, cudaMemcpyAsync(c->amr_small + S_IDMAX, init.data(), sizeof(int) * 17, cudaMemcpyHostToDevice,
-                                     c->stream));
-        AGAL_CUDA(c, cudaMemcpyAsync(c->amr_small + S_NIDS, nn.data(), sizeof(int) * 17, cudaMemcpyHostToDevice,
-                                     c->stream));
+        Ints17 init, nn;
+        for (int L = 0; L < 17; L++) {
+            init.v[L] = INT_MIN;
+            nn.v[L] = L < ML ? c->n_ids[L] : 0;
+        }
+        k_set_ints<<<1, 32, 0, c->stream>>>(c->amr_small + S_IDMAX, init);
+        k_set_ints<<<1, 32, 0, c->stream>>>(c->amr_small + S_NIDS, nn);
         int nmax = 1;
         for (int L = 1; L < ML; L++) nmax = std::max(nmax, c->n_ids[L]);
         dim3 g(grid_for(nmax), ML - 1);
         k_level_max<<<g, NT, 0, c->stream>>>(c->id_set, nmb, c->amr_small + S_NIDS, c->amr_small + S_IDMAX);
         AGAL_CUDA(c, cudaGetLastError());
-        if ((rc = read_small(c, h, S_IDMAX, 17))) return rc;
+        // id_max and the S5 / S6 compaction sizes in one readback
+        if ((rc = read_small(c, h, S_IDMAX, S_MERGE + 17 - S_IDMAX))) return rc;
+        for (int L = 1; L < ML; L++) {
+            if (expect_keep[L] >= 0 && h[S_KEEP - S_IDMAX + L] != expect_keep[L])
+                return agal_set_err(c, AGAL_ERR_STATE, "ID set removal size mismatch");
+            if (expect_merge[L] >= 0 && h[S_MERGE - S_IDMAX + L] != expect_merge[L])
+                return agal_set_err(c, AGAL_ERR_STATE, "ID set merge size mismatch");
+        }
         for (int L = 1; L < ML; L++) c->id_max[L] = h[L] + 1;
         int mx = c->id_max[0];
         for (int L = 1; L < ML; L++) mx = std::max(mx, c->id_max[L]);

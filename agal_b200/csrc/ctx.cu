@@ -102,6 +102,7 @@ void release(agal_ctx *c)
                     c->tiles, c->xfer};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (c->h_small) cudaFreeHost(c->h_small);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->side) cudaStreamDestroy(c->side);
@@ -265,6 +266,10 @@ extern "C" int agal_ctx_create(const agal_params *p, agal_ctx **out)
         c->amr_parts = c->amr + 5 * nmb;
         c->amr_small = c->amr + na - AGAL_AMR_SMALL;
         ALLOC(c->crit, sizeof(double) * nmb + sizeof(int) * 2 * 65536 + 256);
+        if (cudaMallocHost((void **)&c->h_small, sizeof(int) * AGAL_AMR_SMALL) != cudaSuccess) {
+            cudaGetLastError();
+            c->h_small = nullptr;   // the readbacks fall back to pageable memory
+        }
     }
 #undef ALLOC
     cudaMemsetAsync(c->d_status, 0, sizeof(int) * 4, c->stream);

@@ -106,6 +106,7 @@ struct agal_ctx {
     int *amr_a = nullptr, *amr_b = nullptr, *amr_snap = nullptr;   // compaction / snapshot buffers
     int *amr_parts = nullptr;          // per-CTA partial counts of the compactions
     int *amr_small = nullptr;          // small counters read back by the host
+    int *h_small = nullptr;            // [AGAL_AMR_SMALL] pinned host copy of them (a readback per pass stage)
     void *crit = nullptr;              // percentile criterion: block values, histograms, selection state
     long long iter = 0;                // coarse steps taken (M_AdvanceLoop counter i)
     int n_ref_last = 0, n_coarse_last = 0;   // marks acted on by the last refinement pass
@@ -197,7 +198,7 @@ int agal_mark_level(agal_ctx *c, int L, int uniform);
 int agal_freeze_refined(agal_ctx *c, int thaw = 0);
 int agal_build_iface_lists(agal_ctx *c);    // after any mesh change (multi-level cases)
 size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
-#define AGAL_AMR_SMALL 128
+#define AGAL_AMR_SMALL 160
 // After any change of the mesh or launch shapes: the captured graphs no
 // longer match; their executables are kept and updated in place from the next
 // capture (cudaGraphExecUpdate, same topology), else rebuilt.

@@ -52,8 +52,13 @@ constexpr int NT = 256;   // threads per CTA of the per-block kernels
 // Small device counters (amr_small, AGAL_AMR_SMALL ints).
 // S_KEEP / S_MERGE: the sizes of the S5 / S6 compactions per level, checked
 // on the host with the S7 readback (one wait instead of one per level).
-enum { S_NR = 0, S_NC = 1, S_GMAX = 2, S_TOTAL = 3, S_NEW = 8, S_IDMAX = 32, S_NIDS = 64, S_KEEP = 96, S_MERGE = 128 };
-static_assert(S_MERGE + 17 <= AGAL_AMR_SMALL, "small counter layout");
+// S_NEW / S_REM: new and removed blocks per level, read back together after
+// S4.
+enum {
+    S_NR = 0, S_NC = 1, S_GMAX = 2, S_TOTAL = 3, S_NEW = 8, S_IDMAX = 32, S_NIDS = 64, S_KEEP = 96, S_MERGE = 128,
+    S_REM = 160
+};
+static_assert(S_REM + 17 <= AGAL_AMR_SMALL, "small counter layout");
 
 unsigned grid_for(long long n, int per = NT) { return (unsigned)((n + per - 1) / per); }
 
@@ -281,10 +286,11 @@ __global__ void k_coarsen_s2(const int *ref, long long nmb, int qmax, int n, int
     }
 }
 
-__global__ void k_count_new(const int *ref, const int *level, int n, int *cnt)
+// Blocks in refinement state `state` per level (new children, removed ones).
+__global__ void k_count_state(const int *ref, const int *level, int n, int state, int *cnt)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < n && ref[b] == REF_NEW) atomicAdd(&cnt[level[b]], 1);
+    if (b < n && ref[b] == state) atomicAdd(&cnt[level[b]], 1);
 }
 
 __global__ void k_scatter_member(const int *ids, int n, int *member)
@@ -603,16 +609,35 @@ int agal_refine_pass(agal_ctx *c)
     k_add_remove<<<grid_for(idm), NT, 0, c->stream>>>(c->amr_first, nmb, c->dim, NCH, c->dx_cblock, idm, ref, nch,
                                                       c->cblock_level, c->cblock_f_X);
     AGAL_CUDA(c, cudaGetLastError());
+    // The blocks leaving (S5) and joining (S6) each level, read back at once.
+    int n_new[17], n_rem[17];
+    for (int L = 0; L < 17; L++) n_new[L] = n_rem[L] = 0;
+    if (proceed_coarse) {
+        AGAL_CUDA(c, cudaMemsetAsync(c->amr_small + S_REM, 0, sizeof(int) * 17, c->stream));
+        k_count_state<<<grid_for(idm_wnew), NT, 0, c->stream>>>(ref, c->cblock_level, idm_wnew, REF_REMOVE,
+                                                                 c->amr_small + S_REM);
+    }
+    if (proceed_ref) {
+        AGAL_CUDA(c, cudaMemsetAsync(c->amr_small + S_NEW, 0, sizeof(int) * 17, c->stream));
+        k_count_state<<<grid_for(idm_wnew), NT, 0, c->stream>>>(ref, c->cblock_level, idm_wnew, REF_NEW,
+                                                                 c->amr_small + S_NEW);
+    }
+    AGAL_CUDA(c, cudaGetLastError());
+    if ((rc = read_small(c, h, S_NEW, S_REM + 17 - S_NEW))) return rc;
+    for (int L = 0; L < 17; L++) {
+        if (proceed_ref) n_new[L] = h[L];
+        if (proceed_coarse) n_rem[L] = h[S_REM - S_NEW + L];
+    }
     // S5: removed children leave the ID sets and return to the gap stack.
     int expect_keep[17], expect_merge[17];
     for (int L = 0; L < 17; L++) expect_keep[L] = expect_merge[L] = -1;
     if (proceed_coarse) {
         int prev = 0;
         for (int L = 1; L < ML; L++) {
-            int cnt = 0;
-            RemovedAtLevel rl{ref, c->cblock_level, L, c->amr_b + prev};
-            if ((rc = compact(c, rl, idm_wnew, &cnt))) return rc;
+            const int cnt = n_rem[L];
             if (cnt == 0) continue;
+            RemovedAtLevel rl{ref, c->cblock_level, L, c->amr_b + prev};
+            if ((rc = compact_nowait(c, rl, idm_wnew))) return rc;   // cnt blocks, counted above
             int *ids = c->id_set + (long long)L * nmb;
             const int n = c->n_ids[L];
             k_mark_removed_ids<<<grid_for(n), NT, 0, c->stream>>>(ids, n, ref);
@@ -632,12 +657,8 @@ int agal_refine_pass(agal_ctx *c)
     }
     // S6: new children join the ID sets.
     if (proceed_ref) {
-        AGAL_CUDA(c, cudaMemsetAsync(c->amr_small + S_NEW, 0, sizeof(int) * 17, c->stream));
-        k_count_new<<<grid_for(idm_wnew), NT, 0, c->stream>>>(ref, c->cblock_level, idm_wnew, c->amr_small + S_NEW);
-        AGAL_CUDA(c, cudaGetLastError());
-        if ((rc = read_small(c, h, S_NEW, 17))) return rc;
         for (int L = 1; L < ML; L++) {
-            const int cnt = h[L];
+            const int cnt = n_new[L];
             if (cnt == 0) continue;
             int *ids = c->id_set + (long long)L * nmb;
             const int n = c->n_ids[L];

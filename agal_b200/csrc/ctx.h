@@ -198,7 +198,7 @@ int agal_mark_level(agal_ctx *c, int L, int uniform);
 int agal_freeze_refined(agal_ctx *c, int thaw = 0);
 int agal_build_iface_lists(agal_ctx *c);    // after any mesh change (multi-level cases)
 size_t agal_amr_scratch_ints(int64_t nmb);  // the last AGAL_AMR_SMALL ints are amr_small
-#define AGAL_AMR_SMALL 160
+#define AGAL_AMR_SMALL 192
 // After any change of the mesh or launch shapes: the captured graphs no
 // longer match; their executables are kept and updated in place from the next
 // capture (cudaGraphExecUpdate, same topology), else rebuilt.

@@ -675,7 +675,7 @@ def drag_lift(device: int) -> dict:
     return out
 
 
-def _vortex_params(storage: int, p_refine: int, device: int):
+def _vortex_params(storage: int, p_refine: int, device: int, seed: int = 2024):
     """2D periodic flow carrying vortices across the domain: D2Q9 128^2,
     periodic in x and y, uniform u = 0.05 with 30% seeded velocity noise,
     Re 500, up to 3 levels by the percentile rule (refine > p90, coarsen <
@@ -685,7 +685,7 @@ def _vortex_params(storage: int, p_refine: int, device: int):
                              P_REFINE=p_refine, S_CRITERION=_lib.CRITERION_PERCENTILE, ref_pct_hi=0.9,
                              ref_pct_lo=0.5, interp_order=_lib.INTERP_CUBIC, PERIODIC_X=1, PERIODIC_Y=1,
                              bc_preset=_lib.BC_NONE, ic_preset=_lib.IC_UNIFORM, u_ref=0.05, ic_noise=0.3,
-                             seed=2024, v0=0.05 / 500.0, storage=storage, n_maxcblocks=nb * 21 + 64,
+                             seed=seed, v0=0.05 / 500.0, storage=storage, n_maxcblocks=nb * 21 + 64,
                              device=device)
 
 
@@ -713,6 +713,52 @@ def _time_periods(torch, case, period: int, n_periods: int) -> dict:
             "regrid_ms_per_1000_steps": 1000.0 * regrid / steps, "blocks_per_level": case.counts()["n_ids"][:-1]}
 
 
+def _batched_vortices(torch, device: int, weights, thr, horizon: int, base: int, n_cases: int = 8,
+                      spinup: int = 512, window: int = 512) -> dict:
+    """The learned predictor inside a batch: n_cases periodic-vortex cases
+    (other noise seeds) advanced together (one graph branch per case), FP16,
+    once with the percentile rule every `base` coarse steps and once each
+    driven by its own copy of the trained network every base x horizon steps
+    (the rule judging every regrid).  MLUPS over `window` coarse steps after
+    `spinup`, device time on the batch stream, regrids included."""
+    out = {"n_cases": n_cases, "spinup_steps": spinup, "window_steps": window}
+    for name, period, learned in (("plain_fp16", base, False), ("learned_fp16", base * horizon, True)):
+        cases, nets = [], []
+        for i in range(n_cases):
+            c = ag.Case(_vortex_params(_lib.STORE_FP16, period, device, seed=3000 + i))
+            if learned:
+                n = ag.Learner(2, seed=7)
+                n.set_params(weights)
+                n.set_horizon(horizon)
+                n.attach(c, 2, judge_every=1)
+                n.set_thresholds(*thr)
+                nets.append(n)
+            c.set_ic(0)
+            c.refine_near_wall()
+            cases.append(c)
+        with ag.Batch(cases) as b:
+            b.set_worklist(False)
+            b.advance_n(spinup)
+            b.sync()
+            stream = torch.cuda.ExternalStream(b.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            cells = 0
+            e0.record(stream)
+            for _ in range(window // base):
+                cells += base * sum(leaf_cells(c.counts(), 2) for c in cases)
+                b.advance_n(base)
+            e1.record(stream)
+            b.sync()
+            ms = e0.elapsed_time(e1)
+        out[name] = {"mlups": cells / (ms * 1e-3) / 1e6, "ms": ms, "regrids_per_case": window // period}
+        for n in nets:
+            n.close()
+        for c in cases:
+            c.close()
+    out["ratio_learned_vs_plain"] = out["learned_fp16"]["mlups"] / out["plain_fp16"]["mlups"]
+    return out
+
+
 def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epochs: int = 2,
                   window: int = 1024, spinup: int = 1024) -> dict:
     """The learned predictor adapting the grid less often, on the periodic
@@ -722,8 +768,11 @@ def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epoc
     FP16 run driven by the network regrids every horizon x 16 steps, the rule
     judging every regrid (its refinements the network missed are counted and
     applied).  Against the plain FP16 and FP32 runs regridding every 16 steps,
-    after the same spin-up: MLUPS, regrids and regrid time per 1000 coarse
-    steps, and the missed-refinement fraction."""
+    after the same spin-up: MLUPS, device time, regrids and regrid time per
+    1000 coarse steps, and the missed-refinement fraction (the meshes differ, so
+    MLUPS counts different cells: the device time of the same coarse steps is
+    the like-for-like figure); then the same comparison for 8 such cases
+    advanced as one batch (`batched`)."""
     base = 16
     t0 = time.perf_counter()
     src = ag.Case(_vortex_params(_lib.STORE_FP32, base, device))
@@ -781,6 +830,7 @@ def learned_ahead(torch, device: int, horizon: int = 4, n_snap: int = 2000, epoc
         meshes[name] = refined_cells(c)
         c.close()
         out[name] = r
+    out["batched"] = _batched_vortices(torch, device, m.get_params(), thr, horizon, base)
     m.close()
     # both runs end on a regrid of theirs at the same coarse step: the share of
     # the plain FP16 run's refined blocks (per level) the learned run also has

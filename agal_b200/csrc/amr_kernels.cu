@@ -240,6 +240,10 @@ struct AverageArgs {
     int sr;
     const unsigned *sr_ctr;
     unsigned sr_salt;
+    // Non-null: the launch's last CTA advances the rounding counter once all
+    // CTAs have read it (the coarse step's tick), ticket counting the CTAs.
+    unsigned *tick;
+    int *ticket;
 };
 
 
@@ -300,6 +304,16 @@ template <int DIM, int Q, typename T>
 __global__ void __launch_bounds__(Geo<DIM>::NCH * Geo<DIM>::MC) k_average(const AverageArgs a)
 {
     average_body<DIM, Q, T>(a, blockIdx.x);
+    if (a.tick) {
+        __syncthreads();   // every thread of this CTA is past its read of the counter
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(a.ticket, 1) == (int)gridDim.x - 1) {
+                *a.ticket = 0;
+                atomicAdd(a.tick, 1u);
+            }
+        }
+    }
 }
 
 template <int DIM, int Q, typename T>
@@ -764,8 +778,16 @@ template <int DIM, int Q, typename T> struct RunAverage {
         a.ratio = c->tau[L] / c->tau[L + 1];
         if (sizeof(typename ST<T>::C) == 4) a.ratio = (double)((float)c->tau[L] / (float)c->tau[L + 1]);
         a.var = var;
+        a.tick = nullptr;
+        a.ticket = nullptr;
         if (c->rec)   // batch recording: one batched launch per phase (batch.cu)
             return agal_record_args(c, AGAL_OP_AVERAGE, L, &a, sizeof(a), agal_transfer_batch_key(c, false), a.n);
+        if (c->tick_pending && L == c->L0) {   // the coarse step's last launch
+            a.tick = c->d_sr;
+            a.ticket = c->d_status + 3;
+            c->tick_pending = false;
+            c->tick_done = true;
+        }
         constexpr int NT = Geo<DIM>::NCH * Geo<DIM>::MC;
         AGAL_CUDA(c, launch_pdl(k_average<DIM, Q, T>, dim3((unsigned)a.n), dim3(NT), 0, c->stream, a));
         AGAL_CUDA(c, cudaGetLastError());

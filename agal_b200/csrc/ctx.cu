@@ -735,9 +735,22 @@ int agal_record_coarse_step(agal_ctx *c)
 {
     const int mult = 1 << c->L0;
     c->sr_salt = 0;
+    // On multi-level meshes the last launch of the coarse step is the
+    // averaging of the starting level: it carries the tick (no launch of its
+    // own), unless a control-volume pass follows or the batch records.
+    const bool fold = multi_level(c) && c->P.S_FORCE_TYPE != 1 && !c->rec &&
+                      (c->storage == AGAL_STORE_FP16 || c->storage == AGAL_STORE_BF16) &&
+                      c->P.half_rounding == AGAL_ROUND_STOCHASTIC;
+    c->tick_done = false;
     for (int j = 0; j < mult; j++) {
+        c->tick_pending = fold && j == mult - 1;
         int rc = advance_rec(c, c->L0);
+        c->tick_pending = false;
         if (rc) return rc;
+    }
+    if (c->tick_done) {
+        c->tick_done = false;
+        return AGAL_OK;
     }
     return agal_sr_tick(c);
 }

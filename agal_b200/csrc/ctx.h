@@ -87,6 +87,11 @@ struct agal_ctx {
     // the next step launch within the coarse step being recorded.
     unsigned *d_sr = nullptr;
     int sr_salt = 0;
+    // The tick folded into the coarse step's last averaging launch (its last
+    // CTA increments the counter, d_status[3] its CTA ticket): pending while
+    // the last sub-step of a multi-level coarse step is recorded, done once
+    // that launch carries it.
+    bool tick_pending = false, tick_done = false;
     int *meta = nullptr;               // per-block step metadata rows (step_common.cuh Meta<DIM>)
     int *blk_solid = nullptr;          // [nmb] 1 = the block holds a solid cell (geometry cases)
     int *tiles = nullptr;              // root-level tile table of the 2D tile step (step_tile.cu)

@@ -168,11 +168,16 @@ def state_bytes(case, w: dict) -> int:
         ESIZE[w["storage"]]
 
 
+FUSED_FIXUP_BLOCKS = 8192   # grids up to this many blocks apply the stream-guard fix-ups in their last CTA
+
+
 def launches_per_step(counts: dict, amr: bool) -> int:
     """Kernels of one coarse step, from the structure of the level recursion:
-    level L takes 2^L sub-steps, each a fused step and its stream-guard
-    fix-up, and every non-empty level below the finest launches 2^L
-    interpolations and 2^L averagings."""
+    level L takes 2^L sub-steps, each a fused step (plus a separate
+    stream-guard fix-up launch on grids of more than FUSED_FIXUP_BLOCKS
+    blocks), and every non-empty level below the finest launches 2^L
+    interpolations and 2^L averagings; the rounding counter's tick rides on
+    the last averaging."""
     if not amr:
         return 2
     n, ml = counts["n_ids"], counts["max_levels"]
@@ -181,7 +186,7 @@ def launches_per_step(counts: dict, amr: bool) -> int:
         if n[L] == 0:
             continue
         mult = 1 << L
-        total += 2 * mult
+        total += mult * (2 if n[L] > FUSED_FIXUP_BLOCKS else 1)
         if L < ml - 1:
             total += 2 * mult
     return total
